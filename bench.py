@@ -1,0 +1,339 @@
+"""Benchmark of the neko_b200 pressure/Helmholtz solve path.
+
+Workload (one GPU): the large FP64 pressure-type solve -- periodic box
+[0, 2 pi]^3 of 32^3 hexahedra, GLL points displaced by 0.05 sin of the other
+two coordinates, lx = 8 (16.8 M local points), h1 = 1, h2 = 0, mean-free
+Fourier-mode right-hand side, preconditioned CG from x0 = 0 to a residual
+1e-8 times the initial one.  A step is one complete solve.
+
+    python bench.py --gpus N --steps K --warmup W [--impl native|reference]
+                    [--pc jacobi|hsmg]
+
+Under torchrun each rank solves its own copy (replicas, weak scaling; the
+solve itself does not shard).  `value` is solves/s of the whole job from
+device-timed steps (inputs resident in HBM); `e2e` repeats the steps through
+the public API with the right-hand side copied in from pinned host memory
+and the solution copied back inside the timed region.  `roofline` is the
+ax_helm kernel timed with CUDA events on its own stream over the same
+problem; `cpu_baseline` times the CPU oracle on a bounded sample.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}",
+                                      f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout
+                for line in out.strip().splitlines():
+                    self.rows.append([c.strip() for c in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_problem(nb, cfg):
+    return nb.Problem(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"], periodic=cfg["periodic"],
+                      deform=cfg["deform"], dirichlet=cfg["dirichlet"])
+
+
+def make_rhs(nb, P, seed):
+    import torch
+    from neko_b200 import workloads
+    x, y, z, B = (P.field(k) for k in ("x", "y", "z", "B"))
+    b = workloads.config2_rhs_local(x, y, z, B, seed).contiguous()
+    P.gs.op(b, P.n)
+    torch.cuda.synchronize()
+    return b
+
+
+def cpu_baseline_sample(cfg, b, gpu_iters, budget_iters):
+    """Oracle (a one-thread CPU port of the reference's path) on the same
+    workload and right-hand side: setup untimed, then `budget_iters`
+    Jacobi-PCG iterations timed; solves/s extrapolated with the iteration
+    count of the GPU run."""
+    from oracle import oracle as orc
+    O = orc.OracleProblem.box(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"],
+                              periodic=cfg["periodic"])
+    O.deform_sine(cfg["deform"])
+    O.coef()
+    t0 = time.perf_counter()
+    O.cg_jacobi(b, budget_iters, 0.0)
+    dt = time.perf_counter() - t0
+    per_iter = dt / budget_iters
+    return {"value": 1.0 / (per_iter * max(gpu_iters, 1)), "unit": "solves/s", "cores": 1,
+            "kind": "port",
+            "sample": f"{budget_iters} Jacobi-PCG iterations of the same 32^3 lx=8 problem on 1 "
+                      f"host core ({dt:.1f} s); solves/s = 1/(s per iteration x {gpu_iters} "
+                      f"iterations of the GPU run)"}
+
+
+def run_reference(args, cfg, world, rank):
+    """--impl reference: the reference's CPU algorithm (oracle port) on the
+    host cores, same metric/config; rank 0 only."""
+    if rank != 0:
+        return
+    import numpy as np
+    from oracle import oracle as orc
+    from neko_b200 import workloads
+    O = orc.OracleProblem.box(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"],
+                              periodic=cfg["periodic"])
+    O.deform_sine(cfg["deform"])
+    O.coef()
+    x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
+    b = O.gs_add(workloads.config2_rhs_local(x, y, z, B, args.seed))
+    mult = O.f64("mult")
+    r0 = math.sqrt(float(np.sum(b * mult * b)) / O.volume)
+    iters = args.ref_iters
+    for _ in range(args.warmup):
+        O.cg_jacobi(b, 1, 0.0)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.cg_jacobi(b, iters, 0.0)
+        times.append((time.perf_counter() - t0) / iters)
+    per_iter = sorted(times)[len(times) // 2]
+    full_iters = args.ref_full_iters
+    v = 1.0 / (per_iter * full_iters)
+    line = {"impl": "reference", "metric": "Poisson solves/s to 1e-8 rel", "value": v,
+            "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per_iter * full_iters * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "periodic deformed box 32^3 hex, lx=8 (16.8M points), "
+                                   "FP64 Jacobi-PCG to 1e-8 rel", "r0": r0},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
+                             "sample": f"median of {args.steps} runs of {iters} CG iterations; "
+                                       f"solves/s = 1/(s per iteration x {full_iters})"},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--pc", default="jacobi", choices=["jacobi", "hsmg"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--ax-reps", type=int, default=50)
+    ap.add_argument("--cpu-iters", type=int, default=3)
+    ap.add_argument("--ref-iters", type=int, default=2)
+    ap.add_argument("--ref-full-iters", type=int, default=0,
+                    help="iterations of the full solve (default: measured on the GPU path)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    from neko_b200 import workloads
+    cfg = dict(workloads.CONFIG2)
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        if args.ref_full_iters <= 0:
+            args.ref_full_iters = 440  # Jacobi-PCG iterations of this workload (GPU run)
+        run_reference(args, cfg, world, rank)
+        barrier(world)
+        return
+
+    import torch
+    import neko_b200 as nb
+    torch.cuda.set_device(local)
+    P = build_problem(nb, cfg)
+    b = make_rhs(nb, P, args.seed + rank)
+    mult = P.field("mult")
+    r0 = math.sqrt(float((b * mult * b).sum()) / P.volume)
+    tol = cfg["rel_tol"] * r0
+    M = nb.Jacobi() if args.pc == "jacobi" else nb.Hsmg()
+    solver = nb.CG(max_iter=cfg["max_iter"], abs_tol=tol, M=M)
+    Ax = nb.AxHelm()
+    x = P.zeros()
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            mon = solver.solve(Ax, x, b, P.n, P, stream=stream)
+    torch.cuda.synchronize()
+    if not mon.converged:
+        raise RuntimeError(f"warm-up solve did not converge: {mon}")
+
+    # --- device-timed steps (inputs resident in HBM, > L2) ---------------
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    iters = []
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            mon = solver.solve(Ax, x, b, P.n, P, stream=stream)
+            launches += mon.launches
+            iters.append(mon.iter)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    t_dev = max_over_ranks(t_dev, world)
+    value = world * args.steps / t_dev
+
+    # --- end to end through the public API with host buffers -------------
+    hb = b.cpu().pin_memory()
+    hx = torch.empty(P.n, dtype=torch.float64).pin_memory()
+    fdev = torch.empty_like(b)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            fdev.copy_(hb, non_blocking=True)
+            mon_e = solver.solve(Ax, x, fdev, P.n, P, stream=stream)
+            hx.copy_(x, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    e2e = world * args.steps / t_e2e
+
+    # --- ax_helm roofline: events on the launching stream ----------------
+    w = P.zeros()
+    for _ in range(5):
+        Ax.compute(w, x, P, stream=stream)
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.ax_reps):
+        Ax.compute(w, x, P, stream=stream)
+    a1.record(stream)
+    torch.cuda.synchronize()
+    t_ax = a0.elapsed_time(a1) / 1e3 / args.ax_reps
+    peaks, peak_src = measured_peaks()
+    ax_bytes = 72 * P.n  # u, w, h1, G11..G23: 9 x 8 B per point
+    achieved = ax_bytes / t_ax / 1e9
+    ax_gdofs = P.n / t_ax / 1e9
+
+    line = {
+        "metric": "Poisson solves/s to 1e-8 rel", "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"periodic deformed box 32^3 hex, lx=8 (16.8M points), "
+                               f"FP64 {args.pc}-PCG to 1e-8 rel, one solve per step per GPU",
+                   "pc": args.pc, "iterations": iters[-1], "r0": r0, "seed": args.seed,
+                   "l2": "inputs larger than L2 (1.2 GB ax_helm working set)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": P.n * 8,
+                "d2h_bytes_per_step": P.n * 8},
+        "roofline": {"bound": "hbm", "kernel": "ax_helm_kernel<double,8,2>",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "peak_source": peak_src, "bytes_per_launch": ax_bytes,
+                     "launch_ms": t_ax * 1e3, "gdof_s": ax_gdofs},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(cfg, b.cpu().numpy(), iters[-1],
+                                                   args.cpu_iters)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    P.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,197 @@
+/*
+ * neko_b200.h -- C ABI of libnekob200.so, a B200 (sm_100a) device backend for
+ * the pressure/Helmholtz solve path of the Neko spectral-element code.
+ *
+ * Part 1 exports the symbols that Neko's Fortran device layer binds through
+ * `bind(c, name='cuda_*')`, with the same signatures and semantics, so a Neko
+ * build can link this library in place of its own CUDA objects.  As in the
+ * reference, integers arrive by reference, device buffers as plain pointers,
+ * the stream (where the reference passes one) as an opaque handle, and
+ * `real` is double.  Errors in this part print a message and exit, as the
+ * reference's CUDA_CHECK does.
+ *
+ * Part 2 is a native handle API (nb_*) over device-resident problems: mesh,
+ * geometric factors and gather-scatter maps built once and kept in HBM, then
+ * operator applications and complete Krylov solves.  Every nb_* call returns
+ * an nb_status; nb_last_error() describes the last failure of the thread.
+ */
+#ifndef NEKO_B200_H
+#define NEKO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Part 1: drop-in replacements for the reference's cuda_* entry points.
+ * ---------------------------------------------------------------------- */
+
+/* w = A u, the matrix-free Helmholtz operator (h1 part) on nelv elements of
+ * lx^3 points.  Replaces cuda_ax_helm
+ * (src/math/bcknd/device/cuda/ax_helm.cu:63), called from
+ * src/math/bcknd/device/ax_helm_device.F90:234.  Runs on the library's
+ * default stream (the reference uses glb_cmd_queue). */
+void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, void *dxt,
+                  void *dyt, void *dzt, void *h1, void *g11, void *g22,
+                  void *g33, void *g12, void *g13, void *g23, int *nelv,
+                  int *lx);
+
+/* au += h2 B u for one component.  Replaces the addcol4 used for the h2
+ * term of the scalar Ax (ax_helm_device.F90:253-255 ->
+ * src/math/bcknd/device/cuda/math.cu:641). */
+void cuda_addcol4(void *a, void *b, void *c, void *d, int *n, void *stream);
+
+/* Gather: v(dg(k)) = sum of u(gd(k..k+len-1)) for each block, and
+ * v(dg(i)) = u(gd(i)) + u(gd(i+1)) for facet pairs from offset o (op = 1,
+ * add); min/max/mul analogues for op = 2,3,4.  1-based index arrays.
+ * Replaces src/gs/bcknd/device/cuda/gs.cu:51. */
+void cuda_gather_kernel(void *v, int *m, int *o, void *dg, void *u, int *n,
+                        void *gd, int *nb, void *b, void *bo, int *op,
+                        void *stream);
+
+/* Scatter: u(gd(i)) = v(dg(i)).  Replaces src/gs/bcknd/device/cuda/gs.cu:96. */
+void cuda_scatter_kernel(void *v, int *m, void *dg, void *u, int *n, void *gd,
+                         int *nb, void *b, void *bo, void *stream);
+
+/* sum(a*b*c) returned to the host after a stream synchronisation.
+ * Replaces src/math/bcknd/device/cuda/math.cu:906 (cuda_glsc3). */
+double cuda_glsc3(void *a, void *b, void *c, int *n, void *stream);
+/* sum(a*b) -- math.cu:965 */
+double cuda_glsc2(void *a, void *b, int *n, void *stream);
+/* sum(a) -- math.cu:1023 */
+double cuda_glsum(void *a, int *n, void *stream);
+
+/* Vector updates of the Krylov loop (math.cu:60-660). */
+void cuda_copy(void *a, void *b, int *n, void *stream);           /* a = b */
+void cuda_rzero(void *a, int *n, void *stream);                   /* a = 0 */
+void cuda_add2s1(void *a, void *b, double *c1, int *n, void *stream); /* a = c1 a + b */
+void cuda_add2s2(void *a, void *b, double *c1, int *n, void *stream); /* a = a + c1 b */
+void cuda_col2(void *a, void *b, int *n, void *stream);           /* a = a b */
+void cuda_col3(void *a, void *b, void *c, int *n, void *stream);  /* a = b c */
+void cuda_addcol3(void *a, void *b, void *c, int *n, void *stream); /* a += b c */
+void cuda_invcol1(void *a, int *n, void *stream);                 /* a = 1/a */
+void cuda_radd(void *a, double *c, int *n, void *stream);         /* a += c (math.cu:266) */
+
+/* x(msk(i)) = 0 for i = 1..m-1 (msk(0) holds the count).  Replaces
+ * src/bc/bcknd/device/cuda/zero_dirichlet.cu:44. */
+void cuda_zero_dirichlet_apply_scalar(void *msk, void *x, int *m, void *stream);
+
+/* Diagonal of the stiffness matrix from the geometric factors, with the
+ * boundary cross terms of the reference device kernel.  Replaces
+ * src/krylov/bcknd/device/cuda/pc_jacobi.cu:102. */
+void cuda_jacobi_update(void *d, void *dxt, void *dyt, void *dzt, void *G11,
+                        void *G22, void *G33, void *G12, void *G13, void *G23,
+                        int *nel, int *lx);
+
+/* ------------------------------------------------------------------------
+ * Part 2: native handle API.
+ * ---------------------------------------------------------------------- */
+
+typedef enum {
+  NB_OK = 0,
+  NB_ERR_ARG = 1,          /* invalid argument */
+  NB_ERR_UNSUPPORTED = 2,  /* lx or mesh outside the supported set */
+  NB_ERR_OOM = 3,          /* device allocation failed */
+  NB_ERR_CUDA = 4,         /* CUDA runtime error */
+  NB_ERR_NOT_CONVERGED = 5,
+  NB_ERR_NAN = 6,          /* residual became NaN/Inf */
+  NB_ERR_TIMEOUT = 7       /* a bounded device wait expired */
+} nb_status;
+
+typedef struct nb_problem nb_problem;
+
+/* Returns the message of the last failed nb_* call of this thread. */
+const char *nb_last_error(void);
+
+/* Library version string. */
+const char *nb_version(void);
+
+/* Host-only setup helpers (no device needed). */
+
+/* GLL nodes z[lx], weights w[lx] and derivative matrix D[lx*lx]
+ * (column-major, D(i,j) = l_j'(z_i)), the quantities space_t%init builds
+ * with zwgll/dgll (src/sem/space.f90:149-320). */
+nb_status nb_gll(int lx, double *z, double *w, double *D);
+
+/* Gather-scatter maps of a structured box, in the reference layout of
+ * gs_init_mapping (src/gs/gather_scatter.f90:513-1375): 1-based gs id and
+ * local point per entry, block lengths/offsets over the vertex/edge part,
+ * facet pairs from facet_offset on.  Call once with NULL arrays to get the
+ * sizes, then with arrays of those sizes. */
+nb_status nb_box_gs_maps(const int nel[3], const int periodic[3], int lx,
+                         int *nlocal, int *facet_offset, int *nblocks,
+                         int *dof_gs, int *gs_dof, int *blk_len, int *blk_off);
+
+/* Builds a structured box problem on the current device: nel[3] hexahedra
+ * on [lo,hi]^3 (x fastest), optional periodicity, polynomial size lx
+ * (2..16), and an optional smooth deformation of the GLL points
+ * x += a sin(y) sin(z), y += a sin(z) sin(x), z += a sin(x) sin(y).
+ * Geometric factors (G11..G23, B, mult) are computed on the device; the
+ * gather-scatter maps follow the reference's gs_init_mapping
+ * (src/gs/gather_scatter.f90:513-1375) entry for entry.  Faces with no
+ * neighbour become zero-Dirichlet when dirichlet_boundary is non-zero.
+ * Periodic directions need at least 3 elements. */
+nb_status nb_problem_create_box(const int nel[3], const double lo[3],
+                                const double hi[3], const int periodic[3],
+                                int lx, double deform_amp,
+                                int dirichlet_boundary, nb_problem **out);
+nb_status nb_problem_destroy(nb_problem *p);
+
+/* Sizes: n = lx^3 * nelv local dofs. */
+nb_status nb_problem_sizes(const nb_problem *p, int64_t *n, int *nelv, int *lx,
+                           int *nlocal, int *nblocks, int *nmask);
+
+/* Device pointer to a named field of the problem: "x","y","z","g11",
+ * "g22","g33","g12","g13","g23","h1","h2","B","mult","dx","dxt", or a map
+ * "dof_gs","gs_dof","blk_len","blk_off","msk" (int32, 1-based). */
+nb_status nb_problem_field(const nb_problem *p, const char *name, void **dptr);
+
+/* Volume (sum of B) of the problem's mesh. */
+nb_status nb_problem_volume(const nb_problem *p, double *vol);
+
+/* Sets the Helmholtz coefficients from device arrays (n values each; h2 may
+ * be NULL).  ifh2 enables the h2 B u term. */
+nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1,
+                                      const double *h2, int ifh2);
+
+/* w = A u (ax_helm incl. h2 term when enabled), element-local. */
+nb_status nb_ax(nb_problem *p, double *w, const double *u, void *stream);
+/* u = gs_add(u): sum of all local copies of each shared point. */
+nb_status nb_gs_add(nb_problem *p, double *u, void *stream);
+/* x(msk) = 0 for the problem's Dirichlet mask. */
+nb_status nb_bc_apply(nb_problem *p, double *x, void *stream);
+
+typedef enum { NB_PC_JACOBI = 0, NB_PC_HSMG = 1, NB_PC_NONE = 2 } nb_pc_type;
+
+typedef struct {
+  int max_iter;        /* iteration cap */
+  double abs_tol;      /* stop when sqrt(r'*mult*r)/sqrt(volume) < abs_tol */
+  int pc;              /* nb_pc_type */
+  int mixed;           /* 1: FP32 preconditioner, FP64 flexible CG */
+  int coarse_iter;     /* hsmg coarse CG iterations (reference default 10) */
+  double coarse_tol;   /* hsmg coarse CG absolute tolerance (default 1e-9) */
+} nb_solve_opts;
+
+typedef struct {
+  int iter;
+  double res_start;
+  double res_final;
+  int converged;
+  int launches;  /* kernels this solve launched on the device */
+} nb_solve_result;
+
+/* Solves A x = f (f already assembled and masked) from x0 = 0 with
+ * preconditioned CG, entirely on the device.  Follows cg_device_solve
+ * (src/krylov/bcknd/device/cg_device.f90:162-238) with device-resident
+ * scalars.  x and f are device arrays of n doubles. */
+nb_status nb_solve(nb_problem *p, double *x, const double *f,
+                   const nb_solve_opts *opts, nb_solve_result *res,
+                   void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEKO_B200_H */

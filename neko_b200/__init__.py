@@ -1,0 +1,206 @@
+"""neko_b200 -- a B200-native device backend for Neko's pressure/Helmholtz
+solve path (ax_helm, gather-scatter add, CG/flexible CG, hsmg).
+
+The compute lives in libnekob200.so (hand-written sm_100a CUDA, C ABI in
+include/neko_b200.h).  This module is the host-side mirror of the
+reference's operator interfaces, so a solve reads like the reference's
+Fortran:
+
+    ax_t%compute(w, u, coef, msh, Xh)        ->  AxHelm().compute(w, u, coef)
+    gs_t%op(u, n, GS_OP_ADD)                 ->  coef.gs.op(u, n, GS_OP_ADD)
+    bc_list_t%apply(x, n)                    ->  coef.bclst.apply(x, n)
+    ksp_t%solve(Ax, x, f, n, coef, blst, gs_h, niter) -> KspMonitor
+                                             ->  CG(...).solve(Ax, x, f, n, coef, ...)
+
+(src/math/ax.f90:43-84, src/gs/gather_scatter.f90:82-118,
+src/krylov/krylov.f90:136-157, src/krylov/precon.f90:40-66).  Device memory
+is handed over as torch CUDA tensors; torch provides allocation and streams.
+"""
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpts,
+                   SolveResult, check, load)
+
+GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
+
+__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "KspMonitor",
+           "Jacobi", "Hsmg", "GS_OP_ADD", "NekoB200Error", "load", "version"]
+
+
+def version():
+    return load().nb_version().decode()
+
+
+def _stream_handle(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    if not (t.is_cuda and t.is_contiguous()):
+        raise ValueError("expected a contiguous CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class _DeviceView:
+    """__cuda_array_interface__ wrapper so torch can view library memory."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": None}
+
+
+class Problem:
+    """Mesh + GLL space + dofmap + gather-scatter + coefficients (mesh_t,
+    space_t, dofmap_t, gs_t, coef_t) of a structured box, resident on the
+    current CUDA device."""
+
+    def __init__(self, nel, lx, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+                 periodic=(False, False, False), deform=0.0, dirichlet=True):
+        L = load()
+        ne = (ctypes.c_int * 3)(*nel)
+        lo_ = (ctypes.c_double * 3)(*lo)
+        hi_ = (ctypes.c_double * 3)(*hi)
+        per = (ctypes.c_int * 3)(*[int(bool(p)) for p in periodic])
+        h = ctypes.c_void_p()
+        torch.cuda.init()
+        check(L.nb_problem_create_box(ne, lo_, hi_, per, lx, float(deform), int(bool(dirichlet)),
+                                      ctypes.byref(h)))
+        self._h = h
+        n = ctypes.c_int64()
+        nelv, lxo, nloc, nblk, nmsk = (ctypes.c_int() for _ in range(5))
+        check(L.nb_problem_sizes(h, ctypes.byref(n), ctypes.byref(nelv), ctypes.byref(lxo),
+                                 ctypes.byref(nloc), ctypes.byref(nblk), ctypes.byref(nmsk)))
+        self.n, self.nelv, self.lx = n.value, nelv.value, lxo.value
+        self.nlocal, self.nblocks, self.nmask = nloc.value, nblk.value, nmsk.value
+        vol = ctypes.c_double()
+        check(L.nb_problem_volume(h, ctypes.byref(vol)))
+        self.volume = vol.value
+        self.nel, self.periodic, self.deform = tuple(nel), tuple(periodic), deform
+        self.gs = GatherScatter(self)
+        self.bclst = BcList(self)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise ValueError("problem destroyed")
+        return self._h
+
+    _SIZES = {"dx": lambda p: p.lx ** 2, "dxt": lambda p: p.lx ** 2, "zg": lambda p: p.lx,
+              "dof_gs": lambda p: p.nlocal, "gs_dof": lambda p: p.nlocal,
+              "blk_len": lambda p: p.nblocks, "blk_off": lambda p: p.nblocks,
+              "msk": lambda p: p.nmask}
+
+    def field(self, name):
+        """Zero-copy torch view of a device array of the problem."""
+        ptr = ctypes.c_void_p()
+        check(load().nb_problem_field(self.handle, name.encode(), ctypes.byref(ptr)))
+        size = self._SIZES.get(name, lambda p: p.n)(self)
+        typestr = "<i4" if name in ("dof_gs", "gs_dof", "blk_len", "blk_off", "msk") else "<f8"
+        if size == 0:
+            return torch.empty(0, dtype=torch.int32 if typestr == "<i4" else torch.float64,
+                               device="cuda")
+        return torch.as_tensor(_DeviceView(ptr.value, size, typestr), device="cuda")
+
+    def set_coefficients(self, h1, h2=None):
+        """Helmholtz coefficients: A = -div(h1 grad) + h2 B (ifh2 when h2 given)."""
+        h1 = h1.contiguous()
+        h2c = h2.contiguous() if h2 is not None else None
+        check(load().nb_problem_set_coefficients(self.handle, _ptr(h1),
+                                                 _ptr(h2c) if h2c is not None else None,
+                                                 int(h2 is not None)))
+
+    def zeros(self):
+        return torch.zeros(self.n, dtype=torch.float64, device="cuda")
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            load().nb_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class AxHelm:
+    """ax_helm_t: w = A u element by element (no assembly)
+    (src/math/ax_helm.f90:44-77)."""
+
+    def compute(self, w, u, coef, msh=None, Xh=None, stream=None):
+        check(load().nb_ax(coef.handle, _ptr(w), _ptr(u), _stream_handle(stream)))
+
+
+class GatherScatter:
+    """gs_t of a problem: op(u, n, GS_OP_ADD) sums all local copies."""
+
+    def __init__(self, problem):
+        self.problem = problem
+
+    def op(self, u, n=None, op=GS_OP_ADD, stream=None):
+        if op != GS_OP_ADD:
+            raise NotImplementedError("the native gs supports GS_OP_ADD; use the cuda_* "
+                                      "drop-in entry points for mul/min/max")
+        check(load().nb_gs_add(self.problem.handle, _ptr(u), _stream_handle(stream)))
+
+
+class BcList:
+    """bc_list_t with the problem's zero-Dirichlet mask."""
+
+    def __init__(self, problem):
+        self.problem = problem
+
+    def apply(self, x, n=None, stream=None):
+        check(load().nb_bc_apply(self.problem.handle, _ptr(x), _stream_handle(stream)))
+
+
+@dataclass
+class KspMonitor:
+    """ksp_monitor_t (src/krylov/krylov.f90:56-70)."""
+    iter: int
+    res_start: float
+    res_final: float
+    converged: bool
+    launches: int = 0
+
+
+class Jacobi:
+    """pc_jacobi: z = d r with d = 1/gs(diag A) (pc_jacobi.f90:86-170)."""
+    kind = NB_PC_JACOBI
+
+
+class Hsmg:
+    """pc_hsmg: additive 3-level Schwarz/FDM multigrid (pc_hsmg.f90)."""
+    kind = NB_PC_HSMG
+
+    def __init__(self, coarse_iter=10, coarse_tol=1e-9):
+        self.coarse_iter, self.coarse_tol = coarse_iter, coarse_tol
+
+
+class CG:
+    """ksp_t of type 'cg' with preconditioner M (Jacobi, Hsmg or None);
+    stops when sqrt(r' mult r / volume) < abs_tol (krylov.f90:411-421)."""
+
+    def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False):
+        self.max_iter, self.abs_tol, self.mixed = max_iter, abs_tol, mixed
+        self.M = M if M is not None else Jacobi()
+
+    def solve(self, Ax, x, f, n=None, coef=None, blst=None, gs_h=None, niter=None,
+              stream=None):
+        o = SolveOpts()
+        o.max_iter = niter if niter is not None else self.max_iter
+        o.abs_tol = self.abs_tol
+        o.pc = getattr(self.M, "kind", NB_PC_NONE) if self.M is not None else NB_PC_NONE
+        o.mixed = int(self.mixed)
+        o.coarse_iter = getattr(self.M, "coarse_iter", 10)
+        o.coarse_tol = getattr(self.M, "coarse_tol", 1e-9)
+        r = SolveResult()
+        check(load().nb_solve(coef.handle, _ptr(x), _ptr(f), ctypes.byref(o), ctypes.byref(r),
+                              _stream_handle(stream)))
+        return KspMonitor(r.iter, r.res_start, r.res_final, bool(r.converged), r.launches)

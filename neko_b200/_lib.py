@@ -1,0 +1,106 @@
+"""ctypes binding of libnekob200.so (the C ABI declared in include/neko_b200.h).
+
+The library is built in-tree by ``neko_b200/build.py``.  Loading fails with
+an ImportError-style exception when it is missing: there is no fallback
+implementation of any operator.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnekob200.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_IP = ctypes.POINTER(ctypes.c_int)
+_DP = ctypes.POINTER(ctypes.c_double)
+
+NB_OK = 0
+STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR_OOM",
+                4: "NB_ERR_CUDA", 5: "NB_ERR_NOT_CONVERGED", 6: "NB_ERR_NAN",
+                7: "NB_ERR_TIMEOUT"}
+
+NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE = 0, 1, 2
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int), ("abs_tol", ctypes.c_double),
+                ("pc", ctypes.c_int), ("mixed", ctypes.c_int),
+                ("coarse_iter", ctypes.c_int), ("coarse_tol", ctypes.c_double)]
+
+
+class SolveResult(ctypes.Structure):
+    _fields_ = [("iter", ctypes.c_int), ("res_start", ctypes.c_double),
+                ("res_final", ctypes.c_double), ("converged", ctypes.c_int),
+                ("launches", ctypes.c_int)]
+
+
+class NekoB200Error(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+# Signatures of every exported symbol (name -> (restype, argtypes)).
+SIGNATURES = {
+    # drop-in cuda_* entry points
+    "cuda_ax_helm": (None, [_P] * 15 + [_IP, _IP]),
+    "cuda_addcol4": (None, [_P, _P, _P, _P, _IP, _P]),
+    "cuda_gather_kernel": (None, [_P, _IP, _IP, _P, _P, _IP, _P, _IP, _P, _P, _IP, _P]),
+    "cuda_scatter_kernel": (None, [_P, _IP, _P, _P, _IP, _P, _IP, _P, _P, _P]),
+    "cuda_glsc3": (ctypes.c_double, [_P, _P, _P, _IP, _P]),
+    "cuda_glsc2": (ctypes.c_double, [_P, _P, _IP, _P]),
+    "cuda_glsum": (ctypes.c_double, [_P, _IP, _P]),
+    "cuda_copy": (None, [_P, _P, _IP, _P]),
+    "cuda_rzero": (None, [_P, _IP, _P]),
+    "cuda_add2s1": (None, [_P, _P, _DP, _IP, _P]),
+    "cuda_add2s2": (None, [_P, _P, _DP, _IP, _P]),
+    "cuda_col2": (None, [_P, _P, _IP, _P]),
+    "cuda_col3": (None, [_P, _P, _P, _IP, _P]),
+    "cuda_addcol3": (None, [_P, _P, _P, _IP, _P]),
+    "cuda_invcol1": (None, [_P, _IP, _P]),
+    "cuda_radd": (None, [_P, _DP, _IP, _P]),
+    "cuda_zero_dirichlet_apply_scalar": (None, [_P, _P, _IP, _P]),
+    "cuda_jacobi_update": (None, [_P] * 10 + [_IP, _IP]),
+    # native API
+    "nb_last_error": (ctypes.c_char_p, []),
+    "nb_version": (ctypes.c_char_p, []),
+    "nb_gll": (_I, [_I, _DP, _DP, _DP]),
+    "nb_box_gs_maps": (_I, [_IP, _IP, _I, _IP, _IP, _IP, _IP, _IP, _IP, _IP]),
+    "nb_problem_create_box": (_I, [_IP, _DP, _DP, _IP, _I, ctypes.c_double, _I,
+                                   ctypes.POINTER(_P)]),
+    "nb_problem_destroy": (_I, [_P]),
+    "nb_problem_sizes": (_I, [_P, ctypes.POINTER(ctypes.c_int64), _IP, _IP, _IP, _IP, _IP]),
+    "nb_problem_field": (_I, [_P, ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "nb_problem_volume": (_I, [_P, _DP]),
+    "nb_problem_set_coefficients": (_I, [_P, _P, _P, _I]),
+    "nb_ax": (_I, [_P, _P, _P, _P]),
+    "nb_gs_add": (_I, [_P, _P, _P]),
+    "nb_bc_apply": (_I, [_P, _P, _P]),
+    "nb_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult), _P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libnekob200.so and bind every symbol; raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} not found: build it with `python neko_b200/build.py` "
+            "(there is no fallback implementation)")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != NB_OK:
+        raise NekoB200Error(status, load().nb_last_error().decode(errors="replace"))

@@ -1,0 +1,364 @@
+// cg.cu -- preconditioned conjugate gradients entirely on the device.
+//
+// Same iteration as cg_device_solve (src/krylov/bcknd/device/cg_device.f90:
+// 162-238): x0 = 0, r = f; per iteration z = M r, rtz = (r, mult z),
+// beta = rtz/rtz_old (0 first), p = z + beta p, w = A p, gs add, mask,
+// pap = (w, mult p), alpha = rtz/pap, x += alpha p, r -= alpha w,
+// rnorm = sqrt((r, mult r)/volume); stop when rnorm < abs_tol.
+//
+// Differences in form, not in arithmetic: the scalars (rtz, beta, pap,
+// alpha, rnorm) live in device memory and are produced by the last block of
+// each reduction, so no iteration waits for the host (the reference copies
+// three dot products to the host and synchronises per iteration,
+// math.cu:765-797); the vector updates and the mult-weighted inner products
+// are fused (x/r update + (r,mult r) in one pass, z = d r + (r, mult z) in
+// one pass); the gather-scatter and the mask are one launch; and a chunk of
+// iterations is captured in a CUDA graph and replayed, each kernel
+// returning at once after the convergence flag is set, so the iteration
+// count is exact.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "nb_kernels.h"
+#include "nb_precond.h"
+#include "nb_problem.h"
+#include "nb_reduce.cuh"
+
+namespace nb {
+
+__global__ void jacobi_scale_kernel(double *d, const double *h1, const double *h2,
+                                    const double *B, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    double v = d[i] * h1[i];
+    if (h2) v = v + h2[i] * B[i];
+    d[i] = v;
+  }
+}
+
+__global__ void addcol4_kernel(double *w, const double *h2, const double *B, const double *u,
+                               long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    w[i] = w[i] + h2[i] * B[i] * u[i];
+}
+
+// ---------------------------------------------------------------------------
+// CG kernels.  Every kernel returns immediately once st->done is set.
+// ---------------------------------------------------------------------------
+
+// x = 0, p = 0, r = f, rtr = (r, mult r) -> res_start.
+__global__ void __launch_bounds__(kRedThreads)
+    cg_init_kernel(double *__restrict__ x, double *__restrict__ p, double *__restrict__ r,
+                   const double *__restrict__ f, const double *__restrict__ mult, long n,
+                   CgState *st, double *partials, unsigned *counter) {
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    const double ri = f[i];
+    x[i] = 0.0;
+    p[i] = 0.0;
+    r[i] = ri;
+    s += ri * mult[i] * ri;
+  }
+  double tot;
+  if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
+    const double rn = sqrt(tot) * st->norm_fac;
+    st->rtr = tot;
+    st->rnorm = rn;
+    st->res_start = rn;
+    st->rtz1 = 1.0;
+    st->iter = 0;
+    st->nan = 0;
+    st->done = fabs(rn) < 2.220446049250313e-16 ? 1 : 0;
+  }
+}
+
+// z = d r (Jacobi; d == nullptr means no preconditioner) and
+// rtz = (r, mult z); beta from the previous rtz.
+__global__ void __launch_bounds__(kRedThreads)
+    cg_precond_dot_kernel(double *__restrict__ z, const double *__restrict__ r,
+                          const double *__restrict__ d, const double *__restrict__ mult,
+                          long n, CgState *st, double *partials, unsigned *counter) {
+  if (st->done) return;
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    const double ri = r[i];
+    const double zi = d ? ri * d[i] : ri;
+    z[i] = zi;
+    s += ri * mult[i] * zi;
+  }
+  double tot;
+  if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
+    st->rtz2 = st->rtz1;
+    st->rtz1 = tot;
+    st->beta = st->iter == 0 ? 0.0 : tot / st->rtz2;
+  }
+}
+
+// rtz = (r, mult z) for an externally applied preconditioner.
+__global__ void __launch_bounds__(kRedThreads)
+    cg_dot_rz_kernel(const double *__restrict__ z, const double *__restrict__ r,
+                     const double *__restrict__ mult, long n, CgState *st, double *partials,
+                     unsigned *counter) {
+  if (st->done) return;
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads)
+    s += r[i] * mult[i] * z[i];
+  double tot;
+  if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
+    st->rtz2 = st->rtz1;
+    st->rtz1 = tot;
+    st->beta = st->iter == 0 ? 0.0 : tot / st->rtz2;
+  }
+}
+
+// p = z + beta p
+__global__ void cg_update_p_kernel(double *__restrict__ p, const double *__restrict__ z,
+                                   long n, const CgState *st) {
+  if (st->done) return;
+  const double beta = st->beta;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+// pap = (w, mult p); alpha = rtz / pap
+__global__ void __launch_bounds__(kRedThreads)
+    cg_pap_kernel(const double *__restrict__ w, const double *__restrict__ p,
+                  const double *__restrict__ mult, long n, CgState *st, double *partials,
+                  unsigned *counter) {
+  if (st->done) return;
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads)
+    s += w[i] * mult[i] * p[i];
+  double tot;
+  if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
+    st->pap = tot;
+    st->alpha = st->rtz1 / tot;
+  }
+}
+
+// x += alpha p; r -= alpha w; rtr = (r, mult r); convergence test.
+__global__ void __launch_bounds__(kRedThreads)
+    cg_update_xr_kernel(double *__restrict__ x, double *__restrict__ r,
+                        const double *__restrict__ p, const double *__restrict__ w,
+                        const double *__restrict__ mult, long n, CgState *st,
+                        double *partials, unsigned *counter) {
+  if (st->done) return;
+  const double alpha = st->alpha, malpha = -alpha;
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    x[i] = x[i] + alpha * p[i];
+    const double ri = r[i] + malpha * w[i];
+    r[i] = ri;
+    s += ri * mult[i] * ri;
+  }
+  double tot;
+  if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
+    const double rn = sqrt(tot) * st->norm_fac;
+    st->rtr = tot;
+    st->rnorm = rn;
+    st->iter += 1;
+    int done = 0;
+    if (!(rn == rn) || isinf(rn)) {
+      st->nan = 1;
+      done = 1;
+    }
+    if (rn < st->abs_tol) done = 1;
+    if (st->iter >= st->max_iter) done = 1;
+    st->done = done;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Workspace
+// ---------------------------------------------------------------------------
+static nb_status ws_fail(nb_status s, const std::string &m) {
+  set_error(m);
+  return s;
+}
+
+CgWorkspace::~CgWorkspace() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (base) cudaFree(base);
+  if (host_state) cudaFreeHost(host_state);
+}
+
+cudaError_t CgWorkspace::ensure(long n_) {
+  if (base && n == n_) return cudaSuccess;
+  if (graph_exec) {
+    cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+  }
+  if (base) cudaFree(base);
+  base = nullptr;
+  n = n_;
+  const size_t vec = ((size_t)n * 8 + 255) & ~size_t(255);
+  const size_t red = 148 * 8 * sizeof(double) + 256;
+  bytes = 4 * vec + red + sizeof(CgState) + 256;
+  cudaError_t e = cudaMalloc(&base, bytes);
+  if (e != cudaSuccess) {
+    base = nullptr;
+    return e;
+  }
+  char *b = (char *)base;
+  r = (double *)b;
+  z = (double *)(b + vec);
+  p = (double *)(b + 2 * vec);
+  w = (double *)(b + 3 * vec);
+  partials = (double *)(b + 4 * vec);
+  counter = (unsigned *)(b + 4 * vec + 148 * 8 * sizeof(double));
+  st = (CgState *)(b + 4 * vec + red);
+  e = cudaMemset(b + 4 * vec, 0, red + sizeof(CgState));
+  if (e != cudaSuccess) return e;
+  if (!host_state) {
+    e = cudaMallocHost(&host_state, sizeof(CgState));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// One CG iteration (all launches on s), precond chosen by pc.
+static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, double *x,
+                                cudaStream_t s) {
+  const long n = P->n;
+  const int rb = red_blocks(n), eg = stream_grid(n, 256);
+  if (pc) {
+    cudaError_t e = pc->apply(W.z, W.r, &W.st->done, s);
+    if (e != cudaSuccess) return e;
+    cg_dot_rz_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, n, W.st, W.partials,
+                                                W.counter);
+  } else {
+    cg_precond_dot_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.use_jacobi ? P->jdiag : nullptr,
+                                                     P->mult, n, W.st, W.partials, W.counter);
+  }
+  cg_update_p_kernel<<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
+  cudaError_t e = nb::ax_helm<double>(W.w, W.p, P->D, P->D, P->D, P->Dt, P->Dt, P->Dt, P->h1,
+                                      P->g11, P->g22, P->g33, P->g12, P->g13, P->g23, P->nelv,
+                                      P->lx, s, &W.st->done);
+  if (e != cudaSuccess) return e;
+  if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n);
+  e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->done);
+  if (e != cudaSuccess) return e;
+  cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, n, W.st, W.partials, W.counter);
+  cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(x, W.r, W.p, W.w, P->mult, n, W.st,
+                                                 W.partials, W.counter);
+  return cudaGetLastError();
+}
+
+}  // namespace nb
+
+using namespace nb;
+
+void nb_problem::invalidate_solver_cache() {
+  if (solver_ws) {
+    CgWorkspace *W = (CgWorkspace *)solver_ws;
+    if (W->graph_exec) {
+      cudaGraphExecDestroy(W->graph_exec);
+      W->graph_exec = nullptr;
+    }
+  }
+}
+
+namespace nb {
+
+// Runs the whole solve on stream s.  Iterations are replayed from a graph
+// holding `chunk` iterations; the host reads the state once per chunk.
+nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
+                   Precond *pc, nb_solve_result *res, cudaStream_t s) {
+  if (!P->solver_ws) P->solver_ws = new CgWorkspace();
+  CgWorkspace &W = *(CgWorkspace *)P->solver_ws;
+  cudaError_t e = W.ensure(P->n);
+  if (e != cudaSuccess)
+    return ws_fail(e == cudaErrorMemoryAllocation ? NB_ERR_OOM : NB_ERR_CUDA,
+                   std::string("CG workspace: ") + cudaGetErrorString(e));
+  W.use_jacobi = o.pc == NB_PC_JACOBI;
+  CgState init{};
+  init.norm_fac = 1.0 / std::sqrt(P->volume);
+  init.abs_tol = o.abs_tol;
+  init.max_iter = o.max_iter;
+  NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  const long n = P->n;
+  cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(x, W.p, W.r, f, P->mult, n, W.st,
+                                                        W.partials, W.counter);
+  NB_CUDA_TRY(cudaGetLastError());
+  // (Re)capture the iteration graph when the operands changed.
+  const void *key[4] = {x, pc, (const void *)(intptr_t)W.use_jacobi, (const void *)(intptr_t)P->ifh2};
+  bool same = W.graph_exec && !memcmp(key, W.graph_key, sizeof(key));
+  const int chunk = n > (1 << 22) ? 4 : 16;
+  if (!same) {
+    if (W.graph_exec) {
+      cudaGraphExecDestroy(W.graph_exec);
+      W.graph_exec = nullptr;
+    }
+    cudaStream_t cs;
+    NB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaSuccess;
+    for (int k = 0; k < chunk && ce == cudaSuccess; k++) ce = cg_iteration(P, W, pc, x, cs);
+    W.launches_per_iter = 6 + (P->ifh2 ? 1 : 0) + (pc ? pc->launches() : 0);
+    cudaError_t ee = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (ce != cudaSuccess) {
+      if (ee == cudaSuccess) cudaGraphDestroy(g);
+      return ws_fail(NB_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+    }
+    NB_CUDA_TRY(ee);
+    ee = cudaGraphInstantiate(&W.graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    NB_CUDA_TRY(ee);
+    memcpy(W.graph_key, key, sizeof(key));
+  }
+  CgState *hs = (CgState *)W.host_state;
+  int launches = 1;
+  for (;;) {
+    NB_CUDA_TRY(cudaGraphLaunch(W.graph_exec, s));
+    launches += chunk * W.launches_per_iter;
+    NB_CUDA_TRY(cudaMemcpyAsync(hs, W.st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    NB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hs->done) break;
+  }
+  if (res) {
+    res->iter = hs->iter;
+    res->res_start = hs->res_start;
+    res->res_final = hs->iter ? hs->rnorm : hs->res_start;
+    res->converged = !hs->nan && (hs->iter == 0 || hs->rnorm < o.abs_tol);
+    res->launches = launches;
+    // krylov_is_converged (src/krylov/krylov.f90:411-421) also fails a solve
+    // that used the whole iteration budget.
+    if (hs->iter >= o.max_iter) res->converged = 0;
+  }
+  if (hs->nan) return ws_fail(NB_ERR_NAN, "residual became NaN or Inf");
+  return NB_OK;
+}
+
+}  // namespace nb
+
+extern "C" nb_status nb_solve(nb_problem *p, double *x, const double *f,
+                              const nb_solve_opts *opts, nb_solve_result *res, void *stream) {
+  if (!p || !x || !f || !opts) {
+    set_error("null argument");
+    return NB_ERR_ARG;
+  }
+  if (opts->max_iter < 1) {
+    set_error("max_iter must be >= 1");
+    return NB_ERR_ARG;
+  }
+  Precond *pc = nullptr;
+  if (opts->pc == NB_PC_HSMG) {
+    nb_status st = hsmg_get(p, *opts, &pc);
+    if (st != NB_OK) return st;
+  } else if (opts->pc != NB_PC_JACOBI && opts->pc != NB_PC_NONE) {
+    set_error("unknown preconditioner");
+    return NB_ERR_ARG;
+  }
+  return cg_solve(p, x, f, *opts, pc, res, (cudaStream_t)stream);
+}

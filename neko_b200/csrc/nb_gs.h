@@ -1,0 +1,38 @@
+// nb_gs.h -- gather-scatter layouts of the native solver.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "nb_internal.h"
+
+namespace nb {
+
+// Fused-form maps on the host (built once from the reference-layout maps).
+struct GsHostLayout {
+  std::vector<int> seg_ptr;    // nseg + 1 offsets into seg_idx
+  std::vector<int> seg_idx;    // 0-based point indices, map order
+  std::vector<int2> pairs;     // facet pairs, 0-based
+  std::vector<unsigned char> seg_masked, pair_masked;
+  std::vector<int> extra_mask; // masked points outside every segment/pair
+};
+
+// The same on the device (pointers into one allocation owned elsewhere).
+struct GsDevice {
+  int nseg = 0, npairs = 0, nextra = 0;
+  const int *seg_ptr = nullptr, *seg_idx = nullptr;
+  const int2 *pairs = nullptr;
+  const int *extra_mask = nullptr;
+  const unsigned char *seg_masked = nullptr, *pair_masked = nullptr;
+};
+
+void gs_relayout(const GsMaps &m, const std::vector<unsigned char> &masked, long n,
+                 GsHostLayout &h);
+bool gs_pairs_regular(const GsMaps &m);
+
+template <typename T>
+cudaError_t gs_add_fused(const GsDevice &g, T *u, bool with_mask, cudaStream_t s,
+                         const int *skip = nullptr);
+
+}  // namespace nb

@@ -1,0 +1,24 @@
+// nb_kernels.h -- launchers shared between the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "nb_internal.h"
+
+namespace nb {
+
+// Stream used by drop-in entry points that take none (the reference's
+// glb_cmd_queue); the legacy default stream unless set.
+cudaStream_t default_stream();
+void set_default_stream(cudaStream_t s);
+
+template <typename T>
+cudaError_t ax_helm(T *w, const T *u, const T *dx, const T *dy, const T *dz, const T *dxt,
+                    const T *dyt, const T *dzt, const T *h1, const T *g11, const T *g22,
+                    const T *g33, const T *g12, const T *g13, const T *g23, int nelv, int lx,
+                    cudaStream_t s, const int *skip = nullptr);
+
+// Grid size for streaming kernels: a multiple of the SM count.
+int stream_grid(long n, int threads);
+
+}  // namespace nb

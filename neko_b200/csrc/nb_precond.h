@@ -1,0 +1,48 @@
+// nb_precond.h -- Krylov workspace and the preconditioner interface of the
+// native solver (the role of pc_t, src/krylov/precon.f90:40-66).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "nb_problem.h"
+
+namespace nb {
+
+// Device-resident scalars of one CG solve.
+struct CgState {
+  double norm_fac, abs_tol;
+  double rtz1, rtz2, beta, pap, alpha, rtr, rnorm, res_start;
+  int iter, max_iter, done, nan;
+};
+
+// pc_t%solve(z, r): z = M^-1 r on stream s; returns early when *skip != 0.
+struct Precond {
+  virtual ~Precond() {}
+  virtual cudaError_t apply(double *z, const double *r, const int *skip, cudaStream_t s) = 0;
+  // kernels one apply launches
+  virtual int launches() const = 0;
+};
+
+struct CgWorkspace {
+  long n = 0;
+  void *base = nullptr;
+  size_t bytes = 0;
+  double *r = nullptr, *z = nullptr, *p = nullptr, *w = nullptr, *partials = nullptr;
+  unsigned *counter = nullptr;
+  CgState *st = nullptr;
+  void *host_state = nullptr;
+  bool use_jacobi = true;
+  int launches_per_iter = 6;
+  cudaGraphExec_t graph_exec = nullptr;
+  const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  ~CgWorkspace();
+  cudaError_t ensure(long n);
+};
+
+nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
+                   Precond *pc, nb_solve_result *res, cudaStream_t s);
+
+// hsmg preconditioner of problem P, built on first use (pc_hsmg.cu).
+nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out);
+
+}  // namespace nb

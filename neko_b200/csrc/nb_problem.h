@@ -1,0 +1,73 @@
+// nb_problem.h -- the device-resident problem behind the nb_* handle API.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "nb_gs.h"
+#include "nb_internal.h"
+
+namespace nb {
+
+struct HsmgState;  // pc_hsmg.cu
+
+template <int KIND, typename T>
+cudaError_t reduce_to(const T *a, const T *b, const T *c, long n, double *partials,
+                      unsigned *counter, double *out, cudaStream_t s);
+
+cudaError_t jacobi_diag(double *d, const double *dxt, const double *dyt, const double *dzt,
+                        const double *G11, const double *G22, const double *G33,
+                        const double *G12, const double *G13, const double *G23,
+                        const unsigned char *dfrmd, bool device_form, int nel, int lx,
+                        cudaStream_t s);
+
+// d = d * h1 (+ h2 * B)
+__global__ void jacobi_scale_kernel(double *d, const double *h1, const double *h2,
+                                    const double *B, long n);
+// w += h2 * B * u
+__global__ void addcol4_kernel(double *w, const double *h2, const double *B, const double *u,
+                               long n);
+
+}  // namespace nb
+
+struct nb_problem {
+  nb::BoxSpec box{};
+  int lx = 0, nelv = 0, nmask = 0;
+  long n = 0;
+  double deform_amp = 0.0, volume = 0.0;
+  bool ifh2 = false;
+  nb::GsMaps maps;     // reference-layout maps (host copy)
+  nb::GsDevice gsd;    // fused layout (device)
+  void *arena = nullptr;
+  size_t arena_bytes = 0;
+  double *x = nullptr, *y = nullptr, *z = nullptr;
+  double *g11 = nullptr, *g22 = nullptr, *g33 = nullptr, *g12 = nullptr, *g13 = nullptr,
+         *g23 = nullptr;
+  double *h1 = nullptr, *h2 = nullptr, *B = nullptr, *mult = nullptr, *jdiag = nullptr;
+  double *D = nullptr, *Dt = nullptr, *zg = nullptr, *w3 = nullptr;
+  int *dof_gs = nullptr, *gs_dof = nullptr, *blk_len = nullptr, *blk_off = nullptr,
+      *msk = nullptr;
+  unsigned char *dfrmd = nullptr;
+  double *red_partials = nullptr, *red_out = nullptr;
+  unsigned *red_counter = nullptr;
+  // Krylov workspace (allocated on first solve)
+  void *solver_ws = nullptr;
+  size_t solver_ws_bytes = 0;
+  nb::HsmgState *hsmg = nullptr;
+
+  ~nb_problem();
+  cudaError_t update_jacobi(cudaStream_t s);
+  cudaError_t ax(double *w, const double *u, cudaStream_t s) const;
+  void invalidate_solver_cache();
+};
+
+namespace nb {
+void hsmg_free(nb_problem *p);
+
+// Deletes a half-built problem on early return.
+struct nb_problem_guard {
+  nb_problem *p;
+  explicit nb_problem_guard(nb_problem *q) : p(q) {}
+  ~nb_problem_guard() { delete p; }
+  void release() { p = nullptr; }
+};
+}  // namespace nb

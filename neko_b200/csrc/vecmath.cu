@@ -1,0 +1,305 @@
+// vecmath.cu -- vector updates, inner products, zero-Dirichlet apply and the
+// Jacobi diagonal, as drop-in replacements for the reference's device math
+// (src/math/bcknd/device/cuda/math.cu, src/bc/bcknd/device/cuda/
+// zero_dirichlet.cu, src/krylov/bcknd/device/cuda/pc_jacobi.cu), plus the
+// library runtime (error string, default stream, reduction scratch).
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+
+#include "nb_kernels.h"
+#include "nb_reduce.cuh"
+
+namespace nb {
+
+// --------------------------------------------------------------------------
+// runtime
+// --------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+void cuda_check_fatal(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
+    exit(1);
+  }
+}
+
+static cudaStream_t g_default_stream = nullptr;
+cudaStream_t default_stream() { return g_default_stream; }
+void set_default_stream(cudaStream_t s) { g_default_stream = s; }
+
+int stream_grid(long n, int threads) {
+  long b = (n + threads - 1) / threads;
+  const long cap = 148L * 16;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+// Reduction scratch of the drop-in inner products: per device, partials for
+// the largest grid, the arrival counter and the result slot.  Allocated on
+// first use and kept until exit, like the reference's cuda_buffer_reserve
+// (src/device/cuda/buffer.h:60-75).
+struct RedScratch {
+  double *partials = nullptr;
+  unsigned *counter = nullptr;
+  double *result = nullptr;
+};
+static RedScratch g_scratch[64];
+static std::mutex g_scratch_mu;
+
+static RedScratch &scratch() {
+  int dev = 0;
+  cuda_check_fatal(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  RedScratch &s = g_scratch[dev];
+  if (!s.partials) {
+    char *p = nullptr;
+    cuda_check_fatal(cudaMalloc(&p, 148 * 8 * sizeof(double) + 256 + 256), "reduction scratch");
+    cuda_check_fatal(cudaMemset(p, 0, 148 * 8 * sizeof(double) + 512), "reduction scratch");
+    s.partials = (double *)p;
+    s.counter = (unsigned *)(p + 148 * 8 * sizeof(double));
+    s.result = (double *)(p + 148 * 8 * sizeof(double) + 256);
+  }
+  return s;
+}
+
+// --------------------------------------------------------------------------
+// reductions
+// --------------------------------------------------------------------------
+template <int KIND, typename T>
+__global__ void __launch_bounds__(kRedThreads)
+    red_kernel(const T *__restrict__ a, const T *__restrict__ b, const T *__restrict__ c,
+               long n, double *partials, unsigned *counter, double *out) {
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    if (KIND == 3) s += (double)a[i] * (double)b[i] * (double)c[i];
+    if (KIND == 2) s += (double)a[i] * (double)b[i];
+    if (KIND == 1) s += (double)a[i];
+  }
+  grid_sum<kRedThreads>(s, partials, counter, out);
+}
+
+template <int KIND>
+static double host_reduce(const double *a, const double *b, const double *c, long n,
+                          cudaStream_t s) {
+  if (n <= 0) return 0.0;
+  RedScratch &r = scratch();
+  red_kernel<KIND, double><<<red_blocks(n), kRedThreads, 0, s>>>(a, b, c, n, r.partials,
+                                                                  r.counter, r.result);
+  cuda_check_fatal(cudaGetLastError(), "reduction");
+  double h = 0.0;
+  cuda_check_fatal(cudaMemcpyAsync(&h, r.result, sizeof(double), cudaMemcpyDeviceToHost, s),
+                   "reduction D2H");
+  cuda_check_fatal(cudaStreamSynchronize(s), "reduction sync");
+  return h;
+}
+
+// Device-side result variant used by the solver and the tests.
+template <int KIND, typename T>
+cudaError_t reduce_to(const T *a, const T *b, const T *c, long n, double *partials,
+                      unsigned *counter, double *out, cudaStream_t s) {
+  red_kernel<KIND, T><<<red_blocks(n), kRedThreads, 0, s>>>(a, b, c, n, partials, counter, out);
+  return cudaGetLastError();
+}
+template cudaError_t reduce_to<3, double>(const double *, const double *, const double *, long,
+                                          double *, unsigned *, double *, cudaStream_t);
+template cudaError_t reduce_to<1, double>(const double *, const double *, const double *, long,
+                                          double *, unsigned *, double *, cudaStream_t);
+
+// --------------------------------------------------------------------------
+// element-wise kernels
+// --------------------------------------------------------------------------
+#define NB_GRID_STRIDE(i, n) \
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < (n); i += (long)gridDim.x * blockDim.x)
+
+__global__ void k_copy(double *a, const double *b, long n) { NB_GRID_STRIDE(i, n) a[i] = b[i]; }
+__global__ void k_rzero(double *a, long n) { NB_GRID_STRIDE(i, n) a[i] = 0.0; }
+__global__ void k_add2s1(double *a, const double *b, double c, long n) {
+  NB_GRID_STRIDE(i, n) a[i] = c * a[i] + b[i];
+}
+__global__ void k_add2s2(double *a, const double *b, double c, long n) {
+  NB_GRID_STRIDE(i, n) a[i] = a[i] + c * b[i];
+}
+__global__ void k_col2(double *a, const double *b, long n) { NB_GRID_STRIDE(i, n) a[i] = a[i] * b[i]; }
+__global__ void k_col3(double *a, const double *b, const double *c, long n) {
+  NB_GRID_STRIDE(i, n) a[i] = b[i] * c[i];
+}
+__global__ void k_addcol3(double *a, const double *b, const double *c, long n) {
+  NB_GRID_STRIDE(i, n) a[i] = a[i] + b[i] * c[i];
+}
+__global__ void k_addcol4(double *a, const double *b, const double *c, const double *d, long n) {
+  NB_GRID_STRIDE(i, n) a[i] = a[i] + b[i] * c[i] * d[i];
+}
+__global__ void k_invcol1(double *a, long n) { NB_GRID_STRIDE(i, n) a[i] = 1.0 / a[i]; }
+__global__ void k_radd(double *a, double c, long n) { NB_GRID_STRIDE(i, n) a[i] = a[i] + c; }
+
+// zero_dirichlet_apply_scalar_kernel semantics: msk(0) is the count, entries
+// 1..m-1 are 1-based point indices.
+__global__ void k_zero_dirichlet(const int *__restrict__ msk, double *__restrict__ x, int m) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int str = blockDim.x * gridDim.x;
+  for (int i = idx + 1; i < m; i += str) x[msk[i] - 1] = 0.0;
+}
+
+// Stiffness diagonal from the G factors.  DEVICE_FORM adds the boundary
+// cross terms on every face point as the reference device kernel does
+// (pc_jacobi.cu:40-99); otherwise the CPU form applies (pc_jacobi.f90:
+// 174-264): cross terms only at element corners, only for elements flagged
+// deformed.
+template <int LX, bool DEVICE_FORM>
+__global__ void k_jacobi_diag(double *__restrict__ d, const double *__restrict__ dxt,
+                              const double *__restrict__ dyt, const double *__restrict__ dzt,
+                              const double *__restrict__ G11, const double *__restrict__ G22,
+                              const double *__restrict__ G33, const double *__restrict__ G12,
+                              const double *__restrict__ G13, const double *__restrict__ G23,
+                              const unsigned char *__restrict__ dfrmd, int nel) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  constexpr int L3 = LX * LX * LX;
+  const long e = idx / L3;
+  if (e >= nel) return;
+  const int ijk = (int)(idx - e * L3);
+  const int i = ijk % LX, j = (ijk / LX) % LX, k = ijk / (LX * LX);
+  const long o = e * L3;
+  double s = 0.0;
+  for (int l = 0; l < LX; l++) {
+    const double t = dxt[i + LX * l];
+    s += G11[o + l + LX * j + LX * LX * k] * (t * t);
+  }
+  for (int l = 0; l < LX; l++) {
+    const double t = dyt[j + LX * l];
+    s += G22[o + i + LX * l + LX * LX * k] * (t * t);
+  }
+  for (int l = 0; l < LX; l++) {
+    const double t = dzt[k + LX * l];
+    s += G33[o + i + LX * j + LX * LX * l] * (t * t);
+  }
+  const long p = o + ijk;
+  const double xi = dxt[i + LX * i], yj = dyt[j + LX * j], zk = dzt[k + LX * k];
+  const bool bi = i == 0 || i == LX - 1, bj = j == 0 || j == LX - 1, bk = k == 0 || k == LX - 1;
+  if (DEVICE_FORM) {
+    if (bi) s += G12[p] * xi * yj + G13[p] * xi * zk;
+    if (bj) s += G12[p] * yj * xi + G23[p] * yj * zk;
+    if (bk) s += G13[p] * zk * xi + G23[p] * zk * yj;
+  } else if (dfrmd && dfrmd[e] && bi && bj && bk) {
+    // the three corner loops of jacobi_update_lx each hit a corner once
+    s = s + G12[p] * xi * yj + G13[p] * xi * zk;
+    s = s + G12[p] * yj * xi + G23[p] * yj * zk;
+    s = s + G13[p] * zk * xi + G23[p] * zk * yj;
+  }
+  d[p] = s;
+}
+
+cudaError_t jacobi_diag(double *d, const double *dxt, const double *dyt, const double *dzt,
+                        const double *G11, const double *G22, const double *G33,
+                        const double *G12, const double *G13, const double *G23,
+                        const unsigned char *dfrmd, bool device_form, int nel, int lx,
+                        cudaStream_t s) {
+  const long n = (long)nel * lx * lx * lx;
+  const int threads = 256;
+  const int blocks = (int)((n + threads - 1) / threads);
+  if (n == 0) return cudaSuccess;
+#define NB_J(N)                                                                                \
+  case N:                                                                                      \
+    if (device_form)                                                                           \
+      k_jacobi_diag<N, true><<<blocks, threads, 0, s>>>(d, dxt, dyt, dzt, G11, G22, G33, G12,  \
+                                                        G13, G23, dfrmd, nel);                 \
+    else                                                                                       \
+      k_jacobi_diag<N, false><<<blocks, threads, 0, s>>>(d, dxt, dyt, dzt, G11, G22, G33, G12, \
+                                                         G13, G23, dfrmd, nel);                \
+    break;
+  switch (lx) {
+    NB_J(2) NB_J(3) NB_J(4) NB_J(5) NB_J(6) NB_J(7) NB_J(8) NB_J(9) NB_J(10) NB_J(11)
+    NB_J(12) NB_J(13) NB_J(14) NB_J(15) NB_J(16)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef NB_J
+  return cudaGetLastError();
+}
+
+}  // namespace nb
+
+using nb::stream_grid;
+
+#define NB_LAUNCH(kern, n, s, ...)                                              \
+  do {                                                                          \
+    if ((n) > 0) {                                                              \
+      kern<<<stream_grid((n), 256), 256, 0, (cudaStream_t)(s)>>>(__VA_ARGS__);  \
+      nb::cuda_check_fatal(cudaGetLastError(), #kern);                          \
+    }                                                                           \
+  } while (0)
+
+extern "C" {
+
+double cuda_glsc3(void *a, void *b, void *c, int *n, void *stream) {
+  return nb::host_reduce<3>((const double *)a, (const double *)b, (const double *)c, *n,
+                            (cudaStream_t)stream);
+}
+double cuda_glsc2(void *a, void *b, int *n, void *stream) {
+  return nb::host_reduce<2>((const double *)a, (const double *)b, nullptr, *n,
+                            (cudaStream_t)stream);
+}
+double cuda_glsum(void *a, int *n, void *stream) {
+  return nb::host_reduce<1>((const double *)a, nullptr, nullptr, *n, (cudaStream_t)stream);
+}
+
+void cuda_copy(void *a, void *b, int *n, void *s) {
+  NB_LAUNCH(nb::k_copy, *n, s, (double *)a, (const double *)b, *n);
+}
+void cuda_rzero(void *a, int *n, void *s) { NB_LAUNCH(nb::k_rzero, *n, s, (double *)a, *n); }
+void cuda_add2s1(void *a, void *b, double *c1, int *n, void *s) {
+  NB_LAUNCH(nb::k_add2s1, *n, s, (double *)a, (const double *)b, *c1, *n);
+}
+void cuda_add2s2(void *a, void *b, double *c1, int *n, void *s) {
+  NB_LAUNCH(nb::k_add2s2, *n, s, (double *)a, (const double *)b, *c1, *n);
+}
+void cuda_col2(void *a, void *b, int *n, void *s) {
+  NB_LAUNCH(nb::k_col2, *n, s, (double *)a, (const double *)b, *n);
+}
+void cuda_col3(void *a, void *b, void *c, int *n, void *s) {
+  NB_LAUNCH(nb::k_col3, *n, s, (double *)a, (const double *)b, (const double *)c, *n);
+}
+void cuda_addcol3(void *a, void *b, void *c, int *n, void *s) {
+  NB_LAUNCH(nb::k_addcol3, *n, s, (double *)a, (const double *)b, (const double *)c, *n);
+}
+void cuda_addcol4(void *a, void *b, void *c, void *d, int *n, void *s) {
+  NB_LAUNCH(nb::k_addcol4, *n, s, (double *)a, (const double *)b, (const double *)c,
+            (const double *)d, *n);
+}
+void cuda_invcol1(void *a, int *n, void *s) { NB_LAUNCH(nb::k_invcol1, *n, s, (double *)a, *n); }
+void cuda_radd(void *a, double *c, int *n, void *s) {
+  NB_LAUNCH(nb::k_radd, *n, s, (double *)a, *c, *n);
+}
+
+void cuda_zero_dirichlet_apply_scalar(void *msk, void *x, int *m, void *stream) {
+  if (*m <= 1) return;
+  const int threads = 1024;
+  const int blocks = (*m + threads - 1) / threads;
+  nb::k_zero_dirichlet<<<blocks, threads, 0, (cudaStream_t)stream>>>((const int *)msk,
+                                                                     (double *)x, *m);
+  nb::cuda_check_fatal(cudaGetLastError(), "cuda_zero_dirichlet_apply_scalar");
+}
+
+void cuda_jacobi_update(void *d, void *dxt, void *dyt, void *dzt, void *G11, void *G22,
+                        void *G33, void *G12, void *G13, void *G23, int *nel, int *lx) {
+  if (*lx < 2 || *lx > 16) {
+    fprintf(stderr, "cuda_jacobi_update: size not supported: %d\n", *lx);
+    exit(1);
+  }
+  cudaError_t e = nb::jacobi_diag((double *)d, (const double *)dxt, (const double *)dyt,
+                                  (const double *)dzt, (const double *)G11,
+                                  (const double *)G22, (const double *)G33,
+                                  (const double *)G12, (const double *)G13,
+                                  (const double *)G23, nullptr, true, *nel, *lx,
+                                  nb::default_stream());
+  nb::cuda_check_fatal(e, "cuda_jacobi_update");
+}
+
+const char *nb_last_error(void) { return nb::g_last_error.c_str(); }
+const char *nb_version(void) { return "neko_b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,43 @@
+// neko_oracle.h -- internal header of the CPU oracle (test infrastructure).
+// Shared between the setup half (neko_oracle.cpp) and the solve half
+// (neko_oracle_solve.cpp).  Nothing in the neko_b200 product includes it.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace nko {
+struct Mesh;
+}
+// ---------------------------------------------------------------------------
+// Problem object: mesh + space + dofmap + gs maps + coef (+ bc mask).
+// ---------------------------------------------------------------------------
+struct OrProblem {
+  nko::Mesh *meshp = nullptr;
+  int lx = 0, nelv = 0;
+  long n = 0;
+  // space_t (src/sem/space.f90:149-320)
+  std::vector<double> zg, wx, w3, dx, dxt;
+  // dofmap_t (src/sem/dofmap.f90:96-161)
+  std::vector<int64_t> dof;
+  std::vector<double> x, y, z;
+  int glb_mpts = 0, glb_meds = 0;
+  // gs_t local maps (src/gs/gather_scatter.f90:513-1375)
+  int nlocal = 0, local_facet_offset = 0, nlocal_blks = 0;
+  std::vector<int> local_dof_gs, local_gs_dof, blk_len, blk_off;
+  // coef_t (src/sem/coef.f90)
+  std::vector<double> g11, g22, g33, g12, g13, g23, jac, jacinv, B, mult, h1, h2;
+  double volume = 0;
+  bool ifh2 = false;
+  // zero Dirichlet mask, 1-based (src/bc/bc.f90:434-593)
+  std::vector<int> msk;
+};
+
+
+inline long or_lin(int i, int j, int k, int e, int lx) {  // 1-based -> 0-based
+  return (long)(i - 1) + (long)lx * ((j - 1) + (long)lx * ((k - 1) + (long)lx * (e - 1)));
+}
+
+// gs_op_vector(GS_OP_ADD) on a field of P's dofmap.
+void or_gs_add_impl(const OrProblem &P, double *u);
+const int *or_facet_neigh(const OrProblem &P);
+int or_dfrmd_el(const OrProblem &P, int e);

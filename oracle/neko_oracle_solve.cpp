@@ -1,0 +1,240 @@
+// neko_oracle_solve.cpp -- CPU restatement of the solve half of Neko's
+// pressure/Helmholtz path: ax_helm, zero-Dirichlet apply, Jacobi, glsc3 and
+// preconditioned CG.  TEST INFRASTRUCTURE ONLY (see neko_oracle.cpp).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "neko_oracle.h"
+
+namespace {
+
+// ax_helm_lx (src/math/bcknd/cpu/ax_helm_cpu.f90:180-290) plus the h2 term of
+// ax_helm_compute (ax_helm_cpu.f90:156-163).  Dx = Dy = Dz for GLL spaces.
+void ax_helm(const OrProblem &P, double *w, const double *u) {
+  const int lx = P.lx, lxy = lx * lx, lxyz = lxy * lx;
+  const double *Dx = P.dx.data(), *Dxt = P.dxt.data();
+  auto D = [&](int i, int k) { return Dx[i + lx * k]; };
+  auto Dt = [&](int i, int k) { return Dxt[i + lx * k]; };
+  std::vector<double> wur(lxyz), wus(lxyz), wut(lxyz), ur(lxyz), us(lxyz), ut(lxyz);
+  for (int e = 0; e < P.nelv; e++) {
+    const size_t o = (size_t)e * lxyz;
+    const double *ue = u + o;
+    double *we = w + o;
+    for (int j = 0; j < lxy; j++)
+      for (int i = 0; i < lx; i++) {
+        double t = 0.0;
+        for (int k = 0; k < lx; k++) t = t + D(i, k) * ue[k + lx * j];
+        wur[i + lx * j] = t;
+      }
+    for (int k = 0; k < lx; k++)
+      for (int j = 0; j < lx; j++)
+        for (int i = 0; i < lx; i++) {
+          double t = 0.0;
+          for (int l = 0; l < lx; l++) t = t + D(j, l) * ue[i + lx * l + lxy * k];
+          wus[i + lx * j + lxy * k] = t;
+        }
+    for (int k = 0; k < lx; k++)
+      for (int i = 0; i < lxy; i++) {
+        double t = 0.0;
+        for (int l = 0; l < lx; l++) t = t + D(k, l) * ue[i + lxy * l];
+        wut[i + lxy * k] = t;
+      }
+    for (int i = 0; i < lxyz; i++) {
+      const size_t g = o + i;
+      ur[i] = P.h1[g] * (P.g11[g] * wur[i] + P.g12[g] * wus[i] + P.g13[g] * wut[i]);
+      us[i] = P.h1[g] * (P.g12[g] * wur[i] + P.g22[g] * wus[i] + P.g23[g] * wut[i]);
+      ut[i] = P.h1[g] * (P.g13[g] * wur[i] + P.g23[g] * wus[i] + P.g33[g] * wut[i]);
+    }
+    for (int j = 0; j < lxy; j++)
+      for (int i = 0; i < lx; i++) {
+        double t = 0.0;
+        for (int k = 0; k < lx; k++) t = t + Dt(i, k) * ur[k + lx * j];
+        we[i + lx * j] = t;
+      }
+    for (int k = 0; k < lx; k++)
+      for (int j = 0; j < lx; j++)
+        for (int i = 0; i < lx; i++) {
+          double t = 0.0;
+          for (int l = 0; l < lx; l++) t = t + Dt(j, l) * us[i + lx * l + lxy * k];
+          we[i + lx * j + lxy * k] = we[i + lx * j + lxy * k] + t;
+        }
+    for (int k = 0; k < lx; k++)
+      for (int i = 0; i < lxy; i++) {
+        double t = 0.0;
+        for (int l = 0; l < lx; l++) t = t + Dt(k, l) * ut[i + lxy * l];
+        we[i + lxy * k] = we[i + lxy * k] + t;
+      }
+  }
+  if (P.ifh2)
+    for (long i = 0; i < P.n; i++) w[i] = w[i] + P.h2[i] * P.B[i] * u[i];
+}
+
+// zero_dirichlet apply (src/bc/zero_dirichlet.f90:92-172): x(msk) = 0.
+void bc_apply(const OrProblem &P, double *x) {
+  for (int m : P.msk) x[m - 1] = 0.0;
+}
+
+// glsc3 (src/math/math.f90:1286-1306): sequential sum of a*b*c.
+double glsc3(const double *a, const double *b, const double *c, long n) {
+  double t = 0.0;
+  for (long i = 0; i < n; i++) t = t + a[i] * b[i] * c[i];
+  return t;
+}
+
+// jacobi_update_lx (src/krylov/bcknd/cpu/pc_jacobi.f90:174-264) followed by
+// col2(h1), addcol3(h2,B) when ifh2, gs add and invcol1 (pc_jacobi.f90:95-170).
+void jacobi_update(const OrProblem &P, std::vector<double> &d) {
+  const int lx = P.lx, lxy = lx * lx, lxyz = lxy * lx;
+  d.assign(P.n, 0.0);
+  auto dt = [&](int i, int l) { return P.dxt[(i - 1) + lx * (l - 1)]; };
+  for (int e = 1; e <= P.nelv; e++) {
+    const size_t o = (size_t)(e - 1) * lxyz;
+    auto I = [&](int i, int j, int k) { return o + (i - 1) + lx * (j - 1) + lxy * (k - 1); };
+    for (int l = 1; l <= lx; l++)
+      for (int k = 1; k <= lx; k++)
+        for (int j = 1; j <= lx; j++)
+          for (int i = 1; i <= lx; i++)
+            d[I(i, j, k)] = d[I(i, j, k)] + P.g11[I(l, j, k)] * (dt(i, l) * dt(i, l));
+    for (int l = 1; l <= lx; l++)
+      for (int k = 1; k <= lx; k++)
+        for (int j = 1; j <= lx; j++)
+          for (int i = 1; i <= lx; i++)
+            d[I(i, j, k)] = d[I(i, j, k)] + P.g22[I(i, l, k)] * (dt(j, l) * dt(j, l));
+    for (int l = 1; l <= lx; l++)
+      for (int k = 1; k <= lx; k++)
+        for (int j = 1; j <= lx; j++)
+          for (int i = 1; i <= lx; i++)
+            d[I(i, j, k)] = d[I(i, j, k)] + P.g33[I(i, j, l)] * (dt(k, l) * dt(k, l));
+    if (or_dfrmd_el(P, e - 1)) {
+      for (int j = 1; j <= lx; j += lx - 1)
+        for (int k = 1; k <= lx; k += lx - 1) {
+          d[I(1, j, k)] = d[I(1, j, k)] + P.g12[I(1, j, k)] * dt(1, 1) * dt(j, j) +
+                          P.g13[I(1, j, k)] * dt(1, 1) * dt(k, k);
+          d[I(lx, j, k)] = d[I(lx, j, k)] + P.g12[I(lx, j, k)] * dt(lx, lx) * dt(j, j) +
+                           P.g13[I(lx, j, k)] * dt(lx, lx) * dt(k, k);
+        }
+      for (int i = 1; i <= lx; i += lx - 1)
+        for (int k = 1; k <= lx; k += lx - 1) {
+          d[I(i, 1, k)] = d[I(i, 1, k)] + P.g12[I(i, 1, k)] * dt(1, 1) * dt(i, i) +
+                          P.g23[I(i, 1, k)] * dt(1, 1) * dt(k, k);
+          d[I(i, lx, k)] = d[I(i, lx, k)] + P.g12[I(i, lx, k)] * dt(lx, lx) * dt(i, i) +
+                           P.g23[I(i, lx, k)] * dt(lx, lx) * dt(k, k);
+        }
+      for (int i = 1; i <= lx; i += lx - 1)
+        for (int j = 1; j <= lx; j += lx - 1) {
+          d[I(i, j, 1)] = d[I(i, j, 1)] + P.g13[I(i, j, 1)] * dt(1, 1) * dt(i, i) +
+                          P.g23[I(i, j, 1)] * dt(1, 1) * dt(j, j);
+          d[I(i, j, lx)] = d[I(i, j, lx)] + P.g13[I(i, j, lx)] * dt(lx, lx) * dt(i, i) +
+                           P.g23[I(i, j, lx)] * dt(lx, lx) * dt(j, j);
+        }
+    }
+  }
+  for (long i = 0; i < P.n; i++) d[i] = d[i] * P.h1[i];
+  if (P.ifh2)
+    for (long i = 0; i < P.n; i++) d[i] = d[i] + P.h2[i] * P.B[i];
+  or_gs_add_impl(P, d.data());
+  for (long i = 0; i < P.n; i++) d[i] = 1.0 / d[i];
+}
+
+}  // namespace
+
+// cg_solve (src/krylov/bcknd/cpu/cg.f90:140-279): PCG with the deferred
+// x update over CG_P_SPACE = 7 directions and NEKO_BLK_SIZE blocking.
+// Stops when sqrt(r'*mult*r)/sqrt(volume) < abs_tol (krylov.f90:411-421).
+int or_cg_solve_impl(const OrProblem &P, double *x, const double *f, int max_iter,
+                     double abs_tol,
+                     const std::function<void(double *, const double *)> &M,
+                     double *res_start, double *res_final) {
+  const long n = P.n;
+  const int CG_P_SPACE = 7, BLK = 1024;  // NEKO_BLK_SIZE default (configure.ac:30-32)
+  std::vector<double> w(n), r(n), z(n), p((size_t)n * CG_P_SPACE), alpha(CG_P_SPACE);
+  const double norm_fac = 1.0 / std::sqrt(P.volume);
+  double rtz1 = 1.0, rtr = 0.0;
+  for (long i = 0; i < n; i++) {
+    x[i] = 0.0;
+    p[(size_t)(CG_P_SPACE - 1) * n + i] = 0.0;
+    r[i] = f[i];
+    rtr = rtr + (r[i] * P.mult[i] * r[i]);
+  }
+  double rnorm = std::sqrt(rtr) * norm_fac;
+  *res_start = rnorm;
+  *res_final = rnorm;
+  if (std::fabs(rnorm) < 2.220446049250313e-16) return 0;
+  int p_prev = CG_P_SPACE, p_cur = 1, iter;
+  for (iter = 1; iter <= max_iter; iter++) {
+    M(z.data(), r.data());
+    double rtz2 = rtz1;
+    rtz1 = glsc3(r.data(), P.mult.data(), z.data(), n);
+    double beta = rtz1 / rtz2;
+    if (iter == 1) beta = 0.0;
+    double *pc = &p[(size_t)(p_cur - 1) * n], *pp = &p[(size_t)(p_prev - 1) * n];
+    for (long i = 0; i < n; i++) pc[i] = z[i] + beta * pp[i];
+    ax_helm(P, w.data(), pc);
+    or_gs_add_impl(P, w.data());
+    bc_apply(P, w.data());
+    double pap = glsc3(w.data(), P.mult.data(), pc, n);
+    alpha[p_cur - 1] = rtz1 / pap;
+    double tmp = 0.0;  // second_cg_part (cg.f90:261-279)
+    for (long i = 0; i < n; i++) {
+      r[i] = r[i] - alpha[p_cur - 1] * w[i];
+      tmp = tmp + r[i] * r[i] * P.mult[i];
+    }
+    rtr = tmp;
+    rnorm = std::sqrt(rtr) * norm_fac;
+    if (p_cur == CG_P_SPACE || rnorm < abs_tol || iter == max_iter) {
+      for (long i = 0; i < n; i += BLK) {
+        if (i + BLK <= n) {
+          double xp[BLK];
+          for (int k = 0; k < BLK; k++) xp[k] = 0.0;
+          for (int j = 1; j <= p_cur; j++)
+            for (int k = 0; k < BLK; k++)
+              xp[k] = xp[k] + alpha[j - 1] * p[(size_t)(j - 1) * n + i + k];
+          for (int k = 0; k < BLK; k++) x[i + k] = x[i + k] + xp[k];
+        } else {
+          for (long k = 0; k < n - i; k++) {
+            double t = 0.0;
+            for (int j = 1; j <= p_cur; j++) t = t + alpha[j - 1] * p[(size_t)(j - 1) * n + i + k];
+            x[i + k] = x[i + k] + t;
+          }
+        }
+      }
+      p_prev = p_cur;
+      p_cur = 1;
+      if (rnorm < abs_tol) break;
+    } else {
+      p_prev = p_cur;
+      p_cur = p_cur + 1;
+    }
+  }
+  *res_final = rnorm;
+  return iter > max_iter ? max_iter : iter;
+}
+
+extern "C" {
+
+void or_ax_helm(OrProblem *P, double *w, const double *u) { ax_helm(*P, w, u); }
+void or_bc_apply(OrProblem *P, double *x) { bc_apply(*P, x); }
+double or_glsc3(const double *a, const double *b, const double *c, long n) {
+  return glsc3(a, b, c, n);
+}
+void or_jacobi_update(OrProblem *P, double *d_out) {
+  std::vector<double> d;
+  jacobi_update(*P, d);
+  std::memcpy(d_out, d.data(), sizeof(double) * P->n);
+}
+
+// Jacobi-PCG (pc_jacobi.f90 solve: z = d * r).  Returns the iteration count.
+int or_cg_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double abs_tol,
+                 double *res_start, double *res_final) {
+  std::vector<double> d;
+  jacobi_update(*P, d);
+  auto M = [&](double *z, const double *r) {
+    for (long i = 0; i < P->n; i++) z[i] = r[i] * d[i];  // col3 (pc_jacobi.f90:86-92)
+  };
+  return or_cg_solve_impl(*P, x, f, max_iter, abs_tol, M, res_start, res_final);
+}
+
+}  // extern "C"

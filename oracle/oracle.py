@@ -1,0 +1,241 @@
+"""ctypes front end of the CPU oracle (oracle/libneko_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by bench.py's CPU-baseline leg.  It is the checker, never part of the
+neko_b200 product path.  The shared library restates the reference's CPU
+code (see the citations in neko_oracle.cpp / neko_oracle_solve.cpp).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libneko_oracle.so")
+_lib = None
+
+_P = ctypes.c_void_p
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_L = ctypes.POINTER(ctypes.c_int64)
+
+
+def build():
+    """Compile the oracle with its Makefile (g++ only, no GPU needed)."""
+    global _lib
+    if _lib is None:
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        sig = {
+            "or_box_create": (_P, [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [ctypes.c_int] * 4),
+            "or_elements_create": (_P, [ctypes.c_int, _I, _D, ctypes.c_int]),
+            "or_deform_sine": (None, [_P, ctypes.c_double]),
+            "or_coef_init": (None, [_P]),
+            "or_bc_boundary": (None, [_P]),
+            "or_destroy": (None, [_P]),
+            "or_n": (ctypes.c_long, [_P]),
+            "or_nelv": (ctypes.c_int, [_P]),
+            "or_lx": (ctypes.c_int, [_P]),
+            "or_nlocal": (ctypes.c_int, [_P]),
+            "or_local_facet_offset": (ctypes.c_int, [_P]),
+            "or_nblks": (ctypes.c_int, [_P]),
+            "or_nmsk": (ctypes.c_int, [_P]),
+            "or_volume": (ctypes.c_double, [_P]),
+            "or_glb_mpts": (ctypes.c_int, [_P]),
+            "or_glb_meds": (ctypes.c_int, [_P]),
+            "or_dfrmd": (ctypes.c_int, [_P, ctypes.c_int]),
+            "or_get_i64": (None, [_P, ctypes.c_char_p, _L]),
+            "or_get_i32": (None, [_P, ctypes.c_char_p, _I]),
+            "or_get_f64": (None, [_P, ctypes.c_char_p, _D]),
+            "or_set_f64": (None, [_P, ctypes.c_char_p, _D]),
+            "or_set_ifh2": (None, [_P, ctypes.c_int]),
+            "or_gs_add": (None, [_P, _D]),
+            "or_ax_helm": (None, [_P, _D, _D]),
+            "or_bc_apply": (None, [_P, _D]),
+            "or_glsc3": (ctypes.c_double, [_D, _D, _D, ctypes.c_long]),
+            "or_jacobi_update": (None, [_P, _D]),
+            "or_cg_jacobi": (ctypes.c_int, [_P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
+            "or_fd_weights_full": (None, [ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, _D]),
+            "or_zwgll": (None, [ctypes.c_int, _D, _D]),
+            "or_dgll": (None, [ctypes.c_int, _D, _D, _D]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+class OracleProblem:
+    """Mesh + GLL space + dofmap + gs maps (+ coef, bc) built on the CPU the
+    way the reference builds them."""
+
+    def __init__(self, handle):
+        self.h = handle
+        L = lib()
+        self.n = L.or_n(handle)
+        self.nelv = L.or_nelv(handle)
+        self.lx = L.or_lx(handle)
+        self.has_coef = False
+
+    @classmethod
+    def box(cls, nel, lx, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), periodic=(False, False, False)):
+        nx, ny, nz = nel
+        h = lib().or_box_create(nx, ny, nz, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
+                                int(periodic[0]), int(periodic[1]), int(periodic[2]), lx)
+        return cls(h)
+
+    @classmethod
+    def from_elements(cls, ids, xyz, lx):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        nelv = ids.shape[0]
+        h = lib().or_elements_create(nelv, ids.ctypes.data_as(_I), _dp(xyz), lx)
+        return cls(h)
+
+    def deform_sine(self, amp):
+        lib().or_deform_sine(self.h, amp)
+
+    def coef(self):
+        lib().or_coef_init(self.h)
+        self.has_coef = True
+
+    def bc_boundary(self):
+        lib().or_bc_boundary(self.h)
+
+    def close(self):
+        if self.h:
+            lib().or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- sizes ---------------------------------------------------------
+    @property
+    def nlocal(self):
+        return lib().or_nlocal(self.h)
+
+    @property
+    def local_facet_offset(self):
+        return lib().or_local_facet_offset(self.h)
+
+    @property
+    def nblks(self):
+        return lib().or_nblks(self.h)
+
+    @property
+    def volume(self):
+        return lib().or_volume(self.h)
+
+    @property
+    def glb_mpts(self):
+        return lib().or_glb_mpts(self.h)
+
+    @property
+    def glb_meds(self):
+        return lib().or_glb_meds(self.h)
+
+    def dfrmd(self):
+        return np.array([lib().or_dfrmd(self.h, e) for e in range(self.nelv)], dtype=bool)
+
+    # --- arrays --------------------------------------------------------
+    def dof(self):
+        out = np.zeros(self.n, dtype=np.int64)
+        lib().or_get_i64(self.h, b"dof", out.ctypes.data_as(_L))
+        return out
+
+    def i32(self, name):
+        size = {"dof_gs": self.nlocal, "gs_dof": self.nlocal, "blk_len": self.nblks,
+                "blk_off": self.nblks, "msk": lib().or_nmsk(self.h),
+                "facet_neigh": 6 * self.nelv}[name]
+        out = np.zeros(size, dtype=np.int32)
+        if size:
+            lib().or_get_i32(self.h, name.encode(), out.ctypes.data_as(_I))
+        return out
+
+    def f64(self, name):
+        size = {"zg": self.lx, "wx": self.lx, "dx": self.lx ** 2, "dxt": self.lx ** 2,
+                "w3": self.lx ** 3}.get(name, self.n)
+        out = np.zeros(size, dtype=np.float64)
+        lib().or_get_f64(self.h, name.encode(), _dp(out))
+        return out
+
+    def set_f64(self, name, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        assert arr.size == self.n
+        lib().or_set_f64(self.h, name.encode(), _dp(arr))
+
+    def set_ifh2(self, flag):
+        lib().or_set_ifh2(self.h, int(bool(flag)))
+
+    # --- operators -----------------------------------------------------
+    def gs_add(self, u):
+        u = np.array(u, dtype=np.float64, copy=True)
+        lib().or_gs_add(self.h, _dp(u))
+        return u
+
+    def ax_helm(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        w = np.zeros_like(u)
+        lib().or_ax_helm(self.h, _dp(w), _dp(u))
+        return w
+
+    def bc_apply(self, x):
+        x = np.array(x, dtype=np.float64, copy=True)
+        lib().or_bc_apply(self.h, _dp(x))
+        return x
+
+    def jacobi_diag(self):
+        d = np.zeros(self.n)
+        lib().or_jacobi_update(self.h, _dp(d))
+        return d
+
+    def cg_jacobi(self, f, max_iter, abs_tol):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        x = np.zeros_like(f)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        it = lib().or_cg_jacobi(self.h, _dp(x), _dp(f), max_iter, abs_tol,
+                                ctypes.byref(r0), ctypes.byref(r1))
+        return x, it, r0.value, r1.value
+
+
+def fd_weights_full(xi, x, m):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.size - 1
+    c = np.zeros((m + 1) * (n + 1))
+    lib().or_fd_weights_full(xi, _dp(x), n, m, _dp(c))
+    return c.reshape(m + 1, n + 1).T  # c[j, k]
+
+
+def gll(lx):
+    z = np.zeros(lx)
+    w = np.zeros(lx)
+    lib().or_zwgll(lx, _dp(z), _dp(w))
+    d = np.zeros(lx * lx)
+    dt = np.zeros(lx * lx)
+    lib().or_dgll(lx, _dp(z), _dp(d), _dp(dt))
+    return z, w, d.reshape(lx, lx, order="F")
+
+
+def glsc3(a, b, c):
+    a, b, c = (np.ascontiguousarray(v, dtype=np.float64) for v in (a, b, c))
+    return lib().or_glsc3(_dp(a), _dp(b), _dp(c), a.size)

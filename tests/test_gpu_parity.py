@@ -1,0 +1,268 @@
+"""GPU parity of the neko_b200 CUDA path against the CPU oracle.
+
+Tolerances: gather-scatter and map-driven ops are bit-exact (same summation
+order as the reference); FP64 ax_helm agrees to 1e-12 relative (max-norm);
+geometric factors to 1e-12 relative; Krylov iteration counts within +-1.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+AX_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import neko_b200
+    neko_b200.load()
+    return neko_b200
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _cuda(a):
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _pair(nb, oracle, nel, lx, periodic=(False,) * 3, deform=0.0, lo=0.0, hi=1.0, dirichlet=True):
+    P = nb.Problem(nel, lx, lo=(lo,) * 3, hi=(hi,) * 3, periodic=periodic, deform=deform,
+                   dirichlet=dirichlet)
+    O = oracle.OracleProblem.box(nel, lx, lo=(lo,) * 3, hi=(hi,) * 3, periodic=periodic)
+    if deform:
+        O.deform_sine(deform)
+    O.coef()
+    if dirichlet:
+        O.bc_boundary()
+    return P, O
+
+
+CASES = [((8, 8, 8), 8, (False,) * 3, 0.0, 0.0, 1.0),
+         ((3, 4, 5), 5, (False,) * 3, 0.0, 0.0, 1.0),
+         ((4, 4, 4), 8, (True,) * 3, 0.05, 0.0, 2 * np.pi),
+         ((3, 3, 3), 10, (True, False, True), 0.05, 0.0, 2 * np.pi),
+         ((2, 2, 2), 16, (False,) * 3, 0.0, 0.0, 1.0),
+         ((5, 3, 2), 2, (False,) * 3, 0.0, 0.0, 1.0)]
+
+
+@pytest.mark.parametrize("nel,lx,per,amp,lo,hi", CASES)
+def test_geometry_matches_oracle(nb, oracle, nel, lx, per, amp, lo, hi):
+    P, O = _pair(nb, oracle, nel, lx, per, amp, lo, hi)
+    for name in ("x", "y", "z", "B", "mult", "g11", "g22", "g33", "g12", "g13", "g23"):
+        a, b = _np(P.field(name)), O.f64(name)
+        scale = max(np.abs(b).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-12 * scale, name
+    assert abs(P.volume - O.volume) <= 1e-12 * abs(O.volume)
+    for name, oname in (("dof_gs", "dof_gs"), ("gs_dof", "gs_dof"), ("blk_len", "blk_len"),
+                        ("blk_off", "blk_off"), ("msk", "msk")):
+        np.testing.assert_array_equal(_np(P.field(name)), O.i32(oname))
+
+
+@pytest.mark.parametrize("nel,lx,per,amp,lo,hi", CASES)
+def test_ax_helm_matches_oracle(nb, oracle, nel, lx, per, amp, lo, hi):
+    P, O = _pair(nb, oracle, nel, lx, per, amp, lo, hi)
+    rng = np.random.default_rng(7)
+    u = rng.uniform(-1, 1, P.n)
+    w = P.zeros()
+    nb.AxHelm().compute(w, _cuda(u), P)
+    torch.cuda.synchronize()
+    ref = O.ax_helm(u)
+    assert rel_err(_np(w), ref) <= AX_RTOL
+
+
+def test_ax_helm_h2_matches_oracle(nb, oracle):
+    P, O = _pair(nb, oracle, (4, 3, 3), 7, (True, True, True), 0.05, 0.0, 2 * np.pi)
+    rng = np.random.default_rng(3)
+    h1 = rng.uniform(0.5, 2.0, P.n)
+    h2 = rng.uniform(0.0, 100.0, P.n)
+    P.set_coefficients(_cuda(h1), _cuda(h2))
+    O.set_f64("h1", h1)
+    O.set_f64("h2", h2)
+    O.set_ifh2(True)
+    u = rng.uniform(-1, 1, P.n)
+    w = P.zeros()
+    nb.AxHelm().compute(w, _cuda(u), P)
+    torch.cuda.synchronize()
+    assert rel_err(_np(w), O.ax_helm(u)) <= AX_RTOL
+
+
+def test_drop_in_ax_helm(nb, oracle, nblib):
+    """cuda_ax_helm with the reference's argument list."""
+    P, O = _pair(nb, oracle, (4, 4, 4), 8, (True,) * 3, 0.05, 0.0, 2 * np.pi)
+    rng = np.random.default_rng(11)
+    u = _cuda(rng.uniform(-1, 1, P.n))
+    w = P.zeros()
+    f = {k: P.field(k) for k in ("dx", "dxt", "h1", "g11", "g22", "g33", "g12", "g13", "g23")}
+    dx = f["dx"].data_ptr()
+    dxt = f["dxt"].data_ptr()
+    nelv, lx = ctypes.c_int(P.nelv), ctypes.c_int(P.lx)
+    vp = ctypes.c_void_p
+    nblib.cuda_ax_helm(vp(w.data_ptr()), vp(u.data_ptr()), vp(dx), vp(dx), vp(dx), vp(dxt),
+                       vp(dxt), vp(dxt), *(vp(f[k].data_ptr()) for k in
+                                           ("h1", "g11", "g22", "g33", "g12", "g13", "g23")),
+                       ctypes.byref(nelv), ctypes.byref(lx))
+    torch.cuda.synchronize()
+    assert rel_err(_np(w), O.ax_helm(_np(u))) <= AX_RTOL
+
+
+@pytest.mark.parametrize("nel,lx,per,amp,lo,hi", CASES)
+def test_gs_add_bit_exact(nb, oracle, nel, lx, per, amp, lo, hi):
+    P, O = _pair(nb, oracle, nel, lx, per, amp, lo, hi)
+    u = np.random.default_rng(5).standard_normal(P.n)
+    d = _cuda(u)
+    P.gs.op(d, P.n)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_np(d), O.gs_add(u))
+
+
+def _fixtures():
+    with open(os.path.join(GOLD, "gs_face_fixtures.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("t", _fixtures(), ids=lambda t: t["name"])
+def test_drop_in_gather_scatter_on_reference_fixtures(oracle, nblib, t):
+    """cuda_gather_kernel + cuda_scatter_kernel over the oracle's maps of the
+    reference's two-element fixtures reproduce the oracle's gs bit for bit."""
+    pts = t["points"]
+    ids = np.array([[pts[str(r)]["id"] for r in el] for el in t["elements"]], dtype=np.int32)
+    xyz = np.array([[pts[str(r)]["xyz"] for r in el] for el in t["elements"]])
+    O = oracle.OracleProblem.from_elements(ids, xyz, t["lx"])
+    n = O.n
+    u = np.random.default_rng(1).standard_normal(n)
+    dg, gd = _cuda(O.i32("dof_gs")), _cuda(O.i32("gs_dof"))
+    bl, bo = _cuda(O.i32("blk_len")), _cuda(O.i32("blk_off"))
+    ud = _cuda(u)
+    v = torch.zeros(O.nlocal, dtype=torch.float64, device="cuda")
+    m, o, nn, nbk, op = (ctypes.c_int(x) for x in (O.nlocal, O.local_facet_offset, n, O.nblks, 1))
+    vp = ctypes.c_void_p
+    s = vp(torch.cuda.current_stream().cuda_stream)
+    nblib.cuda_gather_kernel(vp(v.data_ptr()), ctypes.byref(m), ctypes.byref(o), vp(dg.data_ptr()),
+                             vp(ud.data_ptr()), ctypes.byref(nn), vp(gd.data_ptr()),
+                             ctypes.byref(nbk), vp(bl.data_ptr()), vp(bo.data_ptr()),
+                             ctypes.byref(op), s)
+    nblib.cuda_scatter_kernel(vp(v.data_ptr()), ctypes.byref(m), vp(dg.data_ptr()),
+                              vp(ud.data_ptr()), ctypes.byref(nn), vp(gd.data_ptr()),
+                              ctypes.byref(nbk), vp(bl.data_ptr()), vp(bo.data_ptr()), s)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(_np(ud), O.gs_add(u))
+
+
+def test_glsc3_golden(nblib):
+    """tests/unit/device_math/test_device_math_parallel.pf:614-647."""
+    n = 4711
+    a = torch.ones(n, dtype=torch.float64, device="cuda")
+    nn = ctypes.c_int(n)
+    vp = ctypes.c_void_p
+    r = nblib.cuda_glsc3(vp(a.data_ptr()), vp(a.data_ptr()), vp(a.data_ptr()), ctypes.byref(nn),
+                         vp(torch.cuda.current_stream().cuda_stream))
+    assert r == 4711.0
+
+
+def test_glsc3_random(nblib, oracle):
+    rng = np.random.default_rng(2)
+    for n in (1, 31, 1000, 262144, 3000017):
+        a, b, c = (rng.standard_normal(n) for _ in range(3))
+        A, Bt, C = _cuda(a), _cuda(b), _cuda(c)
+        nn = ctypes.c_int(n)
+        vp = ctypes.c_void_p
+        r = nblib.cuda_glsc3(vp(A.data_ptr()), vp(Bt.data_ptr()), vp(C.data_ptr()),
+                             ctypes.byref(nn), vp(torch.cuda.current_stream().cuda_stream))
+        exact = float(np.sum(a * b * c, dtype=np.longdouble))
+        assert abs(r - exact) <= 1e-13 * np.sum(np.abs(a * b * c))
+        # deterministic: same bits on a second call
+        r2 = nblib.cuda_glsc3(vp(A.data_ptr()), vp(Bt.data_ptr()), vp(C.data_ptr()),
+                              ctypes.byref(nn), vp(torch.cuda.current_stream().cuda_stream))
+        assert r == r2
+
+
+def test_vector_ops(nblib):
+    rng = np.random.default_rng(4)
+    n = 100003
+    a, b, c = (rng.standard_normal(n) for _ in range(3))
+    vp = ctypes.c_void_p
+    s = vp(torch.cuda.current_stream().cuda_stream)
+    nn = ctypes.c_int(n)
+    A, Bt, C = _cuda(a), _cuda(b), _cuda(c)
+    c1 = ctypes.c_double(0.75)
+    nblib.cuda_add2s2(vp(A.data_ptr()), vp(Bt.data_ptr()), ctypes.byref(c1), ctypes.byref(nn), s)
+    np.testing.assert_allclose(_np(A), a + 0.75 * b, rtol=1e-15, atol=1e-15)
+    nblib.cuda_add2s1(vp(A.data_ptr()), vp(Bt.data_ptr()), ctypes.byref(c1), ctypes.byref(nn), s)
+    np.testing.assert_allclose(_np(A), 0.75 * (a + 0.75 * b) + b, rtol=1e-14, atol=1e-14)
+    nblib.cuda_col3(vp(A.data_ptr()), vp(Bt.data_ptr()), vp(C.data_ptr()), ctypes.byref(nn), s)
+    np.testing.assert_array_equal(_np(A), b * c)
+    nblib.cuda_invcol1(vp(A.data_ptr()), ctypes.byref(nn), s)
+    np.testing.assert_array_equal(_np(A), 1.0 / (b * c))
+
+
+def test_jacobi_diag_matches_oracle(nb, oracle):
+    P, O = _pair(nb, oracle, (4, 4, 4), 8, (True,) * 3, 0.05, 0.0, 2 * np.pi)
+    torch.cuda.synchronize()
+    assert rel_err(_np(P.field("jacobi")), O.jacobi_diag()) <= 1e-12
+
+
+def test_cg_jacobi_config1_shape(nb, oracle):
+    """Config-1 shape (unit box, Dirichlet, sin^3 RHS + continuous noise):
+    iteration counts within +-1 of the oracle, same solution."""
+    P, O = _pair(nb, oracle, (8, 8, 8), 8)
+    x, y, z = O.f64("x"), O.f64("y"), O.f64("z")
+    B, mult = O.f64("B"), O.f64("mult")
+    rng = np.random.default_rng(1234)
+    xi = O.gs_add(rng.normal(0.0, 1e-3, O.n)) * mult
+    fpt = 3 * np.pi ** 2 * np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z) + xi
+    b = O.bc_apply(O.gs_add(B * fpt))
+    r0 = np.sqrt(np.sum(b * mult * b) / O.volume)
+    tol = 1e-10 * r0
+    xo, it_o, rs_o, rf_o = O.cg_jacobi(b, 500, tol)
+    xd = P.zeros()
+    mon = nb.CG(max_iter=500, abs_tol=tol, M=nb.Jacobi()).solve(nb.AxHelm(), xd, _cuda(b), P.n, P)
+    assert abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    assert mon.converged
+    assert abs(mon.res_start - rs_o) <= 1e-12 * rs_o
+    assert rel_err(_np(xd), xo) < 1e-8
+
+
+def test_cg_helmholtz_periodic_deformed(nb, oracle):
+    P, O = _pair(nb, oracle, (4, 4, 4), 8, (True,) * 3, 0.05, 0.0, 2 * np.pi)
+    rng = np.random.default_rng(9)
+    h2 = np.full(P.n, 2.0)
+    P.set_coefficients(_cuda(np.ones(P.n)), _cuda(h2))
+    O.set_f64("h2", h2)
+    O.set_ifh2(True)
+    B = O.f64("B")
+    b = O.gs_add(B * rng.standard_normal(P.n))
+    mult = O.f64("mult")
+    r0 = np.sqrt(np.sum(b * mult * b) / O.volume)
+    xo, it_o, _, _ = O.cg_jacobi(b, 1000, 1e-9 * r0)
+    xd = P.zeros()
+    mon = nb.CG(max_iter=1000, abs_tol=1e-9 * r0, M=nb.Jacobi()).solve(nb.AxHelm(), xd,
+                                                                      _cuda(b), P.n, P)
+    assert abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    assert rel_err(_np(xd), xo) < 1e-7
+
+
+def test_solve_errors_are_returned(nb):
+    P = nb.Problem((3, 3, 3), 4)
+    x = P.zeros()
+    f = torch.ones(P.n, dtype=torch.float64, device="cuda")
+    mon = nb.CG(max_iter=1, abs_tol=1e-30, M=nb.Jacobi()).solve(nb.AxHelm(), x, f, P.n, P)
+    assert mon.iter == 1 and not mon.converged
+    with pytest.raises(nb.NekoB200Error):
+        nb.Problem((2, 4, 4), 4, periodic=(True, False, False))
+    with pytest.raises(nb.NekoB200Error):
+        nb.Problem((3, 3, 3), 17)
+    nanf = torch.full((P.n,), float("nan"), dtype=torch.float64, device="cuda")
+    with pytest.raises(nb.NekoB200Error):
+        nb.CG(max_iter=5, abs_tol=1e-9).solve(nb.AxHelm(), x, nanf, P.n, P)
