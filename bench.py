@@ -201,6 +201,25 @@ def run_reference(args, cfg, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def kernel_only(args, cfg):
+    """A smaller case of one kernel for profilers: nel^3 elements of the
+    config-2 geometry, `--steps` launches after `--warmup`."""
+    import torch
+    import neko_b200 as nb
+    cfg = dict(cfg, nel=(args.nel,) * 3, lx=args.lx)
+    P = build_problem(nb, cfg)
+    u = torch.rand(P.n, dtype=torch.float64, device="cuda")
+    w = P.zeros()
+    s = torch.cuda.Stream()
+    for _ in range(args.warmup + args.steps):
+        if args.kernel_only == "ax":
+            nb.AxHelm().compute(w, u, P, stream=s)
+        else:
+            P.gs.op(u, P.n, stream=s)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel": args.kernel_only, "n": P.n, "launches": args.warmup + args.steps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,12 +234,18 @@ def main():
     ap.add_argument("--ref-full-iters", type=int, default=0,
                     help="iterations of the full solve (default: measured on the GPU path)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-only", choices=["ax", "gs"], default=None,
+                    help="run only this kernel on an nel^3 box (profiling case)")
+    ap.add_argument("--nel", type=int, default=16)
+    ap.add_argument("--lx", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
 
     from neko_b200 import workloads
     cfg = dict(workloads.CONFIG2)
+    if args.kernel_only:
+        return kernel_only(args, cfg)
     world, rank, local = dist_setup()
 
     if args.impl == "reference":

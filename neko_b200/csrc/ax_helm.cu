@@ -13,9 +13,16 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include <cstdint>
+
 #include "nb_kernels.h"
+#include "nb_tma.cuh"
 
 namespace nb {
+
+// Device error word of this translation unit: 0 = ok, 1 = a bulk-copy wait
+// timed out.  Read and cleared by take_device_error().
+__device__ int nb_dev_error = 0;
 
 // Elements per block for each lx (threads = lx*lx*NE).
 template <int LX>
@@ -107,6 +114,205 @@ __global__ void __launch_bounds__(LX *LX *NE)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Streaming variant for the native solver: a persistent kernel in which each
+// CTA walks its share of the elements (e = blockIdx.x + t * gridDim.x) and
+// keeps S elements in flight in a shared-memory ring.  One thread issues, per
+// element, eight 1-D bulk copies (u, h1, G11, G22, G33, G12, G13, G23; each
+// lx^3 contiguous values) completing on the stage's mbarrier, so the bytes
+// in flight per SM are S * 8 * lx^3 * sizeof(T) per CTA regardless of
+// register pressure.  KS thread groups split the k-planes of an element:
+// thread (i, j, kh) computes planes [kh*LX/KS, (kh+1)*LX/KS).
+// ---------------------------------------------------------------------------
+template <typename T, int LX, int S, int KS>
+struct AxTmaCfg {
+  static constexpr int L2 = LX * LX, L3 = L2 * LX, NA = 8;
+  static constexpr int THREADS = ((L2 * KS + 31) / 32) * 32;
+  static constexpr size_t ABYTES = (size_t)L3 * sizeof(T);
+  static constexpr size_t SMEM = S * NA * ABYTES + 3 * ABYTES + 2 * L2 * sizeof(T) + 16 * S;
+};
+
+template <typename T, int LX, int S, int KS>
+__global__ void __launch_bounds__(AxTmaCfg<T, LX, S, KS>::THREADS)
+    ax_helm_tma_kernel(T *__restrict__ w, const T *__restrict__ u, const T *__restrict__ D,
+                       const T *__restrict__ Dt, const T *__restrict__ h1,
+                       const T *__restrict__ g11, const T *__restrict__ g22,
+                       const T *__restrict__ g33, const T *__restrict__ g12,
+                       const T *__restrict__ g13, const T *__restrict__ g23, const int nelv,
+                       const int *__restrict__ skip) {
+  using C = AxTmaCfg<T, LX, S, KS>;
+  constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS;
+  static_assert(LX % KS == 0, "k split must divide lx");
+  if (skip && *skip) return;
+  extern __shared__ __align__(128) unsigned char smem_ring[];
+  T *stage = reinterpret_cast<T *>(smem_ring);
+  T *sur = stage + S * NA * L3, *sus = sur + L3, *sut = sus + L3;
+  T *sD = sut + L3, *sDt = sD + L2;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sDt + L2);
+
+  const int tid = threadIdx.x;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int nt = b < nelv ? (nelv - b + G - 1) / G : 0;
+  if (tid == 0) {
+    for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+    fence_barrier_init();
+  }
+  for (int q = tid; q < L2; q += C::THREADS) {
+    sD[q] = D[q];
+    sDt[q] = Dt[q];
+  }
+  __syncthreads();
+  const T *src[NA] = {u, h1, g11, g22, g33, g12, g13, g23};
+  auto issue = [&](int t, int s) {
+    const long e = b + (long)t * G;
+    mbar_arrive_expect_tx(&full[s], (uint32_t)(NA * C::ABYTES));
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+      bulk_g2s(stage + (size_t)(s * NA + a) * L3, src[a] + e * L3, (uint32_t)C::ABYTES, &full[s]);
+  };
+  if (tid == 0)
+    for (int t = 0; t < S && t < nt; t++) issue(t, t);
+
+  const bool act = tid < L2 * KS;
+  const int col = tid % L2, kh = tid / L2;
+  const int i = col % LX, j = col / LX, k0 = kh * KP;
+  T Di[LX], Dj[LX], Dti[LX], Dtj[LX];
+#pragma unroll
+  for (int l = 0; l < LX; l++) {
+    Di[l] = sD[i + LX * l];
+    Dj[l] = sD[j + LX * l];
+    Dti[l] = sDt[i + LX * l];
+    Dtj[l] = sDt[j + LX * l];
+  }
+
+  int t = 0;
+  bool failed = false;
+  for (; t < nt; t++) {
+    const int s = t % S;
+    const bool ok = mbar_wait(&full[s], (uint32_t)((t / S) & 1));
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    const T *su = stage + (size_t)s * NA * L3;
+    const T *sh = su + L3, *s11 = su + 2 * L3, *s22 = su + 3 * L3, *s33 = su + 4 * L3,
+            *s12 = su + 5 * L3, *s13 = su + 6 * L3, *s23 = su + 7 * L3;
+    if (act) {
+      T ru[LX];
+#pragma unroll
+      for (int l = 0; l < LX; l++) ru[l] = su[col + L2 * l];
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        T ur = 0, us = 0, ut = 0;
+#pragma unroll
+        for (int l = 0; l < LX; l++) {
+          ur += Di[l] * su[l + LX * j + L2 * k];
+          us += Dj[l] * su[i + LX * l + L2 * k];
+          ut += sD[k + LX * l] * ru[l];
+        }
+        const int p = col + L2 * k;
+        const T H = sh[p];
+        const T a11 = s11[p], a22 = s22[p], a33 = s33[p], a12 = s12[p], a13 = s13[p],
+                a23 = s23[p];
+        sur[p] = H * (a11 * ur + a12 * us + a13 * ut);
+        sus[p] = H * (a12 * ur + a22 * us + a23 * ut);
+        sut[p] = H * (a13 * ur + a23 * us + a33 * ut);
+      }
+    }
+    __syncthreads();  // stage s consumed, work planes complete
+    if (tid == 0 && t + S < nt) issue(t + S, s);
+    if (act) {
+      T rt[LX];
+#pragma unroll
+      for (int l = 0; l < LX; l++) rt[l] = sut[col + L2 * l];
+      const long e = b + (long)t * G;
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        T a = 0, c = 0, d = 0;
+#pragma unroll
+        for (int l = 0; l < LX; l++) {
+          a += Dti[l] * sur[l + LX * j + L2 * k];
+          c += Dtj[l] * sus[i + LX * l + L2 * k];
+          d += sDt[k + LX * l] * rt[l];
+        }
+        w[e * L3 + col + L2 * k] = a + c + d;
+      }
+    }
+    __syncthreads();  // work planes free for the next element
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicCAS(&nb_dev_error, 0, 1);
+      // bounded wait for this CTA's copies still in flight
+      for (int q = t; q < nt && q < t + S; q++) mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, int LX, int S, int KS>
+static cudaError_t launch_ax_tma(T *w, const T *u, const T *D, const T *Dt, const T *h1,
+                                 const T *g11, const T *g22, const T *g33, const T *g12,
+                                 const T *g13, const T *g23, int nelv, cudaStream_t st,
+                                 const int *skip) {
+  using C = AxTmaCfg<T, LX, S, KS>;
+  auto kern = ax_helm_tma_kernel<T, LX, S, KS>;
+  static int grid_per_dev[64] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int &g = grid_per_dev[dev & 63];
+  if (g == 0) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::THREADS, C::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    g = (per_sm > 0 ? per_sm : 1) * sms;
+  }
+  if (nelv <= 0) return cudaSuccess;
+  const int grid = nelv < g ? nelv : g;
+  kern<<<grid, C::THREADS, C::SMEM, st>>>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
+                                          skip);
+  return cudaGetLastError();
+}
+
+// Dispatch of the streaming variant; returns cudaErrorNotSupported when no
+// instantiation covers (T, lx) or a pointer is not 16-byte aligned.
+template <typename T>
+cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h1,
+                           const T *g11, const T *g22, const T *g33, const T *g12,
+                           const T *g13, const T *g23, int nelv, int lx, cudaStream_t s,
+                           const int *skip) {
+  const void *ptrs[] = {u, h1, g11, g22, g33, g12, g13, g23};
+  for (const void *p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorNotSupported;
+  if (((size_t)lx * lx * lx * sizeof(T)) % 16) return cudaErrorNotSupported;
+  switch (lx) {
+    case 4: return launch_ax_tma<T, 4, 4, 1>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
+    case 6: return launch_ax_tma<T, 6, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
+    case 8: return launch_ax_tma<T, 8, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
+    case 10: return launch_ax_tma<T, 10, 2, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
+    default: return cudaErrorNotSupported;
+  }
+}
+int take_device_error() {
+  int v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, nb_dev_error, sizeof(int)) != cudaSuccess) return -1;
+  if (v) cudaMemcpyToSymbol(nb_dev_error, &zero, sizeof(int));
+  return v;
+}
+
+template cudaError_t ax_helm_stream<double>(double *, const double *, const double *,
+                                            const double *, const double *, const double *,
+                                            const double *, const double *, const double *,
+                                            const double *, const double *, int, int,
+                                            cudaStream_t, const int *);
+
 template <typename T, int LX>
 static cudaError_t launch_ax(T *w, const T *u, const T *dx, const T *dy, const T *dz,
                              const T *dxt, const T *dyt, const T *dzt, const T *h1,
@@ -180,7 +386,15 @@ extern "C" void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, voi
     fprintf(stderr, "cuda_ax_helm: unsupported lx %d (2..16)\n", *lx);
     exit(1);
   }
-  cudaError_t e = nb::ax_helm<double>(
+  cudaError_t e = cudaErrorNotSupported;
+  if (dx == dy && dx == dz && dxt == dyt && dxt == dzt)
+    e = nb::ax_helm_stream<double>((double *)w, (const double *)u, (const double *)dx,
+                                   (const double *)dxt, (const double *)h1, (const double *)g11,
+                                   (const double *)g22, (const double *)g33, (const double *)g12,
+                                   (const double *)g13, (const double *)g23, *nelv, *lx,
+                                   nb::default_stream());
+  if (e == cudaErrorNotSupported)
+    e = nb::ax_helm<double>(
       (double *)w, (const double *)u, (const double *)dx, (const double *)dy,
       (const double *)dz, (const double *)dxt, (const double *)dyt, (const double *)dzt,
       (const double *)h1, (const double *)g11, (const double *)g22, (const double *)g33,

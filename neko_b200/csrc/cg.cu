@@ -240,9 +240,7 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
                                                      P->mult, n, W.st, W.partials, W.counter);
   }
   cg_update_p_kernel<<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
-  cudaError_t e = nb::ax_helm<double>(W.w, W.p, P->D, P->D, P->D, P->Dt, P->Dt, P->Dt, P->h1,
-                                      P->g11, P->g22, P->g33, P->g12, P->g13, P->g23, P->nelv,
-                                      P->lx, s, &W.st->done);
+  cudaError_t e = P->ax_raw(W.w, W.p, s, &W.st->done);
   if (e != cudaSuccess) return e;
   if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n);
   e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->done);
@@ -336,6 +334,8 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     // that used the whole iteration budget.
     if (hs->iter >= o.max_iter) res->converged = 0;
   }
+  if (take_device_error())
+    return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (bulk copy never completed)");
   if (hs->nan) return ws_fail(NB_ERR_NAN, "residual became NaN or Inf");
   return NB_OK;
 }

@@ -18,6 +18,18 @@ cudaError_t ax_helm(T *w, const T *u, const T *dx, const T *dy, const T *dz, con
                     const T *g33, const T *g12, const T *g13, const T *g23, int nelv, int lx,
                     cudaStream_t s, const int *skip = nullptr);
 
+// Persistent bulk-copy variant of ax_helm (dx = dy = dz); returns
+// cudaErrorNotSupported when it has no instantiation for (T, lx) or the
+// pointers are not 16-byte aligned.
+template <typename T>
+cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h1,
+                           const T *g11, const T *g22, const T *g33, const T *g12,
+                           const T *g13, const T *g23, int nelv, int lx, cudaStream_t s,
+                           const int *skip = nullptr);
+
+// Reads and clears the device error word (0 = no error).
+int take_device_error();
+
 // Grid size for streaming kernels: a multiple of the SM count.
 int stream_grid(long n, int threads);
 

@@ -56,7 +56,9 @@ struct nb_problem {
 
   ~nb_problem();
   cudaError_t update_jacobi(cudaStream_t s);
+  bool use_stream_ax = true;  // NB_AX_KERNEL=classic selects the general kernel
   cudaError_t ax(double *w, const double *u, cudaStream_t s) const;
+  cudaError_t ax_raw(double *w, const double *u, cudaStream_t s, const int *skip) const;
   void invalidate_solver_cache();
 };
 

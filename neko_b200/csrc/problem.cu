@@ -3,6 +3,7 @@
 // and mask uploaded once, and the operator entry points nb_ax / nb_gs_add /
 // nb_bc_apply.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -198,6 +199,7 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
   P->nelv = (int)nelv;
   P->n = n;
   P->deform_amp = deform_amp;
+  if (const char *k = getenv("NB_AX_KERNEL")) P->use_stream_ax = strcmp(k, "classic") != 0;
 
   // host setup: space, vertices, neighbours, maps, mask
   std::vector<double> zg, wx, D, Dt;
@@ -435,9 +437,22 @@ extern "C" nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1
   return NB_OK;
 }
 
+// h1 part of ax_helm: the streaming kernel where it has an instantiation,
+// the general one otherwise.
+cudaError_t nb_problem::ax_raw(double *w, const double *u, cudaStream_t s,
+                               const int *skip) const {
+  cudaError_t e = cudaErrorNotSupported;
+  if (use_stream_ax)
+    e = nb::ax_helm_stream<double>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, lx, s,
+                                   skip);
+  if (e == cudaErrorNotSupported)
+    e = nb::ax_helm<double>(w, u, D, D, D, Dt, Dt, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
+                            lx, s, skip);
+  return e;
+}
+
 cudaError_t nb_problem::ax(double *w, const double *u, cudaStream_t s) const {
-  cudaError_t e = nb::ax_helm<double>(w, u, D, D, D, Dt, Dt, Dt, h1, g11, g22, g33, g12, g13,
-                                      g23, nelv, lx, s);
+  cudaError_t e = ax_raw(w, u, s, nullptr);
   if (e != cudaSuccess || !ifh2) return e;
   addcol4_kernel<<<stream_grid(n, 256), 256, 0, s>>>(w, h2, B, u, n);
   return cudaGetLastError();

@@ -18,6 +18,14 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 AX_RTOL = 1e-12
 
 
+def ax_rtol(lx):
+    """1e-12 relative for lx <= 10 (the benchmark orders).  Above that the
+    derivative-matrix entries grow like lx^2 (D(1,1) = -lx(lx-1)/4) and the
+    16-term contractions of rough random input lose more digits to rounding,
+    so the bound is 1e-11."""
+    return AX_RTOL if lx <= 10 else 1e-11
+
+
 @pytest.fixture(scope="module")
 def nb():
     import neko_b200
@@ -60,9 +68,12 @@ CASES = [((8, 8, 8), 8, (False,) * 3, 0.0, 0.0, 1.0),
 @pytest.mark.parametrize("nel,lx,per,amp,lo,hi", CASES)
 def test_geometry_matches_oracle(nb, oracle, nel, lx, per, amp, lo, hi):
     P, O = _pair(nb, oracle, nel, lx, per, amp, lo, hi)
+    # the off-diagonal G factors are rounding noise on an undeformed box, so
+    # all six are measured against the scale of the diagonal ones
+    gscale = max(np.abs(O.f64(k)).max() for k in ("g11", "g22", "g33"))
     for name in ("x", "y", "z", "B", "mult", "g11", "g22", "g33", "g12", "g13", "g23"):
         a, b = _np(P.field(name)), O.f64(name)
-        scale = max(np.abs(b).max(), 1e-300)
+        scale = gscale if name.startswith("g") else max(np.abs(b).max(), 1e-300)
         assert np.abs(a - b).max() <= 1e-12 * scale, name
     assert abs(P.volume - O.volume) <= 1e-12 * abs(O.volume)
     for name, oname in (("dof_gs", "dof_gs"), ("gs_dof", "gs_dof"), ("blk_len", "blk_len"),
@@ -79,7 +90,21 @@ def test_ax_helm_matches_oracle(nb, oracle, nel, lx, per, amp, lo, hi):
     nb.AxHelm().compute(w, _cuda(u), P)
     torch.cuda.synchronize()
     ref = O.ax_helm(u)
-    assert rel_err(_np(w), ref) <= AX_RTOL
+    assert rel_err(_np(w), ref) <= ax_rtol(lx)
+
+
+@pytest.mark.parametrize("kernel", ["classic", "stream"])
+@pytest.mark.parametrize("lx", [4, 6, 8, 10])
+def test_ax_kernels_agree(nb, oracle, monkeypatch, kernel, lx):
+    """Both ax_helm kernels (general and bulk-copy streaming) against the
+    oracle on a deformed periodic box."""
+    monkeypatch.setenv("NB_AX_KERNEL", kernel)
+    P, O = _pair(nb, oracle, (3, 4, 3), lx, (True,) * 3, 0.05, 0.0, 2 * np.pi)
+    u = np.random.default_rng(lx).uniform(-1, 1, P.n)
+    w = P.zeros()
+    nb.AxHelm().compute(w, _cuda(u), P)
+    torch.cuda.synchronize()
+    assert rel_err(_np(w), O.ax_helm(u)) <= ax_rtol(lx)
 
 
 def test_ax_helm_h2_matches_oracle(nb, oracle):
