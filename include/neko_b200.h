@@ -190,6 +190,19 @@ nb_status nb_solve(nb_problem *p, double *x, const double *f,
                    const nb_solve_opts *opts, nb_solve_result *res,
                    void *stream);
 
+/* sum(a*b*c) over n device values, written to the host double *result,
+ * allocating nothing.  No counterpart in the reference: it is cuda_glsc3 for
+ * callers that must not call cudaMalloc (a solve running under a fixed,
+ * pre-committed device-memory budget; a thread that must not trigger the
+ * device synchronisation cudaMalloc can imply).  Scratch is a static
+ * device array of 128 KB (+256 B) held on every device that loads the
+ * library until exit; n above 33,554,432 is rejected with NB_ERR_ARG.  All
+ * calls share that array, so calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress) and
+ * should come before any stream capture.  Synchronises `stream`. */
+nb_status nb_glsc3_noalloc(const double *a, const double *b, const double *c,
+                           int n, double *result, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

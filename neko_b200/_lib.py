@@ -78,6 +78,7 @@ SIGNATURES = {
     "nb_gs_add": (_I, [_P, _P, _P]),
     "nb_bc_apply": (_I, [_P, _P, _P]),
     "nb_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult), _P]),
+    "nb_glsc3_noalloc": (_I, [_P, _P, _P, _I, _DP, _P]),
 }
 
 _lib = None
