@@ -172,6 +172,7 @@ typedef struct {
   int mixed;           /* 1: FP32 preconditioner, FP64 flexible CG */
   int coarse_iter;     /* hsmg coarse CG iterations (reference default 10) */
   double coarse_tol;   /* hsmg coarse CG absolute tolerance (default 1e-9) */
+  int flexible;        /* 1: flexible CG (Polak-Ribiere beta) with a pc */
 } nb_solve_opts;
 
 typedef struct {
@@ -181,6 +182,11 @@ typedef struct {
   int converged;
   int launches;  /* kernels this solve launched on the device */
 } nb_solve_result;
+
+/* z = M r for preconditioner pc (NB_PC_HSMG), r masked; builds the
+ * preconditioner on first use.  The hsmg_solve of the reference
+ * (src/krylov/pc_hsmg.f90:481-627), exposed for checking and reuse. */
+nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r, void *stream);
 
 /* Solves A x = f (f already assembled and masked) from x0 = 0 with
  * preconditioned CG, entirely on the device.  Follows cg_device_solve

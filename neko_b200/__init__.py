@@ -27,7 +27,7 @@ from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpt
 
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
-__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "KspMonitor",
+__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "KspMonitor",
            "Jacobi", "Hsmg", "GS_OP_ADD", "NekoB200Error", "load", "version"]
 
 
@@ -176,19 +176,28 @@ class Jacobi:
 
 
 class Hsmg:
-    """pc_hsmg: additive 3-level Schwarz/FDM multigrid (pc_hsmg.f90)."""
+    """pc_hsmg: additive 3-level Schwarz/FDM multigrid (pc_hsmg.f90).
+    `solve(z, r, coef)` is pc_t%solve: z = M r (r masked)."""
     kind = NB_PC_HSMG
 
     def __init__(self, coarse_iter=10, coarse_tol=1e-9):
         self.coarse_iter, self.coarse_tol = coarse_iter, coarse_tol
 
+    def solve(self, z, r, coef, n=None, stream=None):
+        check(load().nb_pc_apply(coef.handle, NB_PC_HSMG, _ptr(z), _ptr(r),
+                                 _stream_handle(stream)))
+
 
 class CG:
     """ksp_t of type 'cg' with preconditioner M (Jacobi, Hsmg or None);
-    stops when sqrt(r' mult r / volume) < abs_tol (krylov.f90:411-421)."""
+    stops when sqrt(r' mult r / volume) < abs_tol (krylov.f90:411-421).
+    flexible=True uses the Polak-Ribiere beta of flexible CG, which keeps
+    converging with a non-symmetric preconditioner such as hsmg."""
 
-    def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False):
+    def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False,
+                 flexible=False):
         self.max_iter, self.abs_tol, self.mixed = max_iter, abs_tol, mixed
+        self.flexible = flexible
         self.M = M if M is not None else Jacobi()
 
     def solve(self, Ax, x, f, n=None, coef=None, blst=None, gs_h=None, niter=None,
@@ -200,7 +209,15 @@ class CG:
         o.mixed = int(self.mixed)
         o.coarse_iter = getattr(self.M, "coarse_iter", 10)
         o.coarse_tol = getattr(self.M, "coarse_tol", 1e-9)
+        o.flexible = int(self.flexible)
         r = SolveResult()
         check(load().nb_solve(coef.handle, _ptr(x), _ptr(f), ctypes.byref(o), ctypes.byref(r),
                               _stream_handle(stream)))
         return KspMonitor(r.iter, r.res_start, r.res_final, bool(r.converged), r.launches)
+
+
+class FCG(CG):
+    """Flexible CG: CG with the Polak-Ribiere beta (Notay's FCG(1))."""
+
+    def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False):
+        super().__init__(n, max_iter, M, abs_tol, mixed, flexible=True)

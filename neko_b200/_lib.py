@@ -26,7 +26,8 @@ NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE = 0, 1, 2
 class SolveOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("abs_tol", ctypes.c_double),
                 ("pc", ctypes.c_int), ("mixed", ctypes.c_int),
-                ("coarse_iter", ctypes.c_int), ("coarse_tol", ctypes.c_double)]
+                ("coarse_iter", ctypes.c_int), ("coarse_tol", ctypes.c_double),
+                ("flexible", ctypes.c_int)]
 
 
 class SolveResult(ctypes.Structure):
@@ -79,6 +80,7 @@ SIGNATURES = {
     "nb_bc_apply": (_I, [_P, _P, _P]),
     "nb_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult), _P]),
     "nb_glsc3_noalloc": (_I, [_P, _P, _P, _I, _DP, _P]),
+    "nb_pc_apply": (_I, [_P, _I, _P, _P, _P]),
 }
 
 _lib = None

@@ -53,7 +53,12 @@ __global__ void addcol4_kernel(double *w, const double *h2, const double *B, con
 __global__ void __launch_bounds__(kRedThreads)
     cg_init_kernel(double *__restrict__ x, double *__restrict__ p, double *__restrict__ r,
                    const double *__restrict__ f, const double *__restrict__ mult, long n,
-                   CgState *st, double *partials, unsigned *counter) {
+                   CgState *st, double *partials, unsigned *counter,
+                   const int *__restrict__ outer_skip) {
+  if (outer_skip && *outer_skip) {  // enclosing solve finished: stay idle
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+    return;
+  }
   double s = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads) {
@@ -114,6 +119,29 @@ __global__ void __launch_bounds__(kRedThreads)
     st->rtz2 = st->rtz1;
     st->rtz1 = tot;
     st->beta = st->iter == 0 ? 0.0 : tot / st->rtz2;
+  }
+}
+
+// Flexible variant (Polak-Ribiere): rtz = (r, mult z) and rwz =
+// (w_prev, mult z); beta = -alpha_prev * rwz / rtz_prev, because
+// r_k - r_(k-1) = -alpha_(k-1) w_(k-1) and w still holds w_(k-1) here.
+__global__ void __launch_bounds__(kRedThreads)
+    cg_dot_rz_flex_kernel(const double *__restrict__ z, const double *__restrict__ r,
+                          const double *__restrict__ w_prev, const double *__restrict__ mult,
+                          long n, CgState *st, double *partials, unsigned *counter) {
+  if (st->done) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    const double mz = mult[i] * z[i];
+    s0 += r[i] * mz;
+    s1 += w_prev[i] * mz;
+  }
+  double tot[2];
+  if (grid_sum2<kRedThreads>(s0, s1, partials, counter, tot)) {
+    st->beta = st->iter == 0 ? 0.0 : -st->alpha * tot[1] / st->rtz1;
+    st->rtz2 = st->rtz1;
+    st->rtz1 = tot[0];
   }
 }
 
@@ -201,7 +229,7 @@ cudaError_t CgWorkspace::ensure(long n_) {
   base = nullptr;
   n = n_;
   const size_t vec = ((size_t)n * 8 + 255) & ~size_t(255);
-  const size_t red = 148 * 8 * sizeof(double) + 256;
+  const size_t red = 2 * 148 * 8 * sizeof(double) + 256;  // grid_sum2 needs 2 per block
   bytes = 4 * vec + red + sizeof(CgState) + 256;
   cudaError_t e = cudaMalloc(&base, bytes);
   if (e != cudaSuccess) {
@@ -214,7 +242,7 @@ cudaError_t CgWorkspace::ensure(long n_) {
   p = (double *)(b + 2 * vec);
   w = (double *)(b + 3 * vec);
   partials = (double *)(b + 4 * vec);
-  counter = (unsigned *)(b + 4 * vec + 148 * 8 * sizeof(double));
+  counter = (unsigned *)(b + 4 * vec + 2 * 148 * 8 * sizeof(double));
   st = (CgState *)(b + 4 * vec + red);
   e = cudaMemset(b + 4 * vec, 0, red + sizeof(CgState));
   if (e != cudaSuccess) return e;
@@ -233,8 +261,12 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
   if (pc) {
     cudaError_t e = pc->apply(W.z, W.r, &W.st->done, s);
     if (e != cudaSuccess) return e;
-    cg_dot_rz_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, n, W.st, W.partials,
-                                                W.counter);
+    if (W.flexible)
+      cg_dot_rz_flex_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.w, P->mult, n, W.st,
+                                                       W.partials, W.counter);
+    else
+      cg_dot_rz_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, n, W.st, W.partials,
+                                                  W.counter);
   } else {
     cg_precond_dot_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.use_jacobi ? P->jdiag : nullptr,
                                                      P->mult, n, W.st, W.partials, W.counter);
@@ -278,6 +310,7 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     return ws_fail(e == cudaErrorMemoryAllocation ? NB_ERR_OOM : NB_ERR_CUDA,
                    std::string("CG workspace: ") + cudaGetErrorString(e));
   W.use_jacobi = o.pc == NB_PC_JACOBI;
+  W.flexible = o.flexible != 0 && pc != nullptr;
   CgState init{};
   init.norm_fac = 1.0 / std::sqrt(P->volume);
   init.abs_tol = o.abs_tol;
@@ -285,10 +318,12 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const long n = P->n;
   cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(x, W.p, W.r, f, P->mult, n, W.st,
-                                                        W.partials, W.counter);
+                                                        W.partials, W.counter, nullptr);
   NB_CUDA_TRY(cudaGetLastError());
   // (Re)capture the iteration graph when the operands changed.
-  const void *key[4] = {x, pc, (const void *)(intptr_t)W.use_jacobi, (const void *)(intptr_t)P->ifh2};
+  const void *key[4] = {x, pc,
+                        (const void *)(intptr_t)(W.use_jacobi | (W.flexible << 1)),
+                        (const void *)(intptr_t)P->ifh2};
   bool same = W.graph_exec && !memcmp(key, W.graph_key, sizeof(key));
   const int chunk = n > (1 << 22) ? 4 : 16;
   if (!same) {

@@ -83,15 +83,15 @@ __global__ void gs_add_fused_kernel(T *__restrict__ u, const int *__restrict__ s
                                     const int *__restrict__ extra_mask, int nextra,
                                     const unsigned char *__restrict__ seg_masked,
                                     const unsigned char *__restrict__ pair_masked,
-                                    const int *__restrict__ skip) {
+                                    const int *__restrict__ skip, const T *__restrict__ scale) {
   if (skip && *skip) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < npairs) {
     const int2 p = __ldg(pairs + t);
     T s = u[p.x] + u[p.y];
     if (pair_masked && pair_masked[t]) s = T(0);
-    u[p.x] = s;
-    u[p.y] = s;
+    u[p.x] = scale ? s * scale[p.x] : s;
+    u[p.y] = scale ? s * scale[p.y] : s;
     return;
   }
   int q = t - npairs;
@@ -100,7 +100,10 @@ __global__ void gs_add_fused_kernel(T *__restrict__ u, const int *__restrict__ s
     T s = u[__ldg(seg_idx + a)];
     for (int k = a + 1; k < b; k++) s = s + u[__ldg(seg_idx + k)];
     if (seg_masked && seg_masked[q]) s = T(0);
-    for (int k = a; k < b; k++) u[__ldg(seg_idx + k)] = s;
+    for (int k = a; k < b; k++) {
+      const int idx = __ldg(seg_idx + k);
+      u[idx] = scale ? s * scale[idx] : s;
+    }
     return;
   }
   q -= nseg;
@@ -109,7 +112,7 @@ __global__ void gs_add_fused_kernel(T *__restrict__ u, const int *__restrict__ s
 
 template <typename T>
 cudaError_t gs_add_fused(const GsDevice &g, T *u, bool with_mask, cudaStream_t s,
-                         const int *skip) {
+                         const int *skip, const T *scale) {
   const long total = (long)g.npairs + g.nseg + (with_mask ? g.nextra : 0);
   if (total == 0) return cudaSuccess;
   const int threads = 256;
@@ -117,13 +120,13 @@ cudaError_t gs_add_fused(const GsDevice &g, T *u, bool with_mask, cudaStream_t s
   gs_add_fused_kernel<T><<<blocks, threads, 0, s>>>(
       u, g.seg_ptr, g.seg_idx, g.nseg, g.pairs, g.npairs, g.extra_mask,
       with_mask ? g.nextra : 0, with_mask ? g.seg_masked : nullptr,
-      with_mask ? g.pair_masked : nullptr, skip);
+      with_mask ? g.pair_masked : nullptr, skip, scale);
   return cudaGetLastError();
 }
 template cudaError_t gs_add_fused<double>(const GsDevice &, double *, bool, cudaStream_t,
-                                          const int *);
+                                          const int *, const double *);
 template cudaError_t gs_add_fused<float>(const GsDevice &, float *, bool, cudaStream_t,
-                                         const int *);
+                                         const int *, const float *);
 
 // Host-side re-layout of reference maps into the fused form.  `masked`
 // (n flags, may be empty) marks zero-Dirichlet points.

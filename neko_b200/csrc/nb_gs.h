@@ -31,8 +31,11 @@ void gs_relayout(const GsMaps &m, const std::vector<unsigned char> &masked, long
                  GsHostLayout &h);
 bool gs_pairs_regular(const GsMaps &m);
 
+// u = gs_add(u) over g; masked entries become 0 when with_mask; when scale
+// is given every written entry is multiplied by scale[index] (points outside
+// the maps are not touched).  Returns at once when *skip != 0.
 template <typename T>
 cudaError_t gs_add_fused(const GsDevice &g, T *u, bool with_mask, cudaStream_t s,
-                         const int *skip = nullptr);
+                         const int *skip = nullptr, const T *scale = nullptr);
 
 }  // namespace nb

@@ -32,12 +32,27 @@ struct CgWorkspace {
   CgState *st = nullptr;
   void *host_state = nullptr;
   bool use_jacobi = true;
+  bool flexible = false;
   int launches_per_iter = 6;
   cudaGraphExec_t graph_exec = nullptr;
   const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   ~CgWorkspace();
   cudaError_t ensure(long n);
 };
+
+// CG kernels (cg.cu), shared with the coarse-grid solve of hsmg.
+__global__ void cg_init_kernel(double *x, double *p, double *r, const double *f,
+                               const double *mult, long n, CgState *st, double *partials,
+                               unsigned *counter, const int *outer_skip);
+__global__ void cg_precond_dot_kernel(double *z, const double *r, const double *d,
+                                      const double *mult, long n, CgState *st,
+                                      double *partials, unsigned *counter);
+__global__ void cg_update_p_kernel(double *p, const double *z, long n, const CgState *st);
+__global__ void cg_pap_kernel(const double *w, const double *p, const double *mult, long n,
+                              CgState *st, double *partials, unsigned *counter);
+__global__ void cg_update_xr_kernel(double *x, double *r, const double *p, const double *w,
+                                    const double *mult, long n, CgState *st, double *partials,
+                                    unsigned *counter);
 
 nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
                    Precond *pc, nb_solve_result *res, cudaStream_t s);

@@ -64,6 +64,41 @@ __device__ __forceinline__ bool grid_sum(double v, double *partials, unsigned *c
   return false;
 }
 
+// Two sums at once (same protocol as grid_sum; partials holds 2*gridDim.x
+// values).  Returns true in thread 0 of the last block with out[0..1] set.
+template <int THREADS>
+__device__ __forceinline__ bool grid_sum2(double v0, double v1, double *partials,
+                                          unsigned *counter, double *out) {
+  __shared__ double sh[THREADS / 32];
+  __shared__ bool last;
+  const double b0 = block_sum<THREADS>(v0, sh);
+  const double b1 = block_sum<THREADS>(v1, sh);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = b0;
+    partials[2 * blockIdx.x + 1] = b1;
+    __threadfence();
+    const unsigned done = atomicAdd(counter, 1u);
+    last = done == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double t0 = 0.0, t1 = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS) {
+    t0 += *((volatile double *)partials + 2 * b);
+    t1 += *((volatile double *)partials + 2 * b + 1);
+  }
+  t0 = block_sum<THREADS>(t0, sh);
+  t1 = block_sum<THREADS>(t1, sh);
+  if (threadIdx.x == 0) {
+    *counter = 0;
+    out[0] = t0;
+    out[1] = t1;
+    return true;
+  }
+  return false;
+}
+
 // Number of blocks of a grid-stride reduction over n points: a multiple of
 // the 148 SMs, at most 4 waves, at least one point per thread.
 inline int red_blocks(long n) {

@@ -85,6 +85,7 @@ struct Mesh {
   std::unordered_map<Edge, int, EdgeHash> hte;
   int mfcs = 0, meds = 0;
   std::vector<uint8_t> dfrmd_el;
+  std::vector<int> facet_type;  // (6, nelv)
 
   int pid(int e, int v) const { return points[el[e][v - 1]].id; }
   const double *px(int e, int v) const { return points[el[e][v - 1]].x; }
@@ -115,6 +116,7 @@ struct Mesh {
     el.assign(n, {});
     el_id.assign(n, 0);
     dfrmd_el.assign(n, 0);
+    facet_type.assign(6 * (size_t)n, 0);
   }
 
   // hex_facet_id (hex.f90:109-137): sorted ids of the face's 4 vertices.
@@ -155,6 +157,7 @@ struct Mesh {
   // mesh_mark_labeled_facet (mesh.f90:1633-1650)
   void mark_labeled_facet(int f, int e, int label) {
     labeled[label].push_back({f, e});
+    facet_type[(size_t)e * 6 + (f - 1)] = -label;
   }
 
   // mesh_create_periodic_ids (mesh.f90:1743-1833), tol = 1e-7.
@@ -1126,6 +1129,20 @@ void or_gs_add_impl(const OrProblem &P, double *u) {
   gs_add(P, u, v);
 }
 const int *or_facet_neigh(const OrProblem &P) { return P.meshp->facet_neigh.data(); }
+int or_facet_type(const OrProblem &P, int f, int e) {
+  return P.meshp->facet_type[(size_t)(e - 1) * 6 + (f - 1)];
+}
+void or_all_deformed(OrProblem &P) {
+  std::fill(P.meshp->dfrmd_el.begin(), P.meshp->dfrmd_el.end(), 1);
+}
+void or_coef_init_impl(OrProblem &P) { coef_init(P); }
+void fd_weights_full_impl(double xi, const double *x, int n, int m, double *c) {
+  fd_weights_full(xi, x, n, m, c);
+}
+void zwgll_impl(double *z, double *w, int np) { zwgll(z, w, np); }
+void mxm_impl(const double *a, int n1, const double *b, int n2, double *c, int n3) {
+  mxm(a, n1, b, n2, c, n3);
+}
 int or_dfrmd_el(const OrProblem &P, int e) { return P.meshp->dfrmd_el[e]; }
 
 // ---------------------------------------------------------------------------
@@ -1153,6 +1170,21 @@ static OrProblem *build_common(OrProblem *P, int lx) {
   gs_init_mapping(*P);
   return P;
 }
+
+void or_deform_sine(OrProblem *P, double amp);
+}  // extern "C"
+
+OrProblem *or_level_create(const OrProblem &fine, int lx, bool with_coef) {
+  OrProblem *P = new OrProblem();
+  P->meshp = fine.meshp;
+  P->owns_mesh = false;
+  build_common(P, lx);
+  if (fine.deform_amp != 0.0) or_deform_sine(P, fine.deform_amp);
+  if (with_coef) coef_init(*P);
+  return P;
+}
+
+extern "C" {
 
 OrProblem *or_box_create(int nelx, int nely, int nelz, double x0, double x1,
                          double y0, double y1, double z0, double z1, int px,
@@ -1188,6 +1220,7 @@ OrProblem *or_elements_create(int nelv, const int *ids, const double *xyz, int l
 // x += a sin(y) sin(z), y += a sin(z) sin(x), z += a sin(x) sin(y), all
 // evaluated at the undeformed point.
 void or_deform_sine(OrProblem *P, double amp) {
+  P->deform_amp = amp;
   for (long i = 0; i < P->n; i++) {
     double x = P->x[i], y = P->y[i], z = P->z[i];
     P->x[i] = x + amp * std::sin(y) * std::sin(z);
@@ -1201,7 +1234,20 @@ void or_coef_init(OrProblem *P) { coef_init(*P); }
 // Mark every face with facet_neigh == 0 as zero-Dirichlet
 // (examples/poisson/setup.f90:2-30) and build the mask as bc_finalize_base
 // does (bc.f90:434-593): gs-add an indicator, keep entries > 0.5.
-void or_bc_boundary(OrProblem *P) {
+void or_bc_boundary(OrProblem *P) { or_bc_boundary_impl(*P); }
+
+// Strong (Dirichlet) boundary faces get facet_type 1, as the pressure bc
+// factory does for strong boundaries (src/fluid/fluid_pnpn_bc_fctry.f90:
+// 158-167); the FDM of the Schwarz smoother then drops those rows
+// (fdm.f90:417-441).  Applied to every face without a neighbour.
+void or_mark_dirichlet_facets(OrProblem *P) {
+  for (int e = 0; e < P->nelv; e++)
+    for (int f = 0; f < 6; f++)
+      if (P->meshp->facet_neigh[(size_t)e * 6 + f] == 0) P->meshp->facet_type[(size_t)e * 6 + f] = 1;
+}
+}  // extern "C"
+void or_bc_boundary_impl(OrProblem &PP) {
+  OrProblem *P = &PP;
   int lx = P->lx;
   std::vector<double> t(P->n, 0.0);
   for (int e = 1; e <= P->nelv; e++)
@@ -1227,9 +1273,10 @@ void or_bc_boundary(OrProblem *P) {
   for (long i = 0; i < P->n; i++)
     if (t[i] > 0.5) P->msk.push_back((int)(i + 1));
 }
+extern "C" {
 
 void or_destroy(OrProblem *P) {
-  delete P->meshp;
+  if (P->owns_mesh) delete P->meshp;
   delete P;
 }
 

@@ -13,6 +13,8 @@ struct Mesh;
 // ---------------------------------------------------------------------------
 struct OrProblem {
   nko::Mesh *meshp = nullptr;
+  bool owns_mesh = true;
+  double deform_amp = 0.0;
   int lx = 0, nelv = 0;
   long n = 0;
   // space_t (src/sem/space.f90:149-320)
@@ -40,4 +42,17 @@ inline long or_lin(int i, int j, int k, int e, int lx) {  // 1-based -> 0-based
 // gs_op_vector(GS_OP_ADD) on a field of P's dofmap.
 void or_gs_add_impl(const OrProblem &P, double *u);
 const int *or_facet_neigh(const OrProblem &P);
+// facet_type(f, e) of the mesh (src/mesh/mesh.f90:1633-1650): -label for a
+// labeled zone, 0 otherwise.  f, e are 1-based.
+int or_facet_type(const OrProblem &P, int f, int e);
+// Marks every element deformed (mesh_all_deformed, mesh.f90:470-473).
+void or_all_deformed(OrProblem &P);
+// A problem on the same mesh at another polynomial size: dofmap,
+// coordinates (same deformation), gs maps; coef when with_coef.
+OrProblem *or_level_create(const OrProblem &fine, int lx, bool with_coef);
+void or_coef_init_impl(OrProblem &P);
+void or_bc_boundary_impl(OrProblem &P);
+void fd_weights_full_impl(double xi, const double *x, int n, int m, double *c);
+void zwgll_impl(double *z, double *w, int np);
+void mxm_impl(const double *a, int n1, const double *b, int n2, double *c, int n3);
 int or_dfrmd_el(const OrProblem &P, int e);

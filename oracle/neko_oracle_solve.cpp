@@ -141,6 +141,8 @@ void jacobi_update(const OrProblem &P, std::vector<double> &d) {
 
 }  // namespace
 
+void or_jacobi_diag(const OrProblem &P, std::vector<double> &d) { jacobi_update(P, d); }
+
 // cg_solve (src/krylov/bcknd/cpu/cg.f90:140-279): PCG with the deferred
 // x update over CG_P_SPACE = 7 directions and NEKO_BLK_SIZE blocking.
 // Stops when sqrt(r'*mult*r)/sqrt(volume) < abs_tol (krylov.f90:411-421).
@@ -208,6 +210,52 @@ int or_cg_solve_impl(const OrProblem &P, double *x, const double *f, int max_ite
       p_prev = p_cur;
       p_cur = p_cur + 1;
     }
+  }
+  *res_final = rnorm;
+  return iter > max_iter ? max_iter : iter;
+}
+
+// Flexible CG (Notay's FCG(1), Polak-Ribiere beta): new work, the reference
+// has no flexible CG.  beta_k = (z_k, mult (r_k - r_k-1)) / (z_k-1, mult
+// r_k-1); x updated every iteration (the device CG form,
+// cg_device.f90:205-231).  Same stopping rule as cg_solve.
+int or_fcg_solve_impl(const OrProblem &P, double *x, const double *f, int max_iter,
+                      double abs_tol, const std::function<void(double *, const double *)> &M,
+                      double *res_start, double *res_final) {
+  const long n = P.n;
+  std::vector<double> w(n), r(n), r_old(n), z(n), p(n, 0.0);
+  const double norm_fac = 1.0 / std::sqrt(P.volume);
+  double rtr = 0.0, rtz_old = 1.0;
+  for (long i = 0; i < n; i++) {
+    x[i] = 0.0;
+    r[i] = f[i];
+    rtr = rtr + r[i] * P.mult[i] * r[i];
+  }
+  double rnorm = std::sqrt(rtr) * norm_fac;
+  *res_start = rnorm;
+  *res_final = rnorm;
+  if (std::fabs(rnorm) < 2.220446049250313e-16) return 0;
+  int iter;
+  for (iter = 1; iter <= max_iter; iter++) {
+    M(z.data(), r.data());
+    const double rtz = glsc3(r.data(), P.mult.data(), z.data(), n);
+    double beta = 0.0;
+    if (iter > 1) beta = (rtz - glsc3(r_old.data(), P.mult.data(), z.data(), n)) / rtz_old;
+    rtz_old = rtz;
+    for (long i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+    ax_helm(P, w.data(), p.data());
+    or_gs_add_impl(P, w.data());
+    bc_apply(P, w.data());
+    const double alpha = rtz / glsc3(w.data(), P.mult.data(), p.data(), n);
+    double t = 0.0;
+    for (long i = 0; i < n; i++) {
+      x[i] = x[i] + alpha * p[i];
+      r_old[i] = r[i];
+      r[i] = r[i] - alpha * w[i];
+      t = t + r[i] * P.mult[i] * r[i];
+    }
+    rnorm = std::sqrt(t) * norm_fac;
+    if (rnorm < abs_tol) break;
   }
   *res_final = rnorm;
   return iter > max_iter ? max_iter : iter;

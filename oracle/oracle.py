@@ -40,6 +40,7 @@ def lib():
             "or_deform_sine": (None, [_P, ctypes.c_double]),
             "or_coef_init": (None, [_P]),
             "or_bc_boundary": (None, [_P]),
+            "or_mark_dirichlet_facets": (None, [_P]),
             "or_destroy": (None, [_P]),
             "or_n": (ctypes.c_long, [_P]),
             "or_nelv": (ctypes.c_int, [_P]),
@@ -66,6 +67,13 @@ def lib():
             "or_fd_weights_full": (None, [ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, _D]),
             "or_zwgll": (None, [ctypes.c_int, _D, _D]),
             "or_dgll": (None, [ctypes.c_int, _D, _D, _D]),
+            "or_hsmg_create": (_P, [_P, ctypes.c_int, ctypes.c_double]),
+            "or_hsmg_destroy": (None, [_P]),
+            "or_hsmg_apply": (None, [_P, _D, _D]),
+            "or_hsmg_schwarz_fine": (None, [_P, _D, _D]),
+            "or_hsmg_sizes": (ctypes.c_long, [_P, ctypes.c_int]),
+            "or_cg_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
+            "or_fcg_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -114,8 +122,12 @@ class OracleProblem:
         lib().or_coef_init(self.h)
         self.has_coef = True
 
-    def bc_boundary(self):
+    def bc_boundary(self, strong=True):
+        """Zero-Dirichlet on every face without a neighbour; with strong=True
+        those faces also get facet_type 1 (strong bc) for the FDM."""
         lib().or_bc_boundary(self.h)
+        if strong:
+            lib().or_mark_dirichlet_facets(self.h)
 
     def close(self):
         if self.h:
@@ -216,6 +228,51 @@ class OracleProblem:
         it = lib().or_cg_jacobi(self.h, _dp(x), _dp(f), max_iter, abs_tol,
                                 ctypes.byref(r0), ctypes.byref(r1))
         return x, it, r0.value, r1.value
+
+
+class OracleHsmg:
+    """hsmg_t of an OracleProblem (coef and bc must be set up first)."""
+
+    def __init__(self, P, coarse_iter=10, coarse_tol=1e-9):
+        self.P = P
+        self.h = lib().or_hsmg_create(P.h, coarse_iter, coarse_tol)
+
+    def apply(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        lib().or_hsmg_apply(self.h, _dp(z), _dp(r))
+        return z
+
+    def schwarz_fine(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        e = np.zeros_like(r)
+        lib().or_hsmg_schwarz_fine(self.h, _dp(e), _dp(r))
+        return e
+
+    @property
+    def last_coarse_iter(self):
+        return lib().or_hsmg_sizes(self.h, 4)
+
+    def cg(self, f, max_iter, abs_tol, flexible=False):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        x = np.zeros_like(f)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        fn = lib().or_fcg_hsmg if flexible else lib().or_cg_hsmg
+        it = fn(self.P.h, self.h, _dp(x), _dp(f), max_iter, abs_tol,
+                ctypes.byref(r0), ctypes.byref(r1))
+        return x, it, r0.value, r1.value
+
+    def close(self):
+        if self.h:
+            lib().or_hsmg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fd_weights_full(xi, x, m):
