@@ -139,30 +139,44 @@ def make_rhs(nb, P, seed):
     return b
 
 
-def cpu_baseline_sample(cfg, b, gpu_iters, budget_iters):
-    """Oracle (a one-thread CPU port of the reference's path) on the same
-    workload and right-hand side: setup untimed, then `budget_iters`
-    Jacobi-PCG iterations timed; solves/s extrapolated with the iteration
-    count of the GPU run."""
+def oracle_iteration_time(cfg, b, pc, iters):
+    """Seconds per Krylov iteration of the CPU oracle (a one-thread port of
+    the reference's CPU path) on this workload: setup untimed, `iters`
+    iterations timed."""
     from oracle import oracle as orc
     O = orc.OracleProblem.box(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"],
                               periodic=cfg["periodic"])
     O.deform_sine(cfg["deform"])
     O.coef()
-    t0 = time.perf_counter()
-    O.cg_jacobi(b, budget_iters, 0.0)
-    dt = time.perf_counter() - t0
-    per_iter = dt / budget_iters
+    if pc == "hsmg":
+        H = orc.OracleHsmg(O)
+        t0 = time.perf_counter()
+        H.cg(b, iters, 0.0, flexible=True)
+        dt = time.perf_counter() - t0
+        H.close()
+    else:
+        t0 = time.perf_counter()
+        O.cg_jacobi(b, iters, 0.0)
+        dt = time.perf_counter() - t0
+    O.close()
+    return dt / iters, dt
+
+
+def cpu_baseline_sample(cfg, b, pc, gpu_iters, budget_iters):
+    per_iter, dt = oracle_iteration_time(cfg, b, pc, budget_iters)
+    name = "hsmg-FCG" if pc == "hsmg" else "Jacobi-PCG"
     return {"value": 1.0 / (per_iter * max(gpu_iters, 1)), "unit": "solves/s", "cores": 1,
             "kind": "port",
-            "sample": f"{budget_iters} Jacobi-PCG iterations of the same 32^3 lx=8 problem on 1 "
-                      f"host core ({dt:.1f} s); solves/s = 1/(s per iteration x {gpu_iters} "
-                      f"iterations of the GPU run)"}
+            "sample": f"{budget_iters} {name} iterations of the same 32^3 lx=8 problem and "
+                      f"right-hand side on 1 host core ({dt:.1f} s, setup untimed); solves/s = "
+                      f"1/(s per iteration x {gpu_iters} iterations of the solve)"}
 
 
 def run_reference(args, cfg, world, rank):
-    """--impl reference: the reference's CPU algorithm (oracle port) on the
-    host cores, same metric/config; rank 0 only."""
+    """--impl reference: the reference's CPU algorithm (the oracle port; the
+    Fortran reference does not build here) on the host, same metric,
+    workload and preconditioner; each step times --ref-iters iterations and
+    solves/s uses the solve's iteration count.  Rank 0 only."""
     if rank != 0:
         return
     import numpy as np
@@ -177,25 +191,34 @@ def run_reference(args, cfg, world, rank):
     mult = O.f64("mult")
     r0 = math.sqrt(float(np.sum(b * mult * b)) / O.volume)
     iters = args.ref_iters
+    H = orc.OracleHsmg(O) if args.pc == "hsmg" else None
+
+    def run(k):
+        if H is not None:
+            H.cg(b, k, 0.0, flexible=True)
+        else:
+            O.cg_jacobi(b, k, 0.0)
     for _ in range(args.warmup):
-        O.cg_jacobi(b, 1, 0.0)
+        run(1)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.cg_jacobi(b, iters, 0.0)
+        run(iters)
         times.append((time.perf_counter() - t0) / iters)
     per_iter = sorted(times)[len(times) // 2]
     full_iters = args.ref_full_iters
     v = 1.0 / (per_iter * full_iters)
+    name = "hsmg-FCG" if args.pc == "hsmg" else "Jacobi-PCG"
     line = {"impl": "reference", "metric": "Poisson solves/s to 1e-8 rel", "value": v,
             "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": per_iter * full_iters * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "periodic deformed box 32^3 hex, lx=8 (16.8M points), "
-                                   "FP64 Jacobi-PCG to 1e-8 rel", "r0": r0},
+            "config": {"workload": f"periodic deformed box 32^3 hex, lx=8 (16.8M points), "
+                                   f"FP64 {name} to 1e-8 rel", "pc": args.pc, "r0": r0},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
-                             "sample": f"median of {args.steps} runs of {iters} CG iterations; "
-                                       f"solves/s = 1/(s per iteration x {full_iters})"},
+                             "sample": f"median of {args.steps} runs of {iters} {name} "
+                                       f"iterations on 1 host core; solves/s = 1/(s per "
+                                       f"iteration x {full_iters} iterations of the solve)"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -226,13 +249,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--pc", default="jacobi", choices=["jacobi", "hsmg"])
+    ap.add_argument("--pc", default="hsmg", choices=["jacobi", "hsmg"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--ax-reps", type=int, default=50)
-    ap.add_argument("--cpu-iters", type=int, default=3)
-    ap.add_argument("--ref-iters", type=int, default=2)
+    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--ref-iters", type=int, default=1)
     ap.add_argument("--ref-full-iters", type=int, default=0,
-                    help="iterations of the full solve (default: measured on the GPU path)")
+                    help="iterations of the full solve (default: 20 for hsmg-FCG, 1074 for "
+                         "Jacobi-PCG, the counts of this workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-only", choices=["ax", "gs"], default=None,
                     help="run only this kernel on an nel^3 box (profiling case)")
@@ -249,8 +273,8 @@ def main():
     world, rank, local = dist_setup()
 
     if args.impl == "reference":
-        if args.ref_full_iters <= 0:
-            args.ref_full_iters = 440  # Jacobi-PCG iterations of this workload (GPU run)
+        if args.ref_full_iters <= 0:  # iteration counts of this workload's solve
+            args.ref_full_iters = 20 if args.pc == "hsmg" else 1074
         run_reference(args, cfg, world, rank)
         barrier(world)
         return
@@ -353,7 +377,7 @@ def main():
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(cfg, b.cpu().numpy(), iters[-1],
+        line["cpu_baseline"] = cpu_baseline_sample(cfg, b.cpu().numpy(), args.pc, iters[-1],
                                                    args.cpu_iters)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -35,30 +35,56 @@ namespace nb {
 // ---------------------------------------------------------------------------
 
 // e = S (D^-1) S' r on the extended element, ghost layer gathered from the
-// neighbours (fn: 1-based neighbour per face, 0 = none).  One element per
-// threadIdx.y slice, NL*NL threads each.
-template <typename T, int NL, int NE>
+// neighbours (fn: 1-based neighbour per face, 0 = none).  NE elements per
+// block, NL*NL threads each.  Each of the six tensor passes contracts the
+// first index and writes its result with that index moved last
+// (out(m,n,i) = sum_l M(l,i) in(l,m,n)), so after three passes the order is
+// back to (i,j,k) and every pass reads one contiguous line of NL values per
+// thread into registers; the NL x NL matrix of the pass is read as a
+// broadcast.  The inverse eigenvalue sums are rebuilt from the three
+// spectra (zero where the sum is <= eps, as fdm_setup_fast).
+template <typename TIN, typename T, int NL>
+__device__ __forceinline__ void fdm_pass(const T *__restrict__ in, T *__restrict__ out,
+                                         const T *__restrict__ M, int t) {
+  constexpr int N2 = NL * NL;
+  T line[NL];
+#pragma unroll
+  for (int l = 0; l < NL; l++) line[l] = in[NL * t + l];
+#pragma unroll
+  for (int i = 0; i < NL; i++) {
+    T s = 0;
+#pragma unroll
+    for (int l = 0; l < NL; l++) s += M[l + NL * i] * line[l];
+    out[t + N2 * i] = s;
+  }
+}
+
+template <typename TIN, typename T, int NL, int NE>
 __global__ void __launch_bounds__(NL *NL *NE)
-    fdm_kernel(const T *__restrict__ r, const int *__restrict__ fn, const T *__restrict__ S,
+    fdm_kernel(const TIN *__restrict__ r, const int *__restrict__ fn, const T *__restrict__ S,
                const T *__restrict__ lam, const T *__restrict__ eps, T *__restrict__ out,
                int nelv, const int *__restrict__ skip) {
   if (skip && *skip) return;
   constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = NL * NL, N3 = N2 * NL;
+  constexpr int STRIDE = 2 * N3 + 6 * N2 + 3 * NL + 2;
   extern __shared__ __align__(16) unsigned char fdm_smem[];
-  T *base = reinterpret_cast<T *>(fdm_smem) + threadIdx.y * (2 * N3 + 3 * N2 + 3 * NL + 1);
-  T *b0 = base, *b1 = base + N3, *sS = base + 2 * N3, *sL = sS + 3 * N2;
+  T *base = reinterpret_cast<T *>(fdm_smem) + threadIdx.y * STRIDE;
+  T *b0 = base, *b1 = base + N3;
+  T *sS = base + 2 * N3;        // S_x, S_y, S_z: S(l,i) at l + NL*i
+  T *sT = sS + 3 * N2;          // transposes: S(i,l) at l + NL*i
+  T *sL = sT + 3 * N2;          // spectra + eps
   const long e = (long)blockIdx.x * NE + threadIdx.y;
-  const int tid = threadIdx.x;
+  const int t = threadIdx.x;
   const bool active = e < nelv;
   if (active) {
     const int *f = fn + e * 6;
-    for (int q = tid; q < N3; q += N2) {
+    for (int q = t; q < N3; q += N2) {
       const int a = q % NL, b = (q / NL) % NL, c = q / N2;
       const int ea = (a == 0) + (a == NL - 1), eb = (b == 0) + (b == NL - 1),
                 ec = (c == 0) + (c == NL - 1);
       T v = T(0);
       if (ea + eb + ec == 0) {
-        v = r[e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1)];
+        v = (T)r[e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1)];
       } else if (ea + eb + ec == 1) {
         int nb = 0, si = a - 1, sj = b - 1, sk = c - 1;
         if (a == 0) nb = f[0], si = LX - 2;
@@ -67,69 +93,58 @@ __global__ void __launch_bounds__(NL *NL *NE)
         if (b == NL - 1) nb = f[3], sj = 1;
         if (c == 0) nb = f[4], sk = LX - 2;
         if (c == NL - 1) nb = f[5], sk = 1;
-        if (nb) v = r[(long)(nb - 1) * L3 + si + LX * sj + L2 * sk];
+        if (nb) v = (T)r[(long)(nb - 1) * L3 + si + LX * sj + L2 * sk];
       }
       b0[q] = v;
     }
-    for (int q = tid; q < 3 * N2; q += N2) sS[q] = S[e * 3 * N2 + q];
-    for (int q = tid; q < 3 * NL; q += N2) sL[q] = lam[e * 3 * NL + q];
-    if (tid == 0) sL[3 * NL] = eps[e];
+    for (int q = t; q < 3 * N2; q += N2) {
+      const T v = S[e * 3 * N2 + q];
+      const int d = q / N2, w = q % N2, l = w % NL, i = w / NL;
+      sS[q] = v;
+      sT[d * N2 + i + NL * l] = v;
+    }
+    for (int q = t; q < 3 * NL; q += N2) sL[q] = lam[e * 3 * NL + q];
+    if (t == 0) sL[3 * NL] = eps[e];
   }
   __syncthreads();
-  const T *Sx = sS, *Sy = sS + N2, *Sz = sS + 2 * N2;
-  const int t0 = tid % NL, t1 = tid / NL;
-  // forward transform: b1 = Sx' b0 (x), b0 = Sy' b1 (y), b1 = D Sz' b0 (z)
-  if (active)
-    for (int i = 0; i < NL; i++) {
-      T s = 0;
-#pragma unroll
-      for (int l = 0; l < NL; l++) s += Sx[l + NL * i] * b0[l + NL * t0 + N2 * t1];
-      b1[i + NL * t0 + N2 * t1] = s;
-    }
+  if (active) fdm_pass<TIN, T, NL>(b0, b1, sS, t);           // (l,m,n) -> (m,n,i)
   __syncthreads();
-  if (active)
-    for (int j = 0; j < NL; j++) {
-      T s = 0;
-#pragma unroll
-      for (int m = 0; m < NL; m++) s += Sy[m + NL * j] * b1[t0 + NL * m + N2 * t1];
-      b0[t0 + NL * j + N2 * t1] = s;
-    }
+  if (active) fdm_pass<TIN, T, NL>(b1, b0, sS + N2, t);      // -> (n,i,j)
   __syncthreads();
-  if (active) {
-    const T ep = sL[3 * NL];
+  if (active) {                                              // -> (i,j,k), times D^-1
+    T line[NL];
+#pragma unroll
+    for (int l = 0; l < NL; l++) line[l] = b0[NL * t + l];
+    const int i = t % NL, j = t / NL;
+    const T lij = sL[i] + sL[NL + j], ep = sL[3 * NL];
+    const T *M = sS + 2 * N2;
+#pragma unroll
     for (int k = 0; k < NL; k++) {
       T s = 0;
 #pragma unroll
-      for (int n = 0; n < NL; n++) s += Sz[n + NL * k] * b0[t0 + NL * t1 + N2 * n];
-      const T diag = sL[t0] + sL[NL + t1] + sL[2 * NL + k];
-      b1[t0 + NL * t1 + N2 * k] = diag > ep ? s / diag : T(0);
+      for (int l = 0; l < NL; l++) s += M[l + NL * k] * line[l];
+      const T diag = lij + sL[2 * NL + k];
+      b1[t + N2 * k] = diag > ep ? s / diag : T(0);
     }
   }
   __syncthreads();
-  // back transform: Sx (x), Sy (y), Sz (z) -> out
-  if (active)
-    for (int i = 0; i < NL; i++) {
-      T s = 0;
-#pragma unroll
-      for (int l = 0; l < NL; l++) s += Sx[i + NL * l] * b1[l + NL * t0 + N2 * t1];
-      b0[i + NL * t0 + N2 * t1] = s;
-    }
+  if (active) fdm_pass<TIN, T, NL>(b1, b0, sT, t);           // back: S_x
   __syncthreads();
-  if (active)
-    for (int j = 0; j < NL; j++) {
-      T s = 0;
-#pragma unroll
-      for (int m = 0; m < NL; m++) s += Sy[j + NL * m] * b0[t0 + NL * m + N2 * t1];
-      b1[t0 + NL * j + N2 * t1] = s;
-    }
+  if (active) fdm_pass<TIN, T, NL>(b0, b1, sT + N2, t);      // S_y
   __syncthreads();
-  if (active)
+  if (active) {                                              // S_z, store (i,j,k)
+    T line[NL];
+#pragma unroll
+    for (int l = 0; l < NL; l++) line[l] = b1[NL * t + l];
+    const T *M = sT + 2 * N2;
+#pragma unroll
     for (int k = 0; k < NL; k++) {
       T s = 0;
 #pragma unroll
-      for (int n = 0; n < NL; n++) s += Sz[k + NL * n] * b1[t0 + NL * t1 + N2 * n];
-      out[e * N3 + t0 + NL * t1 + N2 * k] = s;
+      for (int l = 0; l < NL; l++) s += M[l + NL * k] * line[l];
+      out[e * N3 + t + N2 * k] = s;
     }
+  }
 }
 
 // e(i,j,k) = ext interior + neighbours' ghost results on the first interior
@@ -220,8 +235,9 @@ static cudaError_t launch_fdm_post(const SchwarzLevel &L, const double *r, doubl
                                    const int *skip, cudaStream_t s) {
   constexpr int NL = LX + 2;
   constexpr int NE = NL * NL >= 64 ? 1 : (128 / (NL * NL));
-  const size_t smem = sizeof(double) * NE * (2 * NL * NL * NL + 3 * NL * NL + 3 * NL + 1);
-  auto kern = fdm_kernel<double, NL, NE>;
+  const size_t smem =
+      sizeof(double) * NE * (2 * NL * NL * NL + 6 * NL * NL + 3 * NL + 2);
+  auto kern = fdm_kernel<double, double, NL, NE>;
   if (smem > 48 * 1024) {
     cudaError_t err =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
