@@ -167,9 +167,15 @@ def cpu_baseline_sample(cfg, b, pc, gpu_iters, budget_iters):
     name = "hsmg-FCG" if pc == "hsmg" else "Jacobi-PCG"
     return {"value": 1.0 / (per_iter * max(gpu_iters, 1)), "unit": "solves/s", "cores": 1,
             "kind": "port",
-            "sample": f"{budget_iters} {name} iterations of the same 32^3 lx=8 problem and "
-                      f"right-hand side on 1 host core ({dt:.1f} s, setup untimed); solves/s = "
+            "sample": f"{budget_iters} {name} iterations of the same 32^3 lx={cfg['lx']} "
+                      f"problem and right-hand side on 1 host core ({dt:.1f} s, setup untimed); solves/s = "
                       f"1/(s per iteration x {gpu_iters} iterations of the solve)"}
+
+
+def workload_name(cfg, solver):
+    npts = cfg["nel"][0] * cfg["nel"][1] * cfg["nel"][2] * cfg["lx"] ** 3
+    return (f"periodic deformed box {cfg['nel'][0]}^3 hex, lx={cfg['lx']} "
+            f"({npts / 1e6:.1f}M points), {solver} to 1e-8 rel")
 
 
 def run_reference(args, cfg, world, rank):
@@ -213,8 +219,8 @@ def run_reference(args, cfg, world, rank):
             "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": per_iter * full_iters * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"periodic deformed box 32^3 hex, lx=8 (16.8M points), "
-                                   f"FP64 {name} to 1e-8 rel", "pc": args.pc, "r0": r0},
+            "config": {"workload": workload_name(cfg, f"FP64 {name}"), "pc": args.pc,
+                       "r0": r0},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
                              "sample": f"median of {args.steps} runs of {iters} {name} "
                                        f"iterations on 1 host core; solves/s = 1/(s per "
@@ -258,6 +264,8 @@ def main():
                     help="iterations of the full solve (default: 20 for hsmg-FCG, 1074 for "
                          "Jacobi-PCG, the counts of this workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision solve measured beside the FP64 one")
     ap.add_argument("--kernel-only", choices=["ax", "gs"], default=None,
                     help="run only this kernel on an nel^3 box (profiling case)")
     ap.add_argument("--nel", type=int, default=16)
@@ -268,6 +276,7 @@ def main():
 
     from neko_b200 import workloads
     cfg = dict(workloads.CONFIG2)
+    cfg["lx"] = args.lx
     if args.kernel_only:
         return kernel_only(args, cfg)
     world, rank, local = dist_setup()
@@ -339,6 +348,47 @@ def main():
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
     e2e = world * args.steps / t_e2e
 
+    # --- mixed precision beside it: FP32 smoothing levels, FP64 FCG ------
+    mixed = None
+    if args.pc == "hsmg" and not args.no_mixed:
+        x64 = x.clone()
+        msolver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Hsmg(mixed=True))
+        for _ in range(args.warmup):
+            mon_m = msolver.solve(Ax, x, b, P.n, P, stream=stream)
+        torch.cuda.synchronize()
+        if not mon_m.converged:
+            raise RuntimeError(f"mixed warm-up solve did not converge: {mon_m}")
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m_launches, m_iters = 0, []
+        barrier(world)
+        torch.cuda.synchronize()
+        m0.record(stream)
+        for _ in range(args.steps):
+            mon_m = msolver.solve(Ax, x, b, P.n, P, stream=stream)
+            m_launches += mon_m.launches
+            m_iters.append(mon_m.iter)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        t_m = max_over_ranks(m0.elapsed_time(m1) / 1e3, world)
+        xa, xb = x, x64
+        if all(cfg["periodic"]):  # the singular problem's solution is fixed up to a constant
+            xa, xb = x - x.mean(), x64 - x64.mean()
+        err = float(torch.linalg.norm(xa - xb) / torch.linalg.norm(xb))
+        v_m = world * args.steps / t_m
+        mixed = {"value": v_m, "unit": "solves/s", "ms_per_step": t_m / args.steps * 1e3,
+                 "iterations": m_iters[-1], "fp64_iterations": iters[-1],
+                 "res_final": mon_m.res_final, "abs_tol": tol,
+                 "err_vs_fp64": err,
+                 "err_reference": "relative L2 distance to the FP64 hsmg-FCG solution of "
+                                  "the same problem (the FP64 path matches the CPU oracle "
+                                  "in the parity tests)",
+                 "speedup_vs_fp64": v_m / value, "gpu_launches": m_launches,
+                 "precision": "FP32 Schwarz/FDM smoothing and restriction/prolongation; "
+                              "FP64 outer FCG, inner products, coarse CG, true residual "
+                              "every 50 iterations"}
+        x.copy_(x64)
+
     # --- ax_helm roofline: events on the launching stream ----------------
     w = P.zeros()
     for _ in range(5):
@@ -360,15 +410,15 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"periodic deformed box 32^3 hex, lx=8 (16.8M points), "
-                               f"FP64 {'Jacobi-PCG' if args.pc == 'jacobi' else 'hsmg-FCG'} "
-                               f"to 1e-8 rel, one solve per step per GPU",
+        "config": {"workload": workload_name(
+                       cfg, f"FP64 {'Jacobi-PCG' if args.pc == 'jacobi' else 'hsmg-FCG'}")
+                       + ", one solve per step per GPU",
                    "pc": args.pc, "iterations": iters[-1], "r0": r0, "seed": args.seed,
-                   "l2": "inputs larger than L2 (1.2 GB ax_helm working set)",
+                   "l2": f"inputs larger than L2 ({72 * P.n / 1e9:.1f} GB ax_helm working set)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": P.n * 8,
                 "d2h_bytes_per_step": P.n * 8},
-        "roofline": {"bound": "hbm", "kernel": "ax_helm_kernel<double,8,2>",
+        "roofline": {"bound": "hbm", "kernel": f"ax_helm_tma_kernel<double,{cfg['lx']}>",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                      "peak_source": peak_src, "bytes_per_launch": ax_bytes,
@@ -376,6 +426,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if mixed is not None:
+        line["mixed"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(cfg, b.cpu().numpy(), args.pc, iters[-1],
                                                    args.cpu_iters)

@@ -163,13 +163,20 @@ nb_status nb_gs_add(nb_problem *p, double *u, void *stream);
 /* x(msk) = 0 for the problem's Dirichlet mask. */
 nb_status nb_bc_apply(nb_problem *p, double *x, void *stream);
 
-typedef enum { NB_PC_JACOBI = 0, NB_PC_HSMG = 1, NB_PC_NONE = 2 } nb_pc_type;
+typedef enum {
+  NB_PC_JACOBI = 0,
+  NB_PC_HSMG = 1,
+  NB_PC_NONE = 2,
+  NB_PC_HSMG_MIXED = 3  /* nb_pc_apply only: hsmg with FP32 smoothing levels */
+} nb_pc_type;
 
 typedef struct {
   int max_iter;        /* iteration cap */
   double abs_tol;      /* stop when sqrt(r'*mult*r)/sqrt(volume) < abs_tol */
   int pc;              /* nb_pc_type */
-  int mixed;           /* 1: FP32 preconditioner, FP64 flexible CG */
+  int mixed;           /* 1: hsmg smoothing levels in FP32 (coarse CG, outer
+                          Krylov, inner products in FP64); true residual
+                          recomputed every 50 iterations */
   int coarse_iter;     /* hsmg coarse CG iterations (reference default 10) */
   double coarse_tol;   /* hsmg coarse CG absolute tolerance (default 1e-9) */
   int flexible;        /* 1: flexible CG (Polak-Ribiere beta) with a pc */
@@ -183,7 +190,8 @@ typedef struct {
   int launches;  /* kernels this solve launched on the device */
 } nb_solve_result;
 
-/* z = M r for preconditioner pc (NB_PC_HSMG), r masked; builds the
+/* z = M r for preconditioner pc (NB_PC_HSMG, or NB_PC_HSMG_MIXED for the
+ * FP32-smoother variant), r masked; builds the
  * preconditioner on first use.  The hsmg_solve of the reference
  * (src/krylov/pc_hsmg.f90:481-627), exposed for checking and reuse. */
 nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r, void *stream);

@@ -177,15 +177,16 @@ class Jacobi:
 
 class Hsmg:
     """pc_hsmg: additive 3-level Schwarz/FDM multigrid (pc_hsmg.f90).
-    `solve(z, r, coef)` is pc_t%solve: z = M r (r masked)."""
+    `solve(z, r, coef)` is pc_t%solve: z = M r (r masked).  mixed=True runs
+    the smoothing levels in FP32 (the coarse CG stays FP64)."""
     kind = NB_PC_HSMG
 
-    def __init__(self, coarse_iter=10, coarse_tol=1e-9):
-        self.coarse_iter, self.coarse_tol = coarse_iter, coarse_tol
+    def __init__(self, coarse_iter=10, coarse_tol=1e-9, mixed=False):
+        self.coarse_iter, self.coarse_tol, self.mixed = coarse_iter, coarse_tol, mixed
 
     def solve(self, z, r, coef, n=None, stream=None):
-        check(load().nb_pc_apply(coef.handle, NB_PC_HSMG, _ptr(z), _ptr(r),
-                                 _stream_handle(stream)))
+        kind = _lib.NB_PC_HSMG_MIXED if self.mixed else NB_PC_HSMG
+        check(load().nb_pc_apply(coef.handle, kind, _ptr(z), _ptr(r), _stream_handle(stream)))
 
 
 class CG:
@@ -206,7 +207,7 @@ class CG:
         o.max_iter = niter if niter is not None else self.max_iter
         o.abs_tol = self.abs_tol
         o.pc = getattr(self.M, "kind", NB_PC_NONE) if self.M is not None else NB_PC_NONE
-        o.mixed = int(self.mixed)
+        o.mixed = int(self.mixed or getattr(self.M, "mixed", False))
         o.coarse_iter = getattr(self.M, "coarse_iter", 10)
         o.coarse_tol = getattr(self.M, "coarse_tol", 1e-9)
         o.flexible = int(self.flexible)

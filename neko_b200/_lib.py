@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR
                 4: "NB_ERR_CUDA", 5: "NB_ERR_NOT_CONVERGED", 6: "NB_ERR_NAN",
                 7: "NB_ERR_TIMEOUT"}
 
-NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE = 0, 1, 2
+NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED = 0, 1, 2, 3
 
 
 class SolveOpts(ctypes.Structure):

@@ -39,7 +39,8 @@ __global__ void jacobi_scale_kernel(double *d, const double *h1, const double *h
 }
 
 __global__ void addcol4_kernel(double *w, const double *h2, const double *B, const double *u,
-                               long n) {
+                               long n, const int *skip) {
+  if (skip && *skip) return;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
        i += (long)gridDim.x * blockDim.x)
     w[i] = w[i] + h2[i] * B[i] * u[i];
@@ -77,6 +78,8 @@ __global__ void __launch_bounds__(kRedThreads)
     st->rtz1 = 1.0;
     st->iter = 0;
     st->nan = 0;
+    st->skip_rc = 1;
+    st->restart = 0;
     st->done = fabs(rn) < 2.220446049250313e-16 ? 1 : 0;
   }
 }
@@ -100,7 +103,8 @@ __global__ void __launch_bounds__(kRedThreads)
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
     st->rtz2 = st->rtz1;
     st->rtz1 = tot;
-    st->beta = st->iter == 0 ? 0.0 : tot / st->rtz2;
+    st->beta = (st->iter == 0 || st->restart) ? 0.0 : tot / st->rtz2;
+    st->restart = 0;
   }
 }
 
@@ -118,7 +122,8 @@ __global__ void __launch_bounds__(kRedThreads)
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
     st->rtz2 = st->rtz1;
     st->rtz1 = tot;
-    st->beta = st->iter == 0 ? 0.0 : tot / st->rtz2;
+    st->beta = (st->iter == 0 || st->restart) ? 0.0 : tot / st->rtz2;
+    st->restart = 0;
   }
 }
 
@@ -139,7 +144,8 @@ __global__ void __launch_bounds__(kRedThreads)
   }
   double tot[2];
   if (grid_sum2<kRedThreads>(s0, s1, partials, counter, tot)) {
-    st->beta = st->iter == 0 ? 0.0 : -st->alpha * tot[1] / st->rtz1;
+    st->beta = (st->iter == 0 || st->restart) ? 0.0 : -st->alpha * tot[1] / st->rtz1;
+    st->restart = 0;
     st->rtz2 = st->rtz1;
     st->rtz1 = tot[0];
   }
@@ -202,6 +208,36 @@ __global__ void __launch_bounds__(kRedThreads)
     if (rn < st->abs_tol) done = 1;
     if (st->iter >= st->max_iter) done = 1;
     st->done = done;
+    st->skip_rc = !(done == 0 && st->recompute_every > 0 && st->iter % st->recompute_every == 0);
+  }
+}
+
+// True residual: r = f - w (w = A x just computed), rtr, rnorm and the
+// convergence test redone on it; the next direction restarts (beta = 0).
+__global__ void __launch_bounds__(kRedThreads)
+    cg_true_residual_kernel(double *__restrict__ r, const double *__restrict__ f,
+                            const double *__restrict__ w, const double *__restrict__ mult, long n,
+                            CgState *st, double *partials, unsigned *counter) {
+  if (st->skip_rc) return;
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    const double ri = f[i] - w[i];
+    r[i] = ri;
+    s += ri * mult[i] * ri;
+  }
+  double tot;
+  if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
+    const double rn = sqrt(tot) * st->norm_fac;
+    st->rtr = tot;
+    st->rnorm = rn;
+    st->restart = 1;
+    st->skip_rc = 1;
+    if (!(rn == rn) || isinf(rn)) {
+      st->nan = 1;
+      st->done = 1;
+    }
+    if (rn < st->abs_tol) st->done = 1;
   }
 }
 
@@ -255,7 +291,7 @@ cudaError_t CgWorkspace::ensure(long n_) {
 
 // One CG iteration (all launches on s), precond chosen by pc.
 static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, double *x,
-                                cudaStream_t s) {
+                                const double *f, cudaStream_t s) {
   const long n = P->n;
   const int rb = red_blocks(n), eg = stream_grid(n, 256);
   if (pc) {
@@ -274,12 +310,21 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
   cg_update_p_kernel<<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
   cudaError_t e = P->ax_raw(W.w, W.p, s, &W.st->done);
   if (e != cudaSuccess) return e;
-  if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n);
+  if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n, &W.st->done);
   e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->done);
   if (e != cudaSuccess) return e;
   cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, n, W.st, W.partials, W.counter);
   cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(x, W.r, W.p, W.w, P->mult, n, W.st,
                                                  W.partials, W.counter);
+  if (W.recompute_every > 0) {  // w = A x, gs, mask; r = f - w (scheduled iterations only)
+    e = P->ax_raw(W.w, x, s, &W.st->skip_rc);
+    if (e != cudaSuccess) return e;
+    if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, x, n, &W.st->skip_rc);
+    e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->skip_rc);
+    if (e != cudaSuccess) return e;
+    cg_true_residual_kernel<<<rb, kRedThreads, 0, s>>>(W.r, f, W.w, P->mult, n, W.st,
+                                                       W.partials, W.counter);
+  }
   return cudaGetLastError();
 }
 
@@ -310,19 +355,23 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     return ws_fail(e == cudaErrorMemoryAllocation ? NB_ERR_OOM : NB_ERR_CUDA,
                    std::string("CG workspace: ") + cudaGetErrorString(e));
   W.use_jacobi = o.pc == NB_PC_JACOBI;
-  W.flexible = o.flexible != 0 && pc != nullptr;
+  W.flexible = (o.flexible != 0 || o.mixed != 0) && pc != nullptr;
+  W.recompute_every = o.mixed ? 50 : 0;
   CgState init{};
   init.norm_fac = 1.0 / std::sqrt(P->volume);
   init.abs_tol = o.abs_tol;
   init.max_iter = o.max_iter;
+  init.recompute_every = W.recompute_every;
+  init.skip_rc = 1;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const long n = P->n;
   cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(x, W.p, W.r, f, P->mult, n, W.st,
                                                         W.partials, W.counter, nullptr);
   NB_CUDA_TRY(cudaGetLastError());
   // (Re)capture the iteration graph when the operands changed.
-  const void *key[4] = {x, pc,
-                        (const void *)(intptr_t)(W.use_jacobi | (W.flexible << 1)),
+  const void *key[5] = {x, f, pc,
+                        (const void *)(intptr_t)(W.use_jacobi | (W.flexible << 1) |
+                                                 ((W.recompute_every > 0) << 2)),
                         (const void *)(intptr_t)P->ifh2};
   bool same = W.graph_exec && !memcmp(key, W.graph_key, sizeof(key));
   const int chunk = n > (1 << 22) ? 4 : 16;
@@ -336,8 +385,9 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     cudaGraph_t g;
     NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t ce = cudaSuccess;
-    for (int k = 0; k < chunk && ce == cudaSuccess; k++) ce = cg_iteration(P, W, pc, x, cs);
-    W.launches_per_iter = 6 + (P->ifh2 ? 1 : 0) + (pc ? pc->launches() : 0);
+    for (int k = 0; k < chunk && ce == cudaSuccess; k++) ce = cg_iteration(P, W, pc, x, f, cs);
+    W.launches_per_iter = 6 + (P->ifh2 ? 1 : 0) + (pc ? pc->launches() : 0) +
+                          (W.recompute_every > 0 ? 3 + (P->ifh2 ? 1 : 0) : 0);
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (ce != cudaSuccess) {

@@ -13,6 +13,9 @@ struct CgState {
   double norm_fac, abs_tol;
   double rtz1, rtz2, beta, pap, alpha, rtr, rnorm, res_start;
   int iter, max_iter, done, nan;
+  int recompute_every;  // > 0: r = f - A x every that many iterations
+  int skip_rc;          // 0 when the current iteration ends with a recompute
+  int restart;          // next beta is 0 (after a recompute)
 };
 
 // pc_t%solve(z, r): z = M^-1 r on stream s; returns early when *skip != 0.
@@ -33,9 +36,10 @@ struct CgWorkspace {
   void *host_state = nullptr;
   bool use_jacobi = true;
   bool flexible = false;
+  int recompute_every = 0;
   int launches_per_iter = 6;
   cudaGraphExec_t graph_exec = nullptr;
-  const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  const void *graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   ~CgWorkspace();
   cudaError_t ensure(long n);
 };

@@ -25,7 +25,7 @@ __global__ void jacobi_scale_kernel(double *d, const double *h1, const double *h
                                     const double *B, long n);
 // w += h2 * B * u
 __global__ void addcol4_kernel(double *w, const double *h2, const double *B, const double *u,
-                               long n);
+                               long n, const int *skip = nullptr);
 
 }  // namespace nb
 
@@ -52,7 +52,7 @@ struct nb_problem {
   // Krylov workspace (allocated on first solve)
   void *solver_ws = nullptr;
   size_t solver_ws_bytes = 0;
-  nb::HsmgState *hsmg = nullptr;
+  nb::HsmgState *hsmg[2] = {nullptr, nullptr};  // hsmg: [0] FP64, [1] mixed
 
   ~nb_problem();
   cudaError_t update_jacobi(cudaStream_t s);
@@ -64,6 +64,8 @@ struct nb_problem {
 
 namespace nb {
 void hsmg_free(nb_problem *p);
+// After new h1: the coarse levels take the new h1 (hsmg_set_h).
+cudaError_t hsmg_refresh_coefficients(nb_problem *p);
 
 // Deletes a half-built problem on early return.
 struct nb_problem_guard {

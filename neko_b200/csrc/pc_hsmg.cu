@@ -18,6 +18,7 @@
 // eigenvalue sums from the three per-direction spectra, so it reads
 // 3 nl^2 + 3 nl values of factors per element instead of nl^3.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -173,16 +174,17 @@ __global__ void schwarz_post_kernel(const T *__restrict__ ext, const int *__rest
 
 // out = (A x A x A) in per element, A(o, i) = TR ? M[i + NI*o] : M[o + NO*i];
 // the input is multiplied by `scale` first when given; ACC adds to out.
-template <typename T, int NI, int NO, bool TR, bool ACC>
-__global__ void tensor3_kernel(const T *__restrict__ in, const T *__restrict__ scale,
-                               const T *__restrict__ M, T *__restrict__ out, long nelv,
+// Computed in T; input/output converted on load/store.
+template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC>
+__global__ void tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
+                               const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
                                const int *__restrict__ skip) {
   if (skip && *skip) return;
   constexpr int I3 = NI * NI * NI, O3 = NO * NO * NO;
   __shared__ T su[I3], s1[NO * NI * NI], s2[NO * NO * NI], sA[NO * NI];
   const long e = blockIdx.x;
   for (int q = threadIdx.x; q < I3; q += blockDim.x)
-    su[q] = scale ? in[e * I3 + q] * scale[e * I3 + q] : in[e * I3 + q];
+    su[q] = scale ? (T)(in[e * I3 + q] * scale[e * I3 + q]) : (T)in[e * I3 + q];
   for (int q = threadIdx.x; q < NO * NI; q += blockDim.x) {
     const int o = q % NO, i = q / NO;
     sA[q] = TR ? M[i + NI * o] : M[o + NO * i];  // sA(o, i) at o + NO*i
@@ -190,27 +192,36 @@ __global__ void tensor3_kernel(const T *__restrict__ in, const T *__restrict__ s
   __syncthreads();
   for (int q = threadIdx.x; q < NO * NI * NI; q += blockDim.x) {  // x: s1(o, j, k)
     const int o = q % NO, jk = q / NO;
-    T s = 0;
-    for (int i = 0; i < NI; i++) s += sA[o + NO * i] * su[i + NI * jk];
-    s1[q] = s;
+    T acc = 0;
+    for (int i = 0; i < NI; i++) acc += sA[o + NO * i] * su[i + NI * jk];
+    s1[q] = acc;
   }
   __syncthreads();
   for (int q = threadIdx.x; q < NO * NO * NI; q += blockDim.x) {  // y: s2(o, p, k)
     const int o = q % NO, p = (q / NO) % NO, k = q / (NO * NO);
-    T s = 0;
-    for (int j = 0; j < NI; j++) s += sA[p + NO * j] * s1[o + NO * j + NO * NI * k];
-    s2[q] = s;
+    T acc = 0;
+    for (int j = 0; j < NI; j++) acc += sA[p + NO * j] * s1[o + NO * j + NO * NI * k];
+    s2[q] = acc;
   }
   __syncthreads();
   for (int q = threadIdx.x; q < O3; q += blockDim.x) {  // z
     const int op = q % (NO * NO), r = q / (NO * NO);
-    T s = 0;
-    for (int k = 0; k < NI; k++) s += sA[r + NO * k] * s2[op + NO * NO * k];
+    T acc = 0;
+    for (int k = 0; k < NI; k++) acc += sA[r + NO * k] * s2[op + NO * NO * k];
     if (ACC)
-      out[e * O3 + q] += s;
+      out[e * O3 + q] = (TOUT)((T)out[e * O3 + q] + acc);
     else
-      out[e * O3 + q] = s;
+      out[e * O3 + q] = (TOUT)acc;
   }
+}
+
+template <typename TA, typename TB>
+__global__ void convert_kernel(TB *__restrict__ b, const TA *__restrict__ a, long n,
+                               const int *__restrict__ skip) {
+  if (skip && *skip) return;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    b[i] = (TB)a[i];
 }
 
 __global__ void mask_kernel(double *x, const int *msk, int m, const int *skip) {
@@ -220,24 +231,24 @@ __global__ void mask_kernel(double *x, const int *msk, int m, const int *skip) {
 }
 
 // ---------------------------------------------------------------------------
-// Schwarz level
+// Schwarz level (smoother precision T)
 // ---------------------------------------------------------------------------
+template <typename T>
 struct SchwarzLevel {
   int lx = 0, nl = 0;
   long nelv = 0, n = 0;
-  nb_problem *P = nullptr;  // the level's problem (gs maps, mask, mult)
-  double *S = nullptr, *lam = nullptr, *eps = nullptr, *wt = nullptr, *ext = nullptr;
+  nb_problem *P = nullptr;  // the level's problem (gs maps, mask)
+  T *S = nullptr, *lam = nullptr, *eps = nullptr, *wt = nullptr, *ext = nullptr;
   int *fn = nullptr;
 };
 
-template <int LX>
-static cudaError_t launch_fdm_post(const SchwarzLevel &L, const double *r, double *e,
-                                   const int *skip, cudaStream_t s) {
+template <typename TIN, typename T, int LX>
+static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
+                                   cudaStream_t s) {
   constexpr int NL = LX + 2;
   constexpr int NE = NL * NL >= 64 ? 1 : (128 / (NL * NL));
-  const size_t smem =
-      sizeof(double) * NE * (2 * NL * NL * NL + 6 * NL * NL + 3 * NL + 2);
-  auto kern = fdm_kernel<double, double, NL, NE>;
+  const size_t smem = sizeof(T) * NE * (2 * NL * NL * NL + 6 * NL * NL + 3 * NL + 2);
+  auto kern = fdm_kernel<TIN, T, NL, NE>;
   if (smem > 48 * 1024) {
     cudaError_t err =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -246,49 +257,37 @@ static cudaError_t launch_fdm_post(const SchwarzLevel &L, const double *r, doubl
   kern<<<(unsigned)((L.nelv + NE - 1) / NE), dim3(NL * NL, NE), smem, s>>>(
       r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
   const long n = L.nelv * LX * LX * LX;
-  schwarz_post_kernel<double, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.ext, L.fn, L.wt, e,
-                                                                             L.nelv, skip);
+  schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.ext, L.fn, L.wt, e,
+                                                                        L.nelv, skip);
   return cudaGetLastError();
 }
 
 // e = Schwarz(r) on level L (r already masked): FDM + overlap + gs + mask.
-static cudaError_t schwarz_apply(const SchwarzLevel &L, const double *r, double *e,
-                                 const int *skip, cudaStream_t s) {
+template <typename TIN, typename T>
+static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
+                                 cudaStream_t s) {
   cudaError_t err;
   switch (L.lx) {
-    case 3: err = launch_fdm_post<3>(L, r, e, skip, s); break;
-    case 4: err = launch_fdm_post<4>(L, r, e, skip, s); break;
-    case 5: err = launch_fdm_post<5>(L, r, e, skip, s); break;
-    case 6: err = launch_fdm_post<6>(L, r, e, skip, s); break;
-    case 7: err = launch_fdm_post<7>(L, r, e, skip, s); break;
-    case 8: err = launch_fdm_post<8>(L, r, e, skip, s); break;
-    case 9: err = launch_fdm_post<9>(L, r, e, skip, s); break;
-    case 10: err = launch_fdm_post<10>(L, r, e, skip, s); break;
-    case 11: err = launch_fdm_post<11>(L, r, e, skip, s); break;
-    case 12: err = launch_fdm_post<12>(L, r, e, skip, s); break;
-    case 13: err = launch_fdm_post<13>(L, r, e, skip, s); break;
-    case 14: err = launch_fdm_post<14>(L, r, e, skip, s); break;
+#define NB_S(N) \
+  case N: err = launch_fdm_post<TIN, T, N>(L, r, e, skip, s); break;
+    NB_S(3) NB_S(4) NB_S(5) NB_S(6) NB_S(7) NB_S(8) NB_S(9) NB_S(10) NB_S(11) NB_S(12)
+    NB_S(13) NB_S(14)
+#undef NB_S
     default: return cudaErrorNotSupported;
   }
   if (err != cudaSuccess) return err;
-  return gs_add_fused<double>(L.P->gsd, e, true, s, skip);
+  return gs_add_fused<T>(L.P->gsd, e, true, s, skip);
 }
 
-template <int NI, int NO, bool TR, bool ACC>
-static void tensor3(const double *in, const double *scale, const double *M, double *out,
-                    long nelv, const int *skip, cudaStream_t s) {
-  tensor3_kernel<double, NI, NO, TR, ACC><<<(unsigned)nelv, 128, 0, s>>>(in, scale, M, out,
-                                                                         nelv, skip);
-}
-
-// restriction (Jt x Jt x Jt) (in * scale) from NI to NO points, J is NI x NO
-static cudaError_t restrict_level(int ni, int no, const double *in, const double *scale,
-                                  const double *J, double *out, long nelv, const int *skip,
-                                  cudaStream_t s) {
-#define NB_R(A, B)                                                        \
-  if (ni == A && no == B) {                                               \
-    tensor3<A, B, true, false>(in, scale, J, out, nelv, skip, s);         \
-    return cudaGetLastError();                                            \
+// restriction (Jt x Jt x Jt)(in * scale) from ni to no points (J: ni x no)
+template <typename TIN, typename TOUT, typename T>
+static cudaError_t restrict_level(int ni, int no, const TIN *in, const TIN *scale, const T *J,
+                                  TOUT *out, long nelv, const int *skip, cudaStream_t s) {
+#define NB_R(A, B)                                                                          \
+  if (ni == A && no == B) {                                                                 \
+    tensor3_kernel<TIN, TOUT, T, A, B, true, false><<<(unsigned)nelv, 128, 0, s>>>(         \
+        in, scale, J, out, nelv, skip);                                                     \
+    return cudaGetLastError();                                                              \
   }
   NB_R(4, 2) NB_R(3, 2) NB_R(5, 4) NB_R(6, 4) NB_R(7, 4) NB_R(8, 4) NB_R(9, 4) NB_R(10, 4)
   NB_R(11, 4) NB_R(12, 4) NB_R(13, 4) NB_R(14, 4) NB_R(4, 3)
@@ -296,13 +295,15 @@ static cudaError_t restrict_level(int ni, int no, const double *in, const double
   return cudaErrorNotSupported;
 }
 
-// prolongation out += (J x J x J) in from NI to NO points, J is NO x NI
-static cudaError_t prolong_add(int ni, int no, const double *in, const double *J, double *out,
-                               long nelv, const int *skip, cudaStream_t s) {
-#define NB_P(A, B)                                                        \
-  if (ni == A && no == B) {                                               \
-    tensor3<A, B, false, true>(in, nullptr, J, out, nelv, skip, s);       \
-    return cudaGetLastError();                                            \
+// prolongation out += (J x J x J) in from ni to no points (J: no x ni)
+template <typename TIN, typename TOUT, typename T>
+static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *out, long nelv,
+                               const int *skip, cudaStream_t s) {
+#define NB_P(A, B)                                                                          \
+  if (ni == A && no == B) {                                                                 \
+    tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, 128, 0, s>>>(         \
+        in, nullptr, J, out, nelv, skip);                                                   \
+    return cudaGetLastError();                                                              \
   }
   NB_P(2, 4) NB_P(2, 3) NB_P(4, 5) NB_P(4, 6) NB_P(4, 7) NB_P(4, 8) NB_P(4, 9) NB_P(4, 10)
   NB_P(4, 11) NB_P(4, 12) NB_P(4, 13) NB_P(4, 14) NB_P(3, 4)
@@ -311,51 +312,60 @@ static cudaError_t prolong_add(int ni, int no, const double *in, const double *J
 }
 
 // ---------------------------------------------------------------------------
-// The preconditioner
+// The preconditioner.  T is the precision of the smoothing levels (double
+// for the FP64 path, float for the mixed path); the coarse CG is FP64.
 // ---------------------------------------------------------------------------
 struct HsmgState : public Precond {
   nb_problem *fine = nullptr, *mid = nullptr, *crs = nullptr;
-  SchwarzLevel sf, sm;
-  double *Jfm = nullptr, *Jmc = nullptr;  // prolongations (fine x mid), (mid x crs)
-  double *w_mid = nullptr, *e_mid = nullptr, *r_crs = nullptr, *e_crs = nullptr;
-  double *rc = nullptr, *zc = nullptr, *pc = nullptr, *wc = nullptr;
-  CgState *stc = nullptr;
-  double *partials = nullptr;
-  unsigned *counter = nullptr;
   void *arena = nullptr;
   int niter = 10;
   double tol = 1e-9;
-
+  bool mixed = false;
   ~HsmgState() override {
     if (arena) cudaFree(arena);
     if (mid) nb_problem_destroy(mid);
     if (crs) nb_problem_destroy(crs);
   }
+};
+
+template <typename T>
+struct HsmgImpl : public HsmgState {
+  SchwarzLevel<T> sf, sm;
+  T *Jfm = nullptr, *Jmc = nullptr;  // prolongations (fine x mid), (mid x crs)
+  T *mult_f = nullptr, *mult_m = nullptr;
+  T *zf = nullptr;                   // smoother-precision fine output (float path)
+  T *w_mid = nullptr, *e_mid = nullptr;
+  double *r_crs = nullptr, *e_crs = nullptr;
+  double *rc = nullptr, *zc = nullptr, *pc = nullptr, *wc = nullptr;
+  CgState *stc = nullptr;
+  double *partials = nullptr;
+  unsigned *counter = nullptr;
 
   int launches() const override {
     // 2 Schwarz x (fdm, post, gs) + restrict x2 + gs x2 + coarse (init +
-    // niter x 6) + prolong x2 + final gs
-    return 6 + 2 + 2 + 1 + niter * 6 + 2 + 1;
+    // niter x 6) + prolong x2 + final gs (+ convert)
+    return 6 + 2 + 2 + 1 + niter * 6 + 2 + 1 + (sizeof(T) == 4 ? 1 : 0);
   }
 
   cudaError_t apply(double *z, const double *r, const int *skip, cudaStream_t s) override {
     cudaError_t e;
     const long nelv = fine->nelv;
-    // fine Schwarz: z = S_f r
-    if ((e = schwarz_apply(sf, r, z, skip, s)) != cudaSuccess) return e;
+    T *zs = sizeof(T) == 8 ? reinterpret_cast<T *>(z) : zf;
+    // fine Schwarz: zs = S_f r
+    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, s)) != cudaSuccess) return e;
     // restrict (r * mult) to the middle level, assemble, mask
-    if ((e = restrict_level(fine->lx, mid->lx, r, fine->mult, Jfm, w_mid, nelv, skip, s)) !=
-        cudaSuccess)
+    if ((e = restrict_level<double, T, T>(fine->lx, mid->lx, r, fine->mult, Jfm, w_mid, nelv,
+                                          skip, s)) != cudaSuccess)
       return e;
-    if ((e = gs_add_fused<double>(mid->gsd, w_mid, true, s, skip)) != cudaSuccess) return e;
+    if ((e = gs_add_fused<T>(mid->gsd, w_mid, true, s, skip)) != cudaSuccess) return e;
     // middle Schwarz: e_mid = S_m w
-    if ((e = schwarz_apply(sm, w_mid, e_mid, skip, s)) != cudaSuccess) return e;
-    // restrict (w * mult_mid) to the coarse level, assemble, mask
-    if ((e = restrict_level(mid->lx, crs->lx, w_mid, mid->mult, Jmc, r_crs, nelv, skip, s)) !=
-        cudaSuccess)
+    if ((e = schwarz_apply<T, T>(sm, w_mid, e_mid, skip, s)) != cudaSuccess) return e;
+    // restrict (w * mult_mid) to the coarse level (FP64), assemble, mask
+    if ((e = restrict_level<T, double, T>(mid->lx, crs->lx, w_mid, mult_m, Jmc, r_crs, nelv,
+                                          skip, s)) != cudaSuccess)
       return e;
     if ((e = gs_add_fused<double>(crs->gsd, r_crs, true, s, skip)) != cudaSuccess) return e;
-    // coarse CG (Jacobi), niter iterations or abs tol
+    // coarse CG (Jacobi), niter iterations or abs tol, FP64
     const long nc = crs->n;
     const int rb = red_blocks(nc), eg = stream_grid(nc, 256);
     cg_init_kernel<<<rb, kRedThreads, 0, s>>>(e_crs, pc, rc, r_crs, crs->mult, nc, stc, partials,
@@ -370,20 +380,48 @@ struct HsmgState : public Precond {
       cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(e_crs, rc, pc, wc, crs->mult, nc, stc,
                                                      partials, counter);
     }
-    // prolong: e_mid += J e_crs; z += J e_mid; z = mult * gs(z)
-    if ((e = prolong_add(crs->lx, mid->lx, e_crs, Jmc, e_mid, nelv, skip, s)) != cudaSuccess)
+    // prolong: e_mid += J e_crs; zs += J e_mid; z = mult * gs(zs)
+    if ((e = prolong_add<double, T, T>(crs->lx, mid->lx, e_crs, Jmc, e_mid, nelv, skip, s)) !=
+        cudaSuccess)
       return e;
-    if ((e = prolong_add(mid->lx, fine->lx, e_mid, Jfm, z, nelv, skip, s)) != cudaSuccess)
+    if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s)) !=
+        cudaSuccess)
       return e;
-    if ((e = gs_add_fused<double>(fine->gsd, z, false, s, skip, fine->mult)) != cudaSuccess)
-      return e;
+    if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, mult_f)) != cudaSuccess) return e;
+    if (sizeof(T) == 4)
+      convert_kernel<T, double><<<stream_grid(fine->n, 256), 256, 0, s>>>(z, zs, fine->n, skip);
     return cudaGetLastError();
   }
 };
 
 void hsmg_free(nb_problem *p) {
-  delete p->hsmg;
-  p->hsmg = nullptr;
+  for (auto &h : p->hsmg) {
+    delete h;
+    h = nullptr;
+  }
+}
+
+// hsmg_set_h (pc_hsmg.f90:367-379): the coarse h1 is the first n_crs values
+// of the fine h1 and the coarse problem has no h2; its Jacobi diagonal
+// follows.  The mesh is marked all-deformed (pc_hsmg.f90:267), which turns on
+// the corner cross terms of that diagonal.
+static cudaError_t hsmg_set_h(nb_problem *P, nb_problem *C) {
+  cudaError_t e;
+  if ((e = cudaMemcpy(C->h1, P->h1, C->n * 8, cudaMemcpyDeviceToDevice)) != cudaSuccess ||
+      (e = cudaMemset(C->dfrmd, 1, C->nelv)) != cudaSuccess)
+    return e;
+  C->ifh2 = false;
+  C->invalidate_solver_cache();
+  return C->update_jacobi(nullptr);
+}
+
+cudaError_t hsmg_refresh_coefficients(nb_problem *p) {
+  for (auto *h : p->hsmg) {
+    if (!h) continue;
+    cudaError_t e = hsmg_set_h(p, h->crs);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 static nb_status hfail(nb_status st, const std::string &m) {
@@ -399,50 +437,147 @@ static void facet_types(const std::vector<int> &fn, bool dirichlet, std::vector<
     ft[q] = fn[q] ? 0 : (dirichlet ? 1 : -(int)(q % 6 + 1));
 }
 
-static nb_status build_schwarz(nb_problem *L, bool dirichlet, SchwarzLevel &S,
-                               std::vector<double> &hostS, std::vector<double> &hostL,
-                               std::vector<double> &hostE, std::vector<double> &hostW,
-                               std::vector<int> &hostF) {
-  S.P = L;
-  S.lx = L->lx;
-  S.nl = L->lx + 2;
-  S.nelv = L->nelv;
-  S.n = L->n;
+struct SchwarzHost {
+  std::vector<double> S, lam, eps, wt;
+  std::vector<int> fn;
+};
+
+static nb_status build_schwarz_host(nb_problem *L, bool dirichlet, SchwarzHost &H) {
   std::vector<double> x(L->n), y(L->n), z(L->n);
   if (cudaMemcpy(x.data(), L->x, L->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
       cudaMemcpy(y.data(), L->y, L->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
       cudaMemcpy(z.data(), L->z, L->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
     return hfail(NB_ERR_CUDA, "hsmg: coordinate copy failed");
-  box_facet_neigh(L->box, hostF);
+  box_facet_neigh(L->box, H.fn);
   std::vector<int> ft;
-  facet_types(hostF, dirichlet, ft);
+  facet_types(H.fn, dirichlet, ft);
   FdmHost F;
   fdm_build(L->lx, L->nelv, x, y, z, ft, L->maps, F);
-  hostS.swap(F.S);
-  hostL.swap(F.lam);
-  hostE.swap(F.eps);
-  schwarz_weights(L->lx, L->nelv, hostF, L->maps, hostW);
+  H.S.swap(F.S);
+  H.lam.swap(F.lam);
+  H.eps.swap(F.eps);
+  schwarz_weights(L->lx, L->nelv, H.fn, L->maps, H.wt);
+  return NB_OK;
+}
+
+// Device arena layout helper: offsets in 256-byte slices.
+struct Slicer {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+template <typename T>
+static std::vector<T> cast_vec(const std::vector<double> &v) {
+  return std::vector<T>(v.begin(), v.end());
+}
+
+// Allocates and fills the device side of HsmgImpl<T>.
+template <typename T>
+static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const SchwarzHost &hm,
+                             const std::vector<double> &Jfm, const std::vector<double> &Jmc) {
+  nb_problem *P = H->fine, *M = H->mid, *C = H->crs;
+  const long nelv = P->nelv, n = P->n, nm = M->n, nc = C->n;
+  const int nlf = P->lx + 2, nlm = M->lx + 2;
+  const bool f32 = sizeof(T) == 4;
+  Slicer c;
+  const size_t o_Sf = c.take(hf.S.size() * sizeof(T)), o_Lf = c.take(hf.lam.size() * sizeof(T)),
+               o_Ef = c.take(hf.eps.size() * sizeof(T)), o_Wf = c.take(hf.wt.size() * sizeof(T)),
+               o_Ff = c.take(hf.fn.size() * 4),
+               o_Xf = c.take((size_t)nelv * nlf * nlf * nlf * sizeof(T));
+  const size_t o_Sm = c.take(hm.S.size() * sizeof(T)), o_Lm = c.take(hm.lam.size() * sizeof(T)),
+               o_Em = c.take(hm.eps.size() * sizeof(T)), o_Wm = c.take(hm.wt.size() * sizeof(T)),
+               o_Fm = c.take(hm.fn.size() * 4),
+               o_Xm = c.take((size_t)nelv * nlm * nlm * nlm * sizeof(T));
+  const size_t o_Jfm = c.take(Jfm.size() * sizeof(T)), o_Jmc = c.take(Jmc.size() * sizeof(T));
+  const size_t o_mf = f32 ? c.take(n * sizeof(T)) : 0, o_mm = c.take(nm * sizeof(T));
+  const size_t o_zf = f32 ? c.take(n * sizeof(T)) : 0;
+  const size_t o_wm = c.take(nm * sizeof(T)), o_em = c.take(nm * sizeof(T));
+  const size_t o_rc = c.take(nc * 8), o_ec = c.take(nc * 8), o_r = c.take(nc * 8),
+               o_z = c.take(nc * 8), o_p = c.take(nc * 8), o_w = c.take(nc * 8);
+  const size_t o_st = c.take(sizeof(CgState)), o_part = c.take(2 * 148 * 8 * 8 + 64);
+  if (cudaMalloc(&H->arena, c.off) != cudaSuccess) return hfail(NB_ERR_OOM, "hsmg: device arena");
+  char *A = (char *)H->arena;
+  auto Tp = [&](size_t o) { return (T *)(A + o); };
+  auto Dp = [&](size_t o) { return (double *)(A + o); };
+  auto setlev = [&](SchwarzLevel<T> &L, nb_problem *Q, size_t oS, size_t oL, size_t oE, size_t oW,
+                    size_t oF, size_t oX) {
+    L.P = Q;
+    L.lx = Q->lx;
+    L.nl = Q->lx + 2;
+    L.nelv = Q->nelv;
+    L.n = Q->n;
+    L.S = Tp(oS), L.lam = Tp(oL), L.eps = Tp(oE), L.wt = Tp(oW), L.fn = (int *)(A + oF);
+    L.ext = Tp(oX);
+  };
+  setlev(H->sf, P, o_Sf, o_Lf, o_Ef, o_Wf, o_Ff, o_Xf);
+  setlev(H->sm, M, o_Sm, o_Lm, o_Em, o_Wm, o_Fm, o_Xm);
+  H->Jfm = Tp(o_Jfm), H->Jmc = Tp(o_Jmc);
+  H->mult_f = f32 ? Tp(o_mf) : reinterpret_cast<T *>(P->mult);
+  H->mult_m = Tp(o_mm);
+  H->zf = f32 ? Tp(o_zf) : nullptr;
+  H->w_mid = Tp(o_wm), H->e_mid = Tp(o_em);
+  H->r_crs = Dp(o_rc), H->e_crs = Dp(o_ec), H->rc = Dp(o_r), H->zc = Dp(o_z), H->pc = Dp(o_p),
+  H->wc = Dp(o_w);
+  H->stc = (CgState *)(A + o_st);
+  H->partials = Dp(o_part);
+  H->counter = (unsigned *)(A + o_part + 2 * 148 * 8 * 8);
+  auto upv = [&](size_t o, const std::vector<double> &v) {
+    std::vector<T> t = cast_vec<T>(v);
+    return t.empty() ? cudaSuccess
+                     : cudaMemcpy(A + o, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice);
+  };
+  auto upi = [&](size_t o, const std::vector<int> &v) {
+    return cudaMemcpy(A + o, v.data(), v.size() * 4, cudaMemcpyHostToDevice);
+  };
+  std::vector<double> hm_mult(nm), hf_mult;
+  if (cudaMemcpy(hm_mult.data(), M->mult, nm * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return hfail(NB_ERR_CUDA, "hsmg: mult copy failed");
+  if (f32) {
+    hf_mult.resize(n);
+    if (cudaMemcpy(hf_mult.data(), P->mult, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return hfail(NB_ERR_CUDA, "hsmg: mult copy failed");
+  }
+  CgState cs{};
+  cs.norm_fac = 1.0 / std::sqrt(C->volume);
+  cs.abs_tol = H->tol;
+  cs.max_iter = H->niter;
+  cs.done = 1;
+  if (upv(o_Sf, hf.S) || upv(o_Lf, hf.lam) || upv(o_Ef, hf.eps) || upv(o_Wf, hf.wt) ||
+      upi(o_Ff, hf.fn) || upv(o_Sm, hm.S) || upv(o_Lm, hm.lam) || upv(o_Em, hm.eps) ||
+      upv(o_Wm, hm.wt) || upi(o_Fm, hm.fn) || upv(o_Jfm, Jfm) || upv(o_Jmc, Jmc) ||
+      upv(o_mm, hm_mult) || (f32 && upv(o_mf, hf_mult)) ||
+      cudaMemcpy(A + o_st, &cs, sizeof(cs), cudaMemcpyHostToDevice) ||
+      cudaMemset(A + o_part, 0, 2 * 148 * 8 * 8 + 64))
+    return hfail(NB_ERR_CUDA, "hsmg: upload failed");
   return NB_OK;
 }
 
 nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   const int niter = o.coarse_iter > 0 ? o.coarse_iter : 10;
   const double tol = o.coarse_tol > 0 ? o.coarse_tol : 1e-9;
-  if (P->hsmg && (P->hsmg->niter != niter || P->hsmg->tol != tol)) {
+  const bool mixed = o.mixed != 0;
+  HsmgState *&slot = P->hsmg[mixed ? 1 : 0];
+  if (slot && (slot->niter != niter || slot->tol != tol)) {
     P->invalidate_solver_cache();
-    hsmg_free(P);
+    delete slot;
+    slot = nullptr;
   }
-  if (P->hsmg) {
-    *out = P->hsmg;
+  if (slot) {
+    *out = slot;
     return NB_OK;
   }
   const int lx = P->lx;
   if (lx < 3 || lx > 14) return hfail(NB_ERR_UNSUPPORTED, "hsmg supports lx 3..14");
   const int lx_mid = lx < 5 ? std::max(lx - 1, 3) : 4, lx_crs = 2;
-  HsmgState *H = new HsmgState();
+  HsmgState *H = mixed ? (HsmgState *)new HsmgImpl<float>() : (HsmgState *)new HsmgImpl<double>();
   H->fine = P;
   H->niter = niter;
   H->tol = tol;
+  H->mixed = mixed;
   const bool dirichlet = P->nmask > 0;
   nb_status st = nb_problem_create_box(P->box.nel, P->box.lo, P->box.hi, P->box.periodic,
                                        lx_mid, P->deform_amp, dirichlet, &H->mid);
@@ -453,25 +588,13 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
     delete H;
     return st;
   }
-  // hsmg_set_h (pc_hsmg.f90:367-379): coarse h1 = first n_crs values of the
-  // fine h1, no h2; the mesh is marked all-deformed (pc_hsmg.f90:267), which
-  // turns on the corner cross terms of the coarse Jacobi diagonal.
-  nb_problem *C = H->crs;
-  if (cudaMemcpy(C->h1, P->h1, C->n * 8, cudaMemcpyDeviceToDevice) != cudaSuccess ||
-      cudaMemset(C->dfrmd, 1, C->nelv) != cudaSuccess) {
+  if (hsmg_set_h(P, H->crs) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
     delete H;
-    return hfail(NB_ERR_CUDA, "hsmg: coarse coefficient copy failed");
+    return hfail(NB_ERR_CUDA, "hsmg: coarse coefficients failed");
   }
-  C->ifh2 = false;
-  if (C->update_jacobi(nullptr) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
-    delete H;
-    return hfail(NB_ERR_CUDA, "hsmg: coarse Jacobi failed");
-  }
-  // host setup of both Schwarz levels
-  std::vector<double> Sf, Lf, Ef, Wf, Sm, Lm, Em, Wm;
-  std::vector<int> Ff, Fm;
-  if ((st = build_schwarz(P, dirichlet, H->sf, Sf, Lf, Ef, Wf, Ff)) != NB_OK ||
-      (st = build_schwarz(H->mid, dirichlet, H->sm, Sm, Lm, Em, Wm, Fm)) != NB_OK) {
+  SchwarzHost hf, hm;
+  if ((st = build_schwarz_host(P, dirichlet, hf)) != NB_OK ||
+      (st = build_schwarz_host(H->mid, dirichlet, hm)) != NB_OK) {
     delete H;
     return st;
   }
@@ -481,69 +604,24 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   gll_space(lx_crs, zc, tmp, t2, t3);
   lagrange_matrix(zf, zm, Jfm);
   lagrange_matrix(zm, zc, Jmc);
-  // one device arena for everything
-  const long nelv = P->nelv, nm = H->mid->n, nc = C->n;
-  const int nlf = lx + 2, nlm = lx_mid + 2;
-  size_t off = 0;
-  auto take = [&](size_t bytes) {
-    size_t o = off;
-    off += (bytes + 255) & ~size_t(255);
-    return o;
-  };
-  const size_t o_Sf = take(Sf.size() * 8), o_Lf = take(Lf.size() * 8), o_Ef = take(Ef.size() * 8),
-               o_Wf = take(Wf.size() * 8), o_Ff = take(Ff.size() * 4),
-               o_Xf = take((size_t)nelv * nlf * nlf * nlf * 8);
-  const size_t o_Sm = take(Sm.size() * 8), o_Lm = take(Lm.size() * 8), o_Em = take(Em.size() * 8),
-               o_Wm = take(Wm.size() * 8), o_Fm = take(Fm.size() * 4),
-               o_Xm = take((size_t)nelv * nlm * nlm * nlm * 8);
-  const size_t o_Jfm = take(Jfm.size() * 8), o_Jmc = take(Jmc.size() * 8);
-  const size_t o_wm = take(nm * 8), o_em = take(nm * 8), o_rc = take(nc * 8), o_ec = take(nc * 8);
-  const size_t o_r = take(nc * 8), o_z = take(nc * 8), o_p = take(nc * 8), o_w = take(nc * 8);
-  const size_t o_st = take(sizeof(CgState)), o_part = take(2 * 148 * 8 * 8 + 64);
-  if (cudaMalloc(&H->arena, off) != cudaSuccess) {
+  st = mixed ? upload_impl((HsmgImpl<float> *)H, hf, hm, Jfm, Jmc)
+             : upload_impl((HsmgImpl<double> *)H, hf, hm, Jfm, Jmc);
+  if (st != NB_OK) {
     delete H;
-    return hfail(NB_ERR_OOM, "hsmg: device arena");
+    return st;
   }
-  char *A = (char *)H->arena;
-  auto D = [&](size_t o) { return (double *)(A + o); };
-  H->sf.S = D(o_Sf), H->sf.lam = D(o_Lf), H->sf.eps = D(o_Ef), H->sf.wt = D(o_Wf);
-  H->sf.fn = (int *)(A + o_Ff), H->sf.ext = D(o_Xf);
-  H->sm.S = D(o_Sm), H->sm.lam = D(o_Lm), H->sm.eps = D(o_Em), H->sm.wt = D(o_Wm);
-  H->sm.fn = (int *)(A + o_Fm), H->sm.ext = D(o_Xm);
-  H->Jfm = D(o_Jfm), H->Jmc = D(o_Jmc);
-  H->w_mid = D(o_wm), H->e_mid = D(o_em), H->r_crs = D(o_rc), H->e_crs = D(o_ec);
-  H->rc = D(o_r), H->zc = D(o_z), H->pc = D(o_p), H->wc = D(o_w);
-  H->stc = (CgState *)(A + o_st);
-  H->partials = D(o_part);
-  H->counter = (unsigned *)(A + o_part + 2 * 148 * 8 * 8);
-  auto up = [&](size_t o, const void *src, size_t bytes) {
-    return bytes ? cudaMemcpy(A + o, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
-  };
-  CgState cs{};
-  cs.norm_fac = 1.0 / std::sqrt(C->volume);
-  cs.abs_tol = tol;
-  cs.max_iter = niter;
-  cs.done = 1;
-  if (up(o_Sf, Sf.data(), Sf.size() * 8) || up(o_Lf, Lf.data(), Lf.size() * 8) ||
-      up(o_Ef, Ef.data(), Ef.size() * 8) || up(o_Wf, Wf.data(), Wf.size() * 8) ||
-      up(o_Ff, Ff.data(), Ff.size() * 4) || up(o_Sm, Sm.data(), Sm.size() * 8) ||
-      up(o_Lm, Lm.data(), Lm.size() * 8) || up(o_Em, Em.data(), Em.size() * 8) ||
-      up(o_Wm, Wm.data(), Wm.size() * 8) || up(o_Fm, Fm.data(), Fm.size() * 4) ||
-      up(o_Jfm, Jfm.data(), Jfm.size() * 8) || up(o_Jmc, Jmc.data(), Jmc.size() * 8) ||
-      up(o_st, &cs, sizeof(cs)) || cudaMemset(A + o_part, 0, 2 * 148 * 8 * 8 + 64)) {
-    delete H;
-    return hfail(NB_ERR_CUDA, "hsmg: upload failed");
-  }
-  P->hsmg = H;
+  slot = H;
   *out = H;
   return NB_OK;
 }
 
 // Exposed for tests: z = M r with the problem's hsmg (built on demand).
-nb_status hsmg_apply_once(nb_problem *P, double *z, const double *r, cudaStream_t s) {
+nb_status hsmg_apply_once(nb_problem *P, double *z, const double *r, cudaStream_t s, int mixed) {
   nb_solve_opts o{};
-  o.coarse_iter = P->hsmg ? P->hsmg->niter : 10;
-  o.coarse_tol = P->hsmg ? P->hsmg->tol : 1e-9;
+  const HsmgState *h = P->hsmg[mixed ? 1 : 0];
+  o.coarse_iter = h ? h->niter : 10;
+  o.coarse_tol = h ? h->tol : 1e-9;
+  o.mixed = mixed;
   Precond *pc = nullptr;
   nb_status st = hsmg_get(P, o, &pc);
   if (st != NB_OK) return st;
@@ -561,9 +639,9 @@ extern "C" nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double 
     set_error("null argument");
     return NB_ERR_ARG;
   }
-  if (pc != NB_PC_HSMG) {
-    set_error("nb_pc_apply: only NB_PC_HSMG");
+  if (pc != NB_PC_HSMG && pc != NB_PC_HSMG_MIXED) {
+    set_error("nb_pc_apply: pc must be NB_PC_HSMG or NB_PC_HSMG_MIXED");
     return NB_ERR_ARG;
   }
-  return hsmg_apply_once(p, z, r, (cudaStream_t)stream);
+  return hsmg_apply_once(p, z, r, (cudaStream_t)stream, pc == NB_PC_HSMG_MIXED);
 }

@@ -166,7 +166,7 @@ static nb_status fail(nb_status s, const std::string &msg) {
 nb_problem::~nb_problem() {
   if (arena) cudaFree(arena);
   if (solver_ws) delete (nb::CgWorkspace *)solver_ws;
-  if (hsmg) hsmg_free(this);
+  hsmg_free(this);
 }
 
 extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
@@ -433,6 +433,7 @@ extern "C" nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1
   p->ifh2 = ifh2 != 0;
   p->invalidate_solver_cache();
   NB_TRY(p->update_jacobi(nullptr));
+  NB_TRY(nb::hsmg_refresh_coefficients(p));
   NB_TRY(cudaDeviceSynchronize());
   return NB_OK;
 }
@@ -454,7 +455,7 @@ cudaError_t nb_problem::ax_raw(double *w, const double *u, cudaStream_t s,
 cudaError_t nb_problem::ax(double *w, const double *u, cudaStream_t s) const {
   cudaError_t e = ax_raw(w, u, s, nullptr);
   if (e != cudaSuccess || !ifh2) return e;
-  addcol4_kernel<<<stream_grid(n, 256), 256, 0, s>>>(w, h2, B, u, n);
+  addcol4_kernel<<<stream_grid(n, 256), 256, 0, s>>>(w, h2, B, u, n, nullptr);
   return cudaGetLastError();
 }
 

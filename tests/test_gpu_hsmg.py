@@ -102,3 +102,91 @@ def test_hsmg_rejects_bad_lx(nb):
     z = P.zeros()
     with pytest.raises(nb.NekoB200Error):
         nb.Hsmg().solve(z, P.zeros(), P)
+
+
+@pytest.mark.parametrize("nel,lx,per,amp,hi", [CASES[0], CASES[2], CASES[3]])
+def test_hsmg_mixed_apply_close_to_fp64(nb, oracle, nel, lx, per, amp, hi):
+    """FP32 smoothing levels: one application within FP32 accuracy of the
+    FP64 oracle (1e-5 relative, max-norm)."""
+    P, O = _pair(nb, oracle, nel, lx, per, amp, hi)
+    H = oracle.OracleHsmg(O)
+    rng = np.random.default_rng(11)
+    r = O.bc_apply(O.gs_add(O.f64("B") * rng.standard_normal(P.n)))
+    if all(per):
+        r -= r.sum() / r.size
+        r = O.gs_add(r * O.f64("mult"))
+    ref = H.apply(r)
+    z = P.zeros()
+    nb.Hsmg(mixed=True).solve(z, _cuda(r), P)
+    torch.cuda.synchronize()
+    err = np.abs(_np(z) - ref).max() / np.abs(ref).max()
+    assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("nel,lx,per,amp,hi", [CASES[0], CASES[2], CASES[3]])
+def test_mixed_fcg_reaches_fp64_solution(nb, oracle, nel, lx, per, amp, hi):
+    """Mixed path (FP32 smoother, FP64 FCG + inner products + coarse solve,
+    true residual every 50 iterations) reaches the same 1e-8 relative
+    residual; its error against the FP64 oracle solution is stated."""
+    from neko_b200 import workloads
+    P, O = _pair(nb, oracle, nel, lx, per, amp, hi)
+    H = oracle.OracleHsmg(O)
+    x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
+    b = O.bc_apply(O.gs_add(workloads.config2_rhs_local(x, y, z, B, 5)))
+    mult = O.f64("mult")
+    r0 = np.sqrt(np.sum(b * mult * b) / O.volume)
+    xo, it_o, _, _ = H.cg(b, 200, 1e-8 * r0, flexible=True)
+    xd = P.zeros()
+    mon = nb.FCG(max_iter=200, abs_tol=1e-8 * r0, M=nb.Hsmg(mixed=True)).solve(
+        nb.AxHelm(), xd, _cuda(b), P.n, P)
+    assert mon.converged and mon.res_final < 1e-8 * r0
+    assert mon.iter <= it_o + 3, (mon.iter, it_o)
+    xdn = _np(xd)
+    if all(per):
+        xdn, xo = xdn - xdn.mean(), xo - xo.mean()
+    err = np.linalg.norm(xdn - xo) / np.linalg.norm(xo)
+    assert err < 1e-6, err
+
+
+def test_true_residual_recompute_long_solve(nb):
+    """More than 50 iterations in mixed mode: the scheduled true-residual
+    replacement keeps the residual finite and small."""
+    P = nb.Problem((6, 6, 6), 8)
+    rng = np.random.default_rng(2)
+    f = P.zeros()
+    f.copy_(torch.as_tensor(rng.standard_normal(P.n), device="cuda"))
+    P.gs.op(f)
+    P.bclst.apply(f)
+    r0 = float(torch.sqrt((f * P.field("mult") * f).sum() / P.volume))
+    x = P.zeros()
+    mon = nb.FCG(max_iter=60, abs_tol=1e-30 * r0, M=nb.Hsmg(mixed=True)).solve(
+        nb.AxHelm(), x, f, P.n, P)
+    # 60 iterations cross the replacement at iteration 50; the residual must
+    # stay finite and far below the starting one.
+    assert mon.iter == 60 and not mon.converged
+    assert np.isfinite(mon.res_final) and mon.res_final < 1e-9 * r0
+
+
+def test_hsmg_follows_new_coefficients(nb):
+    """set_coefficients after the preconditioner was built hands the new h1
+    to the coarse level (hsmg_set_h): the result equals a preconditioner
+    built after the change."""
+    rng = np.random.default_rng(5)
+    r = None
+    out = []
+    for late in (True, False):
+        P = nb.Problem((4, 3, 3), 6)
+        if r is None:
+            r = P.zeros()
+            r.copy_(torch.as_tensor(rng.standard_normal(P.n), device="cuda"))
+            P.gs.op(r)
+            P.bclst.apply(r)
+        h1 = 1.5 + P.field("x") * P.field("y")
+        z = P.zeros()
+        if late:
+            nb.Hsmg().solve(z, r, P)  # built with h1 = 1
+        P.set_coefficients(h1)
+        nb.Hsmg().solve(z, r, P)
+        torch.cuda.synchronize()
+        out.append(_np(z))
+    assert np.array_equal(out[0], out[1])
