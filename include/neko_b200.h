@@ -190,10 +190,18 @@ typedef struct {
   int launches;  /* kernels this solve launched on the device */
 } nb_solve_result;
 
+/* Builds (or rebuilds, when the settings changed) the problem's hsmg
+ * preconditioner: levels lx -> 4 -> 2, Schwarz/FDM smoothers, coarse
+ * Jacobi-CG of coarse_iter iterations to abs tol coarse_tol (<= 0: the
+ * reference defaults 10 and 1e-9).  mixed = 1 builds the FP32-smoother
+ * variant, kept beside the FP64 one.  Replaces hsmg_init /
+ * hsmg_init_from_components (src/krylov/pc_hsmg.f90:145-365). */
+nb_status nb_hsmg_init(nb_problem *p, int mixed, int coarse_iter, double coarse_tol);
+
 /* z = M r for preconditioner pc (NB_PC_HSMG, or NB_PC_HSMG_MIXED for the
- * FP32-smoother variant), r masked; builds the
- * preconditioner on first use.  The hsmg_solve of the reference
- * (src/krylov/pc_hsmg.f90:481-627), exposed for checking and reuse. */
+ * FP32-smoother variant), r masked; uses the settings of the last
+ * nb_hsmg_init of that variant (the defaults when there was none).  The
+ * hsmg_solve of the reference (src/krylov/pc_hsmg.f90:481-627). */
 nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r, void *stream);
 
 /* Solves A x = f (f already assembled and masked) from x0 = 0 with

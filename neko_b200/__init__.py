@@ -184,7 +184,14 @@ class Hsmg:
     def __init__(self, coarse_iter=10, coarse_tol=1e-9, mixed=False):
         self.coarse_iter, self.coarse_tol, self.mixed = coarse_iter, coarse_tol, mixed
 
+    def init(self, coef):
+        """hsmg_init: build the levels for this problem (cached until the
+        settings change)."""
+        check(load().nb_hsmg_init(coef.handle, int(self.mixed), int(self.coarse_iter),
+                                  float(self.coarse_tol)))
+
     def solve(self, z, r, coef, n=None, stream=None):
+        self.init(coef)
         kind = _lib.NB_PC_HSMG_MIXED if self.mixed else NB_PC_HSMG
         check(load().nb_pc_apply(coef.handle, kind, _ptr(z), _ptr(r), _stream_handle(stream)))
 

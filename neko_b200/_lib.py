@@ -81,6 +81,7 @@ SIGNATURES = {
     "nb_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult), _P]),
     "nb_glsc3_noalloc": (_I, [_P, _P, _P, _I, _DP, _P]),
     "nb_pc_apply": (_I, [_P, _I, _P, _P, _P]),
+    "nb_hsmg_init": (_I, [_P, _I, _I, ctypes.c_double]),
 }
 
 _lib = None

@@ -421,6 +421,8 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
   }
   if (take_device_error())
     return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (bulk copy never completed)");
+  if (pc && pc->take_error())
+    return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (coarse-level grid barrier)");
   if (hs->nan) return ws_fail(NB_ERR_NAN, "residual became NaN or Inf");
   return NB_OK;
 }

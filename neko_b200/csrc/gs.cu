@@ -17,6 +17,7 @@
 
 #include "nb_kernels.h"
 #include "nb_gs.h"
+#include "nb_gs_dev.cuh"
 
 namespace nb {
 
@@ -77,50 +78,21 @@ __global__ void scatter_ref_kernel(const double *__restrict__ v, int m,
 // Fused in-place gs add (+ mask) over the re-laid-out maps.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void gs_add_fused_kernel(T *__restrict__ u, const int *__restrict__ seg_ptr,
-                                    const int *__restrict__ seg_idx, int nseg,
-                                    const int2 *__restrict__ pairs, int npairs,
-                                    const int *__restrict__ extra_mask, int nextra,
-                                    const unsigned char *__restrict__ seg_masked,
-                                    const unsigned char *__restrict__ pair_masked,
+__global__ void gs_add_fused_kernel(T *__restrict__ u, const GsDevice g, bool with_mask,
                                     const int *__restrict__ skip, const T *__restrict__ scale) {
   if (skip && *skip) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < npairs) {
-    const int2 p = __ldg(pairs + t);
-    T s = u[p.x] + u[p.y];
-    if (pair_masked && pair_masked[t]) s = T(0);
-    u[p.x] = scale ? s * scale[p.x] : s;
-    u[p.y] = scale ? s * scale[p.y] : s;
-    return;
-  }
-  int q = t - npairs;
-  if (q < nseg) {
-    const int a = __ldg(seg_ptr + q), b = __ldg(seg_ptr + q + 1);
-    T s = u[__ldg(seg_idx + a)];
-    for (int k = a + 1; k < b; k++) s = s + u[__ldg(seg_idx + k)];
-    if (seg_masked && seg_masked[q]) s = T(0);
-    for (int k = a; k < b; k++) {
-      const int idx = __ldg(seg_idx + k);
-      u[idx] = scale ? s * scale[idx] : s;
-    }
-    return;
-  }
-  q -= nseg;
-  if (q < nextra) u[__ldg(extra_mask + q)] = T(0);
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t < gs_items(g, with_mask)) gs_add_item<T>(u, g, (int)t, with_mask, scale);
 }
 
 template <typename T>
 cudaError_t gs_add_fused(const GsDevice &g, T *u, bool with_mask, cudaStream_t s,
                          const int *skip, const T *scale) {
-  const long total = (long)g.npairs + g.nseg + (with_mask ? g.nextra : 0);
+  const long total = gs_items(g, with_mask);
   if (total == 0) return cudaSuccess;
   const int threads = 256;
   const int blocks = (int)((total + threads - 1) / threads);
-  gs_add_fused_kernel<T><<<blocks, threads, 0, s>>>(
-      u, g.seg_ptr, g.seg_idx, g.nseg, g.pairs, g.npairs, g.extra_mask,
-      with_mask ? g.nextra : 0, with_mask ? g.seg_masked : nullptr,
-      with_mask ? g.pair_masked : nullptr, skip, scale);
+  gs_add_fused_kernel<T><<<blocks, threads, 0, s>>>(u, g, with_mask, skip, scale);
   return cudaGetLastError();
 }
 template cudaError_t gs_add_fused<double>(const GsDevice &, double *, bool, cudaStream_t,

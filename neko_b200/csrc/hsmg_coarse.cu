@@ -1,0 +1,345 @@
+// hsmg_coarse.cu -- the coarse end of hsmg in one persistent launch.
+//
+// The reference runs the coarse level of pc_hsmg (src/krylov/pc_hsmg.f90:
+// 540-560) as separate steps: restrict the middle-level residual (times
+// mult) to lx = 2, gather-scatter and mask it, run `niter` Jacobi-CG
+// iterations (cg.f90, each with its own vector kernels, Ax, gs and three
+// reductions), then prolong the correction back to the middle level.  On the
+// coarse grid (8 points per element) every one of those steps is a few
+// microseconds of work, so launch latency dominates.  Here they are phases
+// of one cooperative launch separated by grid barriers:
+//
+//   restrict -> | gs + mask (f) -> | init x, r, z = d r, (r,r), (r,z) -> |
+//   per iteration: p = z + beta p, w = A p (element-local), (p, w) -> |
+//                  gs + mask (w) -> | x += alpha p, r -= alpha w,
+//                  z = d r, (r, r), (r, z) -> |  ... -> prolong
+//
+// The arithmetic is that of cg_init / cg_precond_dot / cg_update_p /
+// ax_helm / gs / cg_update_xr, with one change of form: (p, mult gs(w)) is
+// formed as the sum over local points of p * w_local before the gather-
+// scatter.  With p continuous and zero on masked points the two are the
+// same sum (each global point's weights 1/k over its k copies add to one).
+//
+// Reductions are all-reduces: each block writes its partial, passes a grid
+// barrier and adds all partials in block order, so every block holds the
+// same total and takes the same branch.  Barriers are bounded: a block that
+// polls too long sets the error word and returns; the others then time out
+// at the same barrier and return too.
+#include <cmath>
+
+#include "nb_gs_dev.cuh"
+#include "nb_precond.h"
+#include "nb_reduce.cuh"
+
+namespace nb {
+
+constexpr int kCoarseThreads = 512;
+constexpr unsigned kBarrierPolls = 1u << 22;
+
+// Sense-counting grid barrier: bar[0] arrivals, bar[1] generation.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned polls = 0;
+      while (*gen == g) {
+        if (++polls > kBarrierPolls || *(volatile int *)err) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (!ok) atomicExch(err, 1);
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// Two sums over the grid, identical in every block.  buf holds 2 * gridDim
+// doubles; consecutive calls must alternate buffers.
+__device__ __forceinline__ bool grid_allsum2(double v0, double v1, double *buf, unsigned *bar,
+                                             int *err, double &t0, double &t1) {
+  __shared__ double sh[kCoarseThreads / 32];
+  __shared__ double res[2];
+  const double b0 = block_sum<kCoarseThreads>(v0, sh);
+  const double b1 = block_sum<kCoarseThreads>(v1, sh);
+  if (threadIdx.x == 0) {
+    buf[2 * blockIdx.x] = b0;
+    buf[2 * blockIdx.x + 1] = b1;
+  }
+  if (!grid_barrier(bar, err)) return false;
+  double s0 = 0.0, s1 = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += kCoarseThreads) {
+    s0 += __ldcg(buf + 2 * b);
+    s1 += __ldcg(buf + 2 * b + 1);
+  }
+  s0 = block_sum<kCoarseThreads>(s0, sh);
+  s1 = block_sum<kCoarseThreads>(s1, sh);
+  if (threadIdx.x == 0) {
+    res[0] = s0;
+    res[1] = s1;
+  }
+  __syncthreads();
+  t0 = res[0];
+  t1 = res[1];
+  __syncthreads();
+  return true;
+}
+
+// w = A p on one lx = 2 element held by 8 consecutive lanes (lane & 7 is the
+// point (i, j, k) = (bit0, bit1, bit2)); the arithmetic of ax_helm_kernel.
+__device__ __forceinline__ double ax_lx2(double p, int lane, const double *D, const double *Dt,
+                                         double H, double G11, double G22, double G33, double G12,
+                                         double G13, double G23) {
+  const unsigned full = 0xffffffffu;
+  const int b = lane & ~7, q = lane & 7, i = q & 1, j = (q >> 1) & 1, k = q >> 2;
+  const double ux0 = __shfl_sync(full, p, b + 0 + 2 * j + 4 * k);
+  const double ux1 = __shfl_sync(full, p, b + 1 + 2 * j + 4 * k);
+  const double uy0 = __shfl_sync(full, p, b + i + 0 + 4 * k);
+  const double uy1 = __shfl_sync(full, p, b + i + 2 + 4 * k);
+  const double uz0 = __shfl_sync(full, p, b + i + 2 * j + 0);
+  const double uz1 = __shfl_sync(full, p, b + i + 2 * j + 4);
+  double ur = 0, us = 0, ut = 0;
+  ur += D[i] * ux0;
+  ur += D[i + 2] * ux1;
+  us += D[j] * uy0;
+  us += D[j + 2] * uy1;
+  ut += D[k] * uz0;
+  ut += D[k + 2] * uz1;
+  const double a = H * (G11 * ur + G12 * us + G13 * ut);
+  const double c = H * (G12 * ur + G22 * us + G23 * ut);
+  const double d = H * (G13 * ur + G23 * us + G33 * ut);
+  const double a0 = __shfl_sync(full, a, b + 0 + 2 * j + 4 * k);
+  const double a1 = __shfl_sync(full, a, b + 1 + 2 * j + 4 * k);
+  const double c0 = __shfl_sync(full, c, b + i + 0 + 4 * k);
+  const double c1 = __shfl_sync(full, c, b + i + 2 + 4 * k);
+  const double d0 = __shfl_sync(full, d, b + i + 2 * j + 0);
+  const double d1 = __shfl_sync(full, d, b + i + 2 * j + 4);
+  double acc = 0, acc2 = 0, acc3 = 0;
+  acc += Dt[i] * a0;
+  acc += Dt[i + 2] * a1;
+  acc2 += Dt[j] * c0;
+  acc2 += Dt[j + 2] * c1;
+  acc3 += Dt[k] * d0;
+  acc3 += Dt[k + 2] * d1;
+  return acc + acc2 + acc3;
+}
+
+template <typename T, int LM>
+__global__ void __launch_bounds__(kCoarseThreads)
+    hsmg_coarse_kernel(const CoarseArgs<T> a) {
+  if (a.skip && *a.skip) return;
+  constexpr int M3 = LM * LM * LM;
+  const long nc = a.nelv * 8, nm = a.nelv * M3;
+  const long stride = (long)gridDim.x * kCoarseThreads;
+  const long t0 = (long)blockIdx.x * kCoarseThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  __shared__ double sD[4], sDt[4];
+  __shared__ T sJ[LM * 2];
+  if (threadIdx.x < 4) {
+    sD[threadIdx.x] = a.D[threadIdx.x];
+    sDt[threadIdx.x] = a.Dt[threadIdx.x];
+  }
+  if (threadIdx.x < LM * 2) sJ[threadIdx.x] = a.J[threadIdx.x];  // J(m, c) at m + LM*c
+  __syncthreads();
+  int buf = 0;
+  auto allsum2 = [&](double v0, double v1, double &s0, double &s1) {
+    const bool ok = grid_allsum2(v0, v1, a.part + (size_t)buf * 2 * gridDim.x, a.bar, a.err,
+                                 s0, s1);
+    buf ^= 1;
+    return ok;
+  };
+
+  // restrict: f(o,p,r) = sum_k J(k,r) sum_j J(j,p) sum_i J(i,o) (w mult)(i,j,k),
+  // in T and in the order of tensor3_kernel (x, then y, then z).
+  for (long q = t0; q < nc; q += stride) {
+    const long e = q >> 3;
+    const int o = q & 1, pp = (q >> 1) & 1, rr = (q >> 2) & 1;
+    const T *in = a.w_mid + e * M3;
+    const T *sc = a.mult_m + e * M3;
+    T acc_z = 0;
+#pragma unroll
+    for (int k = 0; k < LM; k++) {
+      T acc_y = 0;
+#pragma unroll
+      for (int j = 0; j < LM; j++) {
+        T acc_x = 0;
+#pragma unroll
+        for (int i = 0; i < LM; i++) {
+          const int m = i + LM * (j + LM * k);
+          acc_x += sJ[i + LM * o] * (T)(__ldg(in + m) * __ldg(sc + m));
+        }
+        acc_y += sJ[j + LM * pp] * acc_x;
+      }
+      acc_z += sJ[k + LM * rr] * acc_y;
+    }
+    a.f[q] = (double)acc_z;
+  }
+  if (!grid_barrier(a.bar, a.err)) return;
+  const long nitems = gs_items(a.gs, true);
+  for (long t = t0; t < nitems; t += stride) gs_add_item<double>(a.f, a.gs, (int)t, true, nullptr);
+  if (!grid_barrier(a.bar, a.err)) return;
+
+  // x = 0, p = 0, r = f, z = d r; (r, mult r), (r, mult z)
+  double s_rr = 0.0, s_rz = 0.0;
+  for (long q = t0; q < nc; q += stride) {
+    const double ri = a.f[q], m = __ldg(a.mult + q);
+    a.x[q] = 0.0;
+    a.p[q] = 0.0;
+    a.r[q] = ri;
+    const double zi = ri * __ldg(a.dinv + q);
+    a.z[q] = zi;
+    s_rr += ri * m * ri;
+    s_rz += ri * m * zi;
+  }
+  double rtr, rtz;
+  if (!allsum2(s_rr, s_rz, rtr, rtz)) return;
+  const double norm_fac = a.st->norm_fac, tol = a.st->abs_tol;
+  const int max_iter = a.st->max_iter;
+  double rn = sqrt(rtr) * norm_fac;
+  const double res_start = rn;
+  bool done = fabs(rn) < 2.220446049250313e-16;
+  int iter = 0, nan = 0;
+  double rtz_old = 1.0;
+
+  while (!done) {
+    const double beta = iter == 0 ? 0.0 : rtz / rtz_old;
+    // p = z + beta p; w = A p (local); (p, w_local)
+    double s_pw = 0.0;
+    for (long qb = t0 - lane; qb < nc; qb += stride) {
+      const long q = qb + lane;
+      const bool act = q < nc;
+      double pq = 0, H = 0, G11 = 0, G22 = 0, G33 = 0, G12 = 0, G13 = 0, G23 = 0;
+      if (act) {
+        pq = a.z[q] + beta * a.p[q];
+        a.p[q] = pq;
+        H = __ldg(a.h1 + q);
+        G11 = __ldg(a.g11 + q), G22 = __ldg(a.g22 + q), G33 = __ldg(a.g33 + q);
+        G12 = __ldg(a.g12 + q), G13 = __ldg(a.g13 + q), G23 = __ldg(a.g23 + q);
+      }
+      const double wq = ax_lx2(pq, lane, sD, sDt, H, G11, G22, G33, G12, G13, G23);
+      if (act) {
+        a.w[q] = wq;
+        s_pw += pq * wq;
+      }
+    }
+    double pap, unused;
+    if (!allsum2(s_pw, 0.0, pap, unused)) return;
+    const double alpha = rtz / pap;
+    for (long t = t0; t < nitems; t += stride)
+      gs_add_item<double>(a.w, a.gs, (int)t, true, nullptr);
+    if (!grid_barrier(a.bar, a.err)) return;
+    // x += alpha p; r -= alpha w; z = d r; (r, mult r), (r, mult z)
+    s_rr = 0.0;
+    s_rz = 0.0;
+    const double malpha = -alpha;
+    for (long q = t0; q < nc; q += stride) {
+      a.x[q] = a.x[q] + alpha * a.p[q];
+      const double ri = a.r[q] + malpha * a.w[q], m = __ldg(a.mult + q);
+      a.r[q] = ri;
+      const double zi = ri * __ldg(a.dinv + q);
+      a.z[q] = zi;
+      s_rr += ri * m * ri;
+      s_rz += ri * m * zi;
+    }
+    double rtz_new;
+    if (!allsum2(s_rr, s_rz, rtr, rtz_new)) return;
+    rtz_old = rtz;
+    rtz = rtz_new;
+    rn = sqrt(rtr) * norm_fac;
+    iter += 1;
+    if (!(rn == rn) || isinf(rn)) {
+      nan = 1;
+      done = true;
+    }
+    if (rn < tol || iter >= max_iter) done = true;
+  }
+
+  // prolong: e_mid(o,p,r) += sum_k J(r,k) sum_j J(p,j) sum_i J(o,i) x(i,j,k)
+  for (long q = t0; q < nm; q += stride) {
+    const long e = q / M3;
+    const int m = (int)(q - e * M3), o = m % LM, pp = (m / LM) % LM, rr = m / (LM * LM);
+    const double *in = a.x + e * 8;
+    T acc_z = 0;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      T acc_y = 0;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        T acc_x = 0;
+#pragma unroll
+        for (int i = 0; i < 2; i++) acc_x += sJ[o + LM * i] * (T)in[i + 2 * j + 4 * k];
+        acc_y += sJ[pp + LM * j] * acc_x;
+      }
+      acc_z += sJ[rr + LM * k] * acc_y;
+    }
+    a.e_mid[q] = a.e_mid[q] + acc_z;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.st->iter = iter;
+    a.st->rnorm = rn;
+    a.st->res_start = res_start;
+    a.st->nan = nan;
+  }
+}
+
+template <typename T, int LM>
+static cudaError_t launch_coarse(const CoarseArgs<T> &a, int max_blocks, cudaStream_t s) {
+  auto kern = hsmg_coarse_kernel<T, LM>;
+  static int cap[64] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int &c = cap[dev & 63];
+  if (c == 0) {
+    int per_sm = 0, sms = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCoarseThreads, 0)) !=
+            cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+      return e;
+    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+    c = sms;  // one block per SM: co-resident, few barrier arrivals
+  }
+  const long work = a.nelv * LM * LM * LM;
+  long g = (work + kCoarseThreads - 1) / kCoarseThreads;
+  if (g > c) g = c;
+  if (g > max_blocks) g = max_blocks;
+  if (g < 1) g = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)g);
+  cfg.blockDim = dim3(kCoarseThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+template <typename T>
+cudaError_t hsmg_coarse_solve(const CoarseArgs<T> &a, int lm, int max_blocks, cudaStream_t s) {
+  switch (lm) {
+    case 3: return launch_coarse<T, 3>(a, max_blocks, s);
+    case 4: return launch_coarse<T, 4>(a, max_blocks, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+template cudaError_t hsmg_coarse_solve<double>(const CoarseArgs<double> &, int, int,
+                                               cudaStream_t);
+template cudaError_t hsmg_coarse_solve<float>(const CoarseArgs<float> &, int, int, cudaStream_t);
+
+}  // namespace nb

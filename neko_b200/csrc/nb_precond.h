@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "nb_gs.h"
 #include "nb_problem.h"
 
 namespace nb {
@@ -24,6 +25,8 @@ struct Precond {
   virtual cudaError_t apply(double *z, const double *r, const int *skip, cudaStream_t s) = 0;
   // kernels one apply launches
   virtual int launches() const = 0;
+  // nonzero when a bounded device wait of an apply expired; clears it
+  virtual int take_error() { return 0; }
 };
 
 struct CgWorkspace {
@@ -60,6 +63,31 @@ __global__ void cg_update_xr_kernel(double *x, double *r, const double *p, const
 
 nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
                    Precond *pc, nb_solve_result *res, cudaStream_t s);
+
+// Operands of the persistent coarse-level launch of hsmg (hsmg_coarse.cu).
+// T is the precision of the middle level; the coarse level is FP64.
+template <typename T>
+struct CoarseArgs {
+  long nelv = 0;
+  const T *w_mid = nullptr, *mult_m = nullptr;  // middle-level residual and weights
+  const T *J = nullptr;                         // lm x 2 interpolation, column-major
+  T *e_mid = nullptr;                           // += prolonged correction
+  double *f = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *w = nullptr;
+  const double *h1 = nullptr, *g11 = nullptr, *g22 = nullptr, *g33 = nullptr, *g12 = nullptr,
+               *g13 = nullptr, *g23 = nullptr, *D = nullptr, *Dt = nullptr;
+  const double *dinv = nullptr, *mult = nullptr;  // inverse Jacobi diagonal, weights
+  GsDevice gs;
+  CgState *st = nullptr;    // norm_fac, abs_tol, max_iter in; iter, rnorm out
+  double *part = nullptr;   // 2 x 2 x (grid) doubles
+  unsigned *bar = nullptr;  // barrier arrivals and generation, zero at rest
+  int *err = nullptr;       // set to 1 when a barrier wait expired
+  const int *skip = nullptr;
+};
+constexpr int kCoarseMaxBlocks = 1024;
+
+// Restrict, solve and prolong in one cooperative launch (lm = 3 or 4).
+template <typename T>
+cudaError_t hsmg_coarse_solve(const CoarseArgs<T> &a, int lm, int max_blocks, cudaStream_t s);
 
 // hsmg preconditioner of problem P, built on first use (pc_hsmg.cu).
 nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out);

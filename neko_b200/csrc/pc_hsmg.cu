@@ -148,6 +148,184 @@ __global__ void __launch_bounds__(NL *NL *NE)
   }
 }
 
+// The same FDM for even NL, register-blocked: each thread carries two lines
+// (t and t + NL*NL/2) through every pass, so each broadcast load of two
+// matrix entries feeds four FMAs instead of one.  Passes run in place on one
+// padded buffer per element (a, b, c) at a + (NL+1)(b + NL c): a thread
+// reads its lines into registers, the block syncs, and the outputs are
+// written rotated (out(m,n,i) at m + (NL+1)(n + NL i)); the odd row pitch
+// keeps the line reads free of bank conflicts.  Every sum runs over l in
+// ascending order from zero, as in fdm_kernel, so the two kernels agree
+// bit for bit.
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+  using type = double2;
+};
+template <>
+struct Pair<float> {
+  using type = float2;
+};
+
+template <typename T, int NL>
+struct Fdm2Cfg {
+  static constexpr int N2 = NL * NL, NLP = NL + 1, TPE = N2 / 2;
+  static constexpr int NE = TPE >= 128 ? 2 : (TPE >= 64 ? 4 : (TPE >= 32 ? 8 : 16));
+  static constexpr int BUF = NLP * N2;
+  static constexpr int STR = ((BUF + 3 * N2 + 3 * NL + 2) + 3) / 4 * 4;  // per element
+  static constexpr int THREADS = NE * TPE;
+  static constexpr size_t SMEM = (size_t)NE * STR * sizeof(T);
+};
+
+// out_i = sum_l M(l, i) x_l for two lines; M(l, i) at l + NL*i.
+template <typename T, int NL>
+__device__ __forceinline__ void fdm_fwd2(const T *__restrict__ M, const T (&x0)[NL],
+                                         const T (&x1)[NL], T (&o0)[NL], T (&o1)[NL]) {
+  using V = typename Pair<T>::type;
+#pragma unroll
+  for (int i = 0; i < NL; i++) {
+    T s0 = 0, s1 = 0;
+#pragma unroll
+    for (int l = 0; l < NL; l += 2) {
+      const V m = *reinterpret_cast<const V *>(M + l + NL * i);
+      s0 += m.x * x0[l];
+      s1 += m.x * x1[l];
+      s0 += m.y * x0[l + 1];
+      s1 += m.y * x1[l + 1];
+    }
+    o0[i] = s0;
+    o1[i] = s1;
+  }
+}
+
+// out_i = sum_l M(i, l) x_l for two lines; M(i, l) at i + NL*l.
+template <typename T, int NL>
+__device__ __forceinline__ void fdm_bwd2(const T *__restrict__ M, const T (&x0)[NL],
+                                         const T (&x1)[NL], T (&o0)[NL], T (&o1)[NL]) {
+  using V = typename Pair<T>::type;
+#pragma unroll
+  for (int i = 0; i < NL; i++) o0[i] = o1[i] = T(0);
+#pragma unroll
+  for (int l = 0; l < NL; l++) {
+#pragma unroll
+    for (int i = 0; i < NL; i += 2) {
+      const V m = *reinterpret_cast<const V *>(M + i + NL * l);
+      o0[i] += m.x * x0[l];
+      o0[i + 1] += m.y * x0[l];
+      o1[i] += m.x * x1[l];
+      o1[i + 1] += m.y * x1[l];
+    }
+  }
+}
+
+template <typename TIN, typename T, int NL>
+__global__ void __launch_bounds__(Fdm2Cfg<T, NL>::THREADS)
+    fdm2_kernel(const TIN *__restrict__ r, const int *__restrict__ fn, const T *__restrict__ S,
+                const T *__restrict__ lam, const T *__restrict__ eps, T *__restrict__ out,
+                int nelv, const int *__restrict__ skip) {
+  if (skip && *skip) return;
+  using C = Fdm2Cfg<T, NL>;
+  constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = C::N2, N3 = N2 * NL,
+                NLP = C::NLP, TPE = C::TPE;
+  static_assert(NL % 2 == 0, "fdm2_kernel needs an even line length");
+  extern __shared__ __align__(16) unsigned char fdm2_smem[];
+  const int el = threadIdx.x / TPE, t = threadIdx.x - el * TPE;
+  T *B = reinterpret_cast<T *>(fdm2_smem) + el * C::STR;
+  T *sS = B + C::BUF;  // S_x, S_y, S_z: S(l,i) at l + NL*i
+  T *sL = sS + 3 * N2; // spectra + eps
+  const long e = (long)blockIdx.x * C::NE + el;
+  const bool active = e < nelv;
+  if (active) {
+    const int *f = fn + e * 6;
+    for (int q = t; q < N3; q += TPE) {
+      const int a = q % NL, b = (q / NL) % NL, c = q / N2;
+      const int ea = (a == 0) + (a == NL - 1), eb = (b == 0) + (b == NL - 1),
+                ec = (c == 0) + (c == NL - 1);
+      T v = T(0);
+      if (ea + eb + ec == 0) {
+        v = (T)r[e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1)];
+      } else if (ea + eb + ec == 1) {
+        int nb = 0, si = a - 1, sj = b - 1, sk = c - 1;
+        if (a == 0) nb = f[0], si = LX - 2;
+        if (a == NL - 1) nb = f[1], si = 1;
+        if (b == 0) nb = f[2], sj = LX - 2;
+        if (b == NL - 1) nb = f[3], sj = 1;
+        if (c == 0) nb = f[4], sk = LX - 2;
+        if (c == NL - 1) nb = f[5], sk = 1;
+        if (nb) v = (T)r[(long)(nb - 1) * L3 + si + LX * sj + L2 * sk];
+      }
+      B[a + NLP * (b + NL * c)] = v;
+    }
+    for (int q = t; q < 3 * N2; q += TPE) sS[q] = S[e * 3 * N2 + q];
+    for (int q = t; q < 3 * NL; q += TPE) sL[q] = lam[e * 3 * NL + q];
+    if (t == 0) sL[3 * NL] = eps[e];
+  }
+  __syncthreads();
+  const int L0 = t, L1 = t + TPE;
+  T x0[NL], x1[NL], o0[NL], o1[NL];
+  auto load = [&]() {
+#pragma unroll
+    for (int l = 0; l < NL; l++) {
+      x0[l] = B[NLP * L0 + l];
+      x1[l] = B[NLP * L1 + l];
+    }
+  };
+  auto store = [&]() {  // rotated: line (m, n), output i -> m + NLP*(n + NL*i)
+    const int m0 = L0 % NL, n0 = L0 / NL, m1 = L1 % NL, n1 = L1 / NL;
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      B[m0 + NLP * (n0 + NL * i)] = o0[i];
+      B[m1 + NLP * (n1 + NL * i)] = o1[i];
+    }
+  };
+#pragma unroll 1
+  for (int d = 0; d < 2; d++) {  // (a,b,c) -> (b,c,i) -> (c,i,j)
+    if (active) {
+      load();
+      fdm_fwd2<T, NL>(sS + d * N2, x0, x1, o0, o1);
+    }
+    __syncthreads();
+    if (active) store();
+    __syncthreads();
+  }
+  if (active) {  // -> (i,j,k), times D^-1
+    load();
+    fdm_fwd2<T, NL>(sS + 2 * N2, x0, x1, o0, o1);
+    const T ep = sL[3 * NL];
+    const T l0 = sL[L0 % NL] + sL[NL + L0 / NL], l1 = sL[L1 % NL] + sL[NL + L1 / NL];
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+      const T d0 = l0 + sL[2 * NL + k], d1 = l1 + sL[2 * NL + k];
+      o0[k] = d0 > ep ? o0[k] / d0 : T(0);
+      o1[k] = d1 > ep ? o1[k] / d1 : T(0);
+    }
+  }
+  __syncthreads();
+  if (active) store();
+  __syncthreads();
+#pragma unroll 1
+  for (int d = 0; d < 2; d++) {  // back: S_x, S_y
+    if (active) {
+      load();
+      fdm_bwd2<T, NL>(sS + d * N2, x0, x1, o0, o1);
+    }
+    __syncthreads();
+    if (active) store();
+    __syncthreads();
+  }
+  if (active) {  // S_z, store (i,j,k)
+    load();
+    fdm_bwd2<T, NL>(sS + 2 * N2, x0, x1, o0, o1);
+    T *oe = out + e * N3;
+#pragma unroll
+    for (int k = 0; k < NL; k++) {
+      oe[L0 + N2 * k] = o0[k];
+      oe[L1 + N2 * k] = o1[k];
+    }
+  }
+}
+
 // e(i,j,k) = ext interior + neighbours' ghost results on the first interior
 // layers (x, then y, then z, as the extrude passes add them), times the
 // overlap weight.
@@ -246,16 +424,28 @@ template <typename TIN, typename T, int LX>
 static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
                                    cudaStream_t s) {
   constexpr int NL = LX + 2;
-  constexpr int NE = NL * NL >= 64 ? 1 : (128 / (NL * NL));
-  const size_t smem = sizeof(T) * NE * (2 * NL * NL * NL + 6 * NL * NL + 3 * NL + 2);
-  auto kern = fdm_kernel<TIN, T, NL, NE>;
-  if (smem > 48 * 1024) {
-    cudaError_t err =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
+  if constexpr (NL % 2 == 0) {
+    using C = Fdm2Cfg<T, NL>;
+    auto kern = fdm2_kernel<TIN, T, NL>;
+    if (C::SMEM > 48 * 1024) {
+      cudaError_t err =
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+      if (err != cudaSuccess) return err;
+    }
+    kern<<<(unsigned)((L.nelv + C::NE - 1) / C::NE), C::THREADS, C::SMEM, s>>>(
+        r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
+  } else {
+    constexpr int NE = NL * NL >= 64 ? 1 : (128 / (NL * NL));
+    const size_t smem = sizeof(T) * NE * (2 * NL * NL * NL + 6 * NL * NL + 3 * NL + 2);
+    auto kern = fdm_kernel<TIN, T, NL, NE>;
+    if (smem > 48 * 1024) {
+      cudaError_t err =
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (err != cudaSuccess) return err;
+    }
+    kern<<<(unsigned)((L.nelv + NE - 1) / NE), dim3(NL * NL, NE), smem, s>>>(
+        r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
   }
-  kern<<<(unsigned)((L.nelv + NE - 1) / NE), dim3(NL * NL, NE), smem, s>>>(
-      r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
   const long n = L.nelv * LX * LX * LX;
   schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.ext, L.fn, L.wt, e,
                                                                         L.nelv, skip);
@@ -321,7 +511,24 @@ struct HsmgState : public Precond {
   int niter = 10;
   double tol = 1e-9;
   bool mixed = false;
+  // The fine-level Schwarz runs on `side` while the middle and coarse levels
+  // run on the caller's stream (the two branches of the additive scheme
+  // share only the input r).
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaError_t ensure_side() {
+    if (side) return cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming)) != cudaSuccess)
+      return e;
+    return cudaSuccess;
+  }
   ~HsmgState() override {
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (arena) cudaFree(arena);
     if (mid) nb_problem_destroy(mid);
     if (crs) nb_problem_destroy(crs);
@@ -338,21 +545,34 @@ struct HsmgImpl : public HsmgState {
   double *r_crs = nullptr, *e_crs = nullptr;
   double *rc = nullptr, *zc = nullptr, *pc = nullptr, *wc = nullptr;
   CgState *stc = nullptr;
-  double *partials = nullptr;
-  unsigned *counter = nullptr;
+  CoarseArgs<T> ca;
 
   int launches() const override {
-    // 2 Schwarz x (fdm, post, gs) + restrict x2 + gs x2 + coarse (init +
-    // niter x 6) + prolong x2 + final gs (+ convert)
-    return 6 + 2 + 2 + 1 + niter * 6 + 2 + 1 + (sizeof(T) == 4 ? 1 : 0);
+    // 2 Schwarz x (fdm, post, gs) + restrict + gs + coarse (one launch) +
+    // prolong + final gs (+ convert)
+    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0);
+  }
+
+  int take_error() override {
+    int v = 0;
+    if (cudaMemcpy(&v, ca.err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (v) {  // leave the barrier words at rest for the next launch
+      cudaMemset(ca.err, 0, sizeof(int));
+      cudaMemset(ca.bar, 0, 2 * sizeof(unsigned));
+    }
+    return v;
   }
 
   cudaError_t apply(double *z, const double *r, const int *skip, cudaStream_t s) override {
     cudaError_t e;
     const long nelv = fine->nelv;
     T *zs = sizeof(T) == 8 ? reinterpret_cast<T *>(z) : zf;
-    // fine Schwarz: zs = S_f r
-    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, s)) != cudaSuccess) return e;
+    // fine Schwarz on the side stream: zs = S_f r
+    if ((e = ensure_side()) != cudaSuccess || (e = cudaEventRecord(ev_fork, s)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(side, ev_fork, 0)) != cudaSuccess)
+      return e;
+    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_join, side)) != cudaSuccess) return e;
     // restrict (r * mult) to the middle level, assemble, mask
     if ((e = restrict_level<double, T, T>(fine->lx, mid->lx, r, fine->mult, Jfm, w_mid, nelv,
                                           skip, s)) != cudaSuccess)
@@ -360,30 +580,12 @@ struct HsmgImpl : public HsmgState {
     if ((e = gs_add_fused<T>(mid->gsd, w_mid, true, s, skip)) != cudaSuccess) return e;
     // middle Schwarz: e_mid = S_m w
     if ((e = schwarz_apply<T, T>(sm, w_mid, e_mid, skip, s)) != cudaSuccess) return e;
-    // restrict (w * mult_mid) to the coarse level (FP64), assemble, mask
-    if ((e = restrict_level<T, double, T>(mid->lx, crs->lx, w_mid, mult_m, Jmc, r_crs, nelv,
-                                          skip, s)) != cudaSuccess)
-      return e;
-    if ((e = gs_add_fused<double>(crs->gsd, r_crs, true, s, skip)) != cudaSuccess) return e;
-    // coarse CG (Jacobi), niter iterations or abs tol, FP64
-    const long nc = crs->n;
-    const int rb = red_blocks(nc), eg = stream_grid(nc, 256);
-    cg_init_kernel<<<rb, kRedThreads, 0, s>>>(e_crs, pc, rc, r_crs, crs->mult, nc, stc, partials,
-                                              counter, skip);
-    for (int it = 0; it < niter; it++) {
-      cg_precond_dot_kernel<<<rb, kRedThreads, 0, s>>>(zc, rc, crs->jdiag, crs->mult, nc, stc,
-                                                       partials, counter);
-      cg_update_p_kernel<<<eg, 256, 0, s>>>(pc, zc, nc, stc);
-      if ((e = crs->ax_raw(wc, pc, s, &stc->done)) != cudaSuccess) return e;
-      if ((e = gs_add_fused<double>(crs->gsd, wc, true, s, &stc->done)) != cudaSuccess) return e;
-      cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(wc, pc, crs->mult, nc, stc, partials, counter);
-      cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(e_crs, rc, pc, wc, crs->mult, nc, stc,
-                                                     partials, counter);
-    }
-    // prolong: e_mid += J e_crs; zs += J e_mid; z = mult * gs(zs)
-    if ((e = prolong_add<double, T, T>(crs->lx, mid->lx, e_crs, Jmc, e_mid, nelv, skip, s)) !=
-        cudaSuccess)
-      return e;
+    // restrict (w * mult_mid) to the coarse level (FP64), assemble, mask,
+    // niter Jacobi-CG iterations (or abs tol), e_mid += J e_crs: one launch
+    ca.skip = skip;
+    if ((e = hsmg_coarse_solve<T>(ca, mid->lx, kCoarseMaxBlocks, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, ev_join, 0)) != cudaSuccess) return e;
+    // prolong: zs += J e_mid; z = mult * gs(zs)
     if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s)) !=
         cudaSuccess)
       return e;
@@ -498,7 +700,8 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
   const size_t o_wm = c.take(nm * sizeof(T)), o_em = c.take(nm * sizeof(T));
   const size_t o_rc = c.take(nc * 8), o_ec = c.take(nc * 8), o_r = c.take(nc * 8),
                o_z = c.take(nc * 8), o_p = c.take(nc * 8), o_w = c.take(nc * 8);
-  const size_t o_st = c.take(sizeof(CgState)), o_part = c.take(2 * 148 * 8 * 8 + 64);
+  const size_t o_st = c.take(sizeof(CgState)),
+               o_part = c.take(2 * 2 * kCoarseMaxBlocks * sizeof(double) + 64);
   if (cudaMalloc(&H->arena, c.off) != cudaSuccess) return hfail(NB_ERR_OOM, "hsmg: device arena");
   char *A = (char *)H->arena;
   auto Tp = [&](size_t o) { return (T *)(A + o); };
@@ -523,8 +726,18 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
   H->r_crs = Dp(o_rc), H->e_crs = Dp(o_ec), H->rc = Dp(o_r), H->zc = Dp(o_z), H->pc = Dp(o_p),
   H->wc = Dp(o_w);
   H->stc = (CgState *)(A + o_st);
-  H->partials = Dp(o_part);
-  H->counter = (unsigned *)(A + o_part + 2 * 148 * 8 * 8);
+  CoarseArgs<T> &ca = H->ca;
+  ca.nelv = nelv;
+  ca.w_mid = H->w_mid, ca.mult_m = H->mult_m, ca.J = H->Jmc, ca.e_mid = H->e_mid;
+  ca.f = H->r_crs, ca.x = H->e_crs, ca.r = H->rc, ca.z = H->zc, ca.p = H->pc, ca.w = H->wc;
+  ca.h1 = C->h1, ca.g11 = C->g11, ca.g22 = C->g22, ca.g33 = C->g33, ca.g12 = C->g12,
+  ca.g13 = C->g13, ca.g23 = C->g23, ca.D = C->D, ca.Dt = C->Dt;
+  ca.dinv = C->jdiag, ca.mult = C->mult;
+  ca.gs = C->gsd;
+  ca.st = H->stc;
+  ca.part = Dp(o_part);
+  ca.bar = (unsigned *)(A + o_part + 2 * 2 * kCoarseMaxBlocks * sizeof(double));
+  ca.err = (int *)(ca.bar + 2);
   auto upv = [&](size_t o, const std::vector<double> &v) {
     std::vector<T> t = cast_vec<T>(v);
     return t.empty() ? cudaSuccess
@@ -551,7 +764,7 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
       upv(o_Wm, hm.wt) || upi(o_Fm, hm.fn) || upv(o_Jfm, Jfm) || upv(o_Jmc, Jmc) ||
       upv(o_mm, hm_mult) || (f32 && upv(o_mf, hf_mult)) ||
       cudaMemcpy(A + o_st, &cs, sizeof(cs), cudaMemcpyHostToDevice) ||
-      cudaMemset(A + o_part, 0, 2 * 148 * 8 * 8 + 64))
+      cudaMemset(A + o_part, 0, 2 * 2 * kCoarseMaxBlocks * sizeof(double) + 64))
     return hfail(NB_ERR_CUDA, "hsmg: upload failed");
   return NB_OK;
 }
@@ -627,10 +840,29 @@ nb_status hsmg_apply_once(nb_problem *P, double *z, const double *r, cudaStream_
   if (st != NB_OK) return st;
   NB_CUDA_TRY(pc->apply(z, r, nullptr, s));
   NB_CUDA_TRY(cudaStreamSynchronize(s));
+  if (pc->take_error()) {
+    set_error("a bounded device wait expired (coarse-level grid barrier)");
+    return NB_ERR_TIMEOUT;
+  }
   return NB_OK;
 }
 
 }  // namespace nb
+
+extern "C" nb_status nb_hsmg_init(nb_problem *p, int mixed, int coarse_iter,
+                                  double coarse_tol) {
+  using namespace nb;
+  if (!p) {
+    set_error("null argument");
+    return NB_ERR_ARG;
+  }
+  nb_solve_opts o{};
+  o.mixed = mixed != 0;
+  o.coarse_iter = coarse_iter;
+  o.coarse_tol = coarse_tol;
+  Precond *pc = nullptr;
+  return hsmg_get(p, o, &pc);
+}
 
 extern "C" nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r,
                                  void *stream) {
