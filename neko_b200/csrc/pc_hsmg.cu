@@ -148,15 +148,16 @@ __global__ void __launch_bounds__(NL *NL *NE)
   }
 }
 
-// The same FDM for even NL, register-blocked: each thread carries two lines
-// (t and t + NL*NL/2) through every pass, so each broadcast load of two
-// matrix entries feeds four FMAs instead of one.  Passes run in place on one
-// padded buffer per element (a, b, c) at a + (NL+1)(b + NL c): a thread
-// reads its lines into registers, the block syncs, and the outputs are
-// written rotated (out(m,n,i) at m + (NL+1)(n + NL i)); the odd row pitch
-// keeps the line reads free of bank conflicts.  Every sum runs over l in
-// ascending order from zero, as in fdm_kernel, so the two kernels agree
-// bit for bit.
+// The same FDM for even NL, one line per thread with all NL outputs of the
+// line accumulated at once (NL independent FMA chains), each pair of matrix
+// entries fetched with one 16-byte broadcast load.  The forward passes read
+// S through a transposed copy so that both directions load consecutive
+// output pairs.  The passes alternate between two padded buffers, (a, b, c)
+// at a + (NL+1)(b + NL c); the odd row pitch keeps the line reads free of
+// bank conflicts.  The ghost-layer gather issues all of a thread's global
+// loads before its first shared store.  Every sum runs over l in ascending
+// order from zero, as in fdm_kernel; the eigenvalue scaling multiplies by
+// 1/diag as fdm_setup_fast stores it (src/math/fdm.f90:373-393).
 template <typename T>
 struct Pair;
 template <>
@@ -170,51 +171,27 @@ struct Pair<float> {
 
 template <typename T, int NL>
 struct Fdm2Cfg {
-  static constexpr int N2 = NL * NL, NLP = NL + 1, TPE = N2 / 2;
-  static constexpr int NE = TPE >= 128 ? 2 : (TPE >= 64 ? 4 : (TPE >= 32 ? 8 : 16));
+  static constexpr int N2 = NL * NL, NLP = NL + 1;
+  static constexpr int NE = N2 >= 128 ? 1 : 128 / N2;
   static constexpr int BUF = NLP * N2;
-  static constexpr int STR = ((BUF + 3 * N2 + 3 * NL + 2) + 3) / 4 * 4;  // per element
-  static constexpr int THREADS = NE * TPE;
+  static constexpr int STR = ((2 * BUF + 6 * N2 + 3 * NL + 2) + 3) / 4 * 4;  // per element
+  static constexpr int THREADS = NE * N2;
   static constexpr size_t SMEM = (size_t)NE * STR * sizeof(T);
 };
 
-// out_i = sum_l M(l, i) x_l for two lines; M(l, i) at l + NL*i.
+// o_i = sum_l M(i, l) x_l, M(i, l) at i + NL*l.
 template <typename T, int NL>
-__device__ __forceinline__ void fdm_fwd2(const T *__restrict__ M, const T (&x0)[NL],
-                                         const T (&x1)[NL], T (&o0)[NL], T (&o1)[NL]) {
+__device__ __forceinline__ void fdm_line(const T *__restrict__ M, const T (&x)[NL], T (&o)[NL]) {
   using V = typename Pair<T>::type;
 #pragma unroll
-  for (int i = 0; i < NL; i++) {
-    T s0 = 0, s1 = 0;
-#pragma unroll
-    for (int l = 0; l < NL; l += 2) {
-      const V m = *reinterpret_cast<const V *>(M + l + NL * i);
-      s0 += m.x * x0[l];
-      s1 += m.x * x1[l];
-      s0 += m.y * x0[l + 1];
-      s1 += m.y * x1[l + 1];
-    }
-    o0[i] = s0;
-    o1[i] = s1;
-  }
-}
-
-// out_i = sum_l M(i, l) x_l for two lines; M(i, l) at i + NL*l.
-template <typename T, int NL>
-__device__ __forceinline__ void fdm_bwd2(const T *__restrict__ M, const T (&x0)[NL],
-                                         const T (&x1)[NL], T (&o0)[NL], T (&o1)[NL]) {
-  using V = typename Pair<T>::type;
-#pragma unroll
-  for (int i = 0; i < NL; i++) o0[i] = o1[i] = T(0);
+  for (int i = 0; i < NL; i++) o[i] = T(0);
 #pragma unroll
   for (int l = 0; l < NL; l++) {
 #pragma unroll
     for (int i = 0; i < NL; i += 2) {
       const V m = *reinterpret_cast<const V *>(M + i + NL * l);
-      o0[i] += m.x * x0[l];
-      o0[i + 1] += m.y * x0[l];
-      o1[i] += m.x * x1[l];
-      o1[i + 1] += m.y * x1[l];
+      o[i] += m.x * x[l];
+      o[i + 1] += m.y * x[l];
     }
   }
 }
@@ -227,102 +204,90 @@ __global__ void __launch_bounds__(Fdm2Cfg<T, NL>::THREADS)
   if (skip && *skip) return;
   using C = Fdm2Cfg<T, NL>;
   constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = C::N2, N3 = N2 * NL,
-                NLP = C::NLP, TPE = C::TPE;
+                NLP = C::NLP;
   static_assert(NL % 2 == 0, "fdm2_kernel needs an even line length");
   extern __shared__ __align__(16) unsigned char fdm2_smem[];
-  const int el = threadIdx.x / TPE, t = threadIdx.x - el * TPE;
-  T *B = reinterpret_cast<T *>(fdm2_smem) + el * C::STR;
-  T *sS = B + C::BUF;  // S_x, S_y, S_z: S(l,i) at l + NL*i
-  T *sL = sS + 3 * N2; // spectra + eps
+  const int el = threadIdx.x / N2, t = threadIdx.x - el * N2;
+  T *b0 = reinterpret_cast<T *>(fdm2_smem) + el * C::STR, *b1 = b0 + C::BUF;
+  T *sS = b1 + C::BUF;  // S_x, S_y, S_z: S(l,i) at l + NL*i
+  T *sT = sS + 3 * N2;  // transposes: S(l,i) at i + NL*l
+  T *sL = sT + 3 * N2;  // spectra + eps
   const long e = (long)blockIdx.x * C::NE + el;
   const bool active = e < nelv;
   if (active) {
+    constexpr int NG = (N3 + N2 - 1) / N2;
     const int *f = fn + e * 6;
-    for (int q = t; q < N3; q += TPE) {
+    int nbr[6];
+#pragma unroll
+    for (int d = 0; d < 6; d++) nbr[d] = __ldg(f + d);
+    T v[NG];
+#pragma unroll
+    for (int g = 0; g < NG; g++) {
+      const int q = t + g * N2;
       const int a = q % NL, b = (q / NL) % NL, c = q / N2;
       const int ea = (a == 0) + (a == NL - 1), eb = (b == 0) + (b == NL - 1),
                 ec = (c == 0) + (c == NL - 1);
-      T v = T(0);
-      if (ea + eb + ec == 0) {
-        v = (T)r[e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1)];
-      } else if (ea + eb + ec == 1) {
+      long src = -1;
+      if (q < N3 && ea + eb + ec == 0) {
+        src = e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1);
+      } else if (q < N3 && ea + eb + ec == 1) {
         int nb = 0, si = a - 1, sj = b - 1, sk = c - 1;
-        if (a == 0) nb = f[0], si = LX - 2;
-        if (a == NL - 1) nb = f[1], si = 1;
-        if (b == 0) nb = f[2], sj = LX - 2;
-        if (b == NL - 1) nb = f[3], sj = 1;
-        if (c == 0) nb = f[4], sk = LX - 2;
-        if (c == NL - 1) nb = f[5], sk = 1;
-        if (nb) v = (T)r[(long)(nb - 1) * L3 + si + LX * sj + L2 * sk];
+        if (a == 0) nb = nbr[0], si = LX - 2;
+        if (a == NL - 1) nb = nbr[1], si = 1;
+        if (b == 0) nb = nbr[2], sj = LX - 2;
+        if (b == NL - 1) nb = nbr[3], sj = 1;
+        if (c == 0) nb = nbr[4], sk = LX - 2;
+        if (c == NL - 1) nb = nbr[5], sk = 1;
+        if (nb) src = (long)(nb - 1) * L3 + si + LX * sj + L2 * sk;
       }
-      B[a + NLP * (b + NL * c)] = v;
+      v[g] = src >= 0 ? (T)__ldg(r + src) : T(0);
     }
-    for (int q = t; q < 3 * N2; q += TPE) sS[q] = S[e * 3 * N2 + q];
-    for (int q = t; q < 3 * NL; q += TPE) sL[q] = lam[e * 3 * NL + q];
+#pragma unroll
+    for (int g = 0; g < NG; g++) {
+      const int q = t + g * N2;
+      if (q < N3) b0[q % NL + NLP * (q / NL)] = v[g];
+    }
+    for (int q = t; q < 3 * N2; q += N2) {
+      const T sv = __ldg(S + e * 3 * N2 + q);
+      const int d = q / N2, w = q - d * N2, l = w % NL, i = w / NL;
+      sS[q] = sv;
+      sT[d * N2 + i + NL * l] = sv;
+    }
+    for (int q = t; q < 3 * NL; q += N2) sL[q] = lam[e * 3 * NL + q];
     if (t == 0) sL[3 * NL] = eps[e];
   }
   __syncthreads();
-  const int L0 = t, L1 = t + TPE;
-  T x0[NL], x1[NL], o0[NL], o1[NL];
-  auto load = [&]() {
-#pragma unroll
-    for (int l = 0; l < NL; l++) {
-      x0[l] = B[NLP * L0 + l];
-      x1[l] = B[NLP * L1 + l];
-    }
-  };
-  auto store = [&]() {  // rotated: line (m, n), output i -> m + NLP*(n + NL*i)
-    const int m0 = L0 % NL, n0 = L0 / NL, m1 = L1 % NL, n1 = L1 / NL;
-#pragma unroll
-    for (int i = 0; i < NL; i++) {
-      B[m0 + NLP * (n0 + NL * i)] = o0[i];
-      B[m1 + NLP * (n1 + NL * i)] = o1[i];
-    }
-  };
+  const int m = t % NL, n = t / NL;
+  T x[NL], o[NL];
+  T *src = b0, *dst = b1;
 #pragma unroll 1
-  for (int d = 0; d < 2; d++) {  // (a,b,c) -> (b,c,i) -> (c,i,j)
+  for (int p = 0; p < 6; p++) {
     if (active) {
-      load();
-      fdm_fwd2<T, NL>(sS + d * N2, x0, x1, o0, o1);
-    }
-    __syncthreads();
-    if (active) store();
-    __syncthreads();
-  }
-  if (active) {  // -> (i,j,k), times D^-1
-    load();
-    fdm_fwd2<T, NL>(sS + 2 * N2, x0, x1, o0, o1);
-    const T ep = sL[3 * NL];
-    const T l0 = sL[L0 % NL] + sL[NL + L0 / NL], l1 = sL[L1 % NL] + sL[NL + L1 / NL];
 #pragma unroll
-    for (int k = 0; k < NL; k++) {
-      const T d0 = l0 + sL[2 * NL + k], d1 = l1 + sL[2 * NL + k];
-      o0[k] = d0 > ep ? o0[k] / d0 : T(0);
-      o1[k] = d1 > ep ? o1[k] / d1 : T(0);
-    }
-  }
-  __syncthreads();
-  if (active) store();
-  __syncthreads();
-#pragma unroll 1
-  for (int d = 0; d < 2; d++) {  // back: S_x, S_y
-    if (active) {
-      load();
-      fdm_bwd2<T, NL>(sS + d * N2, x0, x1, o0, o1);
-    }
-    __syncthreads();
-    if (active) store();
-    __syncthreads();
-  }
-  if (active) {  // S_z, store (i,j,k)
-    load();
-    fdm_bwd2<T, NL>(sS + 2 * N2, x0, x1, o0, o1);
-    T *oe = out + e * N3;
+      for (int l = 0; l < NL; l++) x[l] = src[NLP * t + l];
+      // forward passes: o_i = sum_l S(l,i) x_l; backward: o_i = sum_l S(i,l) x_l
+      fdm_line<T, NL>(p < 3 ? sT + p * N2 : sS + (p - 3) * N2, x, o);
+      if (p == 2) {  // line (i, j), output k: times D^-1
+        const T ep = sL[3 * NL], lij = sL[m] + sL[NL + n];
 #pragma unroll
-    for (int k = 0; k < NL; k++) {
-      oe[L0 + N2 * k] = o0[k];
-      oe[L1 + N2 * k] = o1[k];
+        for (int k = 0; k < NL; k++) {
+          const T d = lij + sL[2 * NL + k];
+          o[k] = o[k] * (d > ep ? T(1) / d : T(0));
+        }
+      }
+      if (p < 5) {  // rotated: out(m, n, i) at m + NLP*(n + NL*i)
+#pragma unroll
+        for (int i = 0; i < NL; i++) dst[m + NLP * (n + NL * i)] = o[i];
+      } else {
+        T *oe = out + e * N3;
+#pragma unroll
+        for (int k = 0; k < NL; k++) oe[t + N2 * k] = o[k];
+      }
     }
+    __syncthreads();
+    T *tmp = src;
+    src = dst;
+    dst = tmp;
   }
 }
 
@@ -427,10 +392,14 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
   if constexpr (NL % 2 == 0) {
     using C = Fdm2Cfg<T, NL>;
     auto kern = fdm2_kernel<TIN, T, NL>;
-    if (C::SMEM > 48 * 1024) {
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
       cudaError_t err =
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+      if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       if (err != cudaSuccess) return err;
+      attr_set = true;
     }
     kern<<<(unsigned)((L.nelv + C::NE - 1) / C::NE), C::THREADS, C::SMEM, s>>>(
         r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
