@@ -85,6 +85,29 @@ void cuda_jacobi_update(void *d, void *dxt, void *dyt, void *dzt, void *G11,
                         void *G22, void *G33, void *G12, void *G13, void *G23,
                         int *nel, int *lx);
 
+/* v = (C x B x A) u on nel elements: u has nu^3 points per element, v nv^3;
+ * A is nv x nu, Bt and Ct nu x nv (column-major).  Replaces cuda_tnsr3d
+ * (src/math/bcknd/device/cuda/tensor.cu:60); nu, nv <= 16.  Runs on the
+ * library's default stream (the reference uses glb_cmd_queue). */
+void cuda_tnsr3d(void *v, int *nv, void *u, int *nu, void *A, void *Bt, void *Ct, int *nel);
+
+/* Fast-diagonalisation solve per element of nl^3 points: r <- d * (S_x^T,
+ * S_y^T, S_z^T) r, then e <- (S_x, S_y, S_z) r, with s holding
+ * s(nl,nl,2,3,nel) (eigenvectors and their transposes) and d the inverse
+ * eigenvalue sums.  r is overwritten, as in the reference.  Replaces
+ * src/math/bcknd/device/cuda/fdm.cu:42; nl <= 16. */
+void cuda_fdm_do_fast(void *e, void *r, void *s, void *d, int *nl, int *nel, void *stream);
+
+/* a1 = f1 a1 + f2 a2 on the interior points of face layers l1 (a1) and l2
+ * (a2) from each side, x then y then z.  Replaces
+ * src/math/bcknd/device/cuda/schwarz.cu:45. */
+void cuda_schwarz_extrude(void *arr1, int *l1, double *f1, void *arr2, int *l2, double *f2,
+                          int *nx, int *nel, void *stream);
+/* a ((nx+2)^3 per element) = b (nx^3) inside a zero ghost layer; and back.
+ * Replace schwarz.cu:82 and schwarz.cu:92. */
+void cuda_schwarz_toext3d(void *a, void *b, int *nx, int *nel, void *stream);
+void cuda_schwarz_toreg3d(void *b, void *a, int *nx, int *nel, void *stream);
+
 /* ------------------------------------------------------------------------
  * Part 2: native handle API.
  * ---------------------------------------------------------------------- */

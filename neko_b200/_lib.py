@@ -63,6 +63,11 @@ SIGNATURES = {
     "cuda_radd": (None, [_P, _DP, _IP, _P]),
     "cuda_zero_dirichlet_apply_scalar": (None, [_P, _P, _IP, _P]),
     "cuda_jacobi_update": (None, [_P] * 10 + [_IP, _IP]),
+    "cuda_tnsr3d": (None, [_P, _IP, _P, _IP, _P, _P, _P, _IP]),
+    "cuda_fdm_do_fast": (None, [_P, _P, _P, _P, _IP, _IP, _P]),
+    "cuda_schwarz_extrude": (None, [_P, _IP, _DP, _P, _IP, _DP, _IP, _IP, _P]),
+    "cuda_schwarz_toext3d": (None, [_P, _P, _IP, _IP, _P]),
+    "cuda_schwarz_toreg3d": (None, [_P, _P, _IP, _IP, _P]),
     # native API
     "nb_last_error": (ctypes.c_char_p, []),
     "nb_version": (ctypes.c_char_p, []),

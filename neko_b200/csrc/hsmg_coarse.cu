@@ -36,30 +36,29 @@ namespace nb {
 constexpr int kCoarseThreads = 512;
 constexpr unsigned kBarrierPolls = 1u << 22;
 
-// Sense-counting grid barrier: bar[0] arrivals, bar[1] generation.
+// Grid barrier on one 32-bit word: every block adds 1 except block 0,
+// which adds 2^31 - (blocks - 1), so the word's top bit flips exactly when
+// the last block arrives (the arrive pattern of cooperative grid sync).
+// Arrival is a release and the poll an acquire at gpu scope, so the writes
+// of every block before the barrier are visible to every block after it.
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    volatile unsigned *gen = bar + 1;
-    const unsigned g = *gen;
-    __threadfence();
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      unsigned polls = 0;
-      while (*gen == g) {
-        if (++polls > kBarrierPolls || *(volatile int *)err) {
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
+    const unsigned add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+    unsigned old, v;
+    asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(add)
+                 : "memory");
+    unsigned polls = 0;
+    for (;;) {
+      asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if ((old ^ v) & 0x80000000u) break;
+      if (++polls > kBarrierPolls || *(volatile int *)err) {
+        ok = 0;
+        break;
       }
     }
-    __threadfence();
     if (!ok) atomicExch(err, 1);
     ok_s = ok;
   }

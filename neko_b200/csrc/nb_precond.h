@@ -79,7 +79,7 @@ struct CoarseArgs {
   GsDevice gs;
   CgState *st = nullptr;    // norm_fac, abs_tol, max_iter in; iter, rnorm out
   double *part = nullptr;   // 2 x 2 x (grid) doubles
-  unsigned *bar = nullptr;  // barrier arrivals and generation, zero at rest
+  unsigned *bar = nullptr;  // grid-barrier word (reset with err after a timeout)
   int *err = nullptr;       // set to 1 when a barrier wait expired
   const int *skip = nullptr;
 };

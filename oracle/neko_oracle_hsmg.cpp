@@ -632,6 +632,34 @@ void or_hsmg_fdm_fine(OrHsmg *H, double *e, const double *r_ext) {
   std::vector<double> rr(r_ext, r_ext + H->sch_fine.ext->n);
   fdm_do_fast(H->sch_fine.fdm, e, rr.data());
 }
+// Array-level forms of the device routines cuda_tnsr3d, cuda_fdm_do_fast and
+// cuda_schwarz_{extrude,toext3d,toreg3d} (same argument meaning, host
+// arrays), for the drop-in parity tests.
+void or_tnsr3d(double *v, int nv, const double *u, int nu, const double *A, const double *Bt,
+               const double *Ct, int nel) {
+  for (int e = 0; e < nel; e++)
+    tnsr3d_el(v + (size_t)e * nv * nv * nv, nv, u + (size_t)e * nu * nu * nu, nu, A, Bt, Ct);
+}
+void or_fdm_do_fast(double *e, double *r, const double *s, const double *d, int nl, int nel) {
+  const int nn = nl * nl * nl;
+  const size_t sz = (size_t)nl * nl * 2;
+  for (int ie = 0; ie < nel; ie++) {  // fdm_cpu.f90:12-46
+    const double *se = s + sz * 3 * ie;
+    const double *s1x = se, *s2x = se + nl * nl, *s1y = se + sz, *s2y = se + sz + nl * nl,
+                 *s1z = se + 2 * sz, *s2z = se + 2 * sz + nl * nl;
+    double *ee = e + (size_t)nn * ie, *rr = r + (size_t)nn * ie;
+    tnsr3d_el(ee, nl, rr, nl, s2x, s1y, s1z);
+    for (int i = 0; i < nn; i++) rr[i] = d[(size_t)nn * ie + i] * ee[i];
+    tnsr3d_el(ee, nl, rr, nl, s1x, s2y, s2z);
+  }
+}
+void or_schwarz_extrude(double *a1, int l1, double f1, const double *a2, int l2, double f2,
+                        int nx, int nel) {
+  extrude(a1, l1, f1, a2, l2, f2, nx, nel);
+}
+void or_schwarz_toext3d(double *a, const double *b, int nx, int nel) { toext3d(a, b, nx, nel); }
+void or_schwarz_toreg3d(double *b, const double *a, int nx, int nel) { toreg3d(b, a, nx, nel); }
+
 long or_hsmg_sizes(OrHsmg *H, int which) {
   switch (which) {
     case 0: return H->mid->n;

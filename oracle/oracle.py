@@ -72,6 +72,12 @@ def lib():
             "or_hsmg_apply": (None, [_P, _D, _D]),
             "or_hsmg_schwarz_fine": (None, [_P, _D, _D]),
             "or_hsmg_sizes": (ctypes.c_long, [_P, ctypes.c_int]),
+            "or_tnsr3d": (None, [_D, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, ctypes.c_int]),
+            "or_fdm_do_fast": (None, [_D, _D, _D, _D, ctypes.c_int, ctypes.c_int]),
+            "or_schwarz_extrude": (None, [_D, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+            "or_schwarz_toext3d": (None, [_D, _D, ctypes.c_int, ctypes.c_int]),
+            "or_schwarz_toreg3d": (None, [_D, _D, ctypes.c_int, ctypes.c_int]),
             "or_cg_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
             "or_fcg_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
         }
@@ -296,3 +302,39 @@ def gll(lx):
 def glsc3(a, b, c):
     a, b, c = (np.ascontiguousarray(v, dtype=np.float64) for v in (a, b, c))
     return lib().or_glsc3(_dp(a), _dp(b), _dp(c), a.size)
+
+
+# Array-level forms of the reference's device routines (tensor.cu:60,
+# fdm.cu:42, schwarz.cu:45-100), used to check the drop-in symbols.
+def tnsr3d(u, nu, nv, A, Bt, Ct, nel):
+    v = np.zeros(nel * nv ** 3)
+    lib().or_tnsr3d(_dp(v), nv, _dp(np.ascontiguousarray(u)), nu, _dp(A), _dp(Bt), _dp(Ct), nel)
+    return v
+
+
+def fdm_do_fast(r, s, d, nl, nel):
+    """Returns (e, r_after): the reference overwrites r with d * (first pass)."""
+    e = np.zeros(nel * nl ** 3)
+    rr = np.array(r, dtype=np.float64)
+    lib().or_fdm_do_fast(_dp(e), _dp(rr), _dp(np.ascontiguousarray(s)),
+                         _dp(np.ascontiguousarray(d)), nl, nel)
+    return e, rr
+
+
+def schwarz_extrude(a1, l1, f1, a2, l2, f2, nx, nel):
+    out = np.array(a1, dtype=np.float64)
+    src = out if a2 is a1 else np.ascontiguousarray(a2)
+    lib().or_schwarz_extrude(_dp(out), l1, f1, _dp(src), l2, f2, nx, nel)
+    return out
+
+
+def schwarz_toext3d(b, nx, nel):
+    a = np.zeros(nel * (nx + 2) ** 3)
+    lib().or_schwarz_toext3d(_dp(a), _dp(np.ascontiguousarray(b)), nx, nel)
+    return a
+
+
+def schwarz_toreg3d(a, nx, nel):
+    b = np.zeros(nel * nx ** 3)
+    lib().or_schwarz_toreg3d(_dp(b), _dp(np.ascontiguousarray(a)), nx, nel)
+    return b

@@ -121,3 +121,39 @@ def test_config1_analytic_solution(oracle):
     assert rf < 1e-10 * r0
     assert np.abs(u - exact).max() < 1e-8
     assert abs(P.volume - 1.0) < 1e-12
+
+
+def test_oracle_array_forms_consistent(oracle):
+    """The oracle's array-level tnsr3d / fdm_do_fast / toext3d / toreg3d agree
+    with direct numpy restatements (the drop-in GPU tests check against
+    them)."""
+    rng = np.random.default_rng(3)
+    nu, nv, nel = 4, 6, 3
+    u = rng.standard_normal(nel * nu ** 3)
+    A, Bt, Ct = (rng.standard_normal(nv * nu) for _ in range(3))
+    v = oracle.tnsr3d(u, nu, nv, A, Bt, Ct, nel).reshape(nel, nv, nv, nv)
+    Am = A.reshape(nu, nv).T          # A(i, l) at i + nv*l
+    Bm = Bt.reshape(nv, nu)           # Bt(l, j) at l + nu*j -> B(j, l)
+    Cm = Ct.reshape(nv, nu)
+    U = u.reshape(nel, nu, nu, nu)    # U[e, k, j, i]
+    ref = np.einsum("ai,bj,ck,ekji->ecba", Am, Bm, Cm, U)
+    np.testing.assert_allclose(v, ref, rtol=1e-12, atol=1e-12)
+    nl = 5
+    r = rng.standard_normal(nel * nl ** 3)
+    s = rng.standard_normal(nel * 6 * nl * nl)
+    d = rng.uniform(0.5, 2, nel * nl ** 3)
+    e, r2 = oracle.fdm_do_fast(r, s, d, nl, nel)
+    S = s.reshape(nel, 3, 2, nl * nl)  # s(:,:,m,dir,e)
+    e_ref, r_ref = [], []
+    for k in range(nel):
+        m = lambda mm, dd: S[k, dd, mm]  # noqa: E731
+        t = oracle.tnsr3d(r[k * nl ** 3:(k + 1) * nl ** 3], nl, nl, m(1, 0), m(0, 1), m(0, 2), 1)
+        t = t * d[k * nl ** 3:(k + 1) * nl ** 3]
+        r_ref.append(t)
+        e_ref.append(oracle.tnsr3d(t, nl, nl, m(0, 0), m(1, 1), m(1, 2), 1))
+    np.testing.assert_allclose(e, np.concatenate(e_ref), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(r2, np.concatenate(r_ref), rtol=1e-13, atol=1e-13)
+    b = rng.standard_normal(nel * 27)
+    a = oracle.schwarz_toext3d(b, 3, nel)
+    assert a.size == nel * 125 and np.count_nonzero(a) == b.size
+    np.testing.assert_array_equal(oracle.schwarz_toreg3d(a, 3, nel), b)
