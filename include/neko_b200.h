@@ -235,6 +235,34 @@ nb_status nb_solve(nb_problem *p, double *x, const double *f,
                    const nb_solve_opts *opts, nb_solve_result *res,
                    void *stream);
 
+/* Batched solves.  A batch advances many independent Jacobi-PCG solves
+ * (same iteration as nb_solve with NB_PC_JACOBI) together: one iteration
+ * of every active solve is one persistent Ax launch over a work queue of
+ * (solve, element range) items sorted by lx, one gather-scatter launch and
+ * one vector/reduction launch, replayed from a CUDA graph.  Problems may
+ * differ in size and lx (4, 6, 8, 10); the Ax k-split per lx is chosen by
+ * timing on first use.  Solves can be submitted and released between runs
+ * (continuous batching); each solve's work vectors (4 n doubles) are
+ * charged against hbm_budget_bytes (<= 0: unlimited), and a submit over
+ * budget returns NB_ERR_OOM without side effects.  No counterpart in the
+ * reference, which runs one ksp solve at a time. */
+typedef struct nb_batch nb_batch;
+nb_status nb_batch_create(int64_t hbm_budget_bytes, nb_batch **out);
+void nb_batch_destroy(nb_batch *b);
+/* Adds a solve of p with right-hand side f (assembled, masked) into x
+ * (device buffers that stay valid until release); returns its slot. */
+nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f, double *x,
+                          double abs_tol, int max_iter, int *slot);
+/* Frees a slot (finished or not) and its budget. */
+nb_status nb_batch_release(nb_batch *b, int slot);
+/* Runs up to max_chunks graph replays (<= 0: until every solve finished);
+ * *active receives the number of solves still running. */
+nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void *stream);
+/* State of a slot: *done = 1 once it stopped (converged, NaN or max_iter). */
+nb_status nb_batch_result(nb_batch *b, int slot, int *done, nb_solve_result *res);
+/* Autotuner record for lx: chosen k-split and the candidates' times (ms). */
+nb_status nb_batch_tuning(nb_batch *b, int lx, int *ks, float *ms, int *ncand);
+
 /* sum(a*b*c) over n device values, written to the host double *result,
  * allocating nothing.  No counterpart in the reference: it is cuda_glsc3 for
  * callers that must not call cudaMalloc (a solve running under a fixed,

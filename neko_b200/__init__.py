@@ -28,7 +28,7 @@ from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpt
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
 __all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "KspMonitor",
-           "Jacobi", "Hsmg", "GS_OP_ADD", "NekoB200Error", "load", "version"]
+           "Jacobi", "Hsmg", "Batch", "GS_OP_ADD", "NekoB200Error", "load", "version"]
 
 
 def version():
@@ -229,3 +229,59 @@ class FCG(CG):
 
     def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False):
         super().__init__(n, max_iter, M, abs_tol, mixed, flexible=True)
+
+
+class Batch:
+    """Many Jacobi-PCG solves advanced together (nb_batch_*): one persistent
+    Ax launch over every active solve's elements per iteration, replayed
+    from a CUDA graph.  Solves may be submitted and released between runs;
+    their work vectors are charged against `hbm_budget` bytes (0: none)."""
+
+    def __init__(self, hbm_budget=0):
+        h = ctypes.c_void_p()
+        check(load().nb_batch_create(int(hbm_budget), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, problem, f, x, abs_tol, max_iter=1000):
+        slot = ctypes.c_int()
+        check(load().nb_batch_submit(self._h, problem.handle, _ptr(f), _ptr(x), float(abs_tol),
+                                     int(max_iter), ctypes.byref(slot)))
+        self._keep[slot.value] = (problem, f, x)
+        return slot.value
+
+    def run(self, max_chunks=0, stream=None):
+        """Replays iteration chunks until every solve stopped (or max_chunks);
+        returns the number of solves still running."""
+        active = ctypes.c_int()
+        check(load().nb_batch_run(self._h, int(max_chunks), ctypes.byref(active),
+                                  _stream_handle(stream)))
+        return active.value
+
+    def result(self, slot):
+        done = ctypes.c_int()
+        r = SolveResult()
+        check(load().nb_batch_result(self._h, int(slot), ctypes.byref(done), ctypes.byref(r)))
+        return bool(done.value), KspMonitor(r.iter, r.res_start, r.res_final, bool(r.converged))
+
+    def release(self, slot):
+        check(load().nb_batch_release(self._h, int(slot)))
+        self._keep.pop(slot, None)
+
+    def tuning(self, lx):
+        ks, n = ctypes.c_int(), ctypes.c_int()
+        ms = (ctypes.c_float * 4)()
+        check(load().nb_batch_tuning(self._h, int(lx), ctypes.byref(ks), ms, ctypes.byref(n)))
+        return ks.value, [ms[i] for i in range(min(n.value, 4))]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            load().nb_batch_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -87,6 +87,13 @@ SIGNATURES = {
     "nb_glsc3_noalloc": (_I, [_P, _P, _P, _I, _DP, _P]),
     "nb_pc_apply": (_I, [_P, _I, _P, _P, _P]),
     "nb_hsmg_init": (_I, [_P, _I, _I, ctypes.c_double]),
+    "nb_batch_create": (_I, [ctypes.c_int64, _P]),
+    "nb_batch_destroy": (None, [_P]),
+    "nb_batch_submit": (_I, [_P, _P, _P, _P, ctypes.c_double, _I, _IP]),
+    "nb_batch_release": (_I, [_P, _I]),
+    "nb_batch_run": (_I, [_P, _I, _IP, _P]),
+    "nb_batch_result": (_I, [_P, _I, _IP, _P]),
+    "nb_batch_tuning": (_I, [_P, _I, _IP, ctypes.POINTER(ctypes.c_float), _IP]),
 }
 
 _lib = None

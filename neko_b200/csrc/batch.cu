@@ -1,0 +1,801 @@
+// batch.cu -- many independent Helmholtz solves advanced together.
+//
+// Each slot holds one solve (x = A^-1 f with Jacobi-preconditioned CG, the
+// iteration of cg_device_solve, src/krylov/bcknd/device/cg_device.f90:
+// 162-238) on its own device-resident problem; problems may differ in
+// element count and lx.  One iteration of every active slot is three
+// launches whatever the number of slots:
+//
+//   K3  one persistent launch over a work queue of (slot, element range)
+//       items, sorted by lx: p = z + beta p fused into the load of p, then
+//       w = A p (+ h2 B p) per element, and the slot's (p, w) accumulated;
+//       the block that finishes a slot's last item forms alpha.
+//   K4  gather-scatter add + mask of w over every slot's gs items.
+//   K5  x += alpha p, r -= alpha w, z = d r, (r, mult r), (r, mult z) over
+//       fixed point chunks; the block that finishes a slot's last chunk
+//       forms rnorm, the convergence flag and the next beta.
+//
+// Per-slot sums are formed by the last block of the slot from per-item
+// partials in item order, so they do not depend on scheduling.  (p, mult
+// gs(w)) is formed as the sum of p * w over local points before the
+// gather-scatter: p is continuous and zero on masked points, so the two
+// agree (each global point's weights 1/k over its k copies add to one).
+//
+// The element routine exists per (lx, k-split) and the k-split of each lx
+// is chosen by timing the candidates on the batch's own items the first
+// time an lx appears (the reference autotunes its Ax kernels on first call,
+// src/math/bcknd/device/cuda/ax_helm.cu:270-350).  Iterations are captured
+// in a CUDA graph of `chunk` iterations and replayed until every slot has
+// finished; slots that finished skip their work.  Adding or removing a slot
+// rebuilds the queues and the graph, so solves can join while others run
+// (continuous batching).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "nb_gs_dev.cuh"
+#include "nb_kernels.h"
+#include "nb_problem.h"
+#include "nb_reduce.cuh"
+
+namespace nb {
+
+constexpr int kBT = 256;         // threads of the batched kernels
+constexpr int kItemElems = 8;    // elements per Ax work item
+constexpr long kChunk = 8192;    // points per vector chunk
+constexpr int kGsChunk = 4096;   // gs items per chunk
+
+struct BSlot {
+  int lx, nelv;
+  long n;
+  double *x;
+  const double *f;
+  double *r, *z, *p, *w;
+  const double *g11, *g22, *g33, *g12, *g13, *g23, *h1, *h2, *B, *mult, *dinv, *D, *Dt;
+  GsDevice gs;
+  int ifh2;
+  int ax_first, ax_count, vc_first, vc_count;
+  double rtz, pap, alpha, beta, rtr, rnorm, res_start, abs_tol, norm_fac;
+  int iter, max_iter, done, nan;
+  unsigned ax_counter, vc_counter;
+};
+
+struct AxItem {
+  int slot, e0, ne, lx;
+};
+struct VChunk {
+  int slot, pad;
+  long i0, i1;
+};
+struct GChunk {
+  int slot, t0, t1, pad;
+};
+
+// ---------------------------------------------------------------------------
+// Element routine: w = A p on `ne` elements from e0, NE elements at a time,
+// KS thread groups splitting the k-planes; acc += p * w.
+// ---------------------------------------------------------------------------
+template <int LX, int KS>
+struct AxB {
+  static constexpr int L2 = LX * LX, L3 = L2 * LX, TPE = L2 * KS, NE = kBT / TPE, KP = LX / KS;
+  static constexpr int SMEM = 2 * L2 + NE * 4 * L3;  // doubles
+  static_assert(LX % KS == 0 && NE >= 1, "bad k split");
+};
+
+template <int LX, int KS>
+__device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double beta, double *sm,
+                                         double &acc) {
+  using C = AxB<LX, KS>;
+  constexpr int L2 = C::L2, L3 = C::L3, TPE = C::TPE, NE = C::NE, KP = C::KP;
+  const int tid = threadIdx.x, el = tid / TPE, c = tid - el * TPE, col = c % L2, kh = c / L2;
+  const int i = col % LX, j = col / LX, k0 = kh * KP;
+  double *sD = sm, *sDt = sm + L2;
+  double *su = sm + 2 * L2 + el * 4 * L3, *sur = su + L3, *sus = su + 2 * L3, *sut = su + 3 * L3;
+  for (int q = tid; q < L2; q += kBT) {
+    sD[q] = S.D[q];
+    sDt[q] = S.Dt[q];
+  }
+  __syncthreads();
+  for (int g = 0; g < ne; g += NE) {
+    const long e = e0 + g + el;
+    const bool act = el < NE && g + el < ne;
+    if (act) {
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        const long idx = e * L3 + col + L2 * k;
+        const double pv = S.z[idx] + beta * S.p[idx];
+        S.p[idx] = pv;
+        su[col + L2 * k] = pv;
+      }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        double ur = 0, us = 0, ut = 0;
+#pragma unroll
+        for (int l = 0; l < LX; l++) {
+          ur += sD[i + LX * l] * su[l + LX * j + L2 * k];
+          us += sD[j + LX * l] * su[i + LX * l + L2 * k];
+          ut += sD[k + LX * l] * su[col + L2 * l];
+        }
+        const long idx = e * L3 + col + L2 * k;
+        const double H = __ldg(S.h1 + idx), G11 = __ldg(S.g11 + idx), G22 = __ldg(S.g22 + idx),
+                     G33 = __ldg(S.g33 + idx), G12 = __ldg(S.g12 + idx),
+                     G13 = __ldg(S.g13 + idx), G23 = __ldg(S.g23 + idx);
+        sur[col + L2 * k] = H * (G11 * ur + G12 * us + G13 * ut);
+        sus[col + L2 * k] = H * (G12 * ur + G22 * us + G23 * ut);
+        sut[col + L2 * k] = H * (G13 * ur + G23 * us + G33 * ut);
+      }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        double a = 0, b = 0, d = 0;
+#pragma unroll
+        for (int l = 0; l < LX; l++) {
+          a += sDt[i + LX * l] * sur[l + LX * j + L2 * k];
+          b += sDt[j + LX * l] * sus[i + LX * l + L2 * k];
+          d += sDt[k + LX * l] * sut[col + L2 * l];
+        }
+        const long idx = e * L3 + col + L2 * k;
+        const double pv = su[col + L2 * k];
+        double wv = a + b + d;
+        if (S.ifh2) wv = wv + __ldg(S.h2 + idx) * __ldg(S.B + idx) * pv;
+        S.w[idx] = wv;
+        acc += pv * wv;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// lx and k-split of every supported element routine; the table order is
+// the case order of the switch in batch_ax_kernel.
+struct AxVariant {
+  int lx, ks;
+};
+static const AxVariant kVariants[] = {{4, 1}, {4, 2}, {6, 1}, {6, 2}, {6, 3},
+                                      {8, 1}, {8, 2}, {8, 4}, {10, 1}, {10, 2}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+static int variant_smem_doubles(int v) {
+  switch (v) {
+    case 0: return AxB<4, 1>::SMEM;
+    case 1: return AxB<4, 2>::SMEM;
+    case 2: return AxB<6, 1>::SMEM;
+    case 3: return AxB<6, 2>::SMEM;
+    case 4: return AxB<6, 3>::SMEM;
+    case 5: return AxB<8, 1>::SMEM;
+    case 6: return AxB<8, 2>::SMEM;
+    case 7: return AxB<8, 4>::SMEM;
+    case 8: return AxB<10, 1>::SMEM;
+    default: return AxB<10, 2>::SMEM;
+  }
+}
+
+// var_of_lx[lx] = variant index used for that lx.
+__global__ void __launch_bounds__(kBT)
+    batch_ax_kernel(BSlot *__restrict__ slots, const AxItem *__restrict__ items, int nitems,
+                    unsigned *head, double *part, const int *__restrict__ var_of_lx) {
+  extern __shared__ __align__(16) double bsm[];
+  __shared__ double red[kBT / 32];
+  __shared__ int item_s;
+  __shared__ bool last_s;
+  for (;;) {
+    if (threadIdx.x == 0) item_s = (int)atomicAdd(head, 1u);
+    __syncthreads();
+    const int it = item_s;
+    __syncthreads();
+    if (it >= nitems) return;
+    const AxItem I = items[it];
+    BSlot &S = slots[I.slot];
+    if (S.done) continue;
+    double acc = 0.0;
+    const double beta = S.beta;
+    switch (var_of_lx[I.lx]) {
+#define NB_V(V, LX, KS) \
+  case V: ax_elems<LX, KS>(S, I.e0, I.ne, beta, bsm, acc); break;
+      NB_V(0, 4, 1) NB_V(1, 4, 2) NB_V(2, 6, 1) NB_V(3, 6, 2) NB_V(4, 6, 3)
+      NB_V(5, 8, 1) NB_V(6, 8, 2) NB_V(7, 8, 4) NB_V(8, 10, 1) NB_V(9, 10, 2)
+#undef NB_V
+      default: break;
+    }
+    const double tot = block_sum<kBT>(acc, red);
+    if (threadIdx.x == 0) {
+      part[it] = tot;
+      __threadfence();
+      last_s = atomicAdd(&S.ax_counter, 1u) == (unsigned)S.ax_count - 1;
+    }
+    __syncthreads();
+    if (last_s && threadIdx.x == 0) {
+      __threadfence();
+      double pap = 0.0;
+      for (int q = S.ax_first; q < S.ax_first + S.ax_count; q++)
+        pap += *((volatile double *)part + q);
+      S.ax_counter = 0;
+      S.pap = pap;
+      S.alpha = S.rtz / pap;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kBT)
+    batch_gs_kernel(BSlot *__restrict__ slots, const GChunk *__restrict__ chunks) {
+  const GChunk C = chunks[blockIdx.x];
+  const BSlot &S = slots[C.slot];
+  if (S.done) return;
+  for (int t = C.t0 + threadIdx.x; t < C.t1; t += kBT) gs_add_item<double>(S.w, S.gs, t, true, nullptr);
+}
+
+// Per-slot tail of a chunked two-value reduction: returns true in thread 0
+// of the block that completed the slot's last chunk, with the totals.
+__device__ __forceinline__ bool slot_sum2(BSlot &S, int c, double v0, double v1, double *part,
+                                          double *sh, double &t0, double &t1) {
+  __shared__ bool last_s;
+  const double b0 = block_sum<kBT>(v0, sh);
+  const double b1 = block_sum<kBT>(v1, sh);
+  if (threadIdx.x == 0) {
+    part[2 * c] = b0;
+    part[2 * c + 1] = b1;
+    __threadfence();
+    last_s = atomicAdd(&S.vc_counter, 1u) == (unsigned)S.vc_count - 1;
+  }
+  __syncthreads();
+  if (!last_s || threadIdx.x != 0) return false;
+  __threadfence();
+  t0 = t1 = 0.0;
+  for (int q = S.vc_first; q < S.vc_first + S.vc_count; q++) {
+    t0 += *((volatile double *)part + 2 * q);
+    t1 += *((volatile double *)part + 2 * q + 1);
+  }
+  S.vc_counter = 0;
+  return true;
+}
+
+// x = 0, p = 0, r = f, z = d r; res_start.
+__global__ void __launch_bounds__(kBT)
+    batch_init_kernel(BSlot *__restrict__ slots, const VChunk *__restrict__ chunks, double *part) {
+  __shared__ double sh[kBT / 32];
+  const VChunk C = chunks[blockIdx.x];
+  BSlot &S = slots[C.slot];
+  if (S.done) return;
+  double srr = 0.0, srz = 0.0;
+  for (long i = C.i0 + threadIdx.x; i < C.i1; i += kBT) {
+    const double ri = S.f[i], m = __ldg(S.mult + i);
+    S.x[i] = 0.0;
+    S.p[i] = 0.0;
+    S.r[i] = ri;
+    const double zi = ri * __ldg(S.dinv + i);
+    S.z[i] = zi;
+    srr += ri * m * ri;
+    srz += ri * m * zi;
+  }
+  double rtr, rtz;
+  if (slot_sum2(S, blockIdx.x, srr, srz, part, sh, rtr, rtz)) {
+    const double rn = sqrt(rtr) * S.norm_fac;
+    S.rtr = rtr;
+    S.rnorm = rn;
+    S.res_start = rn;
+    S.rtz = rtz;
+    S.beta = 0.0;
+    S.iter = 0;
+    S.nan = !(rn == rn) || isinf(rn);
+    S.done = S.nan || fabs(rn) < 2.220446049250313e-16;
+  }
+}
+
+// x += alpha p; r -= alpha w; z = d r; (r, mult r), (r, mult z).
+__global__ void __launch_bounds__(kBT)
+    batch_update_kernel(BSlot *__restrict__ slots, const VChunk *__restrict__ chunks, double *part) {
+  __shared__ double sh[kBT / 32];
+  const VChunk C = chunks[blockIdx.x];
+  BSlot &S = slots[C.slot];
+  if (S.done) return;
+  const double alpha = S.alpha, malpha = -alpha;
+  double srr = 0.0, srz = 0.0;
+  for (long i = C.i0 + threadIdx.x; i < C.i1; i += kBT) {
+    S.x[i] = S.x[i] + alpha * S.p[i];
+    const double ri = S.r[i] + malpha * S.w[i], m = __ldg(S.mult + i);
+    S.r[i] = ri;
+    const double zi = ri * __ldg(S.dinv + i);
+    S.z[i] = zi;
+    srr += ri * m * ri;
+    srz += ri * m * zi;
+  }
+  double rtr, rtz;
+  if (slot_sum2(S, blockIdx.x, srr, srz, part, sh, rtr, rtz)) {
+    const double rn = sqrt(rtr) * S.norm_fac;
+    S.rtr = rtr;
+    S.rnorm = rn;
+    S.iter += 1;
+    S.beta = rtz / S.rtz;
+    S.rtz = rtz;
+    int done = 0;
+    if (!(rn == rn) || isinf(rn)) {
+      S.nan = 1;
+      done = 1;
+    }
+    if (rn < S.abs_tol || S.iter >= S.max_iter) done = 1;
+    S.done = done;
+  }
+}
+
+}  // namespace nb
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+using namespace nb;
+
+namespace {
+
+struct SlotHost {
+  bool used = false;
+  nb_problem *P = nullptr;
+  const double *f = nullptr;
+  double *x = nullptr;
+  double *vec = nullptr;  // r, z, p, w
+  size_t bytes = 0;
+  double abs_tol = 0.0;
+  int max_iter = 0;
+  bool started = false;  // init kernel run
+};
+
+}  // namespace
+
+struct nb_batch {
+  size_t budget = 0, used = 0;
+  std::vector<SlotHost> slots;
+  // device tables
+  BSlot *d_slots = nullptr;
+  AxItem *d_items = nullptr;
+  VChunk *d_vchunks = nullptr;
+  GChunk *d_gchunks = nullptr;
+  double *d_part3 = nullptr, *d_part5 = nullptr;
+  unsigned *d_head = nullptr;
+  int *d_var = nullptr;
+  size_t cap_slots = 0, cap_items = 0, cap_vchunks = 0, cap_gchunks = 0;
+  int nitems = 0, nvchunks = 0, ngchunks = 0;
+  std::vector<int> ks_of_lx = std::vector<int>(17, 0);  // 0 = not tuned
+  int var_of_lx[17] = {0};
+  std::vector<float> tune_ms[17];
+  cudaGraphExec_t graph = nullptr;
+  bool dirty = true;
+  int chunk = 8;
+  int smem_bytes = 0;
+  cudaStream_t cap_stream = nullptr;
+  ~nb_batch();
+};
+
+static nb_status bfail(nb_status s, const std::string &m) {
+  set_error(m);
+  return s;
+}
+
+#define NB_BTRY(...)                                                            \
+  do {                                                                          \
+    cudaError_t _e = (__VA_ARGS__);                                             \
+    if (_e != cudaSuccess)                                                      \
+      return bfail(_e == cudaErrorMemoryAllocation ? NB_ERR_OOM : NB_ERR_CUDA,  \
+                   std::string(#__VA_ARGS__) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+nb_batch::~nb_batch() {
+  if (graph) cudaGraphExecDestroy(graph);
+  for (auto &s : slots)
+    if (s.vec) cudaFree(s.vec);
+  cudaFree(d_slots);
+  cudaFree(d_items);
+  cudaFree(d_vchunks);
+  cudaFree(d_gchunks);
+  cudaFree(d_part3);
+  cudaFree(d_part5);
+  cudaFree(d_head);
+  cudaFree(d_var);
+  if (cap_stream) cudaStreamDestroy(cap_stream);
+}
+
+static int variant_index(int lx, int ks) {
+  for (int v = 0; v < kNumVariants; v++)
+    if (kVariants[v].lx == lx && kVariants[v].ks == ks) return v;
+  return -1;
+}
+
+template <typename T>
+static cudaError_t grow(T *&p, size_t &cap, size_t need) {
+  if (need <= cap && p) return cudaSuccess;
+  size_t c = std::max<size_t>(need, 2 * cap);
+  if (c < 16) c = 16;
+  cudaFree(p);
+  p = nullptr;
+  cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+  if (e == cudaSuccess) cap = c;
+  return e;
+}
+
+// Rebuilds the slot table and work queues from the active slots.  Slot
+// descriptors keep their device state (a slot's iteration state lives in
+// its BSlot), so only new slots are initialised.
+static nb_status rebuild(nb_batch *b, std::vector<BSlot> &host_slots) {
+  const int ns = (int)b->slots.size();
+  host_slots.assign(ns, BSlot{});
+  if (b->d_slots && ns > 0) {
+    size_t have = std::min<size_t>(b->cap_slots, ns);
+    NB_BTRY(cudaMemcpy(host_slots.data(), b->d_slots, have * sizeof(BSlot),
+                       cudaMemcpyDeviceToHost));
+  }
+  std::vector<AxItem> items;
+  std::vector<VChunk> vch;
+  std::vector<GChunk> gch;
+  // Ax items sorted by lx, then slot
+  std::vector<int> order;
+  for (int s = 0; s < ns; s++)
+    if (b->slots[s].used) order.push_back(s);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int c) { return b->slots[a].P->lx < b->slots[c].P->lx; });
+  for (int s = 0; s < ns; s++) {
+    BSlot &S = host_slots[s];
+    const SlotHost &H = b->slots[s];
+    if (!H.used) {
+      S.done = 1;
+      S.ax_count = S.vc_count = 0;
+      continue;
+    }
+    nb_problem *P = H.P;
+    S.lx = P->lx;
+    S.nelv = P->nelv;
+    S.n = P->n;
+    S.x = H.x;
+    S.f = H.f;
+    S.r = H.vec;
+    S.z = H.vec + P->n;
+    S.p = H.vec + 2 * P->n;
+    S.w = H.vec + 3 * P->n;
+    S.g11 = P->g11, S.g22 = P->g22, S.g33 = P->g33, S.g12 = P->g12, S.g13 = P->g13,
+    S.g23 = P->g23;
+    S.h1 = P->h1, S.h2 = P->h2, S.B = P->B, S.mult = P->mult, S.dinv = P->jdiag;
+    S.D = P->D, S.Dt = P->Dt;
+    S.gs = P->gsd;
+    S.ifh2 = P->ifh2 ? 1 : 0;
+    if (!H.started) {
+      S.abs_tol = H.abs_tol;
+      S.max_iter = H.max_iter;
+      S.norm_fac = 1.0 / std::sqrt(P->volume);
+      S.done = 0;
+      S.nan = 0;
+      S.iter = 0;
+    }
+    S.ax_counter = S.vc_counter = 0;
+  }
+  for (int s : order) {
+    BSlot &S = host_slots[s];
+    S.ax_first = (int)items.size();
+    for (int e = 0; e < S.nelv; e += kItemElems)
+      items.push_back(AxItem{s, e, std::min(kItemElems, S.nelv - e), S.lx});
+    S.ax_count = (int)items.size() - S.ax_first;
+  }
+  for (int s = 0; s < ns; s++) {
+    if (!b->slots[s].used) continue;
+    BSlot &S = host_slots[s];
+    S.vc_first = (int)vch.size();
+    for (long i = 0; i < S.n; i += kChunk) vch.push_back(VChunk{s, 0, i, std::min(S.n, i + kChunk)});
+    S.vc_count = (int)vch.size() - S.vc_first;
+    const int ng = (int)gs_items(S.gs, true);
+    for (int t = 0; t < ng; t += kGsChunk) gch.push_back(GChunk{s, t, std::min(ng, t + kGsChunk), 0});
+  }
+  NB_BTRY(grow(b->d_slots, b->cap_slots, (size_t)std::max(ns, 1)));
+  NB_BTRY(grow(b->d_items, b->cap_items, std::max<size_t>(items.size(), 1)));
+  NB_BTRY(grow(b->d_vchunks, b->cap_vchunks, std::max<size_t>(vch.size(), 1)));
+  NB_BTRY(grow(b->d_gchunks, b->cap_gchunks, std::max<size_t>(gch.size(), 1)));
+  cudaFree(b->d_part3);
+  cudaFree(b->d_part5);
+  b->d_part3 = b->d_part5 = nullptr;
+  NB_BTRY(cudaMalloc(&b->d_part3, std::max<size_t>(items.size(), 1) * sizeof(double)));
+  NB_BTRY(cudaMalloc(&b->d_part5, 2 * std::max<size_t>(vch.size(), 1) * sizeof(double)));
+  if (ns) NB_BTRY(cudaMemcpy(b->d_slots, host_slots.data(), ns * sizeof(BSlot), cudaMemcpyHostToDevice));
+  if (!items.empty())
+    NB_BTRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(AxItem), cudaMemcpyHostToDevice));
+  if (!vch.empty())
+    NB_BTRY(cudaMemcpy(b->d_vchunks, vch.data(), vch.size() * sizeof(VChunk), cudaMemcpyHostToDevice));
+  if (!gch.empty())
+    NB_BTRY(cudaMemcpy(b->d_gchunks, gch.data(), gch.size() * sizeof(GChunk), cudaMemcpyHostToDevice));
+  b->nitems = (int)items.size();
+  b->nvchunks = (int)vch.size();
+  b->ngchunks = (int)gch.size();
+  return NB_OK;
+}
+
+static int ax_grid() {
+  static int g = 0;
+  if (g == 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g = sms * 3;
+  }
+  return g;
+}
+
+static cudaError_t launch_iteration(nb_batch *b, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(b->d_head, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
+  if (b->nitems > 0) {
+    batch_ax_kernel<<<std::min(ax_grid(), b->nitems), kBT, b->smem_bytes, s>>>(
+        b->d_slots, b->d_items, b->nitems, b->d_head, b->d_part3, b->d_var);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (b->ngchunks > 0) batch_gs_kernel<<<b->ngchunks, kBT, 0, s>>>(b->d_slots, b->d_gchunks);
+  if (b->nvchunks > 0)
+    batch_update_kernel<<<b->nvchunks, kBT, 0, s>>>(b->d_slots, b->d_vchunks, b->d_part5);
+  return cudaGetLastError();
+}
+
+static nb_status set_smem(nb_batch *b) {
+  int mx = 0;
+  for (int lx = 0; lx <= 16; lx++)
+    if (b->ks_of_lx[lx]) {
+      const int v = variant_index(lx, b->ks_of_lx[lx]);
+      mx = std::max(mx, variant_smem_doubles(v));
+    }
+  b->smem_bytes = std::max(mx, 1) * (int)sizeof(double);
+  NB_BTRY(cudaFuncSetAttribute(batch_ax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               b->smem_bytes));
+  int var[17];
+  for (int lx = 0; lx <= 16; lx++)
+    var[lx] = b->ks_of_lx[lx] ? variant_index(lx, b->ks_of_lx[lx]) : -1;
+  NB_BTRY(cudaMemcpy(b->d_var, var, sizeof(var), cudaMemcpyHostToDevice));
+  return NB_OK;
+}
+
+// Times every k-split of lx on the batch's own items of that lx (run before
+// the slots are initialised, so the vectors it touches are rewritten).
+static nb_status autotune_lx(nb_batch *b, int lx, cudaStream_t s) {
+  std::vector<AxItem> all(b->nitems), mine;
+  NB_BTRY(cudaMemcpy(all.data(), b->d_items, all.size() * sizeof(AxItem), cudaMemcpyDeviceToHost));
+  for (auto &it : all)
+    if (it.lx == lx) mine.push_back(it);
+  AxItem *d = nullptr;
+  NB_BTRY(cudaMalloc(&d, mine.size() * sizeof(AxItem)));
+  cudaMemcpy(d, mine.data(), mine.size() * sizeof(AxItem), cudaMemcpyHostToDevice);
+  double *part = nullptr;
+  cudaMalloc(&part, std::max<size_t>(b->nitems, 1) * sizeof(double));
+  float best = 1e30f;
+  int best_ks = 0;
+  b->tune_ms[lx].clear();
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int v = 0; v < kNumVariants; v++) {
+    if (kVariants[v].lx != lx) continue;
+    const int smem = variant_smem_doubles(v) * (int)sizeof(double);
+    if (smem > 200 * 1024) continue;
+    int var[17];
+    for (int q = 0; q <= 16; q++) var[q] = q == lx ? v : -1;
+    cudaMemcpy(b->d_var, var, sizeof(var), cudaMemcpyHostToDevice);
+    cudaFuncSetAttribute(batch_ax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         std::max(smem, b->smem_bytes));
+    float ms = 0;
+    for (int rep = 0; rep < 4; rep++) {
+      cudaMemsetAsync(b->d_head, 0, sizeof(unsigned), s);
+      cudaEventRecord(e0, s);
+      batch_ax_kernel<<<std::min(ax_grid(), (int)mine.size()), kBT, smem, s>>>(
+          b->d_slots, d, (int)mine.size(), b->d_head, part, b->d_var);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep == 0 || t < ms) ms = t;
+    }
+    b->tune_ms[lx].push_back(ms);
+    if (ms < best) {
+      best = ms;
+      best_ks = kVariants[v].ks;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  cudaFree(part);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return bfail(NB_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(err));
+  b->ks_of_lx[lx] = best_ks;
+  return NB_OK;
+}
+
+static nb_status prepare(nb_batch *b, cudaStream_t s) {
+  if (!b->dirty) return NB_OK;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  std::vector<BSlot> hs;
+  nb_status st = rebuild(b, hs);
+  if (st != NB_OK) return st;
+  // autotune any lx seen for the first time (before the new slots start)
+  for (auto &sh : b->slots)
+    if (sh.used && !b->ks_of_lx[sh.P->lx]) {
+      // mark every slot done except those of this lx while timing
+      std::vector<BSlot> tmp = hs;
+      for (size_t q = 0; q < tmp.size(); q++) tmp[q].done = 1;
+      for (size_t q = 0; q < tmp.size(); q++)
+        if (b->slots[q].used && b->slots[q].P->lx == sh.P->lx) {
+          tmp[q].done = 0;
+          tmp[q].beta = 0.0;
+          tmp[q].rtz = 1.0;
+        }
+      NB_BTRY(cudaMemcpy(b->d_slots, tmp.data(), tmp.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
+      st = autotune_lx(b, sh.P->lx, s);
+      if (st != NB_OK) return st;
+      NB_BTRY(cudaMemcpy(b->d_slots, hs.data(), hs.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
+    }
+  st = set_smem(b);
+  if (st != NB_OK) return st;
+  // initialise slots that have not started
+  bool any_new = false;
+  for (auto &sh : b->slots)
+    if (sh.used && !sh.started) any_new = true;
+  if (any_new) {
+    // run the init kernel over all chunks; started slots keep their state
+    // because the kernel only touches slots whose `done` is 0 and whose
+    // iteration has not begun -- mark started slots done temporarily.
+    std::vector<BSlot> tmp = hs;
+    for (size_t q = 0; q < tmp.size(); q++)
+      if (!b->slots[q].used || b->slots[q].started) tmp[q].done = 1;
+    NB_BTRY(cudaMemcpy(b->d_slots, tmp.data(), tmp.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
+    if (b->nvchunks > 0) batch_init_kernel<<<b->nvchunks, kBT, 0, s>>>(b->d_slots, b->d_vchunks, b->d_part5);
+    NB_BTRY(cudaGetLastError());
+    NB_BTRY(cudaStreamSynchronize(s));
+    std::vector<BSlot> after(tmp.size());
+    NB_BTRY(cudaMemcpy(after.data(), b->d_slots, after.size() * sizeof(BSlot), cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < after.size(); q++)
+      if (b->slots[q].used && !b->slots[q].started) {
+        hs[q] = after[q];
+        b->slots[q].started = true;
+      }
+    NB_BTRY(cudaMemcpy(b->d_slots, hs.data(), hs.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
+  }
+  // capture `chunk` iterations
+  if (!b->cap_stream) NB_BTRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+  cudaGraph_t g;
+  NB_BTRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = cudaSuccess;
+  for (int k = 0; k < b->chunk && ce == cudaSuccess; k++) ce = launch_iteration(b, b->cap_stream);
+  cudaError_t ee = cudaStreamEndCapture(b->cap_stream, &g);
+  if (ce != cudaSuccess) {
+    if (ee == cudaSuccess) cudaGraphDestroy(g);
+    return bfail(NB_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(ce));
+  }
+  NB_BTRY(ee);
+  ee = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  NB_BTRY(ee);
+  b->dirty = false;
+  return NB_OK;
+}
+
+extern "C" nb_status nb_batch_create(int64_t hbm_budget_bytes, nb_batch **out) {
+  if (!out) return bfail(NB_ERR_ARG, "null argument");
+  *out = nullptr;
+  nb_batch *b = new nb_batch();
+  b->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : (size_t)-1;
+  if (cudaMalloc(&b->d_head, 256) != cudaSuccess || cudaMalloc(&b->d_var, 17 * sizeof(int)) != cudaSuccess) {
+    delete b;
+    return bfail(NB_ERR_OOM, "batch: device tables");
+  }
+  *out = b;
+  return NB_OK;
+}
+
+extern "C" void nb_batch_destroy(nb_batch *b) { delete b; }
+
+extern "C" nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f, double *x,
+                                     double abs_tol, int max_iter, int *slot) {
+  if (!b || !p || !f || !x || !slot) return bfail(NB_ERR_ARG, "null argument");
+  if (max_iter < 1) return bfail(NB_ERR_ARG, "max_iter must be >= 1");
+  if (variant_index(p->lx, 1) < 0)
+    return bfail(NB_ERR_UNSUPPORTED, "batched solves support lx 4, 6, 8, 10");
+  const size_t bytes = 4 * (size_t)p->n * sizeof(double);
+  if (b->used + bytes > b->budget) return bfail(NB_ERR_OOM, "batch: over the HBM budget");
+  SlotHost h;
+  h.used = true;
+  h.P = p;
+  h.f = f;
+  h.x = x;
+  h.abs_tol = abs_tol;
+  h.max_iter = max_iter;
+  h.bytes = bytes;
+  cudaError_t e = cudaMalloc(&h.vec, bytes);
+  if (e != cudaSuccess) return bfail(NB_ERR_OOM, "batch: slot vectors");
+  cudaMemset(h.vec, 0, bytes);
+  int s = -1;
+  for (size_t q = 0; q < b->slots.size(); q++)
+    if (!b->slots[q].used) {
+      s = (int)q;
+      break;
+    }
+  if (s < 0) {
+    s = (int)b->slots.size();
+    b->slots.push_back(h);
+  } else {
+    b->slots[s] = h;
+  }
+  b->used += bytes;
+  b->dirty = true;
+  *slot = s;
+  return NB_OK;
+}
+
+extern "C" nb_status nb_batch_release(nb_batch *b, int slot) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return bfail(NB_ERR_ARG, "no such slot");
+  SlotHost &h = b->slots[slot];
+  cudaFree(h.vec);
+  b->used -= h.bytes;
+  h = SlotHost{};
+  b->dirty = true;
+  return NB_OK;
+}
+
+// Runs graph chunks until every active slot has finished or max_chunks
+// chunks ran (max_chunks <= 0: no limit).  *active = slots still running.
+extern "C" nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void *stream) {
+  if (!b) return bfail(NB_ERR_ARG, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  nb_status st = prepare(b, s);
+  if (st != NB_OK) return st;
+  const int ns = (int)b->slots.size();
+  std::vector<BSlot> hs(ns);
+  int left = 0;
+  for (int c = 0; max_chunks <= 0 || c < max_chunks; c++) {
+    if (ns == 0) break;
+    NB_BTRY(cudaGraphLaunch(b->graph, s));
+    NB_BTRY(cudaMemcpyAsync(hs.data(), b->d_slots, ns * sizeof(BSlot), cudaMemcpyDeviceToHost, s));
+    NB_BTRY(cudaStreamSynchronize(s));
+    left = 0;
+    for (int q = 0; q < ns; q++)
+      if (b->slots[q].used && !hs[q].done) left++;
+    if (!left) break;
+  }
+  if (active) *active = left;
+  return NB_OK;
+}
+
+extern "C" nb_status nb_batch_result(nb_batch *b, int slot, int *done, nb_solve_result *res) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return bfail(NB_ERR_ARG, "no such slot");
+  if (!b->slots[slot].started) {  // submitted, not yet initialised
+    if (done) *done = 0;
+    if (res) *res = nb_solve_result{};
+    return NB_OK;
+  }
+  BSlot S;
+  NB_BTRY(cudaMemcpy(&S, b->d_slots + slot, sizeof(BSlot), cudaMemcpyDeviceToHost));
+  if (done) *done = S.done;
+  if (res) {
+    res->iter = S.iter;
+    res->res_start = S.res_start;
+    res->res_final = S.iter ? S.rnorm : S.res_start;
+    res->converged = !S.nan && (S.iter == 0 || S.rnorm < S.abs_tol) && S.iter < S.max_iter;
+    res->launches = 0;
+  }
+  return NB_OK;
+}
+
+// k-split chosen for lx (0 = lx not tuned yet) and the timing of each
+// candidate in ms (up to 4 values).
+extern "C" nb_status nb_batch_tuning(nb_batch *b, int lx, int *ks, float *ms, int *ncand) {
+  if (!b || lx < 0 || lx > 16) return bfail(NB_ERR_ARG, "bad argument");
+  if (ks) *ks = b->ks_of_lx[lx];
+  if (ncand) *ncand = (int)b->tune_ms[lx].size();
+  if (ms)
+    for (size_t q = 0; q < b->tune_ms[lx].size() && q < 4; q++) ms[q] = b->tune_ms[lx][q];
+  return NB_OK;
+}
