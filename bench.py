@@ -249,6 +249,127 @@ def kernel_only(args, cfg):
     print(json.dumps({"kernel": args.kernel_only, "n": P.n, "launches": args.warmup + args.steps}))
 
 
+class GeometryCache:
+    """Device-resident problems keyed by (n, lx, deformation seed): mesh,
+    geometric factors and gs maps built once and shared by every solve of
+    that shape."""
+
+    def __init__(self, nb):
+        self.nb, self.problems, self.setup_s = nb, {}, 0.0
+
+    def get(self, spec):
+        from neko_b200 import workloads
+        key = (spec["n"], spec["lx"], spec["dseed"])
+        if key not in self.problems:
+            t0 = time.perf_counter()
+            self.problems[key] = self.nb.Problem((spec["n"],) * 3, spec["lx"],
+                                                 deform=workloads.deform_amplitude(spec["dseed"]),
+                                                 dirichlet=True)
+            self.setup_s += time.perf_counter() - t0
+        return self.problems[key]
+
+    def close(self):
+        for P in self.problems.values():
+            P.close()
+        self.problems.clear()
+
+
+def run_batch(args):
+    """Batched uneven Helmholtz solves: `--batch-count` problems of
+    workloads.uneven_specs, Jacobi-PCG to 1e-8 relative, FP64, advanced
+    together by nb_batch (one persistent Ax launch over every solve's
+    elements per iteration, graph replay, per-lx autotuned k-split), timed
+    against the same solves run one by one through nb_solve."""
+    import torch
+    import neko_b200 as nb
+    from neko_b200 import workloads
+    torch.cuda.set_device(0)
+    specs = workloads.uneven_specs(args.batch_count, seed=args.seed)
+    cache = GeometryCache(nb)
+    reqs = []
+    for sp in specs:
+        P = cache.get(sp)
+        f = workloads.uneven_rhs(P, sp["rhs_seed"])
+        r0 = math.sqrt(float((f * P.field("mult") * f).sum()) / P.volume)
+        reqs.append((sp, P, f, 1e-8 * r0))
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream()
+    # autotune once per lx on a small warm-up batch (the first-use cost)
+    B = nb.Batch()
+    warm = {}
+    for sp, P, f, tol in reqs:
+        warm.setdefault(sp["lx"], (sp, P, f, tol))
+    xs = []
+    for sp, P, f, tol in warm.values():
+        x = P.zeros()
+        xs.append(x)
+        B.submit(P, f, x, tol, 5000, h1=sp["h1"], h2=sp["h2"])
+    with torch.cuda.stream(stream):
+        B.run(stream=stream)
+    tuning = {lx: B.tuning(lx) for lx in sorted(warm)}
+    for q in range(len(warm)):
+        B.release(q)
+    # --- batched ---------------------------------------------------------
+    xb = [P.zeros() for _, P, _, _ in reqs]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    slots = [B.submit(P, f, x, tol, 5000, h1=sp["h1"], h2=sp["h2"])
+             for (sp, P, f, tol), x in zip(reqs, xb)]
+    with torch.cuda.stream(stream):
+        B.run(stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_batch = max(e0.elapsed_time(e1) / 1e3, 1e-9)
+    wall_batch = time.perf_counter() - t0
+    res_b = [B.result(s)[1] for s in slots]
+    # --- one by one ------------------------------------------------------
+    xs_seq, it_seq = [], []
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t1 = time.perf_counter()
+    e2.record(stream)
+    with torch.cuda.stream(stream):
+        for sp, P, f, tol in reqs:
+            h1 = torch.full((P.n,), sp["h1"], dtype=torch.float64, device="cuda")
+            P.set_coefficients(h1, torch.full_like(h1, sp["h2"]))
+            x = P.zeros()
+            mon = nb.CG(max_iter=5000, abs_tol=tol, M=nb.Jacobi()).solve(nb.AxHelm(), x, f, P.n, P,
+                                                                         stream=stream)
+            xs_seq.append(x)
+            it_seq.append(mon.iter)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t_seq = max(e2.elapsed_time(e3) / 1e3, 1e-9)
+    wall_seq = time.perf_counter() - t1
+    d_it = max(abs(a.iter - b) for a, b in zip(res_b, it_seq))
+    err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(xb, xs_seq))
+    conv = sum(1 for r in res_b if r.converged)
+    ndof = sum(P.n for _, P, _, _ in reqs)
+    line = {
+        "metric": "batched uneven Helmholtz solves/s to 1e-8 rel", "value": len(reqs) / t_batch,
+        "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic", "vs_baseline": None,
+        "config": {"workload": f"{len(reqs)} Jacobi-PCG Helmholtz solves, n^3 elements n~U{{2..16}}, "
+                               f"N~{{5,7,9}}, h1~U[0.5,2], h2~U[0,100], 8 deformation seeds, "
+                               f"zero Dirichlet, Fourier RHS ({ndof / 1e6:.0f}M DOF in total)",
+                   "geometries": len(cache.problems), "geometry_setup_s": cache.setup_s},
+        "batched_s": t_batch, "batched_wall_s": wall_batch,
+        "sequential": {"value": len(reqs) / t_seq, "seconds": t_seq, "wall_s": wall_seq,
+                       "path": "nb_solve one by one (set_coefficients + Jacobi-PCG graph)"},
+        "speedup_vs_sequential": t_seq / t_batch,
+        "converged": conv, "max_iter_diff_vs_sequential": d_it,
+        "max_rel_diff_vs_sequential": err,
+        "iterations": {"min": min(r.iter for r in res_b), "max": max(r.iter for r in res_b),
+                       "mean": sum(r.iter for r in res_b) / len(res_b)},
+        "autotune": {str(lx): {"ks": t[0], "candidate_ms": t[1]} for lx, t in tuning.items()},
+    }
+    print(json.dumps(line), flush=True)
+    B.close()
+    cache.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -268,6 +389,10 @@ def main():
                     help="skip the mixed-precision solve measured beside the FP64 one")
     ap.add_argument("--kernel-only", choices=["ax", "gs"], default=None,
                     help="run only this kernel on an nel^3 box (profiling case)")
+    ap.add_argument("--workload", choices=["solve", "batch", "serve"], default="solve",
+                    help="solve: the hsmg-FCG config-2 line (default); batch: batched "
+                         "uneven solves; serve: the served request stream")
+    ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--nel", type=int, default=16)
     ap.add_argument("--lx", type=int, default=8)
     args = ap.parse_args()
@@ -279,6 +404,8 @@ def main():
     cfg["lx"] = args.lx
     if args.kernel_only:
         return kernel_only(args, cfg)
+    if args.workload == "batch":
+        return run_batch(args)
     world, rank, local = dist_setup()
 
     if args.impl == "reference":

@@ -175,7 +175,9 @@ nb_status nb_problem_field(const nb_problem *p, const char *name, void **dptr);
 nb_status nb_problem_volume(const nb_problem *p, double *vol);
 
 /* Sets the Helmholtz coefficients from device arrays (n values each; h2 may
- * be NULL).  ifh2 enables the h2 B u term. */
+ * be NULL).  ifh2 enables the h2 B u term.  Synchronous: waits for all
+ * device work before reading the arrays and returns when the Jacobi
+ * diagonal (and any hsmg coarse level) has been updated. */
 nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1,
                                       const double *h2, int ifh2);
 
@@ -253,6 +255,13 @@ void nb_batch_destroy(nb_batch *b);
  * (device buffers that stay valid until release); returns its slot. */
 nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f, double *x,
                           double abs_tol, int max_iter, int *slot);
+/* The same with constant coefficients h1 > 0, h2 >= 0 (h2 > 0 adds h2 B)
+ * held by the slot instead of the problem's h1/h2 fields; the slot keeps
+ * its own Jacobi diagonal (5 n doubles charged), so one problem's mesh,
+ * geometric factors and gs maps can serve solves with different
+ * coefficients. */
+nb_status nb_batch_submit_coef(nb_batch *b, nb_problem *p, const double *f, double *x,
+                               double abs_tol, int max_iter, double h1, double h2, int *slot);
 /* Frees a slot (finished or not) and its budget. */
 nb_status nb_batch_release(nb_batch *b, int slot);
 /* Runs up to max_chunks graph replays (<= 0: until every solve finished);

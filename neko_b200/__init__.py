@@ -243,10 +243,17 @@ class Batch:
         self._h = h
         self._keep = {}
 
-    def submit(self, problem, f, x, abs_tol, max_iter=1000):
+    def submit(self, problem, f, x, abs_tol, max_iter=1000, h1=None, h2=0.0):
+        """Adds a solve; with h1 given, the solve uses the constant
+        coefficients h1, h2 instead of the problem's fields."""
         slot = ctypes.c_int()
-        check(load().nb_batch_submit(self._h, problem.handle, _ptr(f), _ptr(x), float(abs_tol),
-                                     int(max_iter), ctypes.byref(slot)))
+        if h1 is None:
+            check(load().nb_batch_submit(self._h, problem.handle, _ptr(f), _ptr(x),
+                                         float(abs_tol), int(max_iter), ctypes.byref(slot)))
+        else:
+            check(load().nb_batch_submit_coef(self._h, problem.handle, _ptr(f), _ptr(x),
+                                              float(abs_tol), int(max_iter), float(h1),
+                                              float(h2), ctypes.byref(slot)))
         self._keep[slot.value] = (problem, f, x)
         return slot.value
 

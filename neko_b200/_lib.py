@@ -90,6 +90,8 @@ SIGNATURES = {
     "nb_batch_create": (_I, [ctypes.c_int64, _P]),
     "nb_batch_destroy": (None, [_P]),
     "nb_batch_submit": (_I, [_P, _P, _P, _P, ctypes.c_double, _I, _IP]),
+    "nb_batch_submit_coef": (_I, [_P, _P, _P, _P, ctypes.c_double, _I, ctypes.c_double,
+                                  ctypes.c_double, _IP]),
     "nb_batch_release": (_I, [_P, _I]),
     "nb_batch_run": (_I, [_P, _I, _IP, _P]),
     "nb_batch_result": (_I, [_P, _I, _IP, _P]),

@@ -55,7 +55,8 @@ struct BSlot {
   double *r, *z, *p, *w;
   const double *g11, *g22, *g33, *g12, *g13, *g23, *h1, *h2, *B, *mult, *dinv, *D, *Dt;
   GsDevice gs;
-  int ifh2;
+  int ifh2, coef_scalar;  // coef_scalar: h1, h2 are the constants h1c, h2c
+  double h1c, h2c;
   int ax_first, ax_count, vc_first, vc_count;
   double rtz, pap, alpha, beta, rtr, rnorm, res_start, abs_tol, norm_fac;
   int iter, max_iter, done, nan;
@@ -124,7 +125,7 @@ __device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double 
           ut += sD[k + LX * l] * su[col + L2 * l];
         }
         const long idx = e * L3 + col + L2 * k;
-        const double H = __ldg(S.h1 + idx), G11 = __ldg(S.g11 + idx), G22 = __ldg(S.g22 + idx),
+        const double H = S.coef_scalar ? S.h1c : __ldg(S.h1 + idx), G11 = __ldg(S.g11 + idx), G22 = __ldg(S.g22 + idx),
                      G33 = __ldg(S.g33 + idx), G12 = __ldg(S.g12 + idx),
                      G13 = __ldg(S.g13 + idx), G23 = __ldg(S.g23 + idx);
         sur[col + L2 * k] = H * (G11 * ur + G12 * us + G13 * ut);
@@ -147,7 +148,8 @@ __device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double 
         const long idx = e * L3 + col + L2 * k;
         const double pv = su[col + L2 * k];
         double wv = a + b + d;
-        if (S.ifh2) wv = wv + __ldg(S.h2 + idx) * __ldg(S.B + idx) * pv;
+        if (S.ifh2)
+          wv = wv + (S.coef_scalar ? S.h2c : __ldg(S.h2 + idx)) * __ldg(S.B + idx) * pv;
         S.w[idx] = wv;
         acc += pv * wv;
       }
@@ -328,6 +330,22 @@ __global__ void __launch_bounds__(kBT)
   }
 }
 
+// Jacobi diagonal for constant coefficients: d = 1 / gs(h1 diag(A1) + h2 B),
+// the steps of nb_problem::update_jacobi with scalars (d holds diag(A1)).
+__global__ void batch_dinv_scale_kernel(double *d, double h1, double h2, const double *B, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    double v = d[i] * h1;
+    if (h2 != 0.0) v = v + h2 * B[i];
+    d[i] = v;
+  }
+}
+__global__ void batch_inv_kernel(double *d, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    d[i] = 1.0 / d[i];
+}
+
 }  // namespace nb
 
 // ---------------------------------------------------------------------------
@@ -347,6 +365,8 @@ struct SlotHost {
   double abs_tol = 0.0;
   int max_iter = 0;
   bool started = false;  // init kernel run
+  bool coef_scalar = false;
+  double h1c = 1.0, h2c = 0.0;
 };
 
 }  // namespace
@@ -465,6 +485,13 @@ static nb_status rebuild(nb_batch *b, std::vector<BSlot> &host_slots) {
     S.D = P->D, S.Dt = P->Dt;
     S.gs = P->gsd;
     S.ifh2 = P->ifh2 ? 1 : 0;
+    S.coef_scalar = H.coef_scalar ? 1 : 0;
+    S.h1c = H.h1c;
+    S.h2c = H.h2c;
+    if (H.coef_scalar) {
+      S.dinv = H.vec + 4 * P->n;
+      S.ifh2 = H.h2c != 0.0;
+    }
     if (!H.started) {
       S.abs_tol = H.abs_tol;
       S.max_iter = H.max_iter;
@@ -696,13 +723,14 @@ extern "C" nb_status nb_batch_create(int64_t hbm_budget_bytes, nb_batch **out) {
 
 extern "C" void nb_batch_destroy(nb_batch *b) { delete b; }
 
-extern "C" nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f, double *x,
-                                     double abs_tol, int max_iter, int *slot) {
+static nb_status submit(nb_batch *b, nb_problem *p, const double *f, double *x, double abs_tol,
+                        int max_iter, bool scalar, double h1, double h2, int *slot) {
   if (!b || !p || !f || !x || !slot) return bfail(NB_ERR_ARG, "null argument");
   if (max_iter < 1) return bfail(NB_ERR_ARG, "max_iter must be >= 1");
   if (variant_index(p->lx, 1) < 0)
     return bfail(NB_ERR_UNSUPPORTED, "batched solves support lx 4, 6, 8, 10");
-  const size_t bytes = 4 * (size_t)p->n * sizeof(double);
+  if (scalar && !(h1 > 0.0 && h2 >= 0.0)) return bfail(NB_ERR_ARG, "need h1 > 0, h2 >= 0");
+  const size_t bytes = (scalar ? 5 : 4) * (size_t)p->n * sizeof(double);
   if (b->used + bytes > b->budget) return bfail(NB_ERR_OOM, "batch: over the HBM budget");
   SlotHost h;
   h.used = true;
@@ -712,9 +740,32 @@ extern "C" nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f
   h.abs_tol = abs_tol;
   h.max_iter = max_iter;
   h.bytes = bytes;
+  h.coef_scalar = scalar;
+  h.h1c = h1;
+  h.h2c = h2;
   cudaError_t e = cudaMalloc(&h.vec, bytes);
   if (e != cudaSuccess) return bfail(NB_ERR_OOM, "batch: slot vectors");
-  cudaMemset(h.vec, 0, bytes);
+  e = cudaMemset(h.vec, 0, bytes);
+  if (e == cudaSuccess && scalar) {
+    double *d = h.vec + 4 * p->n;
+    const int fg = stream_grid(p->n, 256);
+    e = jacobi_diag(d, p->Dt, p->Dt, p->Dt, p->g11, p->g22, p->g33, p->g12, p->g13, p->g23,
+                    p->dfrmd, false, p->nelv, p->lx, nullptr);
+    if (e == cudaSuccess) {
+      batch_dinv_scale_kernel<<<fg, 256>>>(d, h1, h2, p->B, p->n);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = gs_add_fused<double>(p->gsd, d, false, nullptr);
+    if (e == cudaSuccess) {
+      batch_inv_kernel<<<fg, 256>>>(d, p->n);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  if (e != cudaSuccess) {
+    cudaFree(h.vec);
+    return bfail(NB_ERR_CUDA, std::string("batch submit: ") + cudaGetErrorString(e));
+  }
   int s = -1;
   for (size_t q = 0; q < b->slots.size(); q++)
     if (!b->slots[q].used) {
@@ -731,6 +782,17 @@ extern "C" nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f
   b->dirty = true;
   *slot = s;
   return NB_OK;
+}
+
+extern "C" nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f, double *x,
+                                     double abs_tol, int max_iter, int *slot) {
+  return submit(b, p, f, x, abs_tol, max_iter, false, 1.0, 0.0, slot);
+}
+
+extern "C" nb_status nb_batch_submit_coef(nb_batch *b, nb_problem *p, const double *f,
+                                          double *x, double abs_tol, int max_iter, double h1,
+                                          double h2, int *slot) {
+  return submit(b, p, f, x, abs_tol, max_iter, true, h1, h2, slot);
 }
 
 extern "C" nb_status nb_batch_release(nb_batch *b, int slot) {

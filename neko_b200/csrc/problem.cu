@@ -428,6 +428,10 @@ extern "C" nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1
                                                  const double *h2, int ifh2) {
   if (!p || !h1) return fail(NB_ERR_ARG, "null argument");
   if (ifh2 && !h2) return fail(NB_ERR_ARG, "ifh2 needs h2");
+  // Synchronous: the inputs may come from any stream, so wait for all work
+  // before reading them (a device-to-device cudaMemcpy orders only with the
+  // legacy stream).
+  NB_TRY(cudaDeviceSynchronize());
   NB_TRY(cudaMemcpy(p->h1, h1, p->n * 8, cudaMemcpyDeviceToDevice));
   if (h2) NB_TRY(cudaMemcpy(p->h2, h2, p->n * 8, cudaMemcpyDeviceToDevice));
   p->ifh2 = ifh2 != 0;

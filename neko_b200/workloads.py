@@ -63,3 +63,38 @@ def config1_pointwise(x, y, z, xi_cont):
     else:
         s = np.sin
     return 3 * pi ** 2 * s(pi * x) * s(pi * y) * s(pi * z) + xi_cont
+
+
+# --- config 4/5: uneven Helmholtz problems -----------------------------------
+N_DEFORM_SEEDS = 8
+
+
+def deform_amplitude(dseed):
+    """Deformation amplitude of deformation seed `dseed` (U[0, 0.1])."""
+    return float(np.random.default_rng(1000 + dseed).uniform(0.0, 0.1))
+
+
+def uneven_specs(count=512, seed=4):
+    """Problem descriptions of the batched / served workloads: a box of n^3
+    elements with n ~ U{2..16}, N ~ {5, 7, 9} (lx = N + 1), h1 ~ U[0.5, 2],
+    h2 ~ U[0, 100], a deformation seed (8 seeds, amplitude U[0, 0.1] each),
+    zero Dirichlet on the box faces and a Fourier-mode right-hand side."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        out.append(dict(n=int(rng.integers(2, 17)), lx=int(rng.choice([5, 7, 9])) + 1,
+                        h1=float(rng.uniform(0.5, 2.0)), h2=float(rng.uniform(0.0, 100.0)),
+                        dseed=int(rng.integers(0, N_DEFORM_SEEDS)), rhs_seed=int(seed * 100003 + i)))
+    return out
+
+
+def uneven_rhs(P, rhs_seed, kmax=3):
+    """B f with f a seeded Fourier series on the unit box (device tensor),
+    assembled and masked."""
+    x, y, z, B = (P.field(k) for k in ("x", "y", "z", "B"))
+    two_pi = 2 * math.pi
+    f = B * fourier_field(two_pi * x, two_pi * y, two_pi * z, rhs_seed, kmax)
+    f = f.contiguous()
+    P.gs.op(f)
+    P.bclst.apply(f)
+    return f

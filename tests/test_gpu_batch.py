@@ -139,3 +139,35 @@ def test_batch_rejects_unsupported_lx(nb):
     with pytest.raises(nb.NekoB200Error):
         B.submit(P, P.zeros(), P.zeros(), 1e-8)
     B.close()
+
+
+def test_scalar_coefficients_share_geometry(nb):
+    """Slots with constant coefficients on one shared problem (mesh, G, gs
+    maps built once) equal solves on problems whose h1/h2 fields hold the
+    same constants."""
+    B = nb.Batch()
+    shared = nb.Problem((3, 4, 3), 8, deform=0.07)
+    rng = np.random.default_rng(17)
+    cases = [(1.3, 0.0), (0.6, 45.0), (1.9, 7.5)]
+    fs, xs, slots = [], [], []
+    for h1, h2 in cases:
+        f = torch.as_tensor(rng.standard_normal(shared.n), device="cuda") * shared.field("B")
+        shared.gs.op(f)
+        shared.bclst.apply(f)
+        x = shared.zeros()
+        fs.append(f)
+        xs.append(x)
+        slots.append(B.submit(shared, f, x, 1e-11, 3000, h1=h1, h2=h2))
+    B.run()
+    for (h1, h2), f, x, s in zip(cases, fs, xs, slots):
+        P = nb.Problem((3, 4, 3), 8, deform=0.07)
+        c1 = torch.full((P.n,), h1, dtype=torch.float64, device="cuda")
+        if h2:
+            P.set_coefficients(c1, torch.full_like(c1, h2))
+        else:
+            P.set_coefficients(c1)
+        xa, ma = _alone(nb, P, f, 1e-11, 3000)
+        done, mon = B.result(s)
+        assert done and mon.converged and abs(mon.iter - ma.iter) <= 1, (mon.iter, ma.iter)
+        assert float(torch.linalg.norm(x - xa) / torch.linalg.norm(xa)) < 1e-9
+    B.close()
