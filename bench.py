@@ -249,31 +249,6 @@ def kernel_only(args, cfg):
     print(json.dumps({"kernel": args.kernel_only, "n": P.n, "launches": args.warmup + args.steps}))
 
 
-class GeometryCache:
-    """Device-resident problems keyed by (n, lx, deformation seed): mesh,
-    geometric factors and gs maps built once and shared by every solve of
-    that shape."""
-
-    def __init__(self, nb):
-        self.nb, self.problems, self.setup_s = nb, {}, 0.0
-
-    def get(self, spec):
-        from neko_b200 import workloads
-        key = (spec["n"], spec["lx"], spec["dseed"])
-        if key not in self.problems:
-            t0 = time.perf_counter()
-            self.problems[key] = self.nb.Problem((spec["n"],) * 3, spec["lx"],
-                                                 deform=workloads.deform_amplitude(spec["dseed"]),
-                                                 dirichlet=True)
-            self.setup_s += time.perf_counter() - t0
-        return self.problems[key]
-
-    def close(self):
-        for P in self.problems.values():
-            P.close()
-        self.problems.clear()
-
-
 def run_batch(args):
     """Batched uneven Helmholtz solves: `--batch-count` problems of
     workloads.uneven_specs, Jacobi-PCG to 1e-8 relative, FP64, advanced
@@ -284,8 +259,9 @@ def run_batch(args):
     import neko_b200 as nb
     from neko_b200 import workloads
     torch.cuda.set_device(0)
+    from neko_b200.serve import GeometryCache
     specs = workloads.uneven_specs(args.batch_count, seed=args.seed)
-    cache = GeometryCache(nb)
+    cache = GeometryCache()
     reqs = []
     for sp in specs:
         P = cache.get(sp)
@@ -370,6 +346,66 @@ def run_batch(args):
     cache.close()
 
 
+def run_serve(args):
+    """Served request stream: open-loop Poisson arrivals at each of
+    --serve-rates, --serve-requests requests per rate drawn as the batched
+    workload, answered (a) by the continuous-batching server under a
+    --serve-budget-gb HBM budget and (b) one request at a time with
+    nb_solve; latency percentiles and solves/s for both."""
+    import numpy as np
+    import torch
+    import neko_b200 as nb
+    from neko_b200 import serve, workloads
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    cache = serve.GeometryCache()
+    pool = serve.RhsPool(cache)
+    all_specs = {rate: workloads.uneven_specs(args.serve_requests, seed=args.seed + 17 * q)
+                 for q, rate in enumerate(rates)}
+    for specs in all_specs.values():  # warm the geometry cache and payloads
+        for sp in specs:
+            pool.get(sp)
+    torch.cuda.synchronize()
+    budget = int(args.serve_budget_gb * 1e9) - cache.device_bytes()
+    B = nb.Batch(hbm_budget=max(budget, 1))
+    warm = {}
+    for specs in all_specs.values():
+        for sp in specs:
+            warm.setdefault(sp["lx"], sp)
+    serve.serve_batched(list(warm.values()), np.zeros(len(warm)), pool, budget, batch=B)
+    out = {}
+    for q, rate in enumerate(rates):
+        specs = all_specs[rate]
+        t_arr = serve.arrivals(rate, len(specs), seed=args.seed + q)
+        lat, it, conv, span, _ = serve.serve_batched(specs, t_arr, pool, budget, batch=B)
+        lat_s, it_s, conv_s, span_s = serve.serve_sequential(specs, t_arr, pool)
+        out[str(int(rate))] = {
+            "batched": dict(serve.percentiles(lat), solves_per_s=len(specs) / span,
+                            converged=int(sum(conv)), mean_iter=float(np.mean(it))),
+            "one_by_one": dict(serve.percentiles(lat_s), solves_per_s=len(specs) / span_s,
+                               converged=int(sum(conv_s)), mean_iter=float(np.mean(it_s))),
+            "max_iter_diff": int(max(abs(a - b) for a, b in zip(it, it_s))),
+            "arrival_span_s": float(t_arr[-1]),
+        }
+    line = {
+        "metric": "served Helmholtz solves: p50/p95/p99 latency (ms) and solves/s",
+        "value": out[str(int(rates[0]))]["batched"]["p99_ms"],
+        "unit": "ms (p99 at the first rate)", "higher_is_better": False, "n_gpus": 1,
+        "dtype": "f64", "data": "synthetic", "vs_baseline": None,
+        "config": {"workload": f"{args.serve_requests} requests per rate, open-loop Poisson "
+                               f"arrivals, shapes/orders/coefficients as the batched workload, "
+                               f"Jacobi-PCG to 1e-8 rel, FP64, HBM budget "
+                               f"{args.serve_budget_gb:.0f} GB, geometry cached by "
+                               f"(n, lx, deformation seed)",
+                   "rates_per_s": rates, "geometries": len(cache.problems),
+                   "geometry_setup_s": cache.setup_s},
+        "rates": out,
+    }
+    print(json.dumps(line), flush=True)
+    B.close()
+    cache.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -393,6 +429,9 @@ def main():
                     help="solve: the hsmg-FCG config-2 line (default); batch: batched "
                          "uneven solves; serve: the served request stream")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--serve-rates", default="200,1000,5000")
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--nel", type=int, default=16)
     ap.add_argument("--lx", type=int, default=8)
     args = ap.parse_args()
@@ -406,6 +445,8 @@ def main():
         return kernel_only(args, cfg)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     world, rank, local = dist_setup()
 
     if args.impl == "reference":

@@ -382,7 +382,10 @@ struct nb_batch {
   double *d_part3 = nullptr, *d_part5 = nullptr;
   unsigned *d_head = nullptr;
   int *d_var = nullptr;
-  size_t cap_slots = 0, cap_items = 0, cap_vchunks = 0, cap_gchunks = 0;
+  size_t cap_slots = 0, cap_items = 0, cap_vchunks = 0, cap_gchunks = 0, cap_part3 = 0,
+         cap_part5 = 0;
+  std::vector<BSlot> mirror;  // slot states as of the end of the last run
+  bool mirror_valid = false;
   int nitems = 0, nvchunks = 0, ngchunks = 0;
   std::vector<int> ks_of_lx = std::vector<int>(17, 0);  // 0 = not tuned
   int var_of_lx[17] = {0};
@@ -522,11 +525,8 @@ static nb_status rebuild(nb_batch *b, std::vector<BSlot> &host_slots) {
   NB_BTRY(grow(b->d_items, b->cap_items, std::max<size_t>(items.size(), 1)));
   NB_BTRY(grow(b->d_vchunks, b->cap_vchunks, std::max<size_t>(vch.size(), 1)));
   NB_BTRY(grow(b->d_gchunks, b->cap_gchunks, std::max<size_t>(gch.size(), 1)));
-  cudaFree(b->d_part3);
-  cudaFree(b->d_part5);
-  b->d_part3 = b->d_part5 = nullptr;
-  NB_BTRY(cudaMalloc(&b->d_part3, std::max<size_t>(items.size(), 1) * sizeof(double)));
-  NB_BTRY(cudaMalloc(&b->d_part5, 2 * std::max<size_t>(vch.size(), 1) * sizeof(double)));
+  NB_BTRY(grow(b->d_part3, b->cap_part3, std::max<size_t>(items.size(), 1)));
+  NB_BTRY(grow(b->d_part5, b->cap_part5, 2 * std::max<size_t>(vch.size(), 1)));
   if (ns) NB_BTRY(cudaMemcpy(b->d_slots, host_slots.data(), ns * sizeof(BSlot), cudaMemcpyHostToDevice));
   if (!items.empty())
     NB_BTRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(AxItem), cudaMemcpyHostToDevice));
@@ -639,6 +639,7 @@ static nb_status autotune_lx(nb_batch *b, int lx, cudaStream_t s) {
 
 static nb_status prepare(nb_batch *b, cudaStream_t s) {
   if (!b->dirty) return NB_OK;
+  b->mirror_valid = false;
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -799,10 +800,22 @@ extern "C" nb_status nb_batch_release(nb_batch *b, int slot) {
   if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
     return bfail(NB_ERR_ARG, "no such slot");
   SlotHost &h = b->slots[slot];
+  if (h.started && !b->dirty) {
+    // The captured queues stay valid: a finished slot is skipped by every
+    // kernel before it touches its vectors; an unfinished one is stopped.
+    const bool finished = b->mirror_valid && slot < (int)b->mirror.size() && b->mirror[slot].done;
+    if (!finished) {
+      const int one = 1;
+      NB_BTRY(cudaMemcpy(&b->d_slots[slot].done, &one, sizeof(int), cudaMemcpyHostToDevice));
+    }
+  } else {
+    b->dirty = true;
+  }
+  NB_BTRY(cudaDeviceSynchronize());
   cudaFree(h.vec);
   b->used -= h.bytes;
   h = SlotHost{};
-  b->dirty = true;
+  if (b->mirror_valid && slot < (int)b->mirror.size()) b->mirror[slot].done = 1;
   return NB_OK;
 }
 
@@ -814,13 +827,16 @@ extern "C" nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void
   nb_status st = prepare(b, s);
   if (st != NB_OK) return st;
   const int ns = (int)b->slots.size();
-  std::vector<BSlot> hs(ns);
+  std::vector<BSlot> &hs = b->mirror;
+  hs.resize(ns);
+  b->mirror_valid = false;
   int left = 0;
   for (int c = 0; max_chunks <= 0 || c < max_chunks; c++) {
     if (ns == 0) break;
     NB_BTRY(cudaGraphLaunch(b->graph, s));
     NB_BTRY(cudaMemcpyAsync(hs.data(), b->d_slots, ns * sizeof(BSlot), cudaMemcpyDeviceToHost, s));
     NB_BTRY(cudaStreamSynchronize(s));
+    b->mirror_valid = true;
     left = 0;
     for (int q = 0; q < ns; q++)
       if (b->slots[q].used && !hs[q].done) left++;
@@ -839,7 +855,10 @@ extern "C" nb_status nb_batch_result(nb_batch *b, int slot, int *done, nb_solve_
     return NB_OK;
   }
   BSlot S;
-  NB_BTRY(cudaMemcpy(&S, b->d_slots + slot, sizeof(BSlot), cudaMemcpyDeviceToHost));
+  if (b->mirror_valid && !b->dirty && slot < (int)b->mirror.size())
+    S = b->mirror[slot];
+  else
+    NB_BTRY(cudaMemcpy(&S, b->d_slots + slot, sizeof(BSlot), cudaMemcpyDeviceToHost));
   if (done) *done = S.done;
   if (res) {
     res->iter = S.iter;

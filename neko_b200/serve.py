@@ -1,0 +1,162 @@
+"""Serving loop for streams of Helmholtz solve requests.
+
+Requests (a problem shape (n, N, deformation seed), constant coefficients
+h1, h2 and a right-hand side) arrive open-loop.  The server keeps every
+shape's mesh, geometric factors and gather-scatter maps resident on the
+device (GeometryCache, keyed by (n, lx, deformation seed)), admits requests
+into a Batch while their work vectors fit the HBM budget, and advances all
+admitted solves together one graph chunk at a time: a request that arrives
+while others are on the GPU joins at the next chunk boundary, and a finished
+request leaves at the next one (continuous batching).  Latency is measured
+from arrival to the chunk boundary at which its solve was seen finished.
+
+The one-by-one server (serve_sequential) answers the same stream with
+nb_solve, one request at a time in arrival order.
+"""
+import collections
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import AxHelm, Batch, CG, Jacobi, NekoB200Error, Problem
+from . import workloads
+from ._lib import NB_ERR_OOM
+
+
+class GeometryCache:
+    """Device-resident problems keyed by (n, lx, deformation seed)."""
+
+    def __init__(self):
+        self.problems = {}
+        self.setup_s = 0.0
+        self.misses = 0
+
+    def key(self, spec):
+        return (spec["n"], spec["lx"], spec["dseed"])
+
+    def get(self, spec):
+        k = self.key(spec)
+        P = self.problems.get(k)
+        if P is None:
+            t0 = time.perf_counter()
+            P = Problem((spec["n"],) * 3, spec["lx"],
+                        deform=workloads.deform_amplitude(spec["dseed"]), dirichlet=True)
+            self.setup_s += time.perf_counter() - t0
+            self.misses += 1
+            self.problems[k] = P
+        return P
+
+    def device_bytes(self):
+        """Approximate HBM held by the cached problems (20 arrays of n)."""
+        return sum(P.n * 8 * 20 for P in self.problems.values())
+
+    def close(self):
+        for P in self.problems.values():
+            P.close()
+        self.problems.clear()
+
+
+class RhsPool:
+    """A few seeded right-hand sides per shape, built once (the request
+    payload: a request uses variant rhs_seed % per_shape of its shape)."""
+
+    def __init__(self, cache, per_shape=2):
+        self.cache, self.per_shape, self.pool = cache, per_shape, {}
+
+    def get(self, spec):
+        P = self.cache.get(spec)
+        v = spec["rhs_seed"] % self.per_shape
+        k = (self.cache.key(spec), v)
+        if k not in self.pool:
+            f = workloads.uneven_rhs(P, 7919 * v + spec["n"])
+            r0 = math.sqrt(float((f * P.field("mult") * f).sum()) / P.volume)
+            self.pool[k] = (f, r0)
+        return P, self.pool[k][0], self.pool[k][1]
+
+
+def arrivals(rate, count, seed):
+    """Open-loop Poisson arrival times (s) of `count` requests at `rate`/s."""
+    gaps = np.random.default_rng(seed).exponential(1.0 / rate, count)
+    return np.cumsum(gaps)
+
+
+def percentiles(lat):
+    a = np.sort(np.asarray(lat, dtype=np.float64))
+    return {"p50_ms": float(np.percentile(a, 50) * 1e3),
+            "p95_ms": float(np.percentile(a, 95) * 1e3),
+            "p99_ms": float(np.percentile(a, 99) * 1e3), "max_ms": float(a[-1] * 1e3)}
+
+
+def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000, chunk_runs=1,
+                  batch=None, stream=None):
+    """Continuous-batching server.  Returns per-request latency (s),
+    iterations, convergence flags, the span of the run (s) and the solutions
+    (request index -> device tensor)."""
+    own = batch is None
+    B = batch if batch is not None else Batch(hbm_budget=budget_bytes)
+    n = len(specs)
+    lat, iters, conv = [None] * n, [0] * n, [False] * n
+    xs, active = {}, {}
+    waiting = collections.deque()
+    nxt, done_count = 0, 0
+    t0 = time.perf_counter()
+    while done_count < n:
+        now = time.perf_counter() - t0
+        while nxt < n and t_arr[nxt] <= now:
+            waiting.append(nxt)
+            nxt += 1
+        while waiting:  # admission in arrival order while the budget allows
+            i = waiting[0]
+            sp = specs[i]
+            P, f, r0 = pool.get(sp)
+            x = torch.empty(P.n, dtype=torch.float64, device="cuda")
+            try:
+                slot = B.submit(P, f, x, rel_tol * r0, max_iter, h1=sp["h1"], h2=sp["h2"])
+            except NekoB200Error as e:  # over budget: wait for slots to free
+                if e.status != NB_ERR_OOM or not active:
+                    raise
+                break
+            waiting.popleft()
+            active[slot] = i
+            xs[i] = x
+        if not active:
+            if nxt < n:
+                time.sleep(max(0.0, t_arr[nxt] - (time.perf_counter() - t0)))
+            continue
+        B.run(max_chunks=chunk_runs, stream=stream)
+        now = time.perf_counter() - t0
+        for slot, i in list(active.items()):
+            done, mon = B.result(slot)
+            if done:
+                lat[i] = now - t_arr[i]
+                iters[i], conv[i] = mon.iter, mon.converged
+                B.release(slot)
+                del active[slot]
+                done_count += 1
+    span = time.perf_counter() - t0
+    if own:
+        B.close()
+    return lat, iters, conv, span, xs
+
+
+def serve_sequential(specs, t_arr, pool, rel_tol=1e-8, max_iter=5000):
+    """One request at a time with nb_solve, in arrival order."""
+    n = len(specs)
+    lat, iters, conv = [None] * n, [0] * n, [False] * n
+    t0 = time.perf_counter()
+    for i, sp in enumerate(specs):
+        now = time.perf_counter() - t0
+        if t_arr[i] > now:
+            time.sleep(t_arr[i] - now)
+        P, f, r0 = pool.get(sp)
+        h1 = torch.full((P.n,), sp["h1"], dtype=torch.float64, device="cuda")
+        P.set_coefficients(h1, torch.full_like(h1, sp["h2"]))
+        x = P.zeros()
+        mon = CG(max_iter=max_iter, abs_tol=rel_tol * r0, M=Jacobi()).solve(AxHelm(), x, f,
+                                                                           P.n, P)
+        torch.cuda.synchronize()
+        lat[i] = time.perf_counter() - t0 - t_arr[i]
+        iters[i], conv[i] = mon.iter, mon.converged
+    return lat, iters, conv, time.perf_counter() - t0
