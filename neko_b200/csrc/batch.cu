@@ -607,6 +607,7 @@ static nb_status autotune_lx(nb_batch *b, int lx, cudaStream_t s) {
     int var[17];
     for (int q = 0; q <= 16; q++) var[q] = q == lx ? v : -1;
     cudaMemcpy(b->d_var, var, sizeof(var), cudaMemcpyHostToDevice);
+    cudaDeviceSynchronize();  // legacy-stream copies before the timed launches on s
     cudaFuncSetAttribute(batch_ax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          std::max(smem, b->smem_bytes));
     float ms = 0;
@@ -660,6 +661,7 @@ static nb_status prepare(nb_batch *b, cudaStream_t s) {
           tmp[q].rtz = 1.0;
         }
       NB_BTRY(cudaMemcpy(b->d_slots, tmp.data(), tmp.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
+      NB_BTRY(cudaDeviceSynchronize());
       st = autotune_lx(b, sh.P->lx, s);
       if (st != NB_OK) return st;
       NB_BTRY(cudaMemcpy(b->d_slots, hs.data(), hs.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
@@ -678,6 +680,7 @@ static nb_status prepare(nb_batch *b, cudaStream_t s) {
     for (size_t q = 0; q < tmp.size(); q++)
       if (!b->slots[q].used || b->slots[q].started) tmp[q].done = 1;
     NB_BTRY(cudaMemcpy(b->d_slots, tmp.data(), tmp.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
+    NB_BTRY(cudaDeviceSynchronize());  // legacy-stream copies before work on s
     if (b->nvchunks > 0) batch_init_kernel<<<b->nvchunks, kBT, 0, s>>>(b->d_slots, b->d_vchunks, b->d_part5);
     NB_BTRY(cudaGetLastError());
     NB_BTRY(cudaStreamSynchronize(s));
@@ -690,6 +693,9 @@ static nb_status prepare(nb_batch *b, cudaStream_t s) {
       }
     NB_BTRY(cudaMemcpy(b->d_slots, hs.data(), hs.size() * sizeof(BSlot), cudaMemcpyHostToDevice));
   }
+  // The tables above were written by legacy-stream copies, which do not
+  // order with the caller's (possibly non-blocking) stream.
+  NB_BTRY(cudaDeviceSynchronize());
   // capture `chunk` iterations
   if (!b->cap_stream) NB_BTRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
   cudaGraph_t g;

@@ -282,6 +282,10 @@ cudaError_t CgWorkspace::ensure(long n_) {
   st = (CgState *)(b + 4 * vec + red);
   e = cudaMemset(b + 4 * vec, 0, red + sizeof(CgState));
   if (e != cudaSuccess) return e;
+  // The memset runs on the legacy stream, which does not order with a
+  // caller's non-blocking stream: finish it before the solve's kernels.
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return e;
   if (!host_state) {
     e = cudaMallocHost(&host_state, sizeof(CgState));
     if (e != cudaSuccess) return e;

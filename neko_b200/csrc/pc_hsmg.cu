@@ -43,7 +43,7 @@ namespace nb {
 // back to (i,j,k) and every pass reads one contiguous line of NL values per
 // thread into registers; the NL x NL matrix of the pass is read as a
 // broadcast.  The inverse eigenvalue sums are rebuilt from the three
-// spectra (zero where the sum is <= eps, as fdm_setup_fast).
+// spectra (1/sum, zero where the sum is <= eps, as fdm_setup_fast).
 template <typename TIN, typename T, int NL>
 __device__ __forceinline__ void fdm_pass(const T *__restrict__ in, T *__restrict__ out,
                                          const T *__restrict__ M, int t) {
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(NL *NL *NE)
 #pragma unroll
       for (int l = 0; l < NL; l++) s += M[l + NL * k] * line[l];
       const T diag = lij + sL[2 * NL + k];
-      b1[t + N2 * k] = diag > ep ? s / diag : T(0);
+      b1[t + N2 * k] = s * (diag > ep ? T(1) / diag : T(0));
     }
   }
   __syncthreads();
@@ -528,6 +528,7 @@ struct HsmgImpl : public HsmgState {
     if (v) {  // leave the barrier words at rest for the next launch
       cudaMemset(ca.err, 0, sizeof(int));
       cudaMemset(ca.bar, 0, 2 * sizeof(unsigned));
+      cudaDeviceSynchronize();
     }
     return v;
   }
@@ -788,6 +789,10 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   lagrange_matrix(zm, zc, Jmc);
   st = mixed ? upload_impl((HsmgImpl<float> *)H, hf, hm, Jfm, Jmc)
              : upload_impl((HsmgImpl<double> *)H, hf, hm, Jfm, Jmc);
+  // The uploads ran on the legacy stream (a pageable cudaMemcpy may return
+  // before its DMA lands); finish them before any caller stream reads them.
+  if (st == NB_OK && cudaDeviceSynchronize() != cudaSuccess)
+    st = hfail(NB_ERR_CUDA, "hsmg: upload failed");
   if (st != NB_OK) {
     delete H;
     return st;
