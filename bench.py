@@ -108,14 +108,37 @@ def dist_setup():
     return world, rank, local
 
 
+def _reduce_device():
+    import torch.distributed as dist
+    return "cpu" if dist.get_backend() == "gloo" else "cuda"
+
+
 def max_over_ranks(v, world):
+    """Largest value over the ranks (device times: the job ends with the
+    slowest rank)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=_reduce_device())
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def shard(items, rank, world):
+    """This rank's share of independent work items (replicas: item i goes
+    to rank i mod world)."""
+    return [it for i, it in enumerate(items) if i % world == rank]
 
 
 def barrier(world):
@@ -258,9 +281,11 @@ def run_batch(args):
     import torch
     import neko_b200 as nb
     from neko_b200 import workloads
-    torch.cuda.set_device(0)
     from neko_b200.serve import GeometryCache
-    specs = workloads.uneven_specs(args.batch_count, seed=args.seed)
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    # replicas: each GPU solves its share of the independent problems
+    specs = shard(workloads.uneven_specs(args.batch_count, seed=args.seed), rank, world)
     cache = GeometryCache()
     reqs = []
     for sp in specs:
@@ -288,6 +313,7 @@ def run_batch(args):
     # --- batched ---------------------------------------------------------
     xb = [P.zeros() for _, P, _, _ in reqs]
     torch.cuda.synchronize()
+    barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream)
@@ -297,12 +323,14 @@ def run_batch(args):
         B.run(stream=stream)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_batch = max(e0.elapsed_time(e1) / 1e3, 1e-9)
+    barrier(world)
+    t_batch = max_over_ranks(max(e0.elapsed_time(e1) / 1e3, 1e-9), world)
     wall_batch = time.perf_counter() - t0
     res_b = [B.result(s)[1] for s in slots]
     # --- one by one ------------------------------------------------------
     xs_seq, it_seq = [], []
     torch.cuda.synchronize()
+    barrier(world)
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t1 = time.perf_counter()
     e2.record(stream)
@@ -317,22 +345,27 @@ def run_batch(args):
             it_seq.append(mon.iter)
     e3.record(stream)
     torch.cuda.synchronize()
-    t_seq = max(e2.elapsed_time(e3) / 1e3, 1e-9)
+    barrier(world)
+    t_seq = max_over_ranks(max(e2.elapsed_time(e3) / 1e3, 1e-9), world)
     wall_seq = time.perf_counter() - t1
     d_it = max(abs(a.iter - b) for a, b in zip(res_b, it_seq))
     err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(xb, xs_seq))
-    conv = sum(1 for r in res_b if r.converged)
-    ndof = sum(P.n for _, P, _, _ in reqs)
+    conv = int(sum_over_ranks(sum(1 for r in res_b if r.converged), world))
+    d_it = int(max_over_ranks(d_it, world))
+    err = max_over_ranks(err, world)
+    ndof = sum_over_ranks(sum(P.n for _, P, _, _ in reqs), world)
+    total = args.batch_count
     line = {
-        "metric": "batched uneven Helmholtz solves/s to 1e-8 rel", "value": len(reqs) / t_batch,
-        "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
-        "data": "synthetic", "vs_baseline": None,
-        "config": {"workload": f"{len(reqs)} Jacobi-PCG Helmholtz solves, n^3 elements n~U{{2..16}}, "
+        "metric": "batched uneven Helmholtz solves/s to 1e-8 rel", "value": total / t_batch,
+        "unit": "solves/s", "n_gpus": world, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic", "vs_baseline": None, "scaling": "strong",
+        "parallelism": "replicas x%d" % world,
+        "config": {"workload": f"{total} Jacobi-PCG Helmholtz solves, n^3 elements n~U{{2..16}}, "
                                f"N~{{5,7,9}}, h1~U[0.5,2], h2~U[0,100], 8 deformation seeds, "
                                f"zero Dirichlet, Fourier RHS ({ndof / 1e6:.0f}M DOF in total)",
                    "geometries": len(cache.problems), "geometry_setup_s": cache.setup_s},
         "batched_s": t_batch, "batched_wall_s": wall_batch,
-        "sequential": {"value": len(reqs) / t_seq, "seconds": t_seq, "wall_s": wall_seq,
+        "sequential": {"value": total / t_seq, "seconds": t_seq, "wall_s": wall_seq,
                        "path": "nb_solve one by one (set_coefficients + Jacobi-PCG graph)"},
         "speedup_vs_sequential": t_seq / t_batch,
         "converged": conv, "max_iter_diff_vs_sequential": d_it,
@@ -341,9 +374,13 @@ def run_batch(args):
                        "mean": sum(r.iter for r in res_b) / len(res_b)},
         "autotune": {str(lx): {"ks": t[0], "candidate_ms": t[1]} for lx, t in tuning.items()},
     }
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     B.close()
     cache.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def run_serve(args):
@@ -429,6 +466,9 @@ def main():
                     help="solve: the hsmg-FCG config-2 line (default); batch: batched "
                          "uneven solves; serve: the served request stream")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--coarse-tol", type=float, default=1e-9,
+                    help="hsmg coarse CG absolute tolerance (reference KSP_ABS_TOL 1e-9; "
+                         "1e-4 is the config-2 variant)")
     ap.add_argument("--serve-rates", default="200,1000,5000")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
@@ -467,7 +507,8 @@ def main():
     if args.pc == "jacobi":
         solver = nb.CG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Jacobi())
     else:  # hsmg is not symmetric: flexible CG (plain CG stalls with it)
-        solver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Hsmg())
+        solver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol,
+                        M=nb.Hsmg(coarse_tol=args.coarse_tol))
     Ax = nb.AxHelm()
     x = P.zeros()
     stream = torch.cuda.Stream()
@@ -520,7 +561,8 @@ def main():
     mixed = None
     if args.pc == "hsmg" and not args.no_mixed:
         x64 = x.clone()
-        msolver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Hsmg(mixed=True))
+        msolver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol,
+                         M=nb.Hsmg(coarse_tol=args.coarse_tol, mixed=True))
         for _ in range(args.warmup):
             mon_m = msolver.solve(Ax, x, b, P.n, P, stream=stream)
         torch.cuda.synchronize()
@@ -582,6 +624,7 @@ def main():
                        cfg, f"FP64 {'Jacobi-PCG' if args.pc == 'jacobi' else 'hsmg-FCG'}")
                        + ", one solve per step per GPU",
                    "pc": args.pc, "iterations": iters[-1], "r0": r0, "seed": args.seed,
+                   "coarse": f"10 Jacobi-CG iterations, abs tol {args.coarse_tol:g}",
                    "l2": f"inputs larger than L2 ({72 * P.n / 1e9:.1f} GB ax_helm working set)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": P.n * 8,
