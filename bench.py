@@ -260,6 +260,25 @@ def kernel_only(args, cfg):
     import neko_b200 as nb
     cfg = dict(cfg, nel=(args.nel,) * 3, lx=args.lx)
     P = build_problem(nb, cfg)
+    if args.kernel_only == "solve":
+        # --warmup FP64 and mixed hsmg-FCG solves, then one of each inside a
+        # profiler window (ncu --profile-from-start off captures only those)
+        b = make_rhs(nb, P, args.seed)
+        r0 = math.sqrt(float((b * P.field("mult") * b).sum()) / P.volume)
+        x = P.zeros()
+        solvers = [nb.FCG(max_iter=cfg["max_iter"], abs_tol=cfg["rel_tol"] * r0,
+                          M=nb.Hsmg(mixed=m)) for m in (False, True)]
+        for _ in range(args.warmup):
+            for sv in solvers:
+                sv.solve(nb.AxHelm(), x, b, P.n, P)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        mons = [sv.solve(nb.AxHelm(), x, b, P.n, P) for sv in solvers]
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"kernel": "solve", "n": P.n, "iterations": [m.iter for m in mons],
+                          "launches": [m.launches for m in mons]}))
+        return
     u = torch.rand(P.n, dtype=torch.float64, device="cuda")
     w = P.zeros()
     s = torch.cuda.Stream()
@@ -460,8 +479,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision solve measured beside the FP64 one")
-    ap.add_argument("--kernel-only", choices=["ax", "gs"], default=None,
-                    help="run only this kernel on an nel^3 box (profiling case)")
+    ap.add_argument("--kernel-only", choices=["ax", "gs", "solve"], default=None,
+                    help="run only this kernel (or one FP64 + one mixed solve inside a "
+                         "profiler window) on an nel^3 box (profiling case)")
     ap.add_argument("--workload", choices=["solve", "batch", "serve"], default="solve",
                     help="solve: the hsmg-FCG config-2 line (default); batch: batched "
                          "uneven solves; serve: the served request stream")

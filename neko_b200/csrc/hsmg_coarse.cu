@@ -267,10 +267,12 @@ __global__ void __launch_bounds__(kCoarseThreads)
   }
 
   // prolong: e_mid(o,p,r) += sum_k J(r,k) sum_j J(p,j) sum_i J(o,i) x(i,j,k)
+  const double *__restrict__ xc = a.x;
+#pragma unroll 4
   for (long q = t0; q < nm; q += stride) {
     const long e = q / M3;
     const int m = (int)(q - e * M3), o = m % LM, pp = (m / LM) % LM, rr = m / (LM * LM);
-    const double *in = a.x + e * 8;
+    const double *in = xc + e * 8;
     T acc_z = 0;
 #pragma unroll
     for (int k = 0; k < 2; k++) {

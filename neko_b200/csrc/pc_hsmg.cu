@@ -480,24 +480,32 @@ struct HsmgState : public Precond {
   int niter = 10;
   double tol = 1e-9;
   bool mixed = false;
-  // The fine-level Schwarz runs on `side` while the middle and coarse levels
-  // run on the caller's stream (the two branches of the additive scheme
-  // share only the input r).
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // The two branches of the additive scheme share only the input r: the
+  // fine-level Schwarz runs on `side`, the middle level and the coarse solve
+  // on `hi`, a stream of the greatest priority, so that the small,
+  // latency-bound coarse-branch kernels get SM slots ahead of the pending
+  // blocks of the large fine-level FDM launch instead of queueing behind it.
+  cudaStream_t side = nullptr, hi = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join_hi = nullptr;
   cudaError_t ensure_side() {
     if (side) return cudaSuccess;
     cudaError_t e;
-    if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+    int lo_prio = 0, hi_prio = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&hi, cudaStreamNonBlocking, hi_prio)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming)) != cudaSuccess)
+        (e = cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ev_join_hi, cudaEventDisableTiming)) != cudaSuccess)
       return e;
     return cudaSuccess;
   }
   ~HsmgState() override {
     if (side) cudaStreamDestroy(side);
+    if (hi) cudaStreamDestroy(hi);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_join_hi) cudaEventDestroy(ev_join_hi);
     if (arena) cudaFree(arena);
     if (mid) nb_problem_destroy(mid);
     if (crs) nb_problem_destroy(crs);
@@ -539,22 +547,28 @@ struct HsmgImpl : public HsmgState {
     T *zs = sizeof(T) == 8 ? reinterpret_cast<T *>(z) : zf;
     // fine Schwarz on the side stream: zs = S_f r
     if ((e = ensure_side()) != cudaSuccess || (e = cudaEventRecord(ev_fork, s)) != cudaSuccess ||
-        (e = cudaStreamWaitEvent(side, ev_fork, 0)) != cudaSuccess)
+        (e = cudaStreamWaitEvent(side, ev_fork, 0)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(hi, ev_fork, 0)) != cudaSuccess)
       return e;
-    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side)) != cudaSuccess) return e;
-    if ((e = cudaEventRecord(ev_join, side)) != cudaSuccess) return e;
+    // middle and coarse levels first, on the high-priority stream:
     // restrict (r * mult) to the middle level, assemble, mask
     if ((e = restrict_level<double, T, T>(fine->lx, mid->lx, r, fine->mult, Jfm, w_mid, nelv,
-                                          skip, s)) != cudaSuccess)
+                                          skip, hi)) != cudaSuccess)
       return e;
-    if ((e = gs_add_fused<T>(mid->gsd, w_mid, true, s, skip)) != cudaSuccess) return e;
+    if ((e = gs_add_fused<T>(mid->gsd, w_mid, true, hi, skip)) != cudaSuccess) return e;
     // middle Schwarz: e_mid = S_m w
-    if ((e = schwarz_apply<T, T>(sm, w_mid, e_mid, skip, s)) != cudaSuccess) return e;
+    if ((e = schwarz_apply<T, T>(sm, w_mid, e_mid, skip, hi)) != cudaSuccess) return e;
     // restrict (w * mult_mid) to the coarse level (FP64), assemble, mask,
     // niter Jacobi-CG iterations (or abs tol), e_mid += J e_crs: one launch
     ca.skip = skip;
-    if ((e = hsmg_coarse_solve<T>(ca, mid->lx, kCoarseMaxBlocks, s)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(s, ev_join, 0)) != cudaSuccess) return e;
+    if ((e = hsmg_coarse_solve<T>(ca, mid->lx, kCoarseMaxBlocks, hi)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_join_hi, hi)) != cudaSuccess) return e;
+    // fine Schwarz on the side stream: zs = S_f r
+    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_join, side)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, ev_join, 0)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(s, ev_join_hi, 0)) != cudaSuccess)
+      return e;
     // prolong: zs += J e_mid; z = mult * gs(zs)
     if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s)) !=
         cudaSuccess)
