@@ -162,10 +162,23 @@ def make_rhs(nb, P, seed):
     return b
 
 
+def host_threads():
+    """Host threads the CPU oracle uses (its element-parallel loops); set
+    NB_ORACLE_THREADS to this process's CPU affinity unless given."""
+    if "NB_ORACLE_THREADS" not in os.environ:
+        try:
+            n = len(os.sched_getaffinity(0))
+        except AttributeError:
+            n = os.cpu_count() or 1
+        os.environ["NB_ORACLE_THREADS"] = str(n)
+    return int(os.environ["NB_ORACLE_THREADS"])
+
+
 def oracle_iteration_time(cfg, b, pc, iters):
-    """Seconds per Krylov iteration of the CPU oracle (a one-thread port of
-    the reference's CPU path) on this workload: setup untimed, `iters`
-    iterations timed."""
+    """Seconds per Krylov iteration of the CPU oracle (the port of the
+    reference's CPU path, element loops on all host threads) on this
+    workload: setup untimed, `iters` iterations timed."""
+    host_threads()
     from oracle import oracle as orc
     O = orc.OracleProblem.box(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"],
                               periodic=cfg["periodic"])
@@ -188,10 +201,11 @@ def oracle_iteration_time(cfg, b, pc, iters):
 def cpu_baseline_sample(cfg, b, pc, gpu_iters, budget_iters):
     per_iter, dt = oracle_iteration_time(cfg, b, pc, budget_iters)
     name = "hsmg-FCG" if pc == "hsmg" else "Jacobi-PCG"
-    return {"value": 1.0 / (per_iter * max(gpu_iters, 1)), "unit": "solves/s", "cores": 1,
+    cores = host_threads()
+    return {"value": 1.0 / (per_iter * max(gpu_iters, 1)), "unit": "solves/s", "cores": cores,
             "kind": "port",
             "sample": f"{budget_iters} {name} iterations of the same 32^3 lx={cfg['lx']} "
-                      f"problem and right-hand side on 1 host core ({dt:.1f} s, setup untimed); solves/s = "
+                      f"problem and right-hand side on {cores} host threads ({dt:.1f} s, setup untimed); solves/s = "
                       f"1/(s per iteration x {gpu_iters} iterations of the solve)"}
 
 
@@ -208,6 +222,7 @@ def run_reference(args, cfg, world, rank):
     solves/s uses the solve's iteration count.  Rank 0 only."""
     if rank != 0:
         return
+    host_threads()
     import numpy as np
     from oracle import oracle as orc
     from neko_b200 import workloads
@@ -244,9 +259,9 @@ def run_reference(args, cfg, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name(cfg, f"FP64 {name}"), "pc": args.pc,
                        "r0": r0},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": host_threads(), "kind": "port",
                              "sample": f"median of {args.steps} runs of {iters} {name} "
-                                       f"iterations on 1 host core; solves/s = 1/(s per "
+                                       f"iterations on {host_threads()} host threads; solves/s = 1/(s per "
                                        f"iteration x {full_iters} iterations of the solve)"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}

@@ -1030,20 +1030,34 @@ static void gs_add(const OrProblem &P, double *u, std::vector<double> &v) {
   v.assign(std::max(m, 1), 0.0);
   const int *dg = P.local_dof_gs.data() - 1, *gd = P.local_gs_dof.data() - 1;
   double *U = u - 1, *V = v.data() - 1;
-  for (int b = 0; b < nb; b++) {
-    int k = P.blk_off[b], bl = P.blk_len[b];
-    double t = U[gd[k + 1]];
-    for (int j = 2; j <= bl; j++) t = t + U[gd[k + j]];
-    V[dg[k + 1]] = t;
-  }
-  for (int i = o; i <= m; i += 2) V[dg[i]] = U[gd[i]] + U[gd[i + 1]];
-  for (int b = 0; b < nb; b++) {
-    int k = P.blk_off[b], bl = P.blk_len[b];
-    double t = V[dg[k + 1]];
-    for (int j = 1; j <= bl; j++) U[gd[k + j]] = t;
-  }
+  // Each phase writes distinct entries per block / pair, so the phases
+  // run element-parallel without changing any sum.
+  parallel_for(nb, [&](long b0, long b1) {
+    for (long b = b0; b < b1; b++) {
+      int k = P.blk_off[b], bl = P.blk_len[b];
+      double t = U[gd[k + 1]];
+      for (int j = 2; j <= bl; j++) t = t + U[gd[k + j]];
+      V[dg[k + 1]] = t;
+    }
+  });
+  const long npair = m >= o ? (m - o + 2) / 2 : 0;
+  parallel_for(npair, [&](long q0, long q1) {
+    for (long q = q0; q < q1; q++) {
+      const int i = o + 2 * (int)q;
+      V[dg[i]] = U[gd[i]] + U[gd[i + 1]];
+    }
+  });
+  parallel_for(nb, [&](long b0, long b1) {
+    for (long b = b0; b < b1; b++) {
+      int k = P.blk_off[b], bl = P.blk_len[b];
+      double t = V[dg[k + 1]];
+      for (int j = 1; j <= bl; j++) U[gd[k + j]] = t;
+    }
+  });
   int start = nb > 0 ? P.blk_off[nb - 1] + P.blk_len[nb - 1] + 1 : 1;
-  for (int i = start; i <= m; i++) U[gd[i]] = V[dg[i]];
+  parallel_for(m - start + 1, [&](long q0, long q1) {
+    for (long q = q0; q < q1; q++) U[gd[start + q]] = V[dg[start + q]];
+  });
 }
 
 namespace {

@@ -3,6 +3,8 @@
 // (neko_oracle_solve.cpp).  Nothing in the neko_b200 product includes it.
 #pragma once
 #include <cstdint>
+#include <cstdlib>
+#include <thread>
 #include <vector>
 
 namespace nko {
@@ -55,4 +57,30 @@ void or_bc_boundary_impl(OrProblem &P);
 void fd_weights_full_impl(double xi, const double *x, int n, int m, double *c);
 void zwgll_impl(double *z, double *w, int np);
 void mxm_impl(const double *a, int n1, const double *b, int n2, double *c, int n3);
+
+// Host threads for element-parallel loops: NB_ORACLE_THREADS, else all
+// hardware threads.  Only loops whose iterations write disjoint elements use
+// it, so results do not depend on the thread count.
+inline int oracle_threads() {
+  const char *v = std::getenv("NB_ORACLE_THREADS");
+  int t = v ? std::atoi(v) : (int)std::thread::hardware_concurrency();
+  return t < 1 ? 1 : t;
+}
+// f(begin, end) over [0, n) in contiguous chunks, one per thread.
+template <typename F>
+void parallel_for(long n, F f) {
+  const int T = oracle_threads();
+  if (T == 1 || n < 2 * T) {
+    f(0L, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long chunk = (n + T - 1) / T;
+  for (int t = 0; t < T; t++) {
+    const long b = t * chunk, e = b + chunk < n ? b + chunk : n;
+    if (b >= e) break;
+    th.emplace_back(f, b, e);
+  }
+  for (auto &x : th) x.join();
+}
 int or_dfrmd_el(const OrProblem &P, int e);

@@ -342,16 +342,18 @@ void fdm_init(Fdm &F, const OrProblem &P) {
 void fdm_do_fast(const Fdm &F, double *e, double *r) {
   const int nl = F.nl, nn = nl * nl * nl;
   const size_t sz = (size_t)nl * nl * 2;
-  for (int ie = 0; ie < F.nelv; ie++) {
-    const double *s = &F.s[sz * 3 * ie];
-    const double *s1x = s, *s2x = s + nl * nl, *s1y = s + sz, *s2y = s + sz + nl * nl,
-                 *s1z = s + 2 * sz, *s2z = s + 2 * sz + nl * nl;
-    double *ee = e + (size_t)nn * ie, *rr = r + (size_t)nn * ie;
-    tnsr3d_el(ee, nl, rr, nl, s2x, s1y, s1z);
-    const double *d = &F.d[(size_t)nn * ie];
-    for (int i = 0; i < nn; i++) rr[i] = d[i] * ee[i];
-    tnsr3d_el(ee, nl, rr, nl, s1x, s2y, s2z);
-  }
+  parallel_for(F.nelv, [&](long ib, long iend) {
+    for (long ie = ib; ie < iend; ie++) {
+      const double *s = &F.s[sz * 3 * ie];
+      const double *s1x = s, *s2x = s + nl * nl, *s1y = s + sz, *s2y = s + sz + nl * nl,
+                   *s1z = s + 2 * sz, *s2z = s + 2 * sz + nl * nl;
+      double *ee = e + (size_t)nn * ie, *rr = r + (size_t)nn * ie;
+      tnsr3d_el(ee, nl, rr, nl, s2x, s1y, s1z);
+      const double *d = &F.d[(size_t)nn * ie];
+      for (int i = 0; i < nn; i++) rr[i] = d[i] * ee[i];
+      tnsr3d_el(ee, nl, rr, nl, s1x, s2y, s2z);
+    }
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -370,7 +372,8 @@ void extrude(double *arr1, int l1, double f1, const double *arr2, int l2, double
              int nelv) {
   const size_t n3 = (size_t)nx * nx * nx;
   auto I = [&](int i, int j, int k) { return (i - 1) + nx * (j - 1) + nx * nx * (k - 1); };
-  for (int ie = 0; ie < nelv; ie++) {
+  parallel_for(nelv, [&](long ib, long iend) {
+  for (long ie = ib; ie < iend; ie++) {
     double *a1 = arr1 + n3 * ie;
     const double *a2 = arr2 + n3 * ie;
     for (int k = 2; k <= nx - 1; k++)
@@ -389,27 +392,32 @@ void extrude(double *arr1, int l1, double f1, const double *arr2, int l2, double
         a1[I(i, j, nx - l1)] = f1 * a1[I(i, j, nx - l1)] + f2 * a2[I(i, j, nx - l2)];
       }
   }
+  });
 }
 
 void toext3d(double *a, const double *b, int n, int nelv) {  // schwarz.f90:366-379
   const int m = n + 2;
-  std::fill(a, a + (size_t)m * m * m * nelv, 0.0);
-  for (int ie = 0; ie < nelv; ie++)
-    for (int k = 1; k <= n; k++)
-      for (int j = 1; j <= n; j++)
-        for (int i = 1; i <= n; i++)
-          a[(size_t)ie * m * m * m + i + m * j + m * m * k] =
-              b[(size_t)ie * n * n * n + (i - 1) + n * (j - 1) + n * n * (k - 1)];
+  parallel_for(nelv, [&](long e0, long e1) {
+    std::fill(a + (size_t)m * m * m * e0, a + (size_t)m * m * m * e1, 0.0);
+    for (long ie = e0; ie < e1; ie++)
+      for (int k = 1; k <= n; k++)
+        for (int j = 1; j <= n; j++)
+          for (int i = 1; i <= n; i++)
+            a[(size_t)ie * m * m * m + i + m * j + m * m * k] =
+                b[(size_t)ie * n * n * n + (i - 1) + n * (j - 1) + n * n * (k - 1)];
+  });
 }
 
 void toreg3d(double *b, const double *a, int n, int nelv) {  // schwarz.f90:345-364
   const int m = n + 2;
-  for (int ie = 0; ie < nelv; ie++)
-    for (int k = 1; k <= n; k++)
-      for (int j = 1; j <= n; j++)
-        for (int i = 1; i <= n; i++)
-          b[(size_t)ie * n * n * n + (i - 1) + n * (j - 1) + n * n * (k - 1)] =
-              a[(size_t)ie * m * m * m + i + m * j + m * m * k];
+  parallel_for(nelv, [&](long e0, long e1) {
+    for (long ie = e0; ie < e1; ie++)
+      for (int k = 1; k <= n; k++)
+        for (int j = 1; j <= n; j++)
+          for (int i = 1; i <= n; i++)
+            b[(size_t)ie * n * n * n + (i - 1) + n * (j - 1) + n * n * (k - 1)] =
+                a[(size_t)ie * m * m * m + i + m * j + m * m * k];
+  });
 }
 
 void wt3d(double *e, const std::vector<double> &wt, int n, int nelv) {  // schwarz.f90:599-633
@@ -417,7 +425,8 @@ void wt3d(double *e, const std::vector<double> &wt, int n, int nelv) {  // schwa
     return wt[(size_t)(a - 1) + n * (b - 1) + (size_t)n * n * (c - 1) + (size_t)n * n * 4 * (d - 1) +
               (size_t)n * n * 12 * ie];
   };
-  for (int ie = 0; ie < nelv; ie++) {
+  parallel_for(nelv, [&](long e0, long e1) {
+  for (long ie = e0; ie < e1; ie++) {
     double *E = e + (size_t)n * n * n * ie;
     auto I = [&](int i, int j, int k) { return (i - 1) + n * (j - 1) + n * n * (k - 1); };
     for (int k = 1; k <= n; k++)
@@ -442,6 +451,7 @@ void wt3d(double *e, const std::vector<double> &wt, int n, int nelv) {  // schwa
         E[I(i, j, n)] *= W(i, j, 4, 3, ie);
       }
   }
+  });
 }
 
 void schwarz_init(Schwarz &S, OrProblem *lev) {
@@ -586,15 +596,19 @@ void or_hsmg_apply(OrHsmg *H, double *z, const double *r) {
   for (long i = 0; i < F.n; i++) H->r[i] = H->r[i] * F.mult[i];
   // restrict fine -> mid: interp_fine_mid%map(w, r, to Yh)
   const int lf = F.lx, lm = M.lx, lc = C.lx;
-  for (int e = 0; e < nelv; e++)
-    tnsr3d_el(&H->w[(size_t)e * lm * lm * lm], lm, &H->r[(size_t)e * lf * lf * lf], lf,
-              H->J_fmT.data(), H->J_fm.data(), H->J_fm.data());
+  parallel_for(nelv, [&](long eb, long ee_) {
+    for (long e = eb; e < ee_; e++)
+      tnsr3d_el(&H->w[(size_t)e * lm * lm * lm], lm, &H->r[(size_t)e * lf * lf * lf], lf,
+                H->J_fmT.data(), H->J_fm.data(), H->J_fm.data());
+  });
   or_gs_add_impl(M, H->w.data());
   schwarz_compute(H->sch_mid, H->e_mid.data(), H->w.data());
   for (long i = 0; i < M.n; i++) H->w[i] = H->w[i] * M.mult[i];
-  for (int e = 0; e < nelv; e++)
-    tnsr3d_el(&H->r_crs[(size_t)e * lc * lc * lc], lc, &H->w[(size_t)e * lm * lm * lm], lm,
-              H->J_mcT.data(), H->J_mc.data(), H->J_mc.data());
+  parallel_for(nelv, [&](long eb, long ee_) {
+    for (long e = eb; e < ee_; e++)
+      tnsr3d_el(&H->r_crs[(size_t)e * lc * lc * lc], lc, &H->w[(size_t)e * lm * lm * lm], lm,
+                H->J_mcT.data(), H->J_mc.data(), H->J_mc.data());
+  });
   or_gs_add_impl(C, H->r_crs.data());
   for (int m : C.msk) H->r_crs[m - 1] = 0.0;
   double rs, rf;
@@ -605,13 +619,17 @@ void or_hsmg_apply(OrHsmg *H, double *z, const double *r) {
       or_cg_solve_impl(C, H->e_crs.data(), H->r_crs.data(), H->niter, H->crs_tol, Mj, &rs, &rf);
   for (int m : C.msk) H->e_crs[m - 1] = 0.0;
   // prolong coarse -> mid, add; mid -> fine, add
-  for (int e = 0; e < nelv; e++)
-    tnsr3d_el(&H->w[(size_t)e * lm * lm * lm], lm, &H->e_crs[(size_t)e * lc * lc * lc], lc,
-              H->J_mc.data(), H->J_mcT.data(), H->J_mcT.data());
+  parallel_for(nelv, [&](long eb, long ee_) {
+    for (long e = eb; e < ee_; e++)
+      tnsr3d_el(&H->w[(size_t)e * lm * lm * lm], lm, &H->e_crs[(size_t)e * lc * lc * lc], lc,
+                H->J_mc.data(), H->J_mcT.data(), H->J_mcT.data());
+  });
   for (long i = 0; i < M.n; i++) H->e_mid[i] = H->e_mid[i] + H->w[i];
-  for (int e = 0; e < nelv; e++)
-    tnsr3d_el(&H->w[(size_t)e * lf * lf * lf], lf, &H->e_mid[(size_t)e * lm * lm * lm], lm,
-              H->J_fm.data(), H->J_fmT.data(), H->J_fmT.data());
+  parallel_for(nelv, [&](long eb, long ee_) {
+    for (long e = eb; e < ee_; e++)
+      tnsr3d_el(&H->w[(size_t)e * lf * lf * lf], lf, &H->e_mid[(size_t)e * lm * lm * lm], lm,
+                H->J_fm.data(), H->J_fmT.data(), H->J_fmT.data());
+  });
   for (long i = 0; i < F.n; i++) z[i] = z[i] + H->w[i];
   or_gs_add_impl(F, z);
   for (long i = 0; i < F.n; i++) z[i] = z[i] * F.mult[i];

@@ -18,8 +18,9 @@ void ax_helm(const OrProblem &P, double *w, const double *u) {
   const double *Dx = P.dx.data(), *Dxt = P.dxt.data();
   auto D = [&](int i, int k) { return Dx[i + lx * k]; };
   auto Dt = [&](int i, int k) { return Dxt[i + lx * k]; };
+  parallel_for(P.nelv, [&](long e0, long e1) {
   std::vector<double> wur(lxyz), wus(lxyz), wut(lxyz), ur(lxyz), us(lxyz), ut(lxyz);
-  for (int e = 0; e < P.nelv; e++) {
+  for (long e = e0; e < e1; e++) {
     const size_t o = (size_t)e * lxyz;
     const double *ue = u + o;
     double *we = w + o;
@@ -68,6 +69,7 @@ void ax_helm(const OrProblem &P, double *w, const double *u) {
         we[i + lxy * k] = we[i + lxy * k] + t;
       }
   }
+  });
   if (P.ifh2)
     for (long i = 0; i < P.n; i++) w[i] = w[i] + P.h2[i] * P.B[i] * u[i];
 }
