@@ -39,11 +39,12 @@
 #include "nb_kernels.h"
 #include "nb_problem.h"
 #include "nb_reduce.cuh"
+#include "nb_tma.cuh"
 
 namespace nb {
 
 constexpr int kBT = 256;         // threads of the batched kernels
-constexpr int kItemElems = 8;    // elements per Ax work item
+constexpr int kItemElems = 24;   // elements per Ax work item
 constexpr long kChunk = 8192;    // points per vector chunk
 constexpr int kGsChunk = 4096;   // gs items per chunk
 
@@ -75,48 +76,89 @@ struct GChunk {
 };
 
 // ---------------------------------------------------------------------------
-// Element routine: w = A p on `ne` elements from e0, NE elements at a time,
-// KS thread groups splitting the k-planes; acc += p * w.
+// Element routine: w = A p on the `ne` elements of one work item, streamed.
+// One thread issues, per element, 1-D bulk copies of the arrays the element
+// needs (z and p for the fused update p = z + beta p, the six G factors, h1
+// unless the slot's coefficients are constants, B when the h2 term is on)
+// into a kBS-stage shared-memory ring that completes on the stage's
+// mbarrier, so the next element's bytes are in flight while this one is
+// computed.  L2 * KS threads compute: thread (i, j, kh) owns column (i, j)
+// and k-planes [kh LX/KS, (kh+1) LX/KS).  acc += p * w.
 // ---------------------------------------------------------------------------
-template <int LX, int KS>
-struct AxB {
-  static constexpr int L2 = LX * LX, L3 = L2 * LX, TPE = L2 * KS, NE = kBT / TPE, KP = LX / KS;
-  static constexpr int SMEM = 2 * L2 + NE * 4 * L3;  // doubles
-  static_assert(LX % KS == 0 && NE >= 1, "bad k split");
-};
+constexpr int kBS = 2;       // ring stages
+constexpr int kMaxNA = 10;   // arrays per element: z, p, 6 G, h1, B
 
 template <int LX, int KS>
-__device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double beta, double *sm,
-                                         double &acc) {
+struct AxB {
+  static constexpr int L2 = LX * LX, L3 = L2 * LX, TH = L2 * KS, KP = LX / KS;
+  static_assert(LX % KS == 0 && TH <= kBT, "bad k split");
+};
+
+// Shared-memory layout for the largest lx of a batch (doubles, then the
+// mbarriers): ring[kBS][kMaxNA][L3] | su, sur, sus, sut [4 L3] | D, Dt [2 L2].
+__host__ __device__ inline size_t batch_smem_bytes(int lxmax) {
+  const size_t L2 = (size_t)lxmax * lxmax, L3 = L2 * lxmax;
+  return ((size_t)kBS * kMaxNA * L3 + 4 * L3 + 2 * L2) * sizeof(double) + kBS * sizeof(uint64_t);
+}
+
+template <int LX, int KS>
+__device__ __forceinline__ bool ax_item(const BSlot &S, const AxItem &I, double beta,
+                                        double *sm, uint64_t *full, unsigned &g, double &acc) {
   using C = AxB<LX, KS>;
-  constexpr int L2 = C::L2, L3 = C::L3, TPE = C::TPE, NE = C::NE, KP = C::KP;
-  const int tid = threadIdx.x, el = tid / TPE, c = tid - el * TPE, col = c % L2, kh = c / L2;
+  constexpr int L2 = C::L2, L3 = C::L3, TH = C::TH, KP = C::KP;
+  const int tid = threadIdx.x, col = tid % L2, kh = tid / L2;
   const int i = col % LX, j = col / LX, k0 = kh * KP;
-  double *sD = sm, *sDt = sm + L2;
-  double *su = sm + 2 * L2 + el * 4 * L3, *sur = su + L3, *sus = su + 2 * L3, *sut = su + 3 * L3;
+  const bool act = tid < TH;
+  double *ring = sm;
+  double *su = sm + (size_t)kBS * kMaxNA * L3, *sur = su + L3, *sus = su + 2 * L3,
+         *sut = su + 3 * L3, *sD = su + 4 * L3, *sDt = sD + L2;
+  const bool cs = S.coef_scalar != 0, h2on = S.ifh2 != 0;
+  const int na = 8 + (cs ? 0 : 1) + (h2on ? 1 : 0);
+  const int aH = 8, aB = cs ? 8 : 9;  // slots of h1 and B in a stage
   for (int q = tid; q < L2; q += kBT) {
     sD[q] = S.D[q];
     sDt[q] = S.Dt[q];
   }
-  __syncthreads();
-  for (int g = 0; g < ne; g += NE) {
-    const long e = e0 + g + el;
-    const bool act = el < NE && g + el < ne;
+  auto issue = [&](int t) {
+    const long e = I.e0 + t;
+    const unsigned st = (g + t) % kBS;
+    double *dst = ring + (size_t)st * kMaxNA * L3;
+    const double *src[kMaxNA] = {S.z, S.p, S.g11, S.g22, S.g33, S.g12, S.g13, S.g23,
+                                 cs ? S.B : S.h1, S.B};
+    mbar_arrive_expect_tx(&full[st], (uint32_t)(na * L3 * sizeof(double)));
+    for (int a = 0; a < na; a++)
+      bulk_g2s(dst + (size_t)a * L3, src[a] + e * L3, (uint32_t)(L3 * sizeof(double)), &full[st]);
+  };
+  if (tid == 0)
+    for (int t = 0; t < kBS && t < I.ne; t++) issue(t);
+  __syncthreads();  // D staged
+  bool ok = true;
+  int t = 0;
+  for (; t < I.ne; t++) {
+    const unsigned st = (g + t) % kBS, par = ((g + t) / kBS) & 1u;
+    const bool got = mbar_wait(&full[st], par);
+    if (__syncthreads_or(!got)) {
+      ok = false;
+      break;
+    }
+    const double *sz = ring + (size_t)st * kMaxNA * L3, *sp = sz + L3, *s11 = sz + 2 * L3,
+                 *s22 = sz + 3 * L3, *s33 = sz + 4 * L3, *s12 = sz + 5 * L3, *s13 = sz + 6 * L3,
+                 *s23 = sz + 7 * L3, *sh = sz + aH * L3, *sB = sz + aB * L3;
+    const long e = I.e0 + t;
     if (act) {
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
-        const int k = k0 + kk;
-        const long idx = e * L3 + col + L2 * k;
-        const double pv = S.z[idx] + beta * S.p[idx];
-        S.p[idx] = pv;
-        su[col + L2 * k] = pv;
+        const int q = col + L2 * (k0 + kk);
+        const double pv = sz[q] + beta * sp[q];
+        su[q] = pv;
+        S.p[e * L3 + q] = pv;
       }
     }
     __syncthreads();
     if (act) {
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
-        const int k = k0 + kk;
+        const int k = k0 + kk, q = col + L2 * k;
         double ur = 0, us = 0, ut = 0;
 #pragma unroll
         for (int l = 0; l < LX; l++) {
@@ -124,20 +166,17 @@ __device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double 
           us += sD[j + LX * l] * su[i + LX * l + L2 * k];
           ut += sD[k + LX * l] * su[col + L2 * l];
         }
-        const long idx = e * L3 + col + L2 * k;
-        const double H = S.coef_scalar ? S.h1c : __ldg(S.h1 + idx), G11 = __ldg(S.g11 + idx), G22 = __ldg(S.g22 + idx),
-                     G33 = __ldg(S.g33 + idx), G12 = __ldg(S.g12 + idx),
-                     G13 = __ldg(S.g13 + idx), G23 = __ldg(S.g23 + idx);
-        sur[col + L2 * k] = H * (G11 * ur + G12 * us + G13 * ut);
-        sus[col + L2 * k] = H * (G12 * ur + G22 * us + G23 * ut);
-        sut[col + L2 * k] = H * (G13 * ur + G23 * us + G33 * ut);
+        const double H = cs ? S.h1c : sh[q];
+        sur[q] = H * (s11[q] * ur + s12[q] * us + s13[q] * ut);
+        sus[q] = H * (s12[q] * ur + s22[q] * us + s23[q] * ut);
+        sut[q] = H * (s13[q] * ur + s23[q] * us + s33[q] * ut);
       }
     }
     __syncthreads();
     if (act) {
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
-        const int k = k0 + kk;
+        const int k = k0 + kk, q = col + L2 * k;
         double a = 0, b = 0, d = 0;
 #pragma unroll
         for (int l = 0; l < LX; l++) {
@@ -145,17 +184,22 @@ __device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double 
           b += sDt[j + LX * l] * sus[i + LX * l + L2 * k];
           d += sDt[k + LX * l] * sut[col + L2 * l];
         }
-        const long idx = e * L3 + col + L2 * k;
-        const double pv = su[col + L2 * k];
+        const double pv = su[q];
         double wv = a + b + d;
-        if (S.ifh2)
-          wv = wv + (S.coef_scalar ? S.h2c : __ldg(S.h2 + idx)) * __ldg(S.B + idx) * pv;
-        S.w[idx] = wv;
+        if (h2on) wv = wv + (cs ? S.h2c : __ldg(S.h2 + e * L3 + q)) * sB[q] * pv;
+        S.w[e * L3 + q] = wv;
         acc += pv * wv;
       }
     }
-    __syncthreads();
+    __syncthreads();  // stage st and the work planes are free
+    if (tid == 0 && t + kBS < I.ne) issue(t + kBS);
   }
+  if (!ok && tid == 0)  // bounded wait for this item's copies still in flight
+    for (int q = t; q < I.ne && q < t + kBS; q++)
+      mbar_wait(&full[(g + q) % kBS], ((g + q) / kBS) & 1u);
+  g += (unsigned)I.ne;  // every thread keeps the same count
+  __syncthreads();
+  return ok;
 }
 
 // lx and k-split of every supported element routine; the table order is
@@ -163,33 +207,29 @@ __device__ __forceinline__ void ax_elems(const BSlot &S, int e0, int ne, double 
 struct AxVariant {
   int lx, ks;
 };
-static const AxVariant kVariants[] = {{4, 1}, {4, 2}, {6, 1}, {6, 2}, {6, 3},
-                                      {8, 1}, {8, 2}, {8, 4}, {10, 1}, {10, 2}};
+static const AxVariant kVariants[] = {{4, 2}, {4, 4}, {6, 3}, {6, 6}, {8, 2},
+                                      {8, 4}, {10, 1}, {10, 2}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-static int variant_smem_doubles(int v) {
-  switch (v) {
-    case 0: return AxB<4, 1>::SMEM;
-    case 1: return AxB<4, 2>::SMEM;
-    case 2: return AxB<6, 1>::SMEM;
-    case 3: return AxB<6, 2>::SMEM;
-    case 4: return AxB<6, 3>::SMEM;
-    case 5: return AxB<8, 1>::SMEM;
-    case 6: return AxB<8, 2>::SMEM;
-    case 7: return AxB<8, 4>::SMEM;
-    case 8: return AxB<10, 1>::SMEM;
-    default: return AxB<10, 2>::SMEM;
-  }
-}
-
-// var_of_lx[lx] = variant index used for that lx.
+// var_of_lx[lx] = variant index used for that lx.  Persistent: every CTA
+// takes items from the queue head until it is exhausted.
 __global__ void __launch_bounds__(kBT)
     batch_ax_kernel(BSlot *__restrict__ slots, const AxItem *__restrict__ items, int nitems,
-                    unsigned *head, double *part, const int *__restrict__ var_of_lx) {
-  extern __shared__ __align__(16) double bsm[];
+                    unsigned *head, double *part, const int *__restrict__ var_of_lx, int lxmax,
+                    int *err) {
+  extern __shared__ __align__(128) double bsm[];
   __shared__ double red[kBT / 32];
   __shared__ int item_s;
   __shared__ bool last_s;
+  const size_t L3m = (size_t)lxmax * lxmax * lxmax;
+  uint64_t *full = reinterpret_cast<uint64_t *>(
+      bsm + (size_t)kBS * kMaxNA * L3m + 4 * L3m + 2 * (size_t)lxmax * lxmax);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < kBS; q++) mbar_init(&full[q], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  unsigned g = 0;  // elements streamed by this CTA (ring stage and phase)
   for (;;) {
     if (threadIdx.x == 0) item_s = (int)atomicAdd(head, 1u);
     __syncthreads();
@@ -201,13 +241,18 @@ __global__ void __launch_bounds__(kBT)
     if (S.done) continue;
     double acc = 0.0;
     const double beta = S.beta;
+    bool ok = true;
     switch (var_of_lx[I.lx]) {
 #define NB_V(V, LX, KS) \
-  case V: ax_elems<LX, KS>(S, I.e0, I.ne, beta, bsm, acc); break;
-      NB_V(0, 4, 1) NB_V(1, 4, 2) NB_V(2, 6, 1) NB_V(3, 6, 2) NB_V(4, 6, 3)
-      NB_V(5, 8, 1) NB_V(6, 8, 2) NB_V(7, 8, 4) NB_V(8, 10, 1) NB_V(9, 10, 2)
+  case V: ok = ax_item<LX, KS>(S, I, beta, bsm, full, g, acc); break;
+      NB_V(0, 4, 2) NB_V(1, 4, 4) NB_V(2, 6, 3) NB_V(3, 6, 6) NB_V(4, 8, 2)
+      NB_V(5, 8, 4) NB_V(6, 10, 1) NB_V(7, 10, 2)
 #undef NB_V
-      default: break;
+      default: ok = false; break;
+    }
+    if (!ok) {  // a copy never completed (or no routine): stop this CTA
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      return;
     }
     const double tot = block_sum<kBT>(acc, red);
     if (threadIdx.x == 0) {
@@ -382,6 +427,8 @@ struct nb_batch {
   double *d_part3 = nullptr, *d_part5 = nullptr;
   unsigned *d_head = nullptr;
   int *d_var = nullptr;
+  int *d_err = nullptr;   // set by the Ax kernel when a bulk copy never completed
+  int lxmax = 0;          // largest lx among the slots (sizes the Ax ring)
   size_t cap_slots = 0, cap_items = 0, cap_vchunks = 0, cap_gchunks = 0, cap_part3 = 0,
          cap_part5 = 0;
   std::vector<BSlot> mirror;  // slot states as of the end of the last run
@@ -423,6 +470,7 @@ nb_batch::~nb_batch() {
   cudaFree(d_part5);
   cudaFree(d_head);
   cudaFree(d_var);
+  cudaFree(d_err);
   if (cap_stream) cudaStreamDestroy(cap_stream);
 }
 
@@ -540,23 +588,24 @@ static nb_status rebuild(nb_batch *b, std::vector<BSlot> &host_slots) {
   return NB_OK;
 }
 
-static int ax_grid() {
-  static int g = 0;
-  if (g == 0) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    g = sms * 3;
-  }
-  return g;
+// CTAs of the persistent Ax launch: the resident count for this smem size.
+static int ax_grid(int smem_bytes) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_ax_kernel, kBT,
+                                                    smem_bytes) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return sms * per_sm;
 }
 
 static cudaError_t launch_iteration(nb_batch *b, cudaStream_t s) {
   cudaError_t e;
   if ((e = cudaMemsetAsync(b->d_head, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
   if (b->nitems > 0) {
-    batch_ax_kernel<<<std::min(ax_grid(), b->nitems), kBT, b->smem_bytes, s>>>(
-        b->d_slots, b->d_items, b->nitems, b->d_head, b->d_part3, b->d_var);
+    batch_ax_kernel<<<std::min(ax_grid(b->smem_bytes), b->nitems), kBT, b->smem_bytes, s>>>(
+        b->d_slots, b->d_items, b->nitems, b->d_head, b->d_part3, b->d_var, b->lxmax, b->d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (b->ngchunks > 0) batch_gs_kernel<<<b->ngchunks, kBT, 0, s>>>(b->d_slots, b->d_gchunks);
@@ -566,13 +615,11 @@ static cudaError_t launch_iteration(nb_batch *b, cudaStream_t s) {
 }
 
 static nb_status set_smem(nb_batch *b) {
-  int mx = 0;
-  for (int lx = 0; lx <= 16; lx++)
-    if (b->ks_of_lx[lx]) {
-      const int v = variant_index(lx, b->ks_of_lx[lx]);
-      mx = std::max(mx, variant_smem_doubles(v));
-    }
-  b->smem_bytes = std::max(mx, 1) * (int)sizeof(double);
+  int mx = 4;
+  for (auto &sh : b->slots)
+    if (sh.used) mx = std::max(mx, sh.P->lx);
+  b->lxmax = mx;
+  b->smem_bytes = (int)batch_smem_bytes(mx);
   NB_BTRY(cudaFuncSetAttribute(batch_ax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                b->smem_bytes));
   int var[17];
@@ -602,8 +649,7 @@ static nb_status autotune_lx(nb_batch *b, int lx, cudaStream_t s) {
   cudaEventCreate(&e1);
   for (int v = 0; v < kNumVariants; v++) {
     if (kVariants[v].lx != lx) continue;
-    const int smem = variant_smem_doubles(v) * (int)sizeof(double);
-    if (smem > 200 * 1024) continue;
+    const int smem = (int)batch_smem_bytes(lx);
     int var[17];
     for (int q = 0; q <= 16; q++) var[q] = q == lx ? v : -1;
     cudaMemcpy(b->d_var, var, sizeof(var), cudaMemcpyHostToDevice);
@@ -614,8 +660,8 @@ static nb_status autotune_lx(nb_batch *b, int lx, cudaStream_t s) {
     for (int rep = 0; rep < 4; rep++) {
       cudaMemsetAsync(b->d_head, 0, sizeof(unsigned), s);
       cudaEventRecord(e0, s);
-      batch_ax_kernel<<<std::min(ax_grid(), (int)mine.size()), kBT, smem, s>>>(
-          b->d_slots, d, (int)mine.size(), b->d_head, part, b->d_var);
+      batch_ax_kernel<<<std::min(ax_grid(smem), (int)mine.size()), kBT, smem, s>>>(
+          b->d_slots, d, (int)mine.size(), b->d_head, part, b->d_var, lx, b->d_err);
       cudaEventRecord(e1, s);
       cudaEventSynchronize(e1);
       float t = 0;
@@ -720,7 +766,11 @@ extern "C" nb_status nb_batch_create(int64_t hbm_budget_bytes, nb_batch **out) {
   *out = nullptr;
   nb_batch *b = new nb_batch();
   b->budget = hbm_budget_bytes > 0 ? (size_t)hbm_budget_bytes : (size_t)-1;
-  if (cudaMalloc(&b->d_head, 256) != cudaSuccess || cudaMalloc(&b->d_var, 17 * sizeof(int)) != cudaSuccess) {
+  if (cudaMalloc(&b->d_head, 256) != cudaSuccess ||
+      cudaMalloc(&b->d_var, 17 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess ||
+      cudaDeviceSynchronize() != cudaSuccess) {
     delete b;
     return bfail(NB_ERR_OOM, "batch: device tables");
   }
@@ -734,7 +784,9 @@ static nb_status submit(nb_batch *b, nb_problem *p, const double *f, double *x, 
                         int max_iter, bool scalar, double h1, double h2, int *slot) {
   if (!b || !p || !f || !x || !slot) return bfail(NB_ERR_ARG, "null argument");
   if (max_iter < 1) return bfail(NB_ERR_ARG, "max_iter must be >= 1");
-  if (variant_index(p->lx, 1) < 0)
+  bool supported = false;
+  for (int v = 0; v < kNumVariants; v++) supported = supported || kVariants[v].lx == p->lx;
+  if (!supported)
     return bfail(NB_ERR_UNSUPPORTED, "batched solves support lx 4, 6, 8, 10");
   if (scalar && !(h1 > 0.0 && h2 >= 0.0)) return bfail(NB_ERR_ARG, "need h1 > 0, h2 >= 0");
   const size_t bytes = (scalar ? 5 : 4) * (size_t)p->n * sizeof(double);
@@ -849,6 +901,13 @@ extern "C" nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void
     if (!left) break;
   }
   if (active) *active = left;
+  int err = 0;
+  NB_BTRY(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(b->d_err, 0, sizeof(int));
+    cudaDeviceSynchronize();
+    return bfail(NB_ERR_TIMEOUT, "batch: a bounded bulk-copy wait expired");
+  }
   return NB_OK;
 }
 
