@@ -296,7 +296,7 @@ cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h
     case 4: return launch_ax_tma<T, 4, 4, 1>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
     case 6: return launch_ax_tma<T, 6, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
     case 8: return launch_ax_tma<T, 8, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
-    case 10: return launch_ax_tma<T, 10, 2, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
+    case 10: return launch_ax_tma<T, 10, 2, 5>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
     default: return cudaErrorNotSupported;
   }
 }
