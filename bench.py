@@ -417,6 +417,73 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def run_axgs(args):
+    """Config 1: unit box 8^3, lx = 8, zero Dirichlet.  (a) ax_helm followed
+    by gs add on a continuous u ~ U[-1,1] (h1 = 1, h2 = 0), 100 times,
+    GDOF/s; (b) the Jacobi-PCG solve of the sin^3 + noise right-hand side to
+    1e-10 relative, solves/s."""
+    import torch
+    import neko_b200 as nb
+    from neko_b200 import workloads
+    torch.cuda.set_device(0)
+    c = workloads.CONFIG1
+    P = nb.Problem(c["nel"], c["lx"], lo=c["lo"], hi=c["hi"], periodic=c["periodic"],
+                   deform=c["deform"], dirichlet=c["dirichlet"])
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    u = torch.rand(P.n, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    P.gs.op(u)
+    u *= P.field("mult")
+    w = P.zeros()
+    Ax = nb.AxHelm()
+    s = torch.cuda.Stream()
+    reps = 100
+    for _ in range(args.warmup):
+        Ax.compute(w, u, P, stream=s)
+        P.gs.op(w, stream=s)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        Ax.compute(w, u, P, stream=s)
+        P.gs.op(w, stream=s)
+    e1.record(s)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    x, y, z = (P.field(k) for k in ("x", "y", "z"))
+    xi = torch.randn(P.n, dtype=torch.float64, device="cuda", generator=g) * 1e-3
+    P.gs.op(xi)
+    xi *= P.field("mult")
+    f = workloads.config1_pointwise(x, y, z, xi) * P.field("B")
+    P.gs.op(f)
+    P.bclst.apply(f)
+    r0 = math.sqrt(float((f * P.field("mult") * f).sum()) / P.volume)
+    solver = nb.CG(max_iter=c["max_iter"], abs_tol=c["rel_tol"] * r0, M=nb.Jacobi())
+    xs = P.zeros()
+    for _ in range(args.warmup):
+        mon = solver.solve(Ax, xs, f, P.n, P, stream=s)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(args.steps):
+        mon = solver.solve(Ax, xs, f, P.n, P, stream=s)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ts = e0.elapsed_time(e1) / 1e3 / args.steps
+    err = float((xs - torch.sin(math.pi * x) * torch.sin(math.pi * y) *
+                 torch.sin(math.pi * z)).abs().max())
+    print(json.dumps({
+        "metric": "ax_helm + gs add GDOF/s (config 1)", "value": P.n / t / 1e9, "unit": "GDOF/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None,
+        "config": {"workload": "unit box 8^3 hex, lx=8 (262,144 points), zero Dirichlet, "
+                               "ax_helm then gs add x100 (working set fits in L2)"},
+        "ms_per_apply": t * 1e3,
+        "solve": {"value": 1.0 / ts, "unit": "solves/s", "iterations": mon.iter,
+                  "converged": mon.converged, "max_error_vs_sin3": err,
+                  "workload": "Jacobi-PCG to 1e-10 rel, f = 3 pi^2 sin^3 + N(0,1e-3)"},
+    }), flush=True)
+    P.close()
+
+
 def run_serve(args):
     """Served request stream: open-loop Poisson arrivals at each of
     --serve-rates, --serve-requests requests per rate drawn as the batched
@@ -497,7 +564,7 @@ def main():
     ap.add_argument("--kernel-only", choices=["ax", "gs", "solve"], default=None,
                     help="run only this kernel (or one FP64 + one mixed solve inside a "
                          "profiler window) on an nel^3 box (profiling case)")
-    ap.add_argument("--workload", choices=["solve", "batch", "serve"], default="solve",
+    ap.add_argument("--workload", choices=["solve", "axgs", "batch", "serve"], default="solve",
                     help="solve: the hsmg-FCG config-2 line (default); batch: batched "
                          "uneven solves; serve: the served request stream")
     ap.add_argument("--batch-count", type=int, default=512)
@@ -522,6 +589,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "axgs":
+        return run_axgs(args)
     world, rank, local = dist_setup()
 
     if args.impl == "reference":
