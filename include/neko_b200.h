@@ -269,6 +269,13 @@ nb_status nb_batch_release(nb_batch *b, int slot);
 nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void *stream);
 /* State of a slot: *done = 1 once it stopped (converged, NaN or max_iter). */
 nb_status nb_batch_result(nb_batch *b, int slot, int *done, nb_solve_result *res);
+/* Self-test of the library's bounded device waits (no counterpart in the
+ * reference): a grid barrier that one block never reaches and an mbarrier
+ * that nothing arrives on, each with a short poll limit; both must return
+ * with their timeout flag set (1) instead of hanging.  Leaves the device
+ * usable. */
+nb_status nb_selftest_bounded_waits(int *barrier_timed_out, int *mbarrier_timed_out);
+
 /* Autotuner record for lx: chosen k-split and the candidates' times (ms). */
 nb_status nb_batch_tuning(nb_batch *b, int lx, int *ks, float *ms, int *ncand);
 

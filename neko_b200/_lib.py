@@ -22,6 +22,7 @@ STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR
 
 NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED = 0, 1, 2, 3
 NB_OK, NB_ERR_ARG, NB_ERR_UNSUPPORTED, NB_ERR_OOM, NB_ERR_CUDA = 0, 1, 2, 3, 4
+NB_ERR_NOT_CONVERGED, NB_ERR_NAN, NB_ERR_TIMEOUT = 5, 6, 7
 
 
 class SolveOpts(ctypes.Structure):
@@ -96,6 +97,7 @@ SIGNATURES = {
     "nb_batch_release": (_I, [_P, _I]),
     "nb_batch_run": (_I, [_P, _I, _IP, _P]),
     "nb_batch_result": (_I, [_P, _I, _IP, _P]),
+    "nb_selftest_bounded_waits": (_I, [_IP, _IP]),
     "nb_batch_tuning": (_I, [_P, _I, _IP, ctypes.POINTER(ctypes.c_float), _IP]),
 }
 

@@ -26,10 +26,12 @@
 // polls too long sets the error word and returns; the others then time out
 // at the same barrier and return too.
 #include <cmath>
+#include <string>
 
 #include "nb_gs_dev.cuh"
 #include "nb_precond.h"
 #include "nb_reduce.cuh"
+#include "nb_tma.cuh"
 
 namespace nb {
 
@@ -41,7 +43,8 @@ constexpr unsigned kBarrierPolls = 1u << 22;
 // the last block arrives (the arrive pattern of cooperative grid sync).
 // Arrival is a release and the poll an acquire at gpu scope, so the writes
 // of every block before the barrier are visible to every block after it.
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err,
+                                             unsigned max_polls = kBarrierPolls) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -54,7 +57,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err) {
     for (;;) {
       asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
       if ((old ^ v) & 0x80000000u) break;
-      if (++polls > kBarrierPolls || *(volatile int *)err) {
+      if (++polls > max_polls || *(volatile int *)err) {
         ok = 0;
         break;
       }
@@ -344,3 +347,62 @@ template cudaError_t hsmg_coarse_solve<double>(const CoarseArgs<double> &, int, 
 template cudaError_t hsmg_coarse_solve<float>(const CoarseArgs<float> &, int, int, cudaStream_t);
 
 }  // namespace nb
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded waits: each probe waits on something that never
+// happens -- a grid barrier that one of two blocks skips, an mbarrier that
+// nothing arrives on -- with a short poll limit, and must come back with
+// its timeout flag set instead of hanging.
+// ---------------------------------------------------------------------------
+namespace nb {
+
+__global__ void barrier_timeout_probe(unsigned *bar, int *err) {
+  if (blockIdx.x == 1) return;  // never arrives
+  grid_barrier(bar, err, 1u << 14);
+}
+
+__global__ void mbarrier_timeout_probe(int *out) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(&bar, 0, 1 << 12);  // nothing arrives
+  if (threadIdx.x == 0) *out = ok ? 0 : 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {  // complete the phase so the barrier is left at rest
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&bar)) : "memory");
+  }
+}
+
+}  // namespace nb
+
+extern "C" nb_status nb_selftest_bounded_waits(int *barrier_timed_out, int *mbarrier_timed_out) {
+  using namespace nb;
+  if (!barrier_timed_out || !mbarrier_timed_out) {
+    set_error("null argument");
+    return NB_ERR_ARG;
+  }
+  int *buf = nullptr;  // bar, err, mbarrier result
+  cudaError_t e = cudaMalloc(&buf, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(buf, 0, 4 * sizeof(int));
+  if (e == cudaSuccess) {
+    barrier_timeout_probe<<<2, 32>>>(reinterpret_cast<unsigned *>(buf), buf + 1);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    mbarrier_timeout_probe<<<1, 32>>>(buf + 2);
+    e = cudaGetLastError();
+  }
+  int h[4] = {0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(h, buf, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) {
+    set_error(std::string("selftest: ") + cudaGetErrorString(e));
+    return NB_ERR_CUDA;
+  }
+  *barrier_timed_out = h[1];
+  *mbarrier_timed_out = h[2];
+  return NB_OK;
+}

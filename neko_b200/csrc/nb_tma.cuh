@@ -55,9 +55,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < kWaitPolls; it++)
+// Bounded wait for phase `parity` of `bar` (at most `polls` polls).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          int polls = kWaitPolls) {
+  for (int it = 0; it < polls; it++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

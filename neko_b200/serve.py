@@ -22,7 +22,7 @@ import torch
 
 from . import AxHelm, Batch, CG, Jacobi, NekoB200Error, Problem
 from . import workloads
-from ._lib import NB_ERR_OOM
+from ._lib import NB_ERR_OOM, NB_ERR_TIMEOUT
 
 
 class GeometryCache:
@@ -89,52 +89,102 @@ def percentiles(lat):
             "p99_ms": float(np.percentile(a, 99) * 1e3), "max_ms": float(a[-1] * 1e3)}
 
 
+# Per-request outcome of the served stream.
+OK, NOT_CONVERGED, NAN, OOM_REJECTED, TIMEOUT, CANCELLED = (
+    "ok", "not_converged", "nan", "oom_rejected", "timeout", "cancelled")
+
+
 def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000, chunk_runs=1,
-                  batch=None, stream=None):
+                  batch=None, stream=None, cancel=None, status=None):
     """Continuous-batching server.  Returns per-request latency (s),
     iterations, convergence flags, the span of the run (s) and the solutions
-    (request index -> device tensor)."""
+    (request index -> device tensor).
+
+    A request may set "max_iter" in its spec.  `cancel` maps request index ->
+    time (s after the start) at which the client withdraws it; a withdrawn
+    request leaves the batch at the next chunk boundary.  When `status` (a
+    list) is given it receives each request's outcome: ok, not_converged,
+    nan, oom_rejected (its work vectors alone exceed the budget, or the
+    device refused the allocation while nothing else was running), timeout
+    (a bounded device wait expired; the requests then running are failed
+    and the batch is rebuilt) or cancelled."""
     own = batch is None
     B = batch if batch is not None else Batch(hbm_budget=budget_bytes)
     n = len(specs)
     lat, iters, conv = [None] * n, [0] * n, [False] * n
+    st = status if status is not None else [None] * n
+    if len(st) < n:
+        st.extend([None] * (n - len(st)))
+    cancel = dict(cancel or {})
     xs, active = {}, {}
     waiting = collections.deque()
     nxt, done_count = 0, 0
     t0 = time.perf_counter()
+
+    def finish(i, outcome, now, mon=None):
+        nonlocal done_count
+        lat[i] = now - t_arr[i]
+        st[i] = outcome
+        if mon is not None:
+            iters[i], conv[i] = mon.iter, mon.converged
+        done_count += 1
+
     while done_count < n:
         now = time.perf_counter() - t0
         while nxt < n and t_arr[nxt] <= now:
             waiting.append(nxt)
             nxt += 1
+        for i in [i for i in waiting if i in cancel and cancel[i] <= now]:
+            waiting.remove(i)
+            finish(i, CANCELLED, now)
         while waiting:  # admission in arrival order while the budget allows
             i = waiting[0]
             sp = specs[i]
             P, f, r0 = pool.get(sp)
             x = torch.empty(P.n, dtype=torch.float64, device="cuda")
             try:
-                slot = B.submit(P, f, x, rel_tol * r0, max_iter, h1=sp["h1"], h2=sp["h2"])
-            except NekoB200Error as e:  # over budget: wait for slots to free
-                if e.status != NB_ERR_OOM or not active:
+                slot = B.submit(P, f, x, rel_tol * r0, sp.get("max_iter", max_iter),
+                                h1=sp["h1"], h2=sp["h2"])
+            except NekoB200Error as e:
+                if e.status != NB_ERR_OOM:
                     raise
-                break
+                if active:  # over budget for now: wait for slots to free
+                    break
+                waiting.popleft()  # cannot fit even alone
+                finish(i, OOM_REJECTED, time.perf_counter() - t0)
+                continue
             waiting.popleft()
             active[slot] = i
             xs[i] = x
         if not active:
-            if nxt < n:
+            if nxt < n and not waiting:
                 time.sleep(max(0.0, t_arr[nxt] - (time.perf_counter() - t0)))
             continue
-        B.run(max_chunks=chunk_runs, stream=stream)
+        failed = None
+        try:
+            B.run(max_chunks=chunk_runs, stream=stream)
+        except NekoB200Error as e:
+            if e.status != NB_ERR_TIMEOUT:
+                raise
+            failed = TIMEOUT
         now = time.perf_counter() - t0
         for slot, i in list(active.items()):
-            done, mon = B.result(slot)
-            if done:
-                lat[i] = now - t_arr[i]
-                iters[i], conv[i] = mon.iter, mon.converged
+            if failed is not None:
                 B.release(slot)
                 del active[slot]
-                done_count += 1
+                finish(i, failed, now)
+                continue
+            done, mon = B.result(slot)
+            if i in cancel and cancel[i] <= now and not done:
+                B.release(slot)
+                del active[slot]
+                finish(i, CANCELLED, now, mon)
+            elif done:
+                outcome = OK if mon.converged else (
+                    NAN if not math.isfinite(mon.res_final) else NOT_CONVERGED)
+                B.release(slot)
+                del active[slot]
+                finish(i, outcome, now, mon)
     span = time.perf_counter() - t0
     if own:
         B.close()
