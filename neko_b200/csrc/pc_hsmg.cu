@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "nb_hsmg.h"
@@ -35,260 +36,204 @@ namespace nb {
 // Kernels
 // ---------------------------------------------------------------------------
 
-// e = S (D^-1) S' r on the extended element, ghost layer gathered from the
-// neighbours (fn: 1-based neighbour per face, 0 = none).  NE elements per
-// block, NL*NL threads each.  Each of the six tensor passes contracts the
-// first index and writes its result with that index moved last
-// (out(m,n,i) = sum_l M(l,i) in(l,m,n)), so after three passes the order is
-// back to (i,j,k) and every pass reads one contiguous line of NL values per
-// thread into registers; the NL x NL matrix of the pass is read as a
-// broadcast.  The inverse eigenvalue sums are rebuilt from the three
-// spectra (1/sum, zero where the sum is <= eps, as fdm_setup_fast).
-template <typename TIN, typename T, int NL>
-__device__ __forceinline__ void fdm_pass(const T *__restrict__ in, T *__restrict__ out,
-                                         const T *__restrict__ M, int t) {
-  constexpr int N2 = NL * NL;
-  T line[NL];
+// e = S (D^-1) S' r on the extended element (NL = lx + 2 points a side),
+// ghost layer gathered from the neighbours (fn: 1-based neighbour per face,
+// 0 = none).  One block (one warp; two for NL >= 13) per element holds the
+// element in shared memory and runs the six tensor passes.  Each pass
+// contracts the first index and writes its result with that index moved
+// last (out(m,n,i) = sum_l M(i,l) in(l,m,n)), so after three passes the
+// order is back to (i,j,k).  A lane owns M lines of the pass and all NL
+// outputs of each: for every l it reads its M line values and the NL matrix
+// entries M(., l), which are the same for the whole warp (broadcast reads),
+// and updates M*NL independent sums, so a matrix read serves M lines.  Lines
+// sit at pos(t, l) = NLP t + C (t >> G) + l, the padding chosen per NL so
+// that the consecutive lines of a warp's reads and rotated writes fall in
+// distinct banks.  The D^-1 scaling of the third forward pass is applied to
+// each value as the first backward pass reads it (the same product, stored
+// one pass later).  The ghost-layer gather and the factor loads are
+// asynchronous copies straight into shared memory (zero-filled where a face
+// has no neighbour) when the input needs no conversion.  Every sum runs over
+// l in ascending order from zero; the eigenvalue scaling multiplies by
+// 1/diag, zero where the sum of the three spectra is <= eps
+// (fdm_setup_fast, src/math/fdm.f90:373-393).
+template <typename T, int NL>
+struct FdmCfg {
+  static constexpr int N2 = NL * NL, N3 = N2 * NL;
+  static constexpr int W = ((N2 + 31) / 32) * NL <= 64 ? 1 : 2;  // warps per element
+  static constexpr int TPE = 32 * W;                             // threads per block
+  static constexpr int M = (N2 + TPE - 1) / TPE;                 // lines per lane
+  static constexpr int LA = (N2 + M - 1) / M;                    // lanes with lines
+  static constexpr int NLP = NL == 16 ? 17 : NL;
+  static constexpr int G = NL == 8 ? 2 : NL == 12 ? 3 : 4;
+  static constexpr int C = (NL % 2 == 0 && NL != 16) ? 1 : 0;
+  static constexpr int BUF = (NLP * (N2 - 1) + ((N2 - 1) >> G) * C + NL + 1) / 2 * 2;
+  static constexpr int STR = 2 * BUF + 3 * N2 + 3 * NL + 1;
+  static constexpr size_t SMEM = ((size_t)STR * sizeof(T) + 15) / 16 * 16;
+  // resident blocks per SM the register allocation is sized for: what the
+  // shared memory allows (228 KB, 1 KB reserved per block), fewer if the
+  // M x NL sums and the operands in flight would not fit in the registers
+  static constexpr int OCC = (int)(233472 / (SMEM + 1024));
+  static constexpr int REGS = 3 * M * NL + 48;
+  static constexpr int RB = 65536 / (TPE * REGS);
+  static constexpr int MINB0 = OCC < RB ? OCC : RB;
+  static constexpr int MINB = MINB0 < 1 ? 1 : MINB0 > 32 / W ? 32 / W : MINB0;
+  __device__ static __forceinline__ int pos(int t, int l) { return NLP * t + (t >> G) * C + l; }
+};
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *sdst, const T *gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gsrc),
+               "n"((int)sizeof(T)), "r"(valid ? (int)sizeof(T) : 0)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// shared[dst] = (T) global[src] (zero when !valid): an asynchronous copy when
+// no conversion is needed, else a load and a store.
+template <typename TIN, typename T>
+__device__ __forceinline__ void gather_elem(T *dst, const TIN *src, bool valid) {
+  if constexpr (std::is_same<TIN, T>::value)
+    cp_async_elem<T>(dst, src, valid);
+  else
+    *dst = valid ? (T)__ldg(src) : T(0);
+}
+
+// One pass over the element: FWD contracts with S(l,i) at Sd[l + NL*i],
+// otherwise with S(i,l) at Sd[i + NL*l].  SCALE multiplies each value read
+// by D^-1 (the first backward pass reads the third forward pass's output);
+// `out` != nullptr writes the natural (i,j,k) order to global memory (last
+// pass) instead of the rotated shared-memory layout.
+template <typename T, int NL, bool FWD, bool SCALE>
+__device__ __forceinline__ void fdm_pass(const T *__restrict__ src, T *__restrict__ dst,
+                                         const T *__restrict__ Sd, const T *__restrict__ sL,
+                                         T *__restrict__ out, int u) {
+  using C = FdmCfg<T, NL>;
+  constexpr int N2 = C::N2, M = C::M, LA = C::LA;
+  if (u >= LA) return;
+  T o[M][NL];
+  int base[M];
+  T ljk[M];  // SCALE: spectra sum of the line's second index, added to the first's
+  T lz[M];
+  const T ep = sL[3 * NL];
 #pragma unroll
-  for (int l = 0; l < NL; l++) line[l] = in[NL * t + l];
+  for (int j = 0; j < M; j++) {
+    const int t = u + LA * j, tt = (LA * M == N2 || t < N2) ? t : N2 - 1;
+    base[j] = C::pos(tt, 0);
+    if (SCALE) {
+      ljk[j] = sL[NL + tt % NL];
+      lz[j] = sL[2 * NL + tt / NL];
+    }
 #pragma unroll
-  for (int i = 0; i < NL; i++) {
-    T s = 0;
+    for (int i = 0; i < NL; i++) o[j][i] = T(0);
+  }
+#pragma unroll 2
+  for (int l = 0; l < NL; l++) {
+    T x[M];
 #pragma unroll
-    for (int l = 0; l < NL; l++) s += M[l + NL * i] * line[l];
-    out[t + N2 * i] = s;
+    for (int j = 0; j < M; j++) {
+      x[j] = src[base[j] + l];
+      if (SCALE) {  // (lx + ly) + lz, as the third forward pass forms it
+        const T d = (sL[l] + ljk[j]) + lz[j];
+        x[j] = x[j] * (d > ep ? T(1) / d : T(0));
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      const T mv = Sd[FWD ? l + NL * i : i + NL * l];
+#pragma unroll
+      for (int j = 0; j < M; j++) o[j][i] += mv * x[j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < M; j++) {
+    const int t = u + LA * j;
+    if (LA * M != N2 && t >= N2) continue;
+    if (out) {
+#pragma unroll
+      for (int k = 0; k < NL; k++) out[t + N2 * k] = o[j][k];
+    } else {
+      const int m = t % NL, n = t / NL;
+#pragma unroll
+      for (int i = 0; i < NL; i++) dst[C::pos(n + NL * i, m)] = o[j][i];
+    }
   }
 }
 
-template <typename TIN, typename T, int NL, int NE>
-__global__ void __launch_bounds__(NL *NL *NE)
+template <typename TIN, typename T, int NL>
+__global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
     fdm_kernel(const TIN *__restrict__ r, const int *__restrict__ fn, const T *__restrict__ S,
                const T *__restrict__ lam, const T *__restrict__ eps, T *__restrict__ out,
                int nelv, const int *__restrict__ skip) {
   if (skip && *skip) return;
-  constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = NL * NL, N3 = N2 * NL;
-  constexpr int STRIDE = 2 * N3 + 6 * N2 + 3 * NL + 2;
+  using C = FdmCfg<T, NL>;
+  constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = C::N2, N3 = C::N3,
+                TPE = C::TPE;
   extern __shared__ __align__(16) unsigned char fdm_smem[];
-  T *base = reinterpret_cast<T *>(fdm_smem) + threadIdx.y * STRIDE;
-  T *b0 = base, *b1 = base + N3;
-  T *sS = base + 2 * N3;        // S_x, S_y, S_z: S(l,i) at l + NL*i
-  T *sT = sS + 3 * N2;          // transposes: S(i,l) at l + NL*i
-  T *sL = sT + 3 * N2;          // spectra + eps
-  const long e = (long)blockIdx.x * NE + threadIdx.y;
-  const int t = threadIdx.x;
-  const bool active = e < nelv;
-  if (active) {
-    const int *f = fn + e * 6;
-    for (int q = t; q < N3; q += N2) {
-      const int a = q % NL, b = (q / NL) % NL, c = q / N2;
-      const int ea = (a == 0) + (a == NL - 1), eb = (b == 0) + (b == NL - 1),
-                ec = (c == 0) + (c == NL - 1);
-      T v = T(0);
-      if (ea + eb + ec == 0) {
-        v = (T)r[e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1)];
-      } else if (ea + eb + ec == 1) {
-        int nb = 0, si = a - 1, sj = b - 1, sk = c - 1;
-        if (a == 0) nb = f[0], si = LX - 2;
-        if (a == NL - 1) nb = f[1], si = 1;
-        if (b == 0) nb = f[2], sj = LX - 2;
-        if (b == NL - 1) nb = f[3], sj = 1;
-        if (c == 0) nb = f[4], sk = LX - 2;
-        if (c == NL - 1) nb = f[5], sk = 1;
-        if (nb) v = (T)r[(long)(nb - 1) * L3 + si + LX * sj + L2 * sk];
-      }
-      b0[q] = v;
-    }
-    for (int q = t; q < 3 * N2; q += N2) {
-      const T v = S[e * 3 * N2 + q];
-      const int d = q / N2, w = q % N2, l = w % NL, i = w / NL;
-      sS[q] = v;
-      sT[d * N2 + i + NL * l] = v;
-    }
-    for (int q = t; q < 3 * NL; q += N2) sL[q] = lam[e * 3 * NL + q];
-    if (t == 0) sL[3 * NL] = eps[e];
-  }
-  __syncthreads();
-  if (active) fdm_pass<TIN, T, NL>(b0, b1, sS, t);           // (l,m,n) -> (m,n,i)
-  __syncthreads();
-  if (active) fdm_pass<TIN, T, NL>(b1, b0, sS + N2, t);      // -> (n,i,j)
-  __syncthreads();
-  if (active) {                                              // -> (i,j,k), times D^-1
-    T line[NL];
-#pragma unroll
-    for (int l = 0; l < NL; l++) line[l] = b0[NL * t + l];
-    const int i = t % NL, j = t / NL;
-    const T lij = sL[i] + sL[NL + j], ep = sL[3 * NL];
-    const T *M = sS + 2 * N2;
-#pragma unroll
-    for (int k = 0; k < NL; k++) {
-      T s = 0;
-#pragma unroll
-      for (int l = 0; l < NL; l++) s += M[l + NL * k] * line[l];
-      const T diag = lij + sL[2 * NL + k];
-      b1[t + N2 * k] = s * (diag > ep ? T(1) / diag : T(0));
-    }
-  }
-  __syncthreads();
-  if (active) fdm_pass<TIN, T, NL>(b1, b0, sT, t);           // back: S_x
-  __syncthreads();
-  if (active) fdm_pass<TIN, T, NL>(b0, b1, sT + N2, t);      // S_y
-  __syncthreads();
-  if (active) {                                              // S_z, store (i,j,k)
-    T line[NL];
-#pragma unroll
-    for (int l = 0; l < NL; l++) line[l] = b1[NL * t + l];
-    const T *M = sT + 2 * N2;
-#pragma unroll
-    for (int k = 0; k < NL; k++) {
-      T s = 0;
-#pragma unroll
-      for (int l = 0; l < NL; l++) s += M[l + NL * k] * line[l];
-      out[e * N3 + t + N2 * k] = s;
-    }
-  }
-}
-
-// The same FDM for even NL, one line per thread with all NL outputs of the
-// line accumulated at once (NL independent FMA chains), each pair of matrix
-// entries fetched with one 16-byte broadcast load.  The forward passes read
-// S through a transposed copy so that both directions load consecutive
-// output pairs.  The passes alternate between two padded buffers, (a, b, c)
-// at a + (NL+1)(b + NL c); the odd row pitch keeps the line reads free of
-// bank conflicts.  The ghost-layer gather issues all of a thread's global
-// loads before its first shared store.  Every sum runs over l in ascending
-// order from zero, as in fdm_kernel; the eigenvalue scaling multiplies by
-// 1/diag as fdm_setup_fast stores it (src/math/fdm.f90:373-393).
-template <typename T>
-struct Pair;
-template <>
-struct Pair<double> {
-  using type = double2;
-};
-template <>
-struct Pair<float> {
-  using type = float2;
-};
-
-template <typename T, int NL>
-struct Fdm2Cfg {
-  static constexpr int N2 = NL * NL, NLP = NL + 1;
-  static constexpr int NE = N2 >= 128 ? 1 : 128 / N2;
-  static constexpr int BUF = NLP * N2;
-  static constexpr int STR = ((2 * BUF + 6 * N2 + 3 * NL + 2) + 3) / 4 * 4;  // per element
-  static constexpr int THREADS = NE * N2;
-  static constexpr size_t SMEM = (size_t)NE * STR * sizeof(T);
-};
-
-// o_i = sum_l M(i, l) x_l, M(i, l) at i + NL*l.
-template <typename T, int NL>
-__device__ __forceinline__ void fdm_line(const T *__restrict__ M, const T (&x)[NL], T (&o)[NL]) {
-  using V = typename Pair<T>::type;
-#pragma unroll
-  for (int i = 0; i < NL; i++) o[i] = T(0);
-#pragma unroll
-  for (int l = 0; l < NL; l++) {
-#pragma unroll
-    for (int i = 0; i < NL; i += 2) {
-      const V m = *reinterpret_cast<const V *>(M + i + NL * l);
-      o[i] += m.x * x[l];
-      o[i + 1] += m.y * x[l];
-    }
-  }
-}
-
-template <typename TIN, typename T, int NL>
-__global__ void __launch_bounds__(Fdm2Cfg<T, NL>::THREADS)
-    fdm2_kernel(const TIN *__restrict__ r, const int *__restrict__ fn, const T *__restrict__ S,
-                const T *__restrict__ lam, const T *__restrict__ eps, T *__restrict__ out,
-                int nelv, const int *__restrict__ skip) {
-  if (skip && *skip) return;
-  using C = Fdm2Cfg<T, NL>;
-  constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = C::N2, N3 = N2 * NL,
-                NLP = C::NLP;
-  static_assert(NL % 2 == 0, "fdm2_kernel needs an even line length");
-  extern __shared__ __align__(16) unsigned char fdm2_smem[];
-  const int el = threadIdx.x / N2, t = threadIdx.x - el * N2;
-  T *b0 = reinterpret_cast<T *>(fdm2_smem) + el * C::STR, *b1 = b0 + C::BUF;
+  T *b0 = reinterpret_cast<T *>(fdm_smem), *b1 = b0 + C::BUF;
   T *sS = b1 + C::BUF;  // S_x, S_y, S_z: S(l,i) at l + NL*i
-  T *sT = sS + 3 * N2;  // transposes: S(l,i) at i + NL*l
-  T *sL = sT + 3 * N2;  // spectra + eps
-  const long e = (long)blockIdx.x * C::NE + el;
-  const bool active = e < nelv;
-  if (active) {
-    constexpr int NG = (N3 + N2 - 1) / N2;
-    const int *f = fn + e * 6;
-    int nbr[6];
-#pragma unroll
-    for (int d = 0; d < 6; d++) nbr[d] = __ldg(f + d);
-    T v[NG];
-#pragma unroll
-    for (int g = 0; g < NG; g++) {
-      const int q = t + g * N2;
-      const int a = q % NL, b = (q / NL) % NL, c = q / N2;
-      const int ea = (a == 0) + (a == NL - 1), eb = (b == 0) + (b == NL - 1),
-                ec = (c == 0) + (c == NL - 1);
-      long src = -1;
-      if (q < N3 && ea + eb + ec == 0) {
-        src = e * L3 + (a - 1) + LX * (b - 1) + L2 * (c - 1);
-      } else if (q < N3 && ea + eb + ec == 1) {
-        int nb = 0, si = a - 1, sj = b - 1, sk = c - 1;
-        if (a == 0) nb = nbr[0], si = LX - 2;
-        if (a == NL - 1) nb = nbr[1], si = 1;
-        if (b == 0) nb = nbr[2], sj = LX - 2;
-        if (b == NL - 1) nb = nbr[3], sj = 1;
-        if (c == 0) nb = nbr[4], sk = LX - 2;
-        if (c == NL - 1) nb = nbr[5], sk = 1;
-        if (nb) src = (long)(nb - 1) * L3 + si + LX * sj + L2 * sk;
+  T *sL = sS + 3 * N2;  // spectra + eps
+  const long e = blockIdx.x;
+  if (e >= nelv) return;
+  const int u = threadIdx.x;
+  {
+    const TIN *re = r + e * L3;
+#pragma unroll 4
+    for (int q = u; q < L3; q += TPE) {  // interior: ext(a+1, b+1, c+1) = r(a, b, c)
+      const int a = q % LX, b = (q / LX) % LX, c = q / L2;
+      gather_elem<TIN, T>(b0 + C::pos((b + 1) + NL * (c + 1), a + 1), re + q, true);
+    }
+#pragma unroll 2
+    for (int q = u; q < 6 * L2; q += TPE) {  // faces: the neighbour's first interior layer
+      const int f = q / L2, w = q - f * L2, s1 = w % LX + 1, s2 = w / LX + 1, dir = f >> 1;
+      const int cb = (f & 1) ? NL - 1 : 0;   // ghost coordinate across the face
+      const int cs = (f & 1) ? 2 : LX - 1;   // its source: the neighbour's layer 1 / LX-2
+      const int a = dir == 0 ? cb : s1, b = dir == 1 ? cb : (dir == 0 ? s1 : s2),
+                c = dir == 2 ? cb : s2;
+      const int sa = dir == 0 ? cs : a, sb = dir == 1 ? cs : b, sc = dir == 2 ? cs : c;
+      const int nb = __ldg(fn + e * 6 + f);
+      gather_elem<TIN, T>(b0 + C::pos(b + NL * c, a),
+                          nb ? r + (long)(nb - 1) * L3 + (sa - 1) + LX * (sb - 1) + L2 * (sc - 1)
+                             : r,
+                          nb != 0);
+    }
+    for (int q = u; q < 12 * LX + 8; q += TPE) {  // edges and corners: zero
+      int a, b, c;
+      if (q < 12 * LX) {
+        const int E = q / LX, s = q - E * LX + 1, D = E >> 2;
+        const int c1 = (E & 1) ? NL - 1 : 0, c2 = (E & 2) ? NL - 1 : 0;
+        a = D == 0 ? s : c1;
+        b = D == 1 ? s : (D == 0 ? c1 : c2);
+        c = D == 2 ? s : c2;
+      } else {
+        const int k = q - 12 * LX;
+        a = (k & 1) ? NL - 1 : 0;
+        b = (k & 2) ? NL - 1 : 0;
+        c = (k & 4) ? NL - 1 : 0;
       }
-      v[g] = src >= 0 ? (T)__ldg(r + src) : T(0);
+      b0[C::pos(b + NL * c, a)] = T(0);
     }
-#pragma unroll
-    for (int g = 0; g < NG; g++) {
-      const int q = t + g * N2;
-      if (q < N3) b0[q % NL + NLP * (q / NL)] = v[g];
-    }
-    for (int q = t; q < 3 * N2; q += N2) {
-      const T sv = __ldg(S + e * 3 * N2 + q);
-      const int d = q / N2, w = q - d * N2, l = w % NL, i = w / NL;
-      sS[q] = sv;
-      sT[d * N2 + i + NL * l] = sv;
-    }
-    for (int q = t; q < 3 * NL; q += N2) sL[q] = lam[e * 3 * NL + q];
-    if (t == 0) sL[3 * NL] = eps[e];
+    for (int q = u; q < 3 * N2; q += TPE) cp_async_elem<T>(sS + q, S + e * 3 * N2 + q, true);
+    for (int q = u; q < 3 * NL; q += TPE) cp_async_elem<T>(sL + q, lam + e * 3 * NL + q, true);
+    if (u == 0) cp_async_elem<T>(sL + 3 * NL, eps + e, true);
+    cp_async_wait_all();
   }
   __syncthreads();
-  const int m = t % NL, n = t / NL;
-  T x[NL], o[NL];
-  T *src = b0, *dst = b1;
-#pragma unroll 1
-  for (int p = 0; p < 6; p++) {
-    if (active) {
-#pragma unroll
-      for (int l = 0; l < NL; l++) x[l] = src[NLP * t + l];
-      // forward passes: o_i = sum_l S(l,i) x_l; backward: o_i = sum_l S(i,l) x_l
-      fdm_line<T, NL>(p < 3 ? sT + p * N2 : sS + (p - 3) * N2, x, o);
-      if (p == 2) {  // line (i, j), output k: times D^-1
-        const T ep = sL[3 * NL], lij = sL[m] + sL[NL + n];
-#pragma unroll
-        for (int k = 0; k < NL; k++) {
-          const T d = lij + sL[2 * NL + k];
-          o[k] = o[k] * (d > ep ? T(1) / d : T(0));
-        }
-      }
-      if (p < 5) {  // rotated: out(m, n, i) at m + NLP*(n + NL*i)
-#pragma unroll
-        for (int i = 0; i < NL; i++) dst[m + NLP * (n + NL * i)] = o[i];
-      } else {
-        T *oe = out + e * N3;
-#pragma unroll
-        for (int k = 0; k < NL; k++) oe[t + N2 * k] = o[k];
-      }
-    }
-    __syncthreads();
-    T *tmp = src;
-    src = dst;
-    dst = tmp;
-  }
+  // forward: b0 -> b1 -> b0 -> b1; backward (D^-1 on the first read): b1 -> b0 -> b1 -> out
+  fdm_pass<T, NL, true, false>(b0, b1, sS, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, true, false>(b1, b0, sS + N2, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, true, false>(b0, b1, sS + 2 * N2, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, false, true>(b1, b0, sS, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, false, false>(b0, b1, sS + N2, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, false, false>(b1, nullptr, sS + 2 * N2, sL, out + e * N3, u);
 }
 
 // e(i,j,k) = ext interior + neighbours' ghost results on the first interior
@@ -389,32 +334,19 @@ template <typename TIN, typename T, int LX>
 static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
                                    cudaStream_t s) {
   constexpr int NL = LX + 2;
-  if constexpr (NL % 2 == 0) {
-    using C = Fdm2Cfg<T, NL>;
-    auto kern = fdm2_kernel<TIN, T, NL>;
-    static bool attr_set = false;  // per instantiation
-    if (!attr_set) {
-      cudaError_t err =
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-      if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-      if (err != cudaSuccess) return err;
-      attr_set = true;
-    }
-    kern<<<(unsigned)((L.nelv + C::NE - 1) / C::NE), C::THREADS, C::SMEM, s>>>(
-        r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
-  } else {
-    constexpr int NE = NL * NL >= 64 ? 1 : (128 / (NL * NL));
-    const size_t smem = sizeof(T) * NE * (2 * NL * NL * NL + 6 * NL * NL + 3 * NL + 2);
-    auto kern = fdm_kernel<TIN, T, NL, NE>;
-    if (smem > 48 * 1024) {
-      cudaError_t err =
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (err != cudaSuccess) return err;
-    }
-    kern<<<(unsigned)((L.nelv + NE - 1) / NE), dim3(NL * NL, NE), smem, s>>>(
-        r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
+  using C = FdmCfg<T, NL>;
+  auto kern = fdm_kernel<TIN, T, NL>;
+  static bool attr_set = false;  // per instantiation
+  if (!attr_set) {
+    cudaError_t err =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (err != cudaSuccess) return err;
+    attr_set = true;
   }
+  kern<<<(unsigned)L.nelv, C::TPE, C::SMEM, s>>>(r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv,
+                                                   skip);
   const long n = L.nelv * LX * LX * LX;
   schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.ext, L.fn, L.wt, e,
                                                                         L.nelv, skip);
