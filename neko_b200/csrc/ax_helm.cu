@@ -16,6 +16,8 @@
 #include <cstdint>
 
 #include "nb_kernels.h"
+#include "nb_precond.h"
+#include "nb_reduce.cuh"
 #include "nb_tma.cuh"
 
 namespace nb {
@@ -300,6 +302,216 @@ cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h
     default: return cudaErrorNotSupported;
   }
 }
+// ---------------------------------------------------------------------------
+// The streaming kernel fused with the two CG steps around it, for a problem
+// with no masked points and no h2 term: p = z + beta p (cg_update_p),
+// w = A p (element-local, before the gather-scatter), and pap = sum over the
+// local points of p * w with alpha = rtz / pap (cg_pap).  p is continuous
+// (z is), so the local sum equals (p, mult gs(w)), the form the reference
+// evaluates after the gather-scatter (cg_device.f90:211-214): each global
+// point's weights 1/k over its k copies add up to one.  The ring carries z
+// and the old p in place of u; each thread forms the new p for its own
+// points, stores it, and the element's operator then reads it from the
+// stage.  Returns at once when st->done is set.
+// ---------------------------------------------------------------------------
+template <int LX, int S, int KS>
+struct AxCgCfg {
+  static constexpr int L2 = LX * LX, L3 = L2 * LX, NA = 9;
+  static constexpr int THREADS = ((L2 * KS + 31) / 32) * 32;
+  static constexpr size_t ABYTES = (size_t)L3 * sizeof(double);
+  static constexpr size_t SMEM = S * NA * ABYTES + 3 * ABYTES + 2 * L2 * sizeof(double) + 16 * S;
+};
+
+template <int LX, int S, int KS>
+__global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
+    ax_cg_fused_kernel(double *__restrict__ w, double *__restrict__ p,
+                       const double *__restrict__ z, const double *__restrict__ D,
+                       const double *__restrict__ Dt, const double *__restrict__ h1,
+                       const double *__restrict__ g11, const double *__restrict__ g22,
+                       const double *__restrict__ g33, const double *__restrict__ g12,
+                       const double *__restrict__ g13, const double *__restrict__ g23,
+                       const int nelv, CgState *st, double *partials, unsigned *counter) {
+  using C = AxCgCfg<LX, S, KS>;
+  constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS, THREADS = C::THREADS;
+  static_assert(LX % KS == 0, "k split must divide lx");
+  if (st->done) return;
+  extern __shared__ __align__(128) unsigned char smem_ring[];
+  double *stage = reinterpret_cast<double *>(smem_ring);
+  double *sur = stage + S * NA * L3, *sus = sur + L3, *sut = sus + L3;
+  double *sD = sut + L3, *sDt = sD + L2;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sDt + L2);
+
+  const int tid = threadIdx.x;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int nt = b < nelv ? (nelv - b + G - 1) / G : 0;
+  const double beta = st->beta;
+  if (tid == 0) {
+    for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+    fence_barrier_init();
+  }
+  for (int q = tid; q < L2; q += THREADS) {
+    sD[q] = D[q];
+    sDt[q] = Dt[q];
+  }
+  __syncthreads();
+  const double *src[NA] = {z, p, h1, g11, g22, g33, g12, g13, g23};
+  auto issue = [&](int t, int s) {
+    const long e = b + (long)t * G;
+    mbar_arrive_expect_tx(&full[s], (uint32_t)(NA * C::ABYTES));
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+      bulk_g2s(stage + (size_t)(s * NA + a) * L3, src[a] + e * L3, (uint32_t)C::ABYTES, &full[s]);
+  };
+  if (tid == 0)
+    for (int t = 0; t < S && t < nt; t++) issue(t, t);
+
+  const bool act = tid < L2 * KS;
+  const int col = tid % L2, kh = tid / L2;
+  const int i = col % LX, j = col / LX, k0 = kh * KP;
+  double Di[LX], Dj[LX], Dti[LX], Dtj[LX];
+#pragma unroll
+  for (int l = 0; l < LX; l++) {
+    Di[l] = sD[i + LX * l];
+    Dj[l] = sD[j + LX * l];
+    Dti[l] = sDt[i + LX * l];
+    Dtj[l] = sDt[j + LX * l];
+  }
+
+  double pap = 0.0;
+  int t = 0;
+  bool failed = false;
+  for (; t < nt; t++) {
+    const int s = t % S;
+    const bool ok = mbar_wait(&full[s], (uint32_t)((t / S) & 1));
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    const long e = b + (long)t * G;
+    const double *sz = stage + (size_t)s * NA * L3;
+    double *su = stage + (size_t)s * NA * L3 + L3;  // old p, replaced by the new
+    const double *sh = su + L3, *s11 = su + 2 * L3, *s22 = su + 3 * L3, *s33 = su + 4 * L3,
+                 *s12 = su + 5 * L3, *s13 = su + 6 * L3, *s23 = su + 7 * L3;
+    if (act) {
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int q = col + L2 * (k0 + kk);
+        const double pn = sz[q] + beta * su[q];
+        su[q] = pn;
+        p[e * L3 + q] = pn;
+      }
+    }
+    __syncthreads();  // the element's new p complete in the stage
+    double ru[LX];
+    if (act) {
+#pragma unroll
+      for (int l = 0; l < LX; l++) ru[l] = su[col + L2 * l];
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        double ur = 0, us = 0, ut = 0;
+#pragma unroll
+        for (int l = 0; l < LX; l++) {
+          ur += Di[l] * su[l + LX * j + L2 * k];
+          us += Dj[l] * su[i + LX * l + L2 * k];
+          ut += sD[k + LX * l] * ru[l];
+        }
+        const int q = col + L2 * k;
+        const double H = sh[q];
+        const double a11 = s11[q], a22 = s22[q], a33 = s33[q], a12 = s12[q], a13 = s13[q],
+                     a23 = s23[q];
+        sur[q] = H * (a11 * ur + a12 * us + a13 * ut);
+        sus[q] = H * (a12 * ur + a22 * us + a23 * ut);
+        sut[q] = H * (a13 * ur + a23 * us + a33 * ut);
+      }
+    }
+    __syncthreads();  // stage s consumed, work planes complete
+    if (tid == 0 && t + S < nt) issue(t + S, s);
+    if (act) {
+      double rt[LX];
+#pragma unroll
+      for (int l = 0; l < LX; l++) rt[l] = sut[col + L2 * l];
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const int k = k0 + kk;
+        double a = 0, c = 0, d = 0;
+#pragma unroll
+        for (int l = 0; l < LX; l++) {
+          a += Dti[l] * sur[l + LX * j + L2 * k];
+          c += Dtj[l] * sus[i + LX * l + L2 * k];
+          d += sDt[k + LX * l] * rt[l];
+        }
+        const double wq = a + c + d;
+        w[e * L3 + col + L2 * k] = wq;
+        pap += ru[k] * wq;
+      }
+    }
+    __syncthreads();  // work planes free for the next element
+  }
+  if (failed) {
+    if (tid == 0) {
+      atomicCAS(&nb_dev_error, 0, 1);
+      // bounded wait for this CTA's copies still in flight
+      for (int q = t; q < nt && q < t + S; q++) mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
+    }
+    __syncthreads();
+  }
+  double tot;  // every block takes part, a failed one with its partial sum
+  if (grid_sum<THREADS>(pap, partials, counter, &tot)) {
+    st->pap = tot;
+    st->alpha = st->rtz1 / tot;
+  }
+}
+
+template <int LX, int S, int KS>
+static cudaError_t launch_ax_cg(double *w, double *p, const double *z, const double *D,
+                                const double *Dt, const double *h1, const double *g11,
+                                const double *g22, const double *g33, const double *g12,
+                                const double *g13, const double *g23, int nelv, CgState *st,
+                                double *partials, unsigned *counter, int max_grid,
+                                cudaStream_t s) {
+  using C = AxCgCfg<LX, S, KS>;
+  auto kern = ax_cg_fused_kernel<LX, S, KS>;
+  static int grid_per_dev[64] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int &g = grid_per_dev[dev & 63];
+  if (g == 0) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::THREADS, C::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    g = (per_sm > 0 ? per_sm : 1) * sms;
+  }
+  if (nelv <= 0) return cudaErrorNotSupported;
+  int grid = nelv < g ? nelv : g;
+  if (grid > max_grid) grid = max_grid;
+  kern<<<grid, C::THREADS, C::SMEM, s>>>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
+                                          st, partials, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, const double *Dt,
+                        const double *h1, const double *g11, const double *g22, const double *g33,
+                        const double *g12, const double *g13, const double *g23, int nelv, int lx,
+                        CgState *st, double *partials, unsigned *counter, int max_grid,
+                        cudaStream_t s) {
+  const void *ptrs[] = {z, p, h1, g11, g22, g33, g12, g13, g23};
+  for (const void *q : ptrs)
+    if (reinterpret_cast<uintptr_t>(q) & 15) return cudaErrorNotSupported;
+  if (((size_t)lx * lx * lx * sizeof(double)) % 16) return cudaErrorNotSupported;
+  switch (lx) {
+    case 6: return launch_ax_cg<6, 3, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, partials, counter, max_grid, s);
+    case 8: return launch_ax_cg<8, 2, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, partials, counter, max_grid, s);
+    case 10: return launch_ax_cg<10, 2, 5>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, partials, counter, max_grid, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
 int take_device_error() {
   int v = 0, zero = 0;
   if (cudaMemcpyFromSymbol(&v, nb_dev_error, sizeof(int)) != cudaSuccess) return -1;

@@ -265,7 +265,7 @@ cudaError_t CgWorkspace::ensure(long n_) {
   base = nullptr;
   n = n_;
   const size_t vec = ((size_t)n * 8 + 255) & ~size_t(255);
-  const size_t red = 2 * 148 * 8 * sizeof(double) + 256;  // grid_sum2 needs 2 per block
+  const size_t red = 2 * kCgMaxPartials * sizeof(double) + 256;  // grid_sum2: 2 per block
   bytes = 4 * vec + red + sizeof(CgState) + 256;
   cudaError_t e = cudaMalloc(&base, bytes);
   if (e != cudaSuccess) {
@@ -278,7 +278,7 @@ cudaError_t CgWorkspace::ensure(long n_) {
   p = (double *)(b + 2 * vec);
   w = (double *)(b + 3 * vec);
   partials = (double *)(b + 4 * vec);
-  counter = (unsigned *)(b + 4 * vec + 2 * 148 * 8 * sizeof(double));
+  counter = (unsigned *)(b + 4 * vec + 2 * kCgMaxPartials * sizeof(double));
   st = (CgState *)(b + 4 * vec + red);
   e = cudaMemset(b + 4 * vec, 0, red + sizeof(CgState));
   if (e != cudaSuccess) return e;
@@ -311,13 +311,24 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
     cg_precond_dot_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.use_jacobi ? P->jdiag : nullptr,
                                                      P->mult, n, W.st, W.partials, W.counter);
   }
-  cg_update_p_kernel<<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
-  cudaError_t e = P->ax_raw(W.w, W.p, s, &W.st->done);
-  if (e != cudaSuccess) return e;
-  if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n, &W.st->done);
+  // p = z + beta p; w = A p; pap: one launch when the problem has no mask and
+  // no h2 term (the local form of pap needs p zero wherever w is masked)
+  cudaError_t e = cudaErrorNotSupported;
+  if (P->nmask == 0 && !P->ifh2 && P->use_stream_ax)
+    e = ax_cg_fused(W.w, W.p, W.z, P->D, P->Dt, P->h1, P->g11, P->g22, P->g33, P->g12, P->g13,
+                    P->g23, (int)P->nelv, P->lx, W.st, W.partials, W.counter, kCgMaxPartials, s);
+  W.fused = e == cudaSuccess;
+  if (e != cudaSuccess && e != cudaErrorNotSupported) return e;
+  if (!W.fused) {
+    cg_update_p_kernel<<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
+    e = P->ax_raw(W.w, W.p, s, &W.st->done);
+    if (e != cudaSuccess) return e;
+    if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n, &W.st->done);
+  }
   e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->done);
   if (e != cudaSuccess) return e;
-  cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, n, W.st, W.partials, W.counter);
+  if (!W.fused)
+    cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, n, W.st, W.partials, W.counter);
   cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(x, W.r, W.p, W.w, P->mult, n, W.st,
                                                  W.partials, W.counter);
   if (W.recompute_every > 0) {  // w = A x, gs, mask; r = f - w (scheduled iterations only)
@@ -390,7 +401,7 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t ce = cudaSuccess;
     for (int k = 0; k < chunk && ce == cudaSuccess; k++) ce = cg_iteration(P, W, pc, x, f, cs);
-    W.launches_per_iter = 6 + (P->ifh2 ? 1 : 0) + (pc ? pc->launches() : 0) +
+    W.launches_per_iter = (W.fused ? 4 : 6 + (P->ifh2 ? 1 : 0)) + (pc ? pc->launches() : 0) +
                           (W.recompute_every > 0 ? 3 + (P->ifh2 ? 1 : 0) : 0);
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);

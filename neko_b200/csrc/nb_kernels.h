@@ -30,6 +30,16 @@ cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h
 // Reads and clears the device error word (0 = no error).
 int take_device_error();
 
+struct CgState;
+// p = z + beta p, w = A p (no gather-scatter) and pap = sum p * w, alpha =
+// rtz / pap in one streaming launch, for problems with no mask and no h2
+// (ax_helm.cu).  cudaErrorNotSupported when lx or alignment is not covered.
+cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, const double *Dt,
+                        const double *h1, const double *g11, const double *g22, const double *g33,
+                        const double *g12, const double *g13, const double *g23, int nelv, int lx,
+                        CgState *st, double *partials, unsigned *counter, int max_grid,
+                        cudaStream_t s);
+
 // Grid size for streaming kernels: a multiple of the SM count.
 int stream_grid(long n, int threads);
 

@@ -29,6 +29,9 @@ struct Precond {
   virtual int take_error() { return 0; }
 };
 
+// Blocks a CG reduction may use (its partial sums live in the workspace).
+constexpr int kCgMaxPartials = 148 * 8;
+
 struct CgWorkspace {
   long n = 0;
   void *base = nullptr;
@@ -39,6 +42,7 @@ struct CgWorkspace {
   void *host_state = nullptr;
   bool use_jacobi = true;
   bool flexible = false;
+  bool fused = false;  // the last captured iteration used ax_cg_fused
   int recompute_every = 0;
   int launches_per_iter = 6;
   cudaGraphExec_t graph_exec = nullptr;
