@@ -32,6 +32,12 @@ sys.path.insert(0, ROOT)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 
+# DRAM bytes per point of ax_helm_tma_kernel measured by ncu on a 24^3-element
+# case (dram__bytes_read.sum + dram__bytes_write.sum, mean of two launches;
+# the part of w still dirty in L2 when the launch ends is not counted).
+AX_TRAFFIC_B_PER_POINT = {8: 70.33}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -704,16 +710,20 @@ def main():
         x.copy_(x64)
 
     # --- ax_helm roofline: events on the launching stream ----------------
+    # three timed loops of ax_reps launches; the median loop's mean launch time
     w = P.zeros()
     for _ in range(5):
         Ax.compute(w, x, P, stream=stream)
-    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a0.record(stream)
-    for _ in range(args.ax_reps):
-        Ax.compute(w, x, P, stream=stream)
-    a1.record(stream)
-    torch.cuda.synchronize()
-    t_ax = a0.elapsed_time(a1) / 1e3 / args.ax_reps
+    loops = []
+    for _ in range(3):
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.ax_reps):
+            Ax.compute(w, x, P, stream=stream)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        loops.append(a0.elapsed_time(a1) / 1e3 / args.ax_reps)
+    t_ax = sorted(loops)[1]
     peaks, peak_src = measured_peaks()
     ax_bytes = 72 * P.n  # u, w, h1, G11..G23: 9 x 8 B per point
     achieved = ax_bytes / t_ax / 1e9
@@ -735,7 +745,11 @@ def main():
                 "d2h_bytes_per_step": P.n * 8},
         "roofline": {"bound": "hbm", "kernel": f"ax_helm_tma_kernel<double,{cfg['lx']}>",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": AX_TRAFFIC_B_PER_POINT.get(cfg["lx"], 0) * P.n or None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                       "point of a 24^3-element launch (profiles/"
+                                       "ax_helm_tma_24cube_lx8_traffic.md), times the points",
                      "peak_source": peak_src, "bytes_per_launch": ax_bytes,
                      "launch_ms": t_ax * 1e3, "gdof_s": ax_gdofs},
         "gpu_launches": launches,

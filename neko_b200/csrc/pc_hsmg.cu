@@ -262,44 +262,87 @@ __global__ void schwarz_post_kernel(const T *__restrict__ ext, const int *__rest
 
 // out = (A x A x A) in per element, A(o, i) = TR ? M[i + NI*o] : M[o + NO*i];
 // the input is multiplied by `scale` first when given; ACC adds to out.
-// Computed in T; input/output converted on load/store.
+// Computed in T; input/output converted on load/store.  One element per
+// block of kT3Threads threads; every per-thread loop has a compile-time trip
+// count, so a thread's global loads are all in flight together.
+constexpr int kT3Threads = 128;
+
 template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC>
-__global__ void tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
-                               const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
-                               const int *__restrict__ skip) {
+__global__ void __launch_bounds__(kT3Threads)
+    tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
+                   const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
+                   const int *__restrict__ skip) {
   if (skip && *skip) return;
-  constexpr int I3 = NI * NI * NI, O3 = NO * NO * NO;
+  constexpr int I3 = NI * NI * NI, O3 = NO * NO * NO, NT = kT3Threads;
   __shared__ T su[I3], s1[NO * NI * NI], s2[NO * NO * NI], sA[NO * NI];
   const long e = blockIdx.x;
-  for (int q = threadIdx.x; q < I3; q += blockDim.x)
-    su[q] = scale ? (T)(in[e * I3 + q] * scale[e * I3 + q]) : (T)in[e * I3 + q];
-  for (int q = threadIdx.x; q < NO * NI; q += blockDim.x) {
+  const int tid = threadIdx.x;
+  {
+    constexpr int R = (I3 + NT - 1) / NT;
+    TIN v[R], c[R];
+#pragma unroll
+    for (int g = 0; g < R; g++) {
+      const int q = tid + g * NT;
+      v[g] = q < I3 ? in[e * I3 + q] : TIN(0);
+      c[g] = (scale && q < I3) ? scale[e * I3 + q] : TIN(1);
+    }
+#pragma unroll
+    for (int g = 0; g < R; g++) {
+      const int q = tid + g * NT;
+      if (q < I3) su[q] = scale ? (T)(v[g] * c[g]) : (T)v[g];
+    }
+  }
+  for (int q = tid; q < NO * NI; q += NT) {
     const int o = q % NO, i = q / NO;
     sA[q] = TR ? M[i + NI * o] : M[o + NO * i];  // sA(o, i) at o + NO*i
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < NO * NI * NI; q += blockDim.x) {  // x: s1(o, j, k)
-    const int o = q % NO, jk = q / NO;
-    T acc = 0;
-    for (int i = 0; i < NI; i++) acc += sA[o + NO * i] * su[i + NI * jk];
-    s1[q] = acc;
+#pragma unroll
+  for (int q0 = 0; q0 < NO * NI * NI; q0 += NT) {  // x: s1(o, j, k)
+    const int q = q0 + tid;
+    if (q < NO * NI * NI) {
+      const int o = q % NO, jk = q / NO;
+      T acc = 0;
+#pragma unroll
+      for (int i = 0; i < NI; i++) acc += sA[o + NO * i] * su[i + NI * jk];
+      s1[q] = acc;
+    }
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < NO * NO * NI; q += blockDim.x) {  // y: s2(o, p, k)
-    const int o = q % NO, p = (q / NO) % NO, k = q / (NO * NO);
-    T acc = 0;
-    for (int j = 0; j < NI; j++) acc += sA[p + NO * j] * s1[o + NO * j + NO * NI * k];
-    s2[q] = acc;
+#pragma unroll
+  for (int q0 = 0; q0 < NO * NO * NI; q0 += NT) {  // y: s2(o, p, k)
+    const int q = q0 + tid;
+    if (q < NO * NO * NI) {
+      const int o = q % NO, p = (q / NO) % NO, k = q / (NO * NO);
+      T acc = 0;
+#pragma unroll
+      for (int j = 0; j < NI; j++) acc += sA[p + NO * j] * s1[o + NO * j + NO * NI * k];
+      s2[q] = acc;
+    }
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < O3; q += blockDim.x) {  // z
-    const int op = q % (NO * NO), r = q / (NO * NO);
-    T acc = 0;
-    for (int k = 0; k < NI; k++) acc += sA[r + NO * k] * s2[op + NO * NO * k];
-    if (ACC)
-      out[e * O3 + q] = (TOUT)((T)out[e * O3 + q] + acc);
-    else
-      out[e * O3 + q] = (TOUT)acc;
+  constexpr int RO = (O3 + NT - 1) / NT;
+  TOUT prev[RO];
+  if (ACC) {
+#pragma unroll
+    for (int g = 0; g < RO; g++) {
+      const int q = tid + g * NT;
+      prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < RO; g++) {  // z
+    const int q = tid + g * NT;
+    if (q < O3) {
+      const int op = q % (NO * NO), r = q / (NO * NO);
+      T acc = 0;
+#pragma unroll
+      for (int k = 0; k < NI; k++) acc += sA[r + NO * k] * s2[op + NO * NO * k];
+      if (ACC)
+        out[e * O3 + q] = (TOUT)((T)prev[g] + acc);
+      else
+        out[e * O3 + q] = (TOUT)acc;
+    }
   }
 }
 
@@ -376,7 +419,7 @@ static cudaError_t restrict_level(int ni, int no, const TIN *in, const TIN *scal
                                   TOUT *out, long nelv, const int *skip, cudaStream_t s) {
 #define NB_R(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
-    tensor3_kernel<TIN, TOUT, T, A, B, true, false><<<(unsigned)nelv, 128, 0, s>>>(         \
+    tensor3_kernel<TIN, TOUT, T, A, B, true, false><<<(unsigned)nelv, kT3Threads, 0, s>>>(         \
         in, scale, J, out, nelv, skip);                                                     \
     return cudaGetLastError();                                                              \
   }
@@ -392,7 +435,7 @@ static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *
                                const int *skip, cudaStream_t s) {
 #define NB_P(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
-    tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, 128, 0, s>>>(         \
+    tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, kT3Threads, 0, s>>>(         \
         in, nullptr, J, out, nelv, skip);                                                   \
     return cudaGetLastError();                                                              \
   }
