@@ -238,26 +238,38 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
 
 // e(i,j,k) = ext interior + neighbours' ghost results on the first interior
 // layers (x, then y, then z, as the extrude passes add them), times the
-// overlap weight.
+// overlap weight.  The neighbour table is read up front and every operand
+// load is issued before the first add, so a thread waits on one round trip.
 template <typename T, int LX>
-__global__ void schwarz_post_kernel(const T *__restrict__ ext, const int *__restrict__ fn,
-                                    const T *__restrict__ wt, T *__restrict__ out, long nelv,
-                                    const int *__restrict__ skip) {
+__global__ void __launch_bounds__(256)
+    schwarz_post_kernel(const T *__restrict__ ext, const int *__restrict__ fn,
+                        const T *__restrict__ wt, T *__restrict__ out, long nelv,
+                        const int *__restrict__ skip) {
   if (skip && *skip) return;
   constexpr int NL = LX + 2, L2 = LX * LX, L3 = L2 * LX, N2 = NL * NL, N3 = N2 * NL;
   const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (p >= nelv * L3) return;
   const long e = p / L3;
   const int q = (int)(p - e * L3), i = q % LX, j = (q / LX) % LX, k = q / L2;
-  const int *f = fn + e * 6;
+  const int2 *f2 = reinterpret_cast<const int2 *>(fn + e * 6);
+  const int2 fa = __ldg(f2), fb = __ldg(f2 + 1), fc = __ldg(f2 + 2);
+  const int f[6] = {fa.x, fa.y, fb.x, fb.y, fc.x, fc.y};
+  // the six candidate neighbour contributions: (condition, address)
+  const bool c[6] = {i == 1 && f[0], i == LX - 2 && f[1], j == 1 && f[2],
+                     j == LX - 2 && f[3], k == 1 && f[4], k == LX - 2 && f[5]};
+  const long in = (long)NL * (j + 1) + (long)N2 * (k + 1), jn = (i + 1) + (long)N2 * (k + 1),
+             kn = (i + 1) + (long)NL * (j + 1);
+  const long off[6] = {(NL - 1) + in, 0 + in, NL * (NL - 1) + jn, 0 + jn, N2 * (NL - 1) + kn,
+                       0 + kn};
+  T g[6];
+#pragma unroll
+  for (int d = 0; d < 6; d++) g[d] = c[d] ? ext[(long)(f[d] - 1) * N3 + off[d]] : T(0);
   T v = ext[e * N3 + (i + 1) + NL * (j + 1) + N2 * (k + 1)];
-  if (i == 1 && f[0]) v += ext[(long)(f[0] - 1) * N3 + (NL - 1) + NL * (j + 1) + N2 * (k + 1)];
-  if (i == LX - 2 && f[1]) v += ext[(long)(f[1] - 1) * N3 + 0 + NL * (j + 1) + N2 * (k + 1)];
-  if (j == 1 && f[2]) v += ext[(long)(f[2] - 1) * N3 + (i + 1) + NL * (NL - 1) + N2 * (k + 1)];
-  if (j == LX - 2 && f[3]) v += ext[(long)(f[3] - 1) * N3 + (i + 1) + 0 + N2 * (k + 1)];
-  if (k == 1 && f[4]) v += ext[(long)(f[4] - 1) * N3 + (i + 1) + NL * (j + 1) + N2 * (NL - 1)];
-  if (k == LX - 2 && f[5]) v += ext[(long)(f[5] - 1) * N3 + (i + 1) + NL * (j + 1) + 0];
-  out[p] = v * wt[p];
+  const T w = wt[p];
+#pragma unroll
+  for (int d = 0; d < 6; d++)
+    if (c[d]) v += g[d];
+  out[p] = v * w;
 }
 
 // out = (A x A x A) in per element, A(o, i) = TR ? M[i + NI*o] : M[o + NO*i];
