@@ -36,6 +36,8 @@
 namespace nb {
 
 constexpr int kCoarseThreads = 512;
+constexpr int kU = 4;   // points per thread whose loads are issued together
+constexpr int kUA = 2;  // the same for the operator phase (nine operands a point)
 constexpr unsigned kBarrierPolls = 1u << 22;
 
 // Grid barrier on one 32-bit word: every block adds 1 except block 0,
@@ -194,17 +196,33 @@ __global__ void __launch_bounds__(kCoarseThreads)
   for (long t = t0; t < nitems; t += stride) gs_add_item<double>(a.f, a.gs, (int)t, true, nullptr);
   if (!grid_barrier(a.bar, a.err)) return;
 
-  // x = 0, p = 0, r = f, z = d r; (r, mult r), (r, mult z)
+  // x = 0, p = 0, r = f, z = d r; (r, mult r), (r, mult z).  Point loops run
+  // in chunks of kU points per thread with every load of a chunk issued
+  // before its first use; sums still follow the points in order.
   double s_rr = 0.0, s_rz = 0.0;
-  for (long q = t0; q < nc; q += stride) {
-    const double ri = a.f[q], m = __ldg(a.mult + q);
-    a.x[q] = 0.0;
-    a.p[q] = 0.0;
-    a.r[q] = ri;
-    const double zi = ri * __ldg(a.dinv + q);
-    a.z[q] = zi;
-    s_rr += ri * m * ri;
-    s_rz += ri * m * zi;
+  for (long q0 = t0; q0 < nc; q0 += kU * stride) {
+    double ri[kU], m[kU], dv[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const long q = q0 + u * stride;
+      const bool ok = q < nc;
+      ri[u] = ok ? a.f[q] : 0.0;
+      m[u] = ok ? __ldg(a.mult + q) : 0.0;
+      dv[u] = ok ? __ldg(a.dinv + q) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const long q = q0 + u * stride;
+      if (q < nc) {
+        a.x[q] = 0.0;
+        a.p[q] = 0.0;
+        a.r[q] = ri[u];
+        const double zi = ri[u] * dv[u];
+        a.z[q] = zi;
+        s_rr += ri[u] * m[u] * ri[u];
+        s_rz += ri[u] * m[u] * zi;
+      }
+    }
   }
   double rtr, rtz;
   if (!allsum2(s_rr, s_rz, rtr, rtz)) return;
@@ -220,21 +238,36 @@ __global__ void __launch_bounds__(kCoarseThreads)
     const double beta = iter == 0 ? 0.0 : rtz / rtz_old;
     // p = z + beta p; w = A p (local); (p, w_local)
     double s_pw = 0.0;
-    for (long qb = t0 - lane; qb < nc; qb += stride) {
-      const long q = qb + lane;
-      const bool act = q < nc;
-      double pq = 0, H = 0, G11 = 0, G22 = 0, G33 = 0, G12 = 0, G13 = 0, G23 = 0;
-      if (act) {
-        pq = a.z[q] + beta * a.p[q];
-        a.p[q] = pq;
-        H = __ldg(a.h1 + q);
-        G11 = __ldg(a.g11 + q), G22 = __ldg(a.g22 + q), G33 = __ldg(a.g33 + q);
-        G12 = __ldg(a.g12 + q), G13 = __ldg(a.g13 + q), G23 = __ldg(a.g23 + q);
+    for (long qb0 = t0 - lane; qb0 < nc; qb0 += kUA * stride) {
+      double zq[kUA], pq[kUA], H[kUA], G11[kUA], G22[kUA], G33[kUA], G12[kUA], G13[kUA], G23[kUA];
+#pragma unroll
+      for (int u = 0; u < kUA; u++) {
+        const long q = qb0 + u * stride + lane;
+        const bool act = q < nc;
+        zq[u] = act ? a.z[q] : 0.0;
+        pq[u] = act ? a.p[q] : 0.0;
+        H[u] = act ? __ldg(a.h1 + q) : 0.0;
+        G11[u] = act ? __ldg(a.g11 + q) : 0.0;
+        G22[u] = act ? __ldg(a.g22 + q) : 0.0;
+        G33[u] = act ? __ldg(a.g33 + q) : 0.0;
+        G12[u] = act ? __ldg(a.g12 + q) : 0.0;
+        G13[u] = act ? __ldg(a.g13 + q) : 0.0;
+        G23[u] = act ? __ldg(a.g23 + q) : 0.0;
       }
-      const double wq = ax_lx2(pq, lane, sD, sDt, H, G11, G22, G33, G12, G13, G23);
-      if (act) {
-        a.w[q] = wq;
-        s_pw += pq * wq;
+#pragma unroll
+      for (int u = 0; u < kUA; u++) {
+        const long qb = qb0 + u * stride;
+        if (qb >= nc) break;  // warp-uniform: qb is the warp's first point
+        const long q = qb + lane;
+        const bool act = q < nc;
+        const double pn = act ? zq[u] + beta * pq[u] : 0.0;
+        if (act) a.p[q] = pn;
+        const double wq =
+            ax_lx2(pn, lane, sD, sDt, H[u], G11[u], G22[u], G33[u], G12[u], G13[u], G23[u]);
+        if (act) {
+          a.w[q] = wq;
+          s_pw += pn * wq;
+        }
       }
     }
     double pap, unused;
@@ -247,14 +280,32 @@ __global__ void __launch_bounds__(kCoarseThreads)
     s_rr = 0.0;
     s_rz = 0.0;
     const double malpha = -alpha;
-    for (long q = t0; q < nc; q += stride) {
-      a.x[q] = a.x[q] + alpha * a.p[q];
-      const double ri = a.r[q] + malpha * a.w[q], m = __ldg(a.mult + q);
-      a.r[q] = ri;
-      const double zi = ri * __ldg(a.dinv + q);
-      a.z[q] = zi;
-      s_rr += ri * m * ri;
-      s_rz += ri * m * zi;
+    for (long q0 = t0; q0 < nc; q0 += kU * stride) {
+      double xq[kU], pq[kU], rq[kU], wq[kU], m[kU], dv[kU];
+#pragma unroll
+      for (int u = 0; u < kU; u++) {
+        const long q = q0 + u * stride;
+        const bool ok = q < nc;
+        xq[u] = ok ? a.x[q] : 0.0;
+        pq[u] = ok ? a.p[q] : 0.0;
+        rq[u] = ok ? a.r[q] : 0.0;
+        wq[u] = ok ? a.w[q] : 0.0;
+        m[u] = ok ? __ldg(a.mult + q) : 0.0;
+        dv[u] = ok ? __ldg(a.dinv + q) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; u++) {
+        const long q = q0 + u * stride;
+        if (q < nc) {
+          a.x[q] = xq[u] + alpha * pq[u];
+          const double ri = rq[u] + malpha * wq[u];
+          a.r[q] = ri;
+          const double zi = ri * dv[u];
+          a.z[q] = zi;
+          s_rr += ri * m[u] * ri;
+          s_rz += ri * m[u] * zi;
+        }
+      }
     }
     double rtz_new;
     if (!allsum2(s_rr, s_rz, rtr, rtz_new)) return;

@@ -39,7 +39,8 @@ namespace nb {
 // e = S (D^-1) S' r on the extended element (NL = lx + 2 points a side),
 // ghost layer gathered from the neighbours (fn: 1-based neighbour per face,
 // 0 = none).  One block (one warp; two for NL >= 13) per element holds the
-// element in shared memory and runs the six tensor passes.  Each pass
+// element in shared memory and runs the six tensor passes; for NL <= 7 one
+// warp holds four elements, eight lanes each.  Each pass
 // contracts the first index and writes its result with that index moved
 // last (out(m,n,i) = sum_l M(i,l) in(l,m,n)), so after three passes the
 // order is back to (i,j,k).  A lane owns M lines of the pass and all NL
@@ -59,16 +60,22 @@ namespace nb {
 template <typename T, int NL>
 struct FdmCfg {
   static constexpr int N2 = NL * NL, N3 = N2 * NL;
-  static constexpr int W = ((N2 + 31) / 32) * NL <= 64 ? 1 : 2;  // warps per element
+  // small elements share a warp: EPW elements of LPE lanes each
+  static constexpr int EPW = NL <= 7 ? 4 : 1;
+  static constexpr int W = EPW > 1 ? 1 : ((N2 + 31) / 32) * NL <= 64 ? 1 : 2;  // warps
   static constexpr int TPE = 32 * W;                             // threads per block
-  static constexpr int M = (N2 + TPE - 1) / TPE;                 // lines per lane
+  static constexpr int LPE = TPE / EPW;                          // lanes per element
+  static constexpr int M = (N2 + LPE - 1) / LPE;                 // lines per lane
   static constexpr int LA = (N2 + M - 1) / M;                    // lanes with lines
   static constexpr int NLP = NL == 16 ? 17 : NL;
   static constexpr int G = NL == 8 ? 2 : NL == 12 ? 3 : 4;
   static constexpr int C = (NL % 2 == 0 && NL != 16) ? 1 : 0;
   static constexpr int BUF = (NLP * (N2 - 1) + ((N2 - 1) >> G) * C + NL + 1) / 2 * 2;
-  static constexpr int STR = 2 * BUF + 3 * N2 + 3 * NL + 1;
-  static constexpr size_t SMEM = ((size_t)STR * sizeof(T) + 15) / 16 * 16;
+  static constexpr int STR0 = 2 * BUF + 3 * N2 + 3 * NL + 1;
+  // per-element stride; with several elements in a warp it is 9 mod 16
+  // values, which keeps the line reads of neighbouring elements in distinct banks
+  static constexpr int STR = EPW > 1 ? STR0 + ((9 - STR0 % 16) + 16) % 16 : STR0;
+  static constexpr size_t SMEM = ((size_t)EPW * STR * sizeof(T) + 15) / 16 * 16;
   // resident blocks per SM the register allocation is sized for: what the
   // shared memory allows (228 KB, 1 KB reserved per block), fewer if the
   // M x NL sums and the operands in flight would not fit in the registers
@@ -170,24 +177,26 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
                int nelv, const int *__restrict__ skip) {
   if (skip && *skip) return;
   using C = FdmCfg<T, NL>;
-  constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = C::N2, N3 = C::N3,
-                TPE = C::TPE;
+  constexpr int LX = NL - 2, L2 = LX * LX, L3 = L2 * LX, N2 = C::N2, N3 = C::N3;
   extern __shared__ __align__(16) unsigned char fdm_smem[];
-  T *b0 = reinterpret_cast<T *>(fdm_smem), *b1 = b0 + C::BUF;
+  const int es = threadIdx.x / C::LPE, ul = threadIdx.x - es * C::LPE;
+  T *b0 = reinterpret_cast<T *>(fdm_smem) + es * C::STR, *b1 = b0 + C::BUF;
   T *sS = b1 + C::BUF;  // S_x, S_y, S_z: S(l,i) at l + NL*i
   T *sL = sS + 3 * N2;  // spectra + eps
-  const long e = blockIdx.x;
-  if (e >= nelv) return;
-  const int u = threadIdx.x;
-  {
+  const long e = (long)blockIdx.x * C::EPW + es;
+  if ((long)blockIdx.x * C::EPW >= nelv) return;
+  const bool active = e < nelv;
+  const int u = active ? ul : C::LPE;  // lanes of a missing element do no work
+  constexpr int LPE = C::LPE;
+  if (active) {
     const TIN *re = r + e * L3;
 #pragma unroll 4
-    for (int q = u; q < L3; q += TPE) {  // interior: ext(a+1, b+1, c+1) = r(a, b, c)
+    for (int q = u; q < L3; q += LPE) {  // interior: ext(a+1, b+1, c+1) = r(a, b, c)
       const int a = q % LX, b = (q / LX) % LX, c = q / L2;
       gather_elem<TIN, T>(b0 + C::pos((b + 1) + NL * (c + 1), a + 1), re + q, true);
     }
 #pragma unroll 2
-    for (int q = u; q < 6 * L2; q += TPE) {  // faces: the neighbour's first interior layer
+    for (int q = u; q < 6 * L2; q += LPE) {  // faces: the neighbour's first interior layer
       const int f = q / L2, w = q - f * L2, s1 = w % LX + 1, s2 = w / LX + 1, dir = f >> 1;
       const int cb = (f & 1) ? NL - 1 : 0;   // ghost coordinate across the face
       const int cs = (f & 1) ? 2 : LX - 1;   // its source: the neighbour's layer 1 / LX-2
@@ -200,7 +209,7 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
                              : r,
                           nb != 0);
     }
-    for (int q = u; q < 12 * LX + 8; q += TPE) {  // edges and corners: zero
+    for (int q = u; q < 12 * LX + 8; q += LPE) {  // edges and corners: zero
       int a, b, c;
       if (q < 12 * LX) {
         const int E = q / LX, s = q - E * LX + 1, D = E >> 2;
@@ -216,11 +225,11 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
       }
       b0[C::pos(b + NL * c, a)] = T(0);
     }
-    for (int q = u; q < 3 * N2; q += TPE) cp_async_elem<T>(sS + q, S + e * 3 * N2 + q, true);
-    for (int q = u; q < 3 * NL; q += TPE) cp_async_elem<T>(sL + q, lam + e * 3 * NL + q, true);
+    for (int q = u; q < 3 * N2; q += LPE) cp_async_elem<T>(sS + q, S + e * 3 * N2 + q, true);
+    for (int q = u; q < 3 * NL; q += LPE) cp_async_elem<T>(sL + q, lam + e * 3 * NL + q, true);
     if (u == 0) cp_async_elem<T>(sL + 3 * NL, eps + e, true);
-    cp_async_wait_all();
   }
+  cp_async_wait_all();
   __syncthreads();
   // forward: b0 -> b1 -> b0 -> b1; backward (D^-1 on the first read): b1 -> b0 -> b1 -> out
   fdm_pass<T, NL, true, false>(b0, b1, sS, sL, nullptr, u);
@@ -400,7 +409,8 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
     if (err != cudaSuccess) return err;
     attr_set = true;
   }
-  kern<<<(unsigned)L.nelv, C::TPE, C::SMEM, s>>>(r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv,
+  kern<<<(unsigned)((L.nelv + C::EPW - 1) / C::EPW), C::TPE, C::SMEM, s>>>(
+      r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv,
                                                    skip);
   const long n = L.nelv * LX * LX * LX;
   schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.ext, L.fn, L.wt, e,
