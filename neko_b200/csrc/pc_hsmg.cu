@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(256)
 }
 
 // out = (A x A x A) in per element, A(o, i) = TR ? M[i + NI*o] : M[o + NO*i];
-// the input is multiplied by `scale` first when given; ACC adds to out.
+// without ACC the input is multiplied by `scale` first when given; ACC adds
+// the result to out, times `scale` at the output point when given.
 // Computed in T; input/output converted on load/store.  One element per
 // block of kT3Threads threads; every per-thread loop has a compile-time trip
 // count, so a thread's global loads are all in flight together.
@@ -305,12 +306,12 @@ __global__ void __launch_bounds__(kT3Threads)
     for (int g = 0; g < R; g++) {
       const int q = tid + g * NT;
       v[g] = q < I3 ? in[e * I3 + q] : TIN(0);
-      c[g] = (scale && q < I3) ? scale[e * I3 + q] : TIN(1);
+      c[g] = (!ACC && scale && q < I3) ? scale[e * I3 + q] : TIN(1);
     }
 #pragma unroll
     for (int g = 0; g < R; g++) {
       const int q = tid + g * NT;
-      if (q < I3) su[q] = scale ? (T)(v[g] * c[g]) : (T)v[g];
+      if (q < I3) su[q] = (!ACC && scale) ? (T)(v[g] * c[g]) : (T)v[g];
     }
   }
   for (int q = tid; q < NO * NI; q += NT) {
@@ -344,11 +345,13 @@ __global__ void __launch_bounds__(kT3Threads)
   __syncthreads();
   constexpr int RO = (O3 + NT - 1) / NT;
   TOUT prev[RO];
+  TIN oscale[RO];
   if (ACC) {
 #pragma unroll
     for (int g = 0; g < RO; g++) {
       const int q = tid + g * NT;
       prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
+      oscale[g] = (scale && q < O3) ? scale[e * O3 + q] : TIN(1);
     }
   }
 #pragma unroll
@@ -359,7 +362,9 @@ __global__ void __launch_bounds__(kT3Threads)
       T acc = 0;
 #pragma unroll
       for (int k = 0; k < NI; k++) acc += sA[r + NO * k] * s2[op + NO * NO * k];
-      if (ACC)
+      if (ACC && scale)
+        out[e * O3 + q] = (TOUT)((T)prev[g] + (T)oscale[g] * acc);
+      else if (ACC)
         out[e * O3 + q] = (TOUT)((T)prev[g] + acc);
       else
         out[e * O3 + q] = (TOUT)acc;
@@ -421,7 +426,7 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
 // e = Schwarz(r) on level L (r already masked): FDM + overlap + gs + mask.
 template <typename TIN, typename T>
 static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, bool assemble = true) {
   cudaError_t err;
   switch (L.lx) {
 #define NB_S(N) \
@@ -431,7 +436,7 @@ static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, c
 #undef NB_S
     default: return cudaErrorNotSupported;
   }
-  if (err != cudaSuccess) return err;
+  if (err != cudaSuccess || !assemble) return err;
   return gs_add_fused<T>(L.P->gsd, e, true, s, skip);
 }
 
@@ -454,11 +459,11 @@ static cudaError_t restrict_level(int ni, int no, const TIN *in, const TIN *scal
 // prolongation out += (J x J x J) in from ni to no points (J: no x ni)
 template <typename TIN, typename TOUT, typename T>
 static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *out, long nelv,
-                               const int *skip, cudaStream_t s) {
+                               const int *skip, cudaStream_t s, const TIN *oscale = nullptr) {
 #define NB_P(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
     tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, kT3Threads, 0, s>>>(         \
-        in, nullptr, J, out, nelv, skip);                                                   \
+        in, oscale, J, out, nelv, skip);                                                    \
     return cudaGetLastError();                                                              \
   }
   NB_P(2, 4) NB_P(2, 3) NB_P(4, 5) NB_P(4, 6) NB_P(4, 7) NB_P(4, 8) NB_P(4, 9) NB_P(4, 10)
@@ -521,10 +526,14 @@ struct HsmgImpl : public HsmgState {
   CgState *stc = nullptr;
   CoarseArgs<T> ca;
 
+  // The fine level has no masked point: its Schwarz gather-scatter merges
+  // into the final one.
+  bool merged_assembly() const { return fine->nmask == 0; }
+
   int launches() const override {
     // 2 Schwarz x (fdm, post, gs) + restrict + gs + coarse (one launch) +
-    // prolong + final gs (+ convert)
-    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0);
+    // prolong + final gs (+ convert); one gs fewer when merged
+    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0) - (merged_assembly() ? 1 : 0);
   }
 
   int take_error() override {
@@ -560,17 +569,24 @@ struct HsmgImpl : public HsmgState {
     ca.skip = skip;
     if ((e = hsmg_coarse_solve<T>(ca, mid->lx, kCoarseMaxBlocks, hi)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(ev_join_hi, hi)) != cudaSuccess) return e;
-    // fine Schwarz on the side stream: zs = S_f r
-    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side)) != cudaSuccess) return e;
+    // fine Schwarz on the side stream: zs = S_f r (left unassembled when the
+    // final gather-scatter takes it, see below)
+    const bool merged = merged_assembly();
+    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side, !merged)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(ev_join, side)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s, ev_join, 0)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(s, ev_join_hi, 0)) != cudaSuccess)
       return e;
-    // prolong: zs += J e_mid; z = mult * gs(zs)
-    if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s)) !=
+    // prolong: zs += J e_mid; z = mult * gs(zs).  Without a mask the fine
+    // Schwarz output's own gather-scatter is folded into this one: wt and
+    // mult are the same at every copy of a point, so
+    // mult gs(gs(wt e) + J e_mid) = gs(wt e + mult J e_mid).
+    if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s,
+                                  merged ? mult_f : nullptr)) != cudaSuccess)
+      return e;
+    if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, merged ? nullptr : mult_f)) !=
         cudaSuccess)
       return e;
-    if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, mult_f)) != cudaSuccess) return e;
     if (sizeof(T) == 4)
       convert_kernel<T, double><<<stream_grid(fine->n, 256), 256, 0, s>>>(z, zs, fine->n, skip);
     return cudaGetLastError();
