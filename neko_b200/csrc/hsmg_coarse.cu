@@ -141,6 +141,67 @@ __device__ __forceinline__ double ax_lx2(double p, int lane, const double *D, co
   return acc + acc2 + acc3;
 }
 
+
+// The thread's first gather-scatter item, its point indices kept in shared
+// memory for the whole launch (the coarse solve runs the same gather-scatter
+// eleven times): kind 0 none, 1 pair, 2 segment of up to kGsCache points,
+// 3 masked point, 4 not cached (longer segment: gs_add_item each time).
+constexpr int kGsCache = 8;
+struct GsSlot {
+  int idx[kGsCache];
+  int kind, len, masked;
+};
+
+__device__ __forceinline__ void gs_cache_item(GsSlot &c, const GsDevice &g, long t) {
+  c.kind = 0;
+  if (t >= gs_items(g, true)) return;
+  if (t < g.npairs) {
+    const int2 p = __ldg(g.pairs + t);
+    c.kind = 1, c.len = 2, c.idx[0] = p.x, c.idx[1] = p.y;
+    c.masked = g.pair_masked ? g.pair_masked[t] : 0;
+    return;
+  }
+  long q = t - g.npairs;
+  if (q < g.nseg) {
+    const int a = __ldg(g.seg_ptr + q), b = __ldg(g.seg_ptr + q + 1);
+    if (b - a > kGsCache) {
+      c.kind = 4;
+      return;
+    }
+    c.kind = 2, c.len = b - a;
+    for (int k = 0; k < b - a; k++) c.idx[k] = __ldg(g.seg_idx + a + k);
+    c.masked = g.seg_masked ? g.seg_masked[q] : 0;
+    return;
+  }
+  q -= g.nseg;
+  c.kind = 3, c.len = 1, c.idx[0] = __ldg(g.extra_mask + q);
+}
+
+// gs_add_item (with mask, no scale) on a cached item: the same sums in the
+// same order.
+__device__ __forceinline__ void gs_cached_add(double *__restrict__ u, const GsSlot &c) {
+  if (c.kind == 1) {
+    double s = u[c.idx[0]] + u[c.idx[1]];
+    if (c.masked) s = 0.0;
+    u[c.idx[0]] = s;
+    u[c.idx[1]] = s;
+  } else if (c.kind == 2) {
+    double v[kGsCache];
+#pragma unroll
+    for (int k = 0; k < kGsCache; k++) v[k] = k < c.len ? u[c.idx[k]] : 0.0;
+    double s = v[0];
+#pragma unroll
+    for (int k = 1; k < kGsCache; k++)
+      if (k < c.len) s = s + v[k];
+    if (c.masked) s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kGsCache; k++)
+      if (k < c.len) u[c.idx[k]] = s;
+  } else if (c.kind == 3) {
+    u[c.idx[0]] = 0.0;
+  }
+}
+
 template <typename T, int LM>
 __global__ void __launch_bounds__(kCoarseThreads)
     hsmg_coarse_kernel(const CoarseArgs<T> a) {
@@ -193,7 +254,20 @@ __global__ void __launch_bounds__(kCoarseThreads)
   }
   if (!grid_barrier(a.bar, a.err)) return;
   const long nitems = gs_items(a.gs, true);
-  for (long t = t0; t < nitems; t += stride) gs_add_item<double>(a.f, a.gs, (int)t, true, nullptr);
+  __shared__ GsSlot gslot[kCoarseThreads];
+  gs_cache_item(gslot[threadIdx.x], a.gs, t0);
+  // gs + mask: the first item from the cache, further ones (more items
+  // than threads) as usual
+  auto gs_phase = [&](double *u) {
+    const GsSlot &c = gslot[threadIdx.x];
+    if (c.kind == 4)
+      gs_add_item<double>(u, a.gs, (int)t0, true, nullptr);
+    else
+      gs_cached_add(u, c);
+    for (long t = t0 + stride; t < nitems; t += stride)
+      gs_add_item<double>(u, a.gs, (int)t, true, nullptr);
+  };
+  gs_phase(a.f);
   if (!grid_barrier(a.bar, a.err)) return;
 
   // x = 0, p = 0, r = f, z = d r; (r, mult r), (r, mult z).  Point loops run
@@ -273,8 +347,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
     double pap, unused;
     if (!allsum2(s_pw, 0.0, pap, unused)) return;
     const double alpha = rtz / pap;
-    for (long t = t0; t < nitems; t += stride)
-      gs_add_item<double>(a.w, a.gs, (int)t, true, nullptr);
+    gs_phase(a.w);
     if (!grid_barrier(a.bar, a.err)) return;
     // x += alpha p; r -= alpha w; z = d r; (r, mult r), (r, mult z)
     s_rr = 0.0;
