@@ -28,6 +28,10 @@
 
 namespace nb {
 
+// Weight of point i: the FP32 copy of mult when the problem keeps one (every
+// value exact in FP32, so the product is the same), else the FP64 array.
+#define MW(i) (multf ? (double)multf[i] : mult[i])
+
 __global__ void jacobi_scale_kernel(double *d, const double *h1, const double *h2,
                                     const double *B, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
@@ -53,7 +57,7 @@ __global__ void addcol4_kernel(double *w, const double *h2, const double *B, con
 // x = 0, p = 0, r = f, rtr = (r, mult r) -> res_start.
 __global__ void __launch_bounds__(kRedThreads)
     cg_init_kernel(double *__restrict__ x, double *__restrict__ p, double *__restrict__ r,
-                   const double *__restrict__ f, const double *__restrict__ mult, long n,
+                   const double *__restrict__ f, const double *__restrict__ mult, const float *__restrict__ multf, long n,
                    CgState *st, double *partials, unsigned *counter,
                    const int *__restrict__ outer_skip) {
   if (outer_skip && *outer_skip) {  // enclosing solve finished: stay idle
@@ -67,7 +71,7 @@ __global__ void __launch_bounds__(kRedThreads)
     x[i] = 0.0;
     p[i] = 0.0;
     r[i] = ri;
-    s += ri * mult[i] * ri;
+    s += ri * MW(i) * ri;
   }
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
@@ -88,7 +92,7 @@ __global__ void __launch_bounds__(kRedThreads)
 // rtz = (r, mult z); beta from the previous rtz.
 __global__ void __launch_bounds__(kRedThreads)
     cg_precond_dot_kernel(double *__restrict__ z, const double *__restrict__ r,
-                          const double *__restrict__ d, const double *__restrict__ mult,
+                          const double *__restrict__ d, const double *__restrict__ mult, const float *__restrict__ multf,
                           long n, CgState *st, double *partials, unsigned *counter) {
   if (st->done) return;
   double s = 0.0;
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(kRedThreads)
     const double ri = r[i];
     const double zi = d ? ri * d[i] : ri;
     z[i] = zi;
-    s += ri * mult[i] * zi;
+    s += ri * MW(i) * zi;
   }
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
@@ -111,13 +115,13 @@ __global__ void __launch_bounds__(kRedThreads)
 // rtz = (r, mult z) for an externally applied preconditioner.
 __global__ void __launch_bounds__(kRedThreads)
     cg_dot_rz_kernel(const double *__restrict__ z, const double *__restrict__ r,
-                     const double *__restrict__ mult, long n, CgState *st, double *partials,
+                     const double *__restrict__ mult, const float *__restrict__ multf, long n, CgState *st, double *partials,
                      unsigned *counter) {
   if (st->done) return;
   double s = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads)
-    s += r[i] * mult[i] * z[i];
+    s += r[i] * MW(i) * z[i];
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
     st->rtz2 = st->rtz1;
@@ -132,13 +136,13 @@ __global__ void __launch_bounds__(kRedThreads)
 // r_k - r_(k-1) = -alpha_(k-1) w_(k-1) and w still holds w_(k-1) here.
 __global__ void __launch_bounds__(kRedThreads)
     cg_dot_rz_flex_kernel(const double *__restrict__ z, const double *__restrict__ r,
-                          const double *__restrict__ w_prev, const double *__restrict__ mult,
+                          const double *__restrict__ w_prev, const double *__restrict__ mult, const float *__restrict__ multf,
                           long n, CgState *st, double *partials, unsigned *counter) {
   if (st->done) return;
   double s0 = 0.0, s1 = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads) {
-    const double mz = mult[i] * z[i];
+    const double mz = MW(i) * z[i];
     s0 += r[i] * mz;
     s1 += w_prev[i] * mz;
   }
@@ -164,13 +168,13 @@ __global__ void cg_update_p_kernel(double *__restrict__ p, const double *__restr
 // pap = (w, mult p); alpha = rtz / pap
 __global__ void __launch_bounds__(kRedThreads)
     cg_pap_kernel(const double *__restrict__ w, const double *__restrict__ p,
-                  const double *__restrict__ mult, long n, CgState *st, double *partials,
+                  const double *__restrict__ mult, const float *__restrict__ multf, long n, CgState *st, double *partials,
                   unsigned *counter) {
   if (st->done) return;
   double s = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads)
-    s += w[i] * mult[i] * p[i];
+    s += w[i] * MW(i) * p[i];
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
     st->pap = tot;
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(kRedThreads)
 __global__ void __launch_bounds__(kRedThreads)
     cg_update_xr_kernel(double *__restrict__ x, double *__restrict__ r,
                         const double *__restrict__ p, const double *__restrict__ w,
-                        const double *__restrict__ mult, long n, CgState *st,
+                        const double *__restrict__ mult, const float *__restrict__ multf, long n, CgState *st,
                         double *partials, unsigned *counter) {
   if (st->done) return;
   const double alpha = st->alpha, malpha = -alpha;
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(kRedThreads)
     x[i] = x[i] + alpha * p[i];
     const double ri = r[i] + malpha * w[i];
     r[i] = ri;
-    s += ri * mult[i] * ri;
+    s += ri * MW(i) * ri;
   }
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
@@ -216,7 +220,7 @@ __global__ void __launch_bounds__(kRedThreads)
 // convergence test redone on it; the next direction restarts (beta = 0).
 __global__ void __launch_bounds__(kRedThreads)
     cg_true_residual_kernel(double *__restrict__ r, const double *__restrict__ f,
-                            const double *__restrict__ w, const double *__restrict__ mult, long n,
+                            const double *__restrict__ w, const double *__restrict__ mult, const float *__restrict__ multf, long n,
                             CgState *st, double *partials, unsigned *counter) {
   if (st->skip_rc) return;
   double s = 0.0;
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(kRedThreads)
        i += (long)gridDim.x * kRedThreads) {
     const double ri = f[i] - w[i];
     r[i] = ri;
-    s += ri * mult[i] * ri;
+    s += ri * MW(i) * ri;
   }
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
@@ -302,14 +306,14 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
     cudaError_t e = pc->apply(W.z, W.r, &W.st->done, s);
     if (e != cudaSuccess) return e;
     if (W.flexible)
-      cg_dot_rz_flex_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.w, P->mult, n, W.st,
+      cg_dot_rz_flex_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.w, P->mult, P->multf, n, W.st,
                                                        W.partials, W.counter);
     else
-      cg_dot_rz_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, n, W.st, W.partials,
+      cg_dot_rz_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, P->multf, n, W.st, W.partials,
                                                   W.counter);
   } else {
     cg_precond_dot_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.use_jacobi ? P->jdiag : nullptr,
-                                                     P->mult, n, W.st, W.partials, W.counter);
+                                                     P->mult, P->multf, n, W.st, W.partials, W.counter);
   }
   // p = z + beta p; w = A p; pap: one launch when the problem has no mask and
   // no h2 term (the local form of pap needs p zero wherever w is masked)
@@ -328,8 +332,8 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
   e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->done);
   if (e != cudaSuccess) return e;
   if (!W.fused)
-    cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, n, W.st, W.partials, W.counter);
-  cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(x, W.r, W.p, W.w, P->mult, n, W.st,
+    cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, P->multf, n, W.st, W.partials, W.counter);
+  cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(x, W.r, W.p, W.w, P->mult, P->multf, n, W.st,
                                                  W.partials, W.counter);
   if (W.recompute_every > 0) {  // w = A x, gs, mask; r = f - w (scheduled iterations only)
     e = P->ax_raw(W.w, x, s, &W.st->skip_rc);
@@ -337,7 +341,7 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
     if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, x, n, &W.st->skip_rc);
     e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->skip_rc);
     if (e != cudaSuccess) return e;
-    cg_true_residual_kernel<<<rb, kRedThreads, 0, s>>>(W.r, f, W.w, P->mult, n, W.st,
+    cg_true_residual_kernel<<<rb, kRedThreads, 0, s>>>(W.r, f, W.w, P->mult, P->multf, n, W.st,
                                                        W.partials, W.counter);
   }
   return cudaGetLastError();
@@ -380,7 +384,7 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
   init.skip_rc = 1;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const long n = P->n;
-  cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(x, W.p, W.r, f, P->mult, n, W.st,
+  cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(x, W.p, W.r, f, P->mult, P->multf, n, W.st,
                                                         W.partials, W.counter, nullptr);
   NB_CUDA_TRY(cudaGetLastError());
   // (Re)capture the iteration graph when the operands changed.

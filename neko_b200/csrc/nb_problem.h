@@ -47,6 +47,7 @@ struct nb_problem {
   int *dof_gs = nullptr, *gs_dof = nullptr, *blk_len = nullptr, *blk_off = nullptr,
       *msk = nullptr;
   unsigned char *dfrmd = nullptr;
+  float *multf = nullptr;  // mult in FP32 when every value is exact there, else null
   double *red_partials = nullptr, *red_out = nullptr;
   unsigned *red_counter = nullptr;
   // Krylov workspace (allocated on first solve)

@@ -122,6 +122,15 @@ __global__ void k_fill(double *a, double v, long n) {
        i += (long)gridDim.x * blockDim.x)
     a[i] = v;
 }
+// f = (float)a; *inexact set when some value changes in FP32
+__global__ void k_to_float(float *f, const double *a, long n, unsigned *inexact) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const float v = (float)a[i];
+    f[i] = v;
+    if ((double)v != a[i]) atomicExch(inexact, 1u);
+  }
+}
 __global__ void k_inv(double *a, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
        i += (long)gridDim.x * blockDim.x)
@@ -263,7 +272,7 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
                o_pr = c.take<int2>(hl.pairs.size()), o_ex = c.take<int>(hl.extra_mask.size()),
                o_sm = c.take<unsigned char>(hl.seg_masked.size()),
                o_pm = c.take<unsigned char>(hl.pair_masked.size());
-  const size_t o_df = c.take<unsigned char>(nelv);
+  const size_t o_df = c.take<unsigned char>(nelv), o_mf = c.take<float>(n);
   const size_t o_red = c.take<double>(148 * 8 + 64);
   P->arena_bytes = c.off;
   cudaError_t ce = cudaMalloc(&P->arena, c.off);
@@ -298,6 +307,7 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
   P->blk_off = (int *)(A + o_bo);
   P->msk = (int *)(A + o_msk);
   P->dfrmd = (unsigned char *)(A + o_df);
+  float *multf = (float *)(A + o_mf);
   P->red_partials = dptr(o_red);
   P->red_counter = (unsigned *)(A + o_red + 148 * 8 * sizeof(double));
   P->red_out = (double *)(A + o_red + 148 * 8 * sizeof(double) + 64);
@@ -355,6 +365,16 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
   NB_TRY(gs_add_fused<double>(P->gsd, P->mult, false, s));
   k_inv<<<fg, 256, 0, s>>>(P->mult, n);
   NB_TRY(cudaGetLastError());
+  {  // keep an FP32 copy of mult when it is exact
+    unsigned inexact = 0;  // the reduction counter as scratch, zero again afterwards
+    NB_TRY(cudaMemcpy(P->red_counter, &inexact, sizeof(unsigned), cudaMemcpyHostToDevice));
+    k_to_float<<<fg, 256, 0, s>>>(multf, P->mult, n, P->red_counter);
+    NB_TRY(cudaGetLastError());
+    NB_TRY(cudaMemcpy(&inexact, P->red_counter, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    const unsigned zero = 0;
+    NB_TRY(cudaMemcpy(P->red_counter, &zero, sizeof(unsigned), cudaMemcpyHostToDevice));
+    P->multf = inexact ? nullptr : multf;
+  }
   NB_TRY(reduce_to<1, double>(P->B, nullptr, nullptr, n, P->red_partials, P->red_counter,
                                P->red_out, s));
   NB_TRY(cudaMemcpy(&P->volume, P->red_out, sizeof(double), cudaMemcpyDeviceToHost));
