@@ -292,6 +292,7 @@ constexpr int kT3Threads = 128;
 template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC>
 __global__ void __launch_bounds__(kT3Threads)
     tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
+                   const float *__restrict__ scale_f,
                    const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
                    const int *__restrict__ skip) {
   if (skip && *skip) return;
@@ -306,7 +307,9 @@ __global__ void __launch_bounds__(kT3Threads)
     for (int g = 0; g < R; g++) {
       const int q = tid + g * NT;
       v[g] = q < I3 ? in[e * I3 + q] : TIN(0);
-      c[g] = (!ACC && scale && q < I3) ? scale[e * I3 + q] : TIN(1);
+      c[g] = (!ACC && scale && q < I3)
+                 ? (scale_f ? (TIN)scale_f[e * I3 + q] : scale[e * I3 + q])
+                 : TIN(1);
     }
 #pragma unroll
     for (int g = 0; g < R; g++) {
@@ -351,7 +354,9 @@ __global__ void __launch_bounds__(kT3Threads)
     for (int g = 0; g < RO; g++) {
       const int q = tid + g * NT;
       prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
-      oscale[g] = (scale && q < O3) ? scale[e * O3 + q] : TIN(1);
+      oscale[g] = (scale && q < O3)
+                      ? (scale_f ? (TIN)scale_f[e * O3 + q] : scale[e * O3 + q])
+                      : TIN(1);
     }
   }
 #pragma unroll
@@ -440,14 +445,17 @@ static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, c
   return gs_add_fused<T>(L.P->gsd, e, true, s, skip);
 }
 
-// restriction (Jt x Jt x Jt)(in * scale) from ni to no points (J: ni x no)
+// restriction (Jt x Jt x Jt)(in * scale) from ni to no points (J: ni x no);
+// scale_f, when given, holds the same values as scale exactly in FP32 and is
+// read instead
 template <typename TIN, typename TOUT, typename T>
 static cudaError_t restrict_level(int ni, int no, const TIN *in, const TIN *scale, const T *J,
-                                  TOUT *out, long nelv, const int *skip, cudaStream_t s) {
+                                  TOUT *out, long nelv, const int *skip, cudaStream_t s,
+                                  const float *scale_f = nullptr) {
 #define NB_R(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
     tensor3_kernel<TIN, TOUT, T, A, B, true, false><<<(unsigned)nelv, kT3Threads, 0, s>>>(         \
-        in, scale, J, out, nelv, skip);                                                     \
+        in, scale, scale_f, J, out, nelv, skip);                                            \
     return cudaGetLastError();                                                              \
   }
   NB_R(4, 2) NB_R(3, 2) NB_R(5, 4) NB_R(6, 4) NB_R(7, 4) NB_R(8, 4) NB_R(9, 4) NB_R(10, 4)
@@ -459,11 +467,12 @@ static cudaError_t restrict_level(int ni, int no, const TIN *in, const TIN *scal
 // prolongation out += (J x J x J) in from ni to no points (J: no x ni)
 template <typename TIN, typename TOUT, typename T>
 static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *out, long nelv,
-                               const int *skip, cudaStream_t s, const TIN *oscale = nullptr) {
+                               const int *skip, cudaStream_t s, const TIN *oscale = nullptr,
+                               const float *oscale_f = nullptr) {
 #define NB_P(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
     tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, kT3Threads, 0, s>>>(         \
-        in, oscale, J, out, nelv, skip);                                                    \
+        in, oscale, oscale_f, J, out, nelv, skip);                                          \
     return cudaGetLastError();                                                              \
   }
   NB_P(2, 4) NB_P(2, 3) NB_P(4, 5) NB_P(4, 6) NB_P(4, 7) NB_P(4, 8) NB_P(4, 9) NB_P(4, 10)
@@ -559,7 +568,7 @@ struct HsmgImpl : public HsmgState {
     // middle and coarse levels first, on the high-priority stream:
     // restrict (r * mult) to the middle level, assemble, mask
     if ((e = restrict_level<double, T, T>(fine->lx, mid->lx, r, fine->mult, Jfm, w_mid, nelv,
-                                          skip, hi)) != cudaSuccess)
+                                          skip, hi, fine->multf)) != cudaSuccess)
       return e;
     if ((e = gs_add_fused<T>(mid->gsd, w_mid, true, hi, skip)) != cudaSuccess) return e;
     // middle Schwarz: e_mid = S_m w
@@ -582,7 +591,9 @@ struct HsmgImpl : public HsmgState {
     // mult are the same at every copy of a point, so
     // mult gs(gs(wt e) + J e_mid) = gs(wt e + mult J e_mid).
     if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s,
-                                  merged ? mult_f : nullptr)) != cudaSuccess)
+                                  merged ? mult_f : nullptr,
+                                  merged && sizeof(T) == 8 ? fine->multf : nullptr)) !=
+        cudaSuccess)
       return e;
     if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, merged ? nullptr : mult_f)) !=
         cudaSuccess)
