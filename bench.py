@@ -799,8 +799,8 @@ def main():
                      "frac": achieved / peaks["hbm_gbs"],
                      "traffic": AX_TRAFFIC_B_PER_POINT.get(cfg["lx"], 0) * P.n or None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per "
-                                       "point of a 24^3-element launch (profiles/"
-                                       "ax_helm_tma_24cube_lx8_traffic.md), times the points",
+                                       "point of a 24^3-element launch of the same kernel "
+                                       "(mean of two launches), times the points",
                      "peak_source": peak_src, "bytes_per_launch": ax_bytes,
                      "launch_ms": t_ax * 1e3, "gdof_s": ax_gdofs},
         "gpu_launches": launches,
