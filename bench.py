@@ -32,10 +32,11 @@ sys.path.insert(0, ROOT)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 
-# DRAM bytes per point of ax_helm_tma_kernel measured by ncu on a 24^3-element
-# case (dram__bytes_read.sum + dram__bytes_write.sum, mean of two launches;
-# the part of w still dirty in L2 when the launch ends is not counted).
-AX_TRAFFIC_B_PER_POINT = {8: 70.33}
+# DRAM bytes per point of ax_cg_fused_kernel measured by ncu on a 24^3-element
+# case (dram__bytes_read.sum + dram__bytes_write.sum per launch over the
+# points; the part of p and w still dirty in L2 when the launch ends is not
+# counted).
+FUSED_TRAFFIC_B_PER_POINT = {}
 
 
 def measured_peaks():
@@ -48,7 +49,8 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks/throttle reasons sampled every 100 ms during the
+    timed region (one nvidia-smi process in loop mode)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -57,29 +59,35 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.rows = []
-        self._stop = threading.Event()
+        self._p = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}",
-                                      f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout
-                for line in out.strip().splitlines():
-                    self.rows.append([c.strip() for c in line.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.3)  # first sample before the timed work starts
+        except Exception:
+            self._p = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is not None:
+            time.sleep(0.15)
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=10)
+            except Exception:
+                self._p.kill()
+            self._t.join(timeout=10)
 
     def summary(self):
         sm = []
@@ -97,7 +105,7 @@ class ClockSampler:
                 continue
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": 100}
 
 
 def dist_setup():
@@ -180,39 +188,46 @@ def host_threads():
     return int(os.environ["NB_ORACLE_THREADS"])
 
 
-def oracle_iteration_time(cfg, b, pc, iters):
-    """Seconds per Krylov iteration of the CPU oracle (the port of the
-    reference's CPU path, element loops on all host threads) on this
-    workload: setup untimed, `iters` iterations timed."""
+def oracle_problem(cfg):
+    """The CPU oracle's copy of the workload's mesh and geometry."""
     host_threads()
     from oracle import oracle as orc
     O = orc.OracleProblem.box(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"],
                               periodic=cfg["periodic"])
     O.deform_sine(cfg["deform"])
     O.coef()
+    return O
+
+
+def oracle_solve(O, b, pc, tol, coarse_tol, max_iter):
+    """One complete FP64 solve of the CPU oracle (the port of the
+    reference's CPU path, element loops on all host threads) from x0 = 0:
+    returns (x, iterations, solve seconds, preconditioner set-up seconds)."""
+    from oracle import oracle as orc
     if pc == "hsmg":
-        H = orc.OracleHsmg(O)
         t0 = time.perf_counter()
-        H.cg(b, iters, 0.0, flexible=True)
+        H = orc.OracleHsmg(O, coarse_tol=coarse_tol)
+        t_setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        x, it, _, _ = H.cg(b, max_iter, tol, flexible=True)
         dt = time.perf_counter() - t0
         H.close()
     else:
+        t_setup = 0.0
         t0 = time.perf_counter()
-        O.cg_jacobi(b, iters, 0.0)
+        x, it, _, _ = O.cg_jacobi(b, max_iter, tol)
         dt = time.perf_counter() - t0
-    O.close()
-    return dt / iters, dt
+    return x, it, dt, t_setup
 
 
-def cpu_baseline_sample(cfg, b, pc, gpu_iters, budget_iters):
-    per_iter, dt = oracle_iteration_time(cfg, b, pc, budget_iters)
-    name = "hsmg-FCG" if pc == "hsmg" else "Jacobi-PCG"
-    cores = host_threads()
-    return {"value": 1.0 / (per_iter * max(gpu_iters, 1)), "unit": "solves/s", "cores": cores,
-            "kind": "port",
-            "sample": f"{budget_iters} {name} iterations of the same 32^3 lx={cfg['lx']} "
-                      f"problem and right-hand side on {cores} host threads ({dt:.1f} s, setup untimed); solves/s = "
-                      f"1/(s per iteration x {gpu_iters} iterations of the solve)"}
+def rel_err_mean_free(a, b, singular):
+    """Relative L2 distance of a to b; for the singular fully periodic
+    problem both are taken mean-free first (its solution is fixed up to a
+    constant)."""
+    import numpy as np
+    if singular:
+        a, b = a - a.mean(), b - b.mean()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 def workload_name(cfg, solver):
@@ -224,51 +239,43 @@ def workload_name(cfg, solver):
 def run_reference(args, cfg, world, rank):
     """--impl reference: the reference's CPU algorithm (the oracle port; the
     Fortran reference does not build here) on the host, same metric,
-    workload and preconditioner; each step times --ref-iters iterations and
-    solves/s uses the solve's iteration count.  Rank 0 only."""
+    workload, preconditioner and tolerance.  Each timed step is one complete
+    solve from x0 = 0 to 1e-8 relative; the --warmup steps are short solves
+    (two iterations each) that warm the host threads and caches.  Rank 0
+    only."""
     if rank != 0:
         return
-    host_threads()
     import numpy as np
-    from oracle import oracle as orc
     from neko_b200 import workloads
-    O = orc.OracleProblem.box(cfg["nel"], cfg["lx"], lo=cfg["lo"], hi=cfg["hi"],
-                              periodic=cfg["periodic"])
-    O.deform_sine(cfg["deform"])
-    O.coef()
+    O = oracle_problem(cfg)
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
     b = O.gs_add(workloads.config2_rhs_local(x, y, z, B, args.seed))
     mult = O.f64("mult")
     r0 = math.sqrt(float(np.sum(b * mult * b)) / O.volume)
-    iters = args.ref_iters
-    H = orc.OracleHsmg(O) if args.pc == "hsmg" else None
-
-    def run(k):
-        if H is not None:
-            H.cg(b, k, 0.0, flexible=True)
-        else:
-            O.cg_jacobi(b, k, 0.0)
+    tol = cfg["rel_tol"] * r0
     for _ in range(args.warmup):
-        run(1)
-    times = []
+        oracle_solve(O, b, args.pc, 0.0, args.coarse_tol, 2)
+    times, iters = [], []
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        run(iters)
-        times.append((time.perf_counter() - t0) / iters)
-    per_iter = sorted(times)[len(times) // 2]
-    full_iters = args.ref_full_iters
-    v = 1.0 / (per_iter * full_iters)
+        _, it, dt, _ = oracle_solve(O, b, args.pc, tol, args.coarse_tol, cfg["max_iter"])
+        times.append(dt)
+        iters.append(it)
+    O.close()
+    total = sum(times)
+    v = args.steps / total
     name = "hsmg-FCG" if args.pc == "hsmg" else "Jacobi-PCG"
+    cores = host_threads()
     line = {"impl": "reference", "metric": "Poisson solves/s to 1e-8 rel", "value": v,
             "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": per_iter * full_iters * 1e3, "higher_is_better": True,
+            "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name(cfg, f"FP64 {name}"), "pc": args.pc,
-                       "r0": r0},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": host_threads(), "kind": "port",
-                             "sample": f"median of {args.steps} runs of {iters} {name} "
-                                       f"iterations on {host_threads()} host threads; solves/s = 1/(s per "
-                                       f"iteration x {full_iters} iterations of the solve)"},
+                       "r0": r0, "iterations": iters[-1], "seed": args.seed},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} complete {name} solves to 1e-8 rel "
+                                       f"({iters[-1]} iterations each) on {cores} host threads, "
+                                       f"each timed from x0 = 0 (preconditioner set-up "
+                                       f"untimed); warm-up: {args.warmup} two-iteration solves"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -301,11 +308,14 @@ def kernel_only(args, cfg):
                           "launches": [m.launches for m in mons]}))
         return
     u = torch.rand(P.n, dtype=torch.float64, device="cuda")
+    z = torch.rand(P.n, dtype=torch.float64, device="cuda")
     w = P.zeros()
     s = torch.cuda.Stream()
     for _ in range(args.warmup + args.steps):
         if args.kernel_only == "ax":
             nb.AxHelm().compute(w, u, P, stream=s)
+        elif args.kernel_only == "fused":
+            nb.AxHelm().update_p_compute(w, u, z, 0.5, P, stream=s)
         else:
             P.gs.op(u, P.n, stream=s)
     torch.cuda.synchronize()
@@ -559,15 +569,11 @@ def main():
     ap.add_argument("--pc", default="hsmg", choices=["jacobi", "hsmg"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--ax-reps", type=int, default=50)
-    ap.add_argument("--cpu-iters", type=int, default=2)
-    ap.add_argument("--ref-iters", type=int, default=1)
-    ap.add_argument("--ref-full-iters", type=int, default=0,
-                    help="iterations of the full solve (default: 20 for hsmg-FCG, 1074 for "
-                         "Jacobi-PCG, the counts of this workload)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU oracle solve (cpu_baseline and the parity fields)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision solve measured beside the FP64 one")
-    ap.add_argument("--kernel-only", choices=["ax", "gs", "solve"], default=None,
+    ap.add_argument("--kernel-only", choices=["ax", "fused", "gs", "solve"], default=None,
                     help="run only this kernel (or one FP64 + one mixed solve inside a "
                          "profiler window) on an nel^3 box (profiling case)")
     ap.add_argument("--workload", choices=["solve", "axgs", "batch", "serve"], default="solve",
@@ -600,8 +606,6 @@ def main():
     world, rank, local = dist_setup()
 
     if args.impl == "reference":
-        if args.ref_full_iters <= 0:  # iteration counts of this workload's solve
-            args.ref_full_iters = 20 if args.pc == "hsmg" else 1074
         run_reference(args, cfg, world, rank)
         barrier(world)
         return
@@ -619,6 +623,10 @@ def main():
     else:  # hsmg is not symmetric: flexible CG (plain CG stalls with it)
         solver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol,
                         M=nb.Hsmg(coarse_tol=args.coarse_tol))
+    msolver = None
+    if args.pc == "hsmg" and not args.no_mixed:
+        msolver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol,
+                         M=nb.Hsmg(coarse_tol=args.coarse_tol, mixed=True))
     Ax = nb.AxHelm()
     x = P.zeros()
     stream = torch.cuda.Stream()
@@ -628,154 +636,142 @@ def main():
     torch.cuda.synchronize()
     if not mon.converged:
         raise RuntimeError(f"warm-up solve did not converge: {mon}")
-
-    # --- device-timed steps (inputs resident in HBM, > L2) ---------------
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches = 0
-    iters = []
-    with ClockSampler(local) as clk:
-        barrier(world)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            mon = solver.solve(Ax, x, b, P.n, P, stream=stream)
-            launches += mon.launches
-            iters.append(mon.iter)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier(world)
-    t_dev = ev0.elapsed_time(ev1) / 1e3
-    t_dev = max_over_ranks(t_dev, world)
-    value = world * args.steps / t_dev
-
-    # --- end to end through the public API with host buffers -------------
-    # Every step uploads its right-hand side from pinned host memory and
-    # downloads its solution.  Pipelined as a serving loop would run it: the
-    # upload of step k+1 and the download of step k-1 run on a copy stream
-    # while step k solves; device staging buffers keep the solver's operands
-    # (and so its captured iteration graph) fixed.  The serial form (copy,
-    # solve, copy on one stream) is reported beside it.
-    hb = b.cpu().pin_memory()
-    hx = [torch.empty(P.n, dtype=torch.float64).pin_memory() for _ in range(2)]
-    fdev = torch.empty_like(b)
-    f_st = [torch.empty_like(b) for _ in range(2)]
-    x_st = [torch.empty_like(b) for _ in range(2)]
-    cstream = torch.cuda.Stream()
-    ev = lambda: torch.cuda.Event()
-    ev_in, ev_used, ev_done, ev_out = ([ev(), ev()] for _ in range(4))
-    barrier(world)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    cstream.wait_stream(stream)
-    with torch.cuda.stream(cstream):
-        f_st[0].copy_(hb, non_blocking=True)
-        ev_in[0].record(cstream)
-    for k in range(args.steps):
-        bk = k % 2
-        if k + 1 < args.steps:  # prefetch the next input while this step solves
-            with torch.cuda.stream(cstream):
-                if k >= 1:
-                    cstream.wait_event(ev_used[1 - bk])
-                f_st[1 - bk].copy_(hb, non_blocking=True)
-                ev_in[1 - bk].record(cstream)
-        with torch.cuda.stream(stream):
-            stream.wait_event(ev_in[bk])
-            fdev.copy_(f_st[bk], non_blocking=True)
-            ev_used[bk].record(stream)
-            mon_e = solver.solve(Ax, x, fdev, P.n, P, stream=stream)
-            if k >= 2:
-                stream.wait_event(ev_out[bk])
-            x_st[bk].copy_(x, non_blocking=True)
-            ev_done[bk].record(stream)
-        with torch.cuda.stream(cstream):
-            cstream.wait_event(ev_done[bk])
-            hx[bk].copy_(x_st[bk], non_blocking=True)
-            ev_out[bk].record(cstream)
-    stream.wait_stream(cstream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
-    e2e = world * args.steps / t_e2e
-    if not torch.equal(hx[(args.steps - 1) % 2], x.cpu()):
-        raise RuntimeError("end-to-end solution read back differs from the device solution")
-    # serial form: upload, solve, download on one stream
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(world)
-    torch.cuda.synchronize()
-    s0.record(stream)
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            fdev.copy_(hb, non_blocking=True)
-            mon_e = solver.solve(Ax, x, fdev, P.n, P, stream=stream)
-            hx[0].copy_(x, non_blocking=True)
-    s1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    e2e_serial = world * args.steps / max_over_ranks(s0.elapsed_time(s1) / 1e3, world)
-
-    # --- mixed precision beside it: FP32 smoothing levels, FP64 FCG ------
-    mixed = None
-    if args.pc == "hsmg" and not args.no_mixed:
-        x64 = x.clone()
-        msolver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol,
-                         M=nb.Hsmg(coarse_tol=args.coarse_tol, mixed=True))
+    x64 = x.clone()
+    xm = None
+    if msolver is not None:
         for _ in range(args.warmup):
             mon_m = msolver.solve(Ax, x, b, P.n, P, stream=stream)
         torch.cuda.synchronize()
         if not mon_m.converged:
             raise RuntimeError(f"mixed warm-up solve did not converge: {mon_m}")
-        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        m_launches, m_iters = 0, []
-        barrier(world)
-        torch.cuda.synchronize()
-        m0.record(stream)
-        for _ in range(args.steps):
-            mon_m = msolver.solve(Ax, x, b, P.n, P, stream=stream)
-            m_launches += mon_m.launches
-            m_iters.append(mon_m.iter)
-        m1.record(stream)
-        torch.cuda.synchronize()
-        barrier(world)
-        t_m = max_over_ranks(m0.elapsed_time(m1) / 1e3, world)
-        xa, xb = x, x64
-        if all(cfg["periodic"]):  # the singular problem's solution is fixed up to a constant
-            xa, xb = x - x.mean(), x64 - x64.mean()
-        err = float(torch.linalg.norm(xa - xb) / torch.linalg.norm(xb))
-        v_m = world * args.steps / t_m
-        mixed = {"value": v_m, "unit": "solves/s", "ms_per_step": t_m / args.steps * 1e3,
-                 "iterations": m_iters[-1], "fp64_iterations": iters[-1],
-                 "res_final": mon_m.res_final, "abs_tol": tol,
-                 "err_vs_fp64": err,
-                 "err_reference": "relative L2 distance to the FP64 hsmg-FCG solution of "
-                                  "the same problem (the FP64 path matches the CPU oracle "
-                                  "in the parity tests)",
-                 "speedup_vs_fp64": v_m / value, "gpu_launches": m_launches,
-                 "precision": "FP32 Schwarz/FDM smoothing and restriction/prolongation; "
-                              "FP64 outer FCG, inner products, coarse CG, true residual "
-                              "every 50 iterations"}
-        x.copy_(x64)
+        xm = x.clone()
 
-    # --- ax_helm roofline: events on the launching stream ----------------
-    # three timed loops of ax_reps launches; the median loop's mean launch time
-    w = P.zeros()
-    for _ in range(5):
-        Ax.compute(w, x, P, stream=stream)
-    loops = []
-    for _ in range(3):
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(args.ax_reps):
-            Ax.compute(w, x, P, stream=stream)
-        a1.record(stream)
+    def timed(fn, steps):
+        """Device time of `steps` calls of fn on `stream`, max over ranks."""
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(world)
         torch.cuda.synchronize()
-        loops.append(a0.elapsed_time(a1) / 1e3 / args.ax_reps)
-    t_ax = sorted(loops)[1]
+        e0.record(stream)
+        out = [fn() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3, world), out
+
+    hb = b.cpu().pin_memory()
+    hx = [torch.empty(P.n, dtype=torch.float64).pin_memory() for _ in range(2)]
+    fdev = torch.empty_like(b)
+    with ClockSampler(local) as clk:
+        # --- device-timed steps (inputs resident in HBM, > L2) -----------
+        t_dev, mons = timed(lambda: solver.solve(Ax, x, b, P.n, P, stream=stream), args.steps)
+        launches = sum(m.launches for m in mons)
+        iters = [m.iter for m in mons]
+        value = world * args.steps / t_dev
+
+        # --- end to end through the public API with host buffers ---------
+        # Every step uploads its right-hand side from pinned host memory and
+        # downloads its solution.  Pipelined as a serving loop would run it:
+        # the upload of step k+1 and the download of step k-1 run on a copy
+        # stream while step k solves; device staging buffers keep the
+        # solver's operands (and so its captured iteration graph) fixed.
+        # The serial form (copy, solve, copy on one stream) is reported
+        # beside it.
+        f_st = [torch.empty_like(b) for _ in range(2)]
+        x_st = [torch.empty_like(b) for _ in range(2)]
+        cstream = torch.cuda.Stream()
+        ev = lambda: torch.cuda.Event()
+        ev_in, ev_used, ev_done, ev_out = ([ev(), ev()] for _ in range(4))
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cstream.wait_stream(stream)
+        with torch.cuda.stream(cstream):
+            f_st[0].copy_(hb, non_blocking=True)
+            ev_in[0].record(cstream)
+        for k in range(args.steps):
+            bk = k % 2
+            if k + 1 < args.steps:  # prefetch the next input while this step solves
+                with torch.cuda.stream(cstream):
+                    if k >= 1:
+                        cstream.wait_event(ev_used[1 - bk])
+                    f_st[1 - bk].copy_(hb, non_blocking=True)
+                    ev_in[1 - bk].record(cstream)
+            with torch.cuda.stream(stream):
+                stream.wait_event(ev_in[bk])
+                fdev.copy_(f_st[bk], non_blocking=True)
+                ev_used[bk].record(stream)
+                solver.solve(Ax, x, fdev, P.n, P, stream=stream)
+                if k >= 2:
+                    stream.wait_event(ev_out[bk])
+                x_st[bk].copy_(x, non_blocking=True)
+                ev_done[bk].record(stream)
+            with torch.cuda.stream(cstream):
+                cstream.wait_event(ev_done[bk])
+                hx[bk].copy_(x_st[bk], non_blocking=True)
+                ev_out[bk].record(cstream)
+        stream.wait_stream(cstream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+        e2e = world * args.steps / t_e2e
+        if not torch.equal(hx[(args.steps - 1) % 2], x.cpu()):
+            raise RuntimeError("end-to-end solution read back differs from the device solution")
+
+        def serial_step():
+            with torch.cuda.stream(stream):
+                fdev.copy_(hb, non_blocking=True)
+                solver.solve(Ax, x, fdev, P.n, P, stream=stream)
+                hx[0].copy_(x, non_blocking=True)
+        t_ser, _ = timed(serial_step, args.steps)
+        e2e_serial = world * args.steps / t_ser
+
+        # --- mixed precision beside it: FP32 smoothing levels, FP64 FCG --
+        mixed = None
+        if msolver is not None:
+            t_m, mons_m = timed(lambda: msolver.solve(Ax, x, b, P.n, P, stream=stream),
+                                args.steps)
+            mon_m = mons_m[-1]
+            v_m = world * args.steps / t_m
+            singular = all(cfg["periodic"])
+            err = rel_err_mean_free(x.cpu().numpy(), x64.cpu().numpy(), singular)
+            mixed = {"value": v_m, "unit": "solves/s", "ms_per_step": t_m / args.steps * 1e3,
+                     "iterations": mon_m.iter, "fp64_iterations": iters[-1],
+                     "res_final": mon_m.res_final, "abs_tol": tol,
+                     "err_vs_fp64": err,
+                     "speedup_vs_fp64": v_m / value,
+                     "gpu_launches": sum(m.launches for m in mons_m),
+                     "precision": "FP32 Schwarz/FDM smoothing and restriction/prolongation; "
+                                  "FP64 outer FCG, inner products, coarse CG, true residual "
+                                  "every 50 iterations"}
+
+        # --- the dominant kernel of the solve, timed with events ----------
+        # The fused CG step (p = z + beta p, w = A p, sum p w: 88 B/point) is
+        # the largest share of the solve's device time; it is timed on its
+        # launching stream, three loops of --ax-reps launches, median loop.
+        # The standalone operator (72 B/point) is timed the same way.
+        w = P.zeros()
+        pd = x64.clone()
+        zd = b.clone()
+        pap = torch.zeros(1, dtype=torch.float64, device="cuda")
+
+        def loop_time(fn):
+            for _ in range(5):
+                fn()
+            loops = []
+            for _ in range(3):
+                t, _ = timed(lambda: [fn() for _ in range(args.ax_reps)], 1)
+                loops.append(t / args.ax_reps)
+            return sorted(loops)[1]
+        t_fused = loop_time(lambda: Ax.update_p_compute(w, pd, zd, 0.0, P, pap=pap, stream=stream))
+        t_ax = loop_time(lambda: Ax.compute(w, x64, P, stream=stream))
     peaks, peak_src = measured_peaks()
-    ax_bytes = 72 * P.n  # u, w, h1, G11..G23: 9 x 8 B per point
-    achieved = ax_bytes / t_ax / 1e9
-    ax_gdofs = P.n / t_ax / 1e9
+    fused_bytes = 88 * P.n  # z, p read; p, w written; h1, G11..G23 read
+    ax_bytes = 72 * P.n     # u, w, h1, G11..G23
+    achieved = fused_bytes / t_fused / 1e9
+    traffic_pp = FUSED_TRAFFIC_B_PER_POINT.get(cfg["lx"])
+    singular = all(cfg["periodic"])
 
     line = {
         "metric": "Poisson solves/s to 1e-8 rel", "value": value, "unit": "solves/s",
@@ -787,30 +783,57 @@ def main():
                        + ", one solve per step per GPU",
                    "pc": args.pc, "iterations": iters[-1], "r0": r0, "seed": args.seed,
                    "coarse": f"10 Jacobi-CG iterations, abs tol {args.coarse_tol:g}",
-                   "l2": f"inputs larger than L2 ({72 * P.n / 1e9:.1f} GB ax_helm working set)",
+                   "l2": f"inputs larger than L2 ({88 * P.n / 1e9:.1f} GB fused-step working set)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": P.n * 8,
                 "d2h_bytes_per_step": P.n * 8,
                 "form": "pipelined: step k+1's upload and step k-1's download overlap "
                         "step k's solve on a second stream",
                 "serial_value": e2e_serial},
-        "roofline": {"bound": "hbm", "kernel": f"ax_helm_tma_kernel<double,{cfg['lx']}>",
+        "roofline": {"bound": "hbm",
+                     "kernel": f"ax_cg_fused_kernel<{cfg['lx']}> (p = z + beta p, w = A p, "
+                               f"sum p w; the solve's largest kernel)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"],
-                     "traffic": AX_TRAFFIC_B_PER_POINT.get(cfg["lx"], 0) * P.n or None,
+                     "traffic": traffic_pp * P.n if traffic_pp else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per "
-                                       "point of a 24^3-element launch of the same kernel "
-                                       "(mean of two launches), times the points",
-                     "peak_source": peak_src, "bytes_per_launch": ax_bytes,
-                     "launch_ms": t_ax * 1e3, "gdof_s": ax_gdofs},
+                                       "point of a 24^3-element launch of the same kernel, "
+                                       "times the points",
+                     "peak_source": peak_src, "bytes_per_launch": fused_bytes,
+                     "launch_ms": t_fused * 1e3, "gdof_s": P.n / t_fused / 1e9},
+        "ax_helm": {"kernel": f"ax_helm_tma_kernel<double,{cfg['lx']}>",
+                    "achieved": ax_bytes / t_ax / 1e9, "unit": "GB/s",
+                    "frac": ax_bytes / t_ax / 1e9 / peaks["hbm_gbs"],
+                    "bytes_per_launch": ax_bytes, "launch_ms": t_ax * 1e3,
+                    "gdof_s": P.n / t_ax / 1e9},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     if mixed is not None:
         line["mixed"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(cfg, b.cpu().numpy(), args.pc, iters[-1],
-                                                   args.cpu_iters)
+        # One complete FP64 solve of the CPU oracle on the same right-hand
+        # side: the CPU baseline (whole solve, host threads), and the parity
+        # of the GPU solves at full size (iterations within +-1, error).
+        O = oracle_problem(cfg)
+        xo, it_o, dt_o, _ = oracle_solve(O, b.cpu().numpy(), args.pc, tol, args.coarse_tol,
+                                         cfg["max_iter"])
+        O.close()
+        cores = host_threads()
+        name = "hsmg-FCG" if args.pc == "hsmg" else "Jacobi-PCG"
+        line["cpu_baseline"] = {
+            "value": 1.0 / dt_o, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"one complete FP64 {name} solve of the same problem and right-hand "
+                      f"side to 1e-8 rel ({it_o} iterations, {dt_o:.1f} s) on {cores} host "
+                      f"threads, preconditioner set-up untimed"}
+        line["parity"] = {
+            "iterations": iters[-1], "iterations_oracle": it_o,
+            "err_vs_oracle": rel_err_mean_free(x64.cpu().numpy(), xo, singular),
+            "err_definition": "relative L2 distance to the CPU oracle's FP64 solution"
+                              + (" (both mean-free: the periodic problem is singular)"
+                                 if singular else "")}
+        if mixed is not None:
+            mixed["err_vs_oracle"] = rel_err_mean_free(xm.cpu().numpy(), xo, singular)
     if rank == 0:
         print(json.dumps(line), flush=True)
     P.close()

@@ -8,7 +8,11 @@
  * reference, integers arrive by reference, device buffers as plain pointers,
  * the stream (where the reference passes one) as an opaque handle, and
  * `real` is double.  Errors in this part print a message and exit, as the
- * reference's CUDA_CHECK does.
+ * reference's CUDA_CHECK does.  Entry points that take no stream launch on
+ * the stream given to nb_set_default_stream(), else on Neko's global
+ * `void *glb_cmd_queue` when the program defines it (the library holds a
+ * weak reference to that symbol, src/device/device_config.h.in:19), else on
+ * the legacy default stream.
  *
  * Part 2 is a native handle API (nb_*) over device-resident problems: mesh,
  * geometric factors and gather-scatter maps built once and kept in HBM, then
@@ -31,8 +35,10 @@ extern "C" {
 /* w = A u, the matrix-free Helmholtz operator (h1 part) on nelv elements of
  * lx^3 points.  Replaces cuda_ax_helm
  * (src/math/bcknd/device/cuda/ax_helm.cu:63), called from
- * src/math/bcknd/device/ax_helm_device.F90:234.  Runs on the library's
- * default stream (the reference uses glb_cmd_queue). */
+ * src/math/bcknd/device/ax_helm_device.F90:234.  Launches on glb_cmd_queue
+ * as the reference does (see the stream rule above).  A bounded device wait
+ * that expires is reported, fatally, by the next synchronising drop-in
+ * (cuda_glsc3, cuda_glsc2, cuda_glsum, cuda_fusedcg_part2). */
 void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, void *dxt,
                   void *dyt, void *dzt, void *h1, void *g11, void *g22,
                   void *g33, void *g12, void *g13, void *g23, int *nelv,
@@ -74,6 +80,24 @@ void cuda_addcol3(void *a, void *b, void *c, int *n, void *stream); /* a += b c 
 void cuda_invcol1(void *a, int *n, void *stream);                 /* a = 1/a */
 void cuda_radd(void *a, double *c, int *n, void *stream);         /* a += c (math.cu:266) */
 
+/* Fused CG helpers of fusedcg_device_solve
+ * (src/krylov/bcknd/device/fusedcg_device.F90:328-414), launched on
+ * glb_cmd_queue.  Replace src/krylov/bcknd/device/cuda/fusedcg_aux.cu:61-87.
+ *   update_p: p = beta po + z.
+ *   update_x: x += sum_{j < p_cur} alpha[j] p[j], p a device array of p_cur
+ *             device pointers, alpha a device array.
+ *   part2:    alpha_d[p_cur-1] = *alpha; a = a - alpha c; returns
+ *             sum(a b a) of the updated a after synchronising the stream. */
+void cuda_fusedcg_update_p(void *p, void *z, void *po, double *beta, int *n);
+void cuda_fusedcg_update_x(void *x, void *p, void *alpha, int *p_cur, int *n);
+double cuda_fusedcg_part2(void *a, void *b, void *c, void *alpha_d, double *alpha,
+                          int *p_cur, int *n);
+
+/* Stream for the Part-1 entry points that take none, overriding
+ * glb_cmd_queue (NULL selects the legacy default stream).  No counterpart in
+ * the reference, where Neko's device layer owns glb_cmd_queue. */
+void nb_set_default_stream(void *stream);
+
 /* x(msk(i)) = 0 for i = 1..m-1 (msk(0) holds the count).  Replaces
  * src/bc/bcknd/device/cuda/zero_dirichlet.cu:44. */
 void cuda_zero_dirichlet_apply_scalar(void *msk, void *x, int *m, void *stream);
@@ -87,8 +111,8 @@ void cuda_jacobi_update(void *d, void *dxt, void *dyt, void *dzt, void *G11,
 
 /* v = (C x B x A) u on nel elements: u has nu^3 points per element, v nv^3;
  * A is nv x nu, Bt and Ct nu x nv (column-major).  Replaces cuda_tnsr3d
- * (src/math/bcknd/device/cuda/tensor.cu:60); nu, nv <= 16.  Runs on the
- * library's default stream (the reference uses glb_cmd_queue). */
+ * (src/math/bcknd/device/cuda/tensor.cu:60); nu, nv <= 16.  Launches on
+ * glb_cmd_queue as the reference does (see the stream rule above). */
 void cuda_tnsr3d(void *v, int *nv, void *u, int *nu, void *A, void *Bt, void *Ct, int *nel);
 
 /* Fast-diagonalisation solve per element of nl^3 points: r <- d * (S_x^T,
@@ -168,7 +192,11 @@ nb_status nb_problem_sizes(const nb_problem *p, int64_t *n, int *nelv, int *lx,
 
 /* Device pointer to a named field of the problem: "x","y","z","g11",
  * "g22","g33","g12","g13","g23","h1","h2","B","mult","dx","dxt", or a map
- * "dof_gs","gs_dof","blk_len","blk_off","msk" (int32, 1-based). */
+ * "dof_gs","gs_dof","blk_len","blk_off","msk" (int32, 1-based), or the
+ * problem's device error word "err" (one int32, see nb_problem_sync).  Every field
+ * is read-only for the caller: the solver keeps derived copies (the Jacobi
+ * diagonal, an FP32 copy of mult, the hsmg levels) that a write through this
+ * pointer would not update.  Change h1/h2 with nb_problem_set_coefficients. */
 nb_status nb_problem_field(const nb_problem *p, const char *name, void **dptr);
 
 /* Volume (sum of B) of the problem's mesh. */
@@ -181,8 +209,27 @@ nb_status nb_problem_volume(const nb_problem *p, double *vol);
 nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1,
                                       const double *h2, int ifh2);
 
-/* w = A u (ax_helm incl. h2 term when enabled), element-local. */
+/* w = A u (ax_helm incl. h2 term when enabled), element-local.
+ * Asynchronous on `stream`; a bounded device wait that expires is recorded
+ * in the problem's error word and reported by the next nb_problem_sync or
+ * nb_solve on the same problem. */
 nb_status nb_ax(nb_problem *p, double *w, const double *u, void *stream);
+/* Synchronises `stream` and reports (then clears) the problem's error word:
+ * NB_ERR_TIMEOUT when an earlier asynchronous call on this problem had a
+ * bounded device wait expire.  No counterpart in the reference, whose
+ * kernels have no bounded waits. */
+nb_status nb_problem_sync(nb_problem *p, void *stream);
+/* The direction update and operator of one CG iteration in one streaming
+ * pass: pdir = z + beta pdir, w = A pdir (element-local, before the
+ * gather-scatter), and *pap = sum over the local points of pdir * w (pap a
+ * device double, may be NULL).  One launch when the problem has no mask and
+ * no h2 term (lx 6, 8, 10); separate passes otherwise.  It fuses what
+ * fusedcg_device_solve does with cuda_fusedcg_update_p followed by
+ * ax_t%compute (src/krylov/bcknd/device/fusedcg_device.F90:382-384), and
+ * adds the curvature sum.  Asynchronous on `stream`; calls on one problem
+ * share its reduction scratch, so they must not overlap on the GPU. */
+nb_status nb_ax_update_p(nb_problem *p, double *w, double *pdir, const double *z,
+                         double beta, double *pap, void *stream);
 /* u = gs_add(u): sum of all local copies of each shared point. */
 nb_status nb_gs_add(nb_problem *p, double *u, void *stream);
 /* x(msk) = 0 for the problem's Dirichlet mask. */

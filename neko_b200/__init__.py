@@ -93,14 +93,15 @@ class Problem:
     _SIZES = {"dx": lambda p: p.lx ** 2, "dxt": lambda p: p.lx ** 2, "zg": lambda p: p.lx,
               "dof_gs": lambda p: p.nlocal, "gs_dof": lambda p: p.nlocal,
               "blk_len": lambda p: p.nblocks, "blk_off": lambda p: p.nblocks,
-              "msk": lambda p: p.nmask}
+              "msk": lambda p: p.nmask, "err": lambda p: 1}
+    _INT_FIELDS = ("dof_gs", "gs_dof", "blk_len", "blk_off", "msk", "err")
 
     def field(self, name):
         """Zero-copy torch view of a device array of the problem."""
         ptr = ctypes.c_void_p()
         check(load().nb_problem_field(self.handle, name.encode(), ctypes.byref(ptr)))
         size = self._SIZES.get(name, lambda p: p.n)(self)
-        typestr = "<i4" if name in ("dof_gs", "gs_dof", "blk_len", "blk_off", "msk") else "<f8"
+        typestr = "<i4" if name in self._INT_FIELDS else "<f8"
         if size == 0:
             return torch.empty(0, dtype=torch.int32 if typestr == "<i4" else torch.float64,
                                device="cuda")
@@ -116,6 +117,12 @@ class Problem:
 
     def zeros(self):
         return torch.zeros(self.n, dtype=torch.float64, device="cuda")
+
+    def sync(self, stream=None):
+        """Wait for `stream` and raise NekoB200Error (NB_ERR_TIMEOUT) when an
+        earlier asynchronous call on this problem had a bounded device wait
+        expire (nb_problem_sync)."""
+        check(load().nb_problem_sync(self.handle, _stream_handle(stream)))
 
     def close(self):
         if getattr(self, "_h", None) is not None:
@@ -135,6 +142,14 @@ class AxHelm:
 
     def compute(self, w, u, coef, msh=None, Xh=None, stream=None):
         check(load().nb_ax(coef.handle, _ptr(w), _ptr(u), _stream_handle(stream)))
+
+    def update_p_compute(self, w, p, z, beta, coef, pap=None, stream=None):
+        """p = z + beta p, then w = A p in one streaming pass; pap (a
+        one-element float64 CUDA tensor, optional) receives sum(p * w) over
+        the local points (nb_ax_update_p)."""
+        check(load().nb_ax_update_p(coef.handle, _ptr(w), _ptr(p), _ptr(z), float(beta),
+                                    _ptr(pap) if pap is not None else None,
+                                    _stream_handle(stream)))
 
 
 class GatherScatter:

@@ -70,6 +70,10 @@ SIGNATURES = {
     "cuda_schwarz_extrude": (None, [_P, _IP, _DP, _P, _IP, _DP, _IP, _IP, _P]),
     "cuda_schwarz_toext3d": (None, [_P, _P, _IP, _IP, _P]),
     "cuda_schwarz_toreg3d": (None, [_P, _P, _IP, _IP, _P]),
+    "cuda_fusedcg_update_p": (None, [_P, _P, _P, _DP, _IP]),
+    "cuda_fusedcg_update_x": (None, [_P, _P, _P, _IP, _IP]),
+    "cuda_fusedcg_part2": (ctypes.c_double, [_P, _P, _P, _P, _DP, _IP, _IP]),
+    "nb_set_default_stream": (None, [_P]),
     # native API
     "nb_last_error": (ctypes.c_char_p, []),
     "nb_version": (ctypes.c_char_p, []),
@@ -83,6 +87,8 @@ SIGNATURES = {
     "nb_problem_volume": (_I, [_P, _DP]),
     "nb_problem_set_coefficients": (_I, [_P, _P, _P, _I]),
     "nb_ax": (_I, [_P, _P, _P, _P]),
+    "nb_problem_sync": (_I, [_P, _P]),
+    "nb_ax_update_p": (_I, [_P, _P, _P, _P, ctypes.c_double, _P, _P]),
     "nb_gs_add": (_I, [_P, _P, _P]),
     "nb_bc_apply": (_I, [_P, _P, _P]),
     "nb_solve": (_I, [_P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveResult), _P]),

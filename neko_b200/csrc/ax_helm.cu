@@ -22,9 +22,11 @@
 
 namespace nb {
 
-// Device error word of this translation unit: 0 = ok, 1 = a bulk-copy wait
-// timed out.  Read and cleared by take_device_error().
-__device__ int nb_dev_error = 0;
+// Error word of the drop-in cuda_ax_helm, which has no problem handle to
+// carry one: 0 = ok, 1 = a bulk-copy wait timed out.  The native entry
+// points pass their problem's own word instead.  Read and cleared by
+// take_dropin_error() (after the synchronising drop-in reductions).
+__device__ int nb_dropin_error = 0;
 
 // Elements per block for each lx (threads = lx*lx*NE).
 template <int LX>
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(AxTmaCfg<T, LX, S, KS>::THREADS)
                        const T *__restrict__ g11, const T *__restrict__ g22,
                        const T *__restrict__ g33, const T *__restrict__ g12,
                        const T *__restrict__ g13, const T *__restrict__ g23, const int nelv,
-                       const int *__restrict__ skip) {
+                       const int *__restrict__ skip, int *__restrict__ err) {
   using C = AxTmaCfg<T, LX, S, KS>;
   constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS;
   static_assert(LX % KS == 0, "k split must divide lx");
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(AxTmaCfg<T, LX, S, KS>::THREADS)
   }
   if (failed) {
     if (tid == 0) {
-      atomicCAS(&nb_dev_error, 0, 1);
+      atomicExch(err ? err : &nb_dropin_error, 1);
       // bounded wait for this CTA's copies still in flight
       for (int q = t; q < nt && q < t + S; q++) mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
     }
@@ -258,7 +260,7 @@ template <typename T, int LX, int S, int KS>
 static cudaError_t launch_ax_tma(T *w, const T *u, const T *D, const T *Dt, const T *h1,
                                  const T *g11, const T *g22, const T *g33, const T *g12,
                                  const T *g13, const T *g23, int nelv, cudaStream_t st,
-                                 const int *skip) {
+                                 const int *skip, int *err) {
   using C = AxTmaCfg<T, LX, S, KS>;
   auto kern = ax_helm_tma_kernel<T, LX, S, KS>;
   static int grid_per_dev[64] = {0};
@@ -279,7 +281,7 @@ static cudaError_t launch_ax_tma(T *w, const T *u, const T *D, const T *Dt, cons
   if (nelv <= 0) return cudaSuccess;
   const int grid = nelv < g ? nelv : g;
   kern<<<grid, C::THREADS, C::SMEM, st>>>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
-                                          skip);
+                                          skip, err);
   return cudaGetLastError();
 }
 
@@ -289,16 +291,16 @@ template <typename T>
 cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h1,
                            const T *g11, const T *g22, const T *g33, const T *g12,
                            const T *g13, const T *g23, int nelv, int lx, cudaStream_t s,
-                           const int *skip) {
+                           const int *skip, int *err) {
   const void *ptrs[] = {u, h1, g11, g22, g33, g12, g13, g23};
   for (const void *p : ptrs)
     if (reinterpret_cast<uintptr_t>(p) & 15) return cudaErrorNotSupported;
   if (((size_t)lx * lx * lx * sizeof(T)) % 16) return cudaErrorNotSupported;
   switch (lx) {
-    case 4: return launch_ax_tma<T, 4, 4, 1>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
-    case 6: return launch_ax_tma<T, 6, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
-    case 8: return launch_ax_tma<T, 8, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
-    case 10: return launch_ax_tma<T, 10, 2, 5>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip);
+    case 4: return launch_ax_tma<T, 4, 4, 1>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip, err);
+    case 6: return launch_ax_tma<T, 6, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip, err);
+    case 8: return launch_ax_tma<T, 8, 3, 2>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip, err);
+    case 10: return launch_ax_tma<T, 10, 2, 5>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, skip, err);
     default: return cudaErrorNotSupported;
   }
 }
@@ -330,11 +332,12 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
                        const double *__restrict__ g11, const double *__restrict__ g22,
                        const double *__restrict__ g33, const double *__restrict__ g12,
                        const double *__restrict__ g13, const double *__restrict__ g23,
-                       const int nelv, CgState *st, double *partials, unsigned *counter) {
+                       const int nelv, CgState *st, double beta_arg, double *pap_out,
+                       double *partials, unsigned *counter, int *__restrict__ err) {
   using C = AxCgCfg<LX, S, KS>;
   constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS, THREADS = C::THREADS;
   static_assert(LX % KS == 0, "k split must divide lx");
-  if (st->done) return;
+  if (st && st->done) return;
   extern __shared__ __align__(128) unsigned char smem_ring[];
   double *stage = reinterpret_cast<double *>(smem_ring);
   double *sur = stage + S * NA * L3, *sus = sur + L3, *sut = sus + L3;
@@ -344,7 +347,7 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
   const int tid = threadIdx.x;
   const int G = gridDim.x, b = blockIdx.x;
   const int nt = b < nelv ? (nelv - b + G - 1) / G : 0;
-  const double beta = st->beta;
+  const double beta = st ? st->beta : beta_arg;
   if (tid == 0) {
     for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
     fence_barrier_init();
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
   }
   if (failed) {
     if (tid == 0) {
-      atomicCAS(&nb_dev_error, 0, 1);
+      atomicExch(err ? err : &nb_dropin_error, 1);
       // bounded wait for this CTA's copies still in flight
       for (int q = t; q < nt && q < t + S; q++) mbar_wait(&full[q % S], (uint32_t)((q / S) & 1));
     }
@@ -458,8 +461,12 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
   }
   double tot;  // every block takes part, a failed one with its partial sum
   if (grid_sum<THREADS>(pap, partials, counter, &tot)) {
-    st->pap = tot;
-    st->alpha = st->rtz1 / tot;
+    if (st) {
+      st->pap = tot;
+      st->alpha = st->rtz1 / tot;
+    } else if (pap_out) {
+      *pap_out = tot;
+    }
   }
 }
 
@@ -468,8 +475,8 @@ static cudaError_t launch_ax_cg(double *w, double *p, const double *z, const dou
                                 const double *Dt, const double *h1, const double *g11,
                                 const double *g22, const double *g33, const double *g12,
                                 const double *g13, const double *g23, int nelv, CgState *st,
-                                double *partials, unsigned *counter, int max_grid,
-                                cudaStream_t s) {
+                                double beta, double *pap_out, double *partials,
+                                unsigned *counter, int max_grid, cudaStream_t s, int *err) {
   using C = AxCgCfg<LX, S, KS>;
   auto kern = ax_cg_fused_kernel<LX, S, KS>;
   static int grid_per_dev[64] = {0};
@@ -491,31 +498,31 @@ static cudaError_t launch_ax_cg(double *w, double *p, const double *z, const dou
   int grid = nelv < g ? nelv : g;
   if (grid > max_grid) grid = max_grid;
   kern<<<grid, C::THREADS, C::SMEM, s>>>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
-                                          st, partials, counter);
+                                          st, beta, pap_out, partials, counter, err);
   return cudaGetLastError();
 }
 
 cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, const double *Dt,
                         const double *h1, const double *g11, const double *g22, const double *g33,
                         const double *g12, const double *g13, const double *g23, int nelv, int lx,
-                        CgState *st, double *partials, unsigned *counter, int max_grid,
-                        cudaStream_t s) {
+                        CgState *st, double beta, double *pap_out, double *partials,
+                        unsigned *counter, int max_grid, cudaStream_t s, int *err) {
   const void *ptrs[] = {z, p, h1, g11, g22, g33, g12, g13, g23};
   for (const void *q : ptrs)
     if (reinterpret_cast<uintptr_t>(q) & 15) return cudaErrorNotSupported;
   if (((size_t)lx * lx * lx * sizeof(double)) % 16) return cudaErrorNotSupported;
   switch (lx) {
-    case 6: return launch_ax_cg<6, 3, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, partials, counter, max_grid, s);
-    case 8: return launch_ax_cg<8, 2, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, partials, counter, max_grid, s);
-    case 10: return launch_ax_cg<10, 2, 5>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, partials, counter, max_grid, s);
+    case 6: return launch_ax_cg<6, 3, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
+    case 8: return launch_ax_cg<8, 2, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
+    case 10: return launch_ax_cg<10, 2, 5>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
     default: return cudaErrorNotSupported;
   }
 }
 
-int take_device_error() {
+int take_dropin_error() {
   int v = 0, zero = 0;
-  if (cudaMemcpyFromSymbol(&v, nb_dev_error, sizeof(int)) != cudaSuccess) return -1;
-  if (v) cudaMemcpyToSymbol(nb_dev_error, &zero, sizeof(int));
+  if (cudaMemcpyFromSymbol(&v, nb_dropin_error, sizeof(int)) != cudaSuccess) return -1;
+  if (v) cudaMemcpyToSymbol(nb_dropin_error, &zero, sizeof(int));
   return v;
 }
 
@@ -523,7 +530,7 @@ template cudaError_t ax_helm_stream<double>(double *, const double *, const doub
                                             const double *, const double *, const double *,
                                             const double *, const double *, const double *,
                                             const double *, const double *, int, int,
-                                            cudaStream_t, const int *);
+                                            cudaStream_t, const int *, int *);
 
 template <typename T, int LX>
 static cudaError_t launch_ax(T *w, const T *u, const T *dx, const T *dy, const T *dz,
@@ -604,7 +611,7 @@ extern "C" void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, voi
                                    (const double *)dxt, (const double *)h1, (const double *)g11,
                                    (const double *)g22, (const double *)g33, (const double *)g12,
                                    (const double *)g13, (const double *)g23, *nelv, *lx,
-                                   nb::default_stream());
+                                   nb::default_stream(), nullptr, nullptr);
   if (e == cudaErrorNotSupported)
     e = nb::ax_helm<double>(
       (double *)w, (const double *)u, (const double *)dx, (const double *)dy,

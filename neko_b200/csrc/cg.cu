@@ -320,7 +320,8 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
   cudaError_t e = cudaErrorNotSupported;
   if (P->nmask == 0 && !P->ifh2 && P->use_stream_ax)
     e = ax_cg_fused(W.w, W.p, W.z, P->D, P->Dt, P->h1, P->g11, P->g22, P->g33, P->g12, P->g13,
-                    P->g23, (int)P->nelv, P->lx, W.st, W.partials, W.counter, kCgMaxPartials, s);
+                    P->g23, (int)P->nelv, P->lx, W.st, 0.0, nullptr, W.partials, W.counter,
+                    kCgMaxPartials, s, P->err);
   W.fused = e == cudaSuccess;
   if (e != cudaSuccess && e != cudaErrorNotSupported) return e;
   if (!W.fused) {
@@ -438,7 +439,9 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     // that used the whole iteration budget.
     if (hs->iter >= o.max_iter) res->converged = 0;
   }
-  if (take_device_error())
+  // the problem's own error word: this solve's operator launches, or an
+  // earlier asynchronous nb_ax on the same problem not yet reported
+  if (P->take_error())
     return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (bulk copy never completed)");
   if (pc && pc->take_error())
     return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (coarse-level grid barrier)");

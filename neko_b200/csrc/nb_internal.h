@@ -23,6 +23,12 @@ void set_error(const std::string &msg);
     }                                                                       \
   } while (0)
 
+// Streaming multiprocessors of the current device (queried once per device).
+int device_sms();
+
+// Capacity, in blocks, of every partial-sum buffer of a grid reduction.
+constexpr int kMaxRedBlocks = 2048;
+
 // Reference-style fatal check for the drop-in cuda_* symbols, which return
 // no status (the reference's CUDA_CHECK prints and exits).
 void cuda_check_fatal(cudaError_t e, const char *what);

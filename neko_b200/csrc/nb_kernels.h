@@ -7,8 +7,9 @@
 
 namespace nb {
 
-// Stream used by drop-in entry points that take none (the reference's
-// glb_cmd_queue); the legacy default stream unless set.
+// Stream used by drop-in entry points that take none: the one set by
+// nb_set_default_stream, else Neko's glb_cmd_queue when the program defines
+// it, else the legacy default stream.
 cudaStream_t default_stream();
 void set_default_stream(cudaStream_t s);
 
@@ -25,20 +26,24 @@ template <typename T>
 cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h1,
                            const T *g11, const T *g22, const T *g33, const T *g12,
                            const T *g13, const T *g23, int nelv, int lx, cudaStream_t s,
-                           const int *skip = nullptr);
+                           const int *skip = nullptr, int *err = nullptr);
 
-// Reads and clears the device error word (0 = no error).
-int take_device_error();
+// Reads and clears the error word of the drop-in cuda_ax_helm (0 = no
+// error); kernels given a null error word record their timeouts there.
+int take_dropin_error();
 
 struct CgState;
-// p = z + beta p, w = A p (no gather-scatter) and pap = sum p * w, alpha =
-// rtz / pap in one streaming launch, for problems with no mask and no h2
-// (ax_helm.cu).  cudaErrorNotSupported when lx or alignment is not covered.
+// p = z + beta p, w = A p (no gather-scatter) and pap = sum p * w in one
+// streaming launch (ax_helm.cu).  With a CG state, beta is read from it,
+// the launch returns at once when st->done is set, and pap and alpha =
+// rtz / pap are written to it; without one, beta is the argument and pap
+// goes to *pap_out (device, may be null).  cudaErrorNotSupported when lx or
+// alignment is not covered.
 cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, const double *Dt,
                         const double *h1, const double *g11, const double *g22, const double *g33,
                         const double *g12, const double *g13, const double *g23, int nelv, int lx,
-                        CgState *st, double *partials, unsigned *counter, int max_grid,
-                        cudaStream_t s);
+                        CgState *st, double beta, double *pap_out, double *partials,
+                        unsigned *counter, int max_grid, cudaStream_t s, int *err);
 
 // Grid size for streaming kernels: a multiple of the SM count.
 int stream_grid(long n, int threads);

@@ -30,7 +30,7 @@ struct Precond {
 };
 
 // Blocks a CG reduction may use (its partial sums live in the workspace).
-constexpr int kCgMaxPartials = 148 * 8;
+constexpr int kCgMaxPartials = kMaxRedBlocks;
 
 struct CgWorkspace {
   long n = 0;

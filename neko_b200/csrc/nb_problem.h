@@ -50,6 +50,10 @@ struct nb_problem {
   float *multf = nullptr;  // mult in FP32 when every value is exact there, else null
   double *red_partials = nullptr, *red_out = nullptr;
   unsigned *red_counter = nullptr;
+  // Device error word of this problem's streaming kernels (1 = a bounded
+  // bulk-copy wait expired); read and cleared by take_error().
+  int *err = nullptr;
+  int take_error();
   // Krylov workspace (allocated on first solve)
   void *solver_ws = nullptr;
   size_t solver_ws_bytes = 0;

@@ -8,6 +8,8 @@
 
 #include <cuda_runtime.h>
 
+#include "nb_internal.h"
+
 namespace nb {
 
 constexpr int kRedThreads = 256;
@@ -99,11 +101,13 @@ __device__ __forceinline__ bool grid_sum2(double v0, double v1, double *partials
   return false;
 }
 
-// Number of blocks of a grid-stride reduction over n points: a multiple of
-// the 148 SMs, at most 4 waves, at least one point per thread.
+// Number of blocks of a grid-stride reduction over n points: eight blocks a
+// multiprocessor of the current device (at most kMaxRedBlocks), at least one
+// point per thread.
 inline int red_blocks(long n) {
   long b = (n + kRedThreads - 1) / kRedThreads;
-  const long cap = 148L * 8;
+  long cap = 8L * device_sms();
+  if (cap > kMaxRedBlocks) cap = kMaxRedBlocks;
   if (b > cap) b = cap;
   if (b < 1) b = 1;
   return (int)b;

@@ -136,6 +136,13 @@ __global__ void k_inv(double *a, long n) {
        i += (long)gridDim.x * blockDim.x)
     a[i] = 1.0 / a[i];
 }
+// p = z + beta p
+__global__ void k_update_p(double *__restrict__ p, const double *__restrict__ z, double beta,
+                           long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
 __global__ void k_mask(double *__restrict__ x, const int *__restrict__ msk, int m) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) x[msk[i] - 1] = 0.0;
@@ -273,7 +280,8 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
                o_sm = c.take<unsigned char>(hl.seg_masked.size()),
                o_pm = c.take<unsigned char>(hl.pair_masked.size());
   const size_t o_df = c.take<unsigned char>(nelv), o_mf = c.take<float>(n);
-  const size_t o_red = c.take<double>(148 * 8 + 64);
+  const size_t o_red = c.take<double>(kMaxRedBlocks + 64);
+  const size_t o_err = c.take<int>(1);
   P->arena_bytes = c.off;
   cudaError_t ce = cudaMalloc(&P->arena, c.off);
   if (ce != cudaSuccess) {
@@ -309,8 +317,9 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
   P->dfrmd = (unsigned char *)(A + o_df);
   float *multf = (float *)(A + o_mf);
   P->red_partials = dptr(o_red);
-  P->red_counter = (unsigned *)(A + o_red + 148 * 8 * sizeof(double));
-  P->red_out = (double *)(A + o_red + 148 * 8 * sizeof(double) + 64);
+  P->red_counter = (unsigned *)(A + o_red + kMaxRedBlocks * sizeof(double));
+  P->red_out = (double *)(A + o_red + kMaxRedBlocks * sizeof(double) + 64);
+  P->err = (int *)(A + o_err);
   P->gsd.nseg = (int)hl.seg_ptr.size() - 1;
   P->gsd.npairs = (int)hl.pairs.size();
   P->gsd.nextra = (int)hl.extra_mask.size();
@@ -325,7 +334,8 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
   auto up = [&](void *dst, const void *src, size_t bytes) {
     return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
   };
-  NB_TRY(cudaMemset(A + o_red, 0, (148 * 8 + 64) * sizeof(double)));
+  NB_TRY(cudaMemset(A + o_red, 0, (kMaxRedBlocks + 64) * sizeof(double)));
+  NB_TRY(cudaMemset(P->err, 0, sizeof(int)));
   NB_TRY(up(P->D, D.data(), D.size() * 8));
   NB_TRY(up(P->Dt, Dt.data(), Dt.size() * 8));
   NB_TRY(up(P->zg, zg.data(), zg.size() * 8));
@@ -429,7 +439,8 @@ extern "C" nb_status nb_problem_field(const nb_problem *p, const char *name, voi
            {"g23", p->g23},   {"h1", p->h1},         {"h2", p->h2},         {"B", p->B},
            {"mult", p->mult}, {"dx", p->D},          {"dxt", p->Dt},        {"zg", p->zg},
            {"jacobi", p->jdiag}, {"dof_gs", p->dof_gs}, {"gs_dof", p->gs_dof},
-           {"blk_len", p->blk_len}, {"blk_off", p->blk_off}, {"msk", p->msk}};
+           {"blk_len", p->blk_len}, {"blk_off", p->blk_off}, {"msk", p->msk},
+           {"err", p->err}};
   for (auto &e : t)
     if (!strcmp(e.k, name)) {
       *dptr = const_cast<void *>(e.v);
@@ -469,7 +480,7 @@ cudaError_t nb_problem::ax_raw(double *w, const double *u, cudaStream_t s,
   cudaError_t e = cudaErrorNotSupported;
   if (use_stream_ax)
     e = nb::ax_helm_stream<double>(w, u, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, lx, s,
-                                   skip);
+                                   skip, err);
   if (e == cudaErrorNotSupported)
     e = nb::ax_helm<double>(w, u, D, D, D, Dt, Dt, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
                             lx, s, skip);
@@ -483,9 +494,53 @@ cudaError_t nb_problem::ax(double *w, const double *u, cudaStream_t s) const {
   return cudaGetLastError();
 }
 
+int nb_problem::take_error() {
+  int v = 0;
+  if (cudaMemcpy(&v, err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  if (v) {
+    const int zero = 0;
+    cudaMemcpy(err, &zero, sizeof(int), cudaMemcpyHostToDevice);
+  }
+  return v;
+}
+
+extern "C" nb_status nb_problem_sync(nb_problem *p, void *stream) {
+  if (!p) return fail(NB_ERR_ARG, "null problem");
+  NB_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  const int v = p->take_error();
+  if (v < 0) return fail(NB_ERR_CUDA, "nb_problem_sync: reading the error word failed");
+  if (v)
+    return fail(NB_ERR_TIMEOUT,
+                "a bounded device wait of an earlier operator application on this problem "
+                "expired (bulk copy never completed); its output is incomplete");
+  return NB_OK;
+}
+
 extern "C" nb_status nb_ax(nb_problem *p, double *w, const double *u, void *stream) {
   if (!p || !w || !u) return fail(NB_ERR_ARG, "null argument");
   NB_TRY(p->ax(w, u, (cudaStream_t)stream));
+  return NB_OK;
+}
+
+extern "C" nb_status nb_ax_update_p(nb_problem *p, double *w, double *pdir, const double *z,
+                                    double beta, double *pap, void *stream) {
+  if (!p || !w || !pdir || !z) return fail(NB_ERR_ARG, "null argument");
+  const cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaErrorNotSupported;
+  if (p->nmask == 0 && !p->ifh2 && p->use_stream_ax)
+    e = ax_cg_fused(w, pdir, z, p->D, p->Dt, p->h1, p->g11, p->g22, p->g33, p->g12, p->g13,
+                    p->g23, p->nelv, p->lx, nullptr, beta, pap, p->red_partials, p->red_counter,
+                    kMaxRedBlocks, s, p->err);
+  if (e != cudaErrorNotSupported) {
+    NB_TRY(e);
+    return NB_OK;
+  }
+  // separate passes: direction update, operator (with its h2 term), sum
+  k_update_p<<<stream_grid(p->n, 256), 256, 0, s>>>(pdir, z, beta, p->n);
+  NB_TRY(cudaGetLastError());
+  NB_TRY(p->ax(w, pdir, s));
+  if (pap)
+    NB_TRY(reduce_to<2, double>(pdir, w, nullptr, p->n, p->red_partials, p->red_counter, pap, s));
   return NB_OK;
 }
 

@@ -26,13 +26,46 @@ void cuda_check_fatal(cudaError_t e, const char *what) {
   }
 }
 
+// Stream of the Part-1 entry points that take none.  A Neko build defines
+// the global `void *glb_cmd_queue` (src/device/device_config.h.in:19) and
+// creates it non-blocking (src/device/cuda_intf.F90:284); the reference's
+// kernels launch on it (src/math/bcknd/device/cuda/ax_helm.cu:77).  The weak
+// reference below resolves to that variable when the executable or an
+// already loaded library defines it and stays null otherwise, so the library
+// also links without Neko.  nb_set_default_stream() overrides both.
+extern "C" {
+extern void *glb_cmd_queue __attribute__((weak));
+}
 static cudaStream_t g_default_stream = nullptr;
-cudaStream_t default_stream() { return g_default_stream; }
-void set_default_stream(cudaStream_t s) { g_default_stream = s; }
+static bool g_default_stream_set = false;
+cudaStream_t default_stream() {
+  if (g_default_stream_set) return g_default_stream;
+  if (&glb_cmd_queue != nullptr) return (cudaStream_t)glb_cmd_queue;
+  return nullptr;
+}
+void set_default_stream(cudaStream_t s) {
+  g_default_stream = s;
+  g_default_stream_set = true;
+}
 
+int device_sms() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0)
+      sms = 148;
+    cache[dev] = sms;
+  }
+  return cache[dev];
+}
+
+// Grid of a grid-stride streaming kernel: 16 blocks a multiprocessor at most.
 int stream_grid(long n, int threads) {
   long b = (n + threads - 1) / threads;
-  const long cap = 148L * 16;
+  const long cap = 16L * device_sms();
   if (b > cap) b = cap;
   if (b < 1) b = 1;
   return (int)b;
@@ -57,13 +90,31 @@ static RedScratch &scratch() {
   RedScratch &s = g_scratch[dev];
   if (!s.partials) {
     char *p = nullptr;
-    cuda_check_fatal(cudaMalloc(&p, 148 * 8 * sizeof(double) + 256 + 256), "reduction scratch");
-    cuda_check_fatal(cudaMemset(p, 0, 148 * 8 * sizeof(double) + 512), "reduction scratch");
+    cuda_check_fatal(cudaMalloc(&p, kMaxRedBlocks * sizeof(double) + 256 + 256),
+                     "reduction scratch");
+    cuda_check_fatal(cudaMemset(p, 0, kMaxRedBlocks * sizeof(double) + 512), "reduction scratch");
+    // the memset runs on the legacy stream: finish it before a caller's
+    // non-blocking stream reads the counter
+    cuda_check_fatal(cudaDeviceSynchronize(), "reduction scratch");
     s.partials = (double *)p;
-    s.counter = (unsigned *)(p + 148 * 8 * sizeof(double));
-    s.result = (double *)(p + 148 * 8 * sizeof(double) + 256);
+    s.counter = (unsigned *)(p + kMaxRedBlocks * sizeof(double));
+    s.result = (double *)(p + kMaxRedBlocks * sizeof(double) + 256);
   }
   return s;
+}
+
+// A bounded device wait of an asynchronous drop-in kernel (cuda_ax_helm's
+// bulk-copy ring) that expired is recorded in a device word; the drop-ins
+// that synchronise (the inner products) read it and stop the program as the
+// reference's CUDA_CHECK does for any CUDA error.
+static void check_dropin_error() {
+  const int e = take_dropin_error();
+  if (e > 0) {
+    fprintf(stderr,
+            "neko_b200: a bounded device wait of an earlier cuda_ax_helm expired "
+            "(bulk copy never completed); its output is incomplete\n");
+    exit(1);
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -95,6 +146,7 @@ static double host_reduce(const double *a, const double *b, const double *c, lon
   cuda_check_fatal(cudaMemcpyAsync(&h, r.result, sizeof(double), cudaMemcpyDeviceToHost, s),
                    "reduction D2H");
   cuda_check_fatal(cudaStreamSynchronize(s), "reduction sync");
+  check_dropin_error();
   return h;
 }
 
@@ -106,6 +158,8 @@ cudaError_t reduce_to(const T *a, const T *b, const T *c, long n, double *partia
   return cudaGetLastError();
 }
 template cudaError_t reduce_to<3, double>(const double *, const double *, const double *, long,
+                                          double *, unsigned *, double *, cudaStream_t);
+template cudaError_t reduce_to<2, double>(const double *, const double *, const double *, long,
                                           double *, unsigned *, double *, cudaStream_t);
 template cudaError_t reduce_to<1, double>(const double *, const double *, const double *, long,
                                           double *, unsigned *, double *, cudaStream_t);
@@ -136,6 +190,37 @@ __global__ void k_addcol4(double *a, const double *b, const double *c, const dou
 }
 __global__ void k_invcol1(double *a, long n) { NB_GRID_STRIDE(i, n) a[i] = 1.0 / a[i]; }
 __global__ void k_radd(double *a, double c, long n) { NB_GRID_STRIDE(i, n) a[i] = a[i] + c; }
+
+// Fused-CG helpers (fusedcg_device_solve, src/krylov/bcknd/device/
+// fusedcg_device.F90:328-414): p = beta po + z; x += sum_j alpha_j p_j over
+// the p_cur stored directions (j ascending, the sum formed first); and
+// a -= alpha c with sum (a b a) of the updated a.
+__global__ void k_fusedcg_update_p(double *__restrict__ p, const double *__restrict__ z,
+                                   const double *__restrict__ po, double beta, long n) {
+  NB_GRID_STRIDE(i, n) p[i] = beta * po[i] + z[i];
+}
+__global__ void k_fusedcg_update_x(double *__restrict__ x, const double *const *__restrict__ p,
+                                   const double *__restrict__ alpha, int p_cur, long n) {
+  NB_GRID_STRIDE(i, n) {
+    double t = 0.0;
+    for (int j = 0; j < p_cur; j++) t += p[j][i] * alpha[j];
+    x[i] += t;
+  }
+}
+__global__ void __launch_bounds__(kRedThreads)
+    k_fusedcg_part2(double *__restrict__ a, const double *__restrict__ b,
+                    const double *__restrict__ c, double alpha, double *alpha_slot, long n,
+                    double *partials, unsigned *counter, double *out) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *alpha_slot = alpha;
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kRedThreads) {
+    const double rt = a[i] - alpha * c[i];
+    s += rt * b[i] * rt;
+    a[i] = rt;
+  }
+  grid_sum<kRedThreads>(s, partials, counter, out);
+}
 
 // zero_dirichlet_apply_scalar_kernel semantics: msk(0) is the count, entries
 // 1..m-1 are 1-based point indices.
@@ -274,6 +359,35 @@ void cuda_invcol1(void *a, int *n, void *s) { NB_LAUNCH(nb::k_invcol1, *n, s, (d
 void cuda_radd(void *a, double *c, int *n, void *s) {
   NB_LAUNCH(nb::k_radd, *n, s, (double *)a, *c, *n);
 }
+
+// The reference's fused-CG entry points take no stream and launch on
+// glb_cmd_queue (src/krylov/bcknd/device/cuda/fusedcg_aux.cu:61-87).
+void cuda_fusedcg_update_p(void *p, void *z, void *po, double *beta, int *n) {
+  NB_LAUNCH(nb::k_fusedcg_update_p, *n, nb::default_stream(), (double *)p, (const double *)z,
+            (const double *)po, *beta, *n);
+}
+void cuda_fusedcg_update_x(void *x, void *p, void *alpha, int *p_cur, int *n) {
+  NB_LAUNCH(nb::k_fusedcg_update_x, *n, nb::default_stream(), (double *)x,
+            (const double *const *)p, (const double *)alpha, *p_cur, *n);
+}
+double cuda_fusedcg_part2(void *a, void *b, void *c, void *alpha_d, double *alpha, int *p_cur,
+                          int *n) {
+  const cudaStream_t s = nb::default_stream();
+  nb::RedScratch &r = nb::scratch();
+  const long nn = *n > 0 ? *n : 0;
+  nb::k_fusedcg_part2<<<nb::red_blocks(nn), nb::kRedThreads, 0, s>>>(
+      (double *)a, (const double *)b, (const double *)c, *alpha,
+      (double *)alpha_d + (*p_cur - 1), nn, r.partials, r.counter, r.result);
+  nb::cuda_check_fatal(cudaGetLastError(), "cuda_fusedcg_part2");
+  double h = 0.0;
+  nb::cuda_check_fatal(cudaMemcpyAsync(&h, r.result, sizeof(double), cudaMemcpyDeviceToHost, s),
+                       "cuda_fusedcg_part2 D2H");
+  nb::cuda_check_fatal(cudaStreamSynchronize(s), "cuda_fusedcg_part2 sync");
+  nb::check_dropin_error();
+  return h;
+}
+
+void nb_set_default_stream(void *stream) { nb::set_default_stream((cudaStream_t)stream); }
 
 void cuda_zero_dirichlet_apply_scalar(void *msk, void *x, int *m, void *stream) {
   if (*m <= 1) return;

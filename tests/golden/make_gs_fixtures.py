@@ -52,7 +52,9 @@ def parse(text):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_gs_fixtures.py <root of the reference checkout>")
+    root = sys.argv[1]
     with open(os.path.join(root, PF)) as f:
         tests = parse(f.read())
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "gs_face_fixtures.json")

@@ -1,0 +1,128 @@
+"""Parity at the benchmark sizes: the large pressure-type solve (periodic
+deformed box [0, 2 pi]^3 of 32^3 hexahedra, lx = 8, 16.8 M points; and
+lx = 10, 32.8 M points) against one complete FP64 solve of the CPU oracle
+on the same right-hand side.
+
+Bars (the same as the small-mesh tests): flexible-CG iteration counts within
++-1 of the oracle's (pc_hsmg.f90:481-627 preconditioning
+cg_device.f90:162-238's iteration), FP64 solutions within 1e-7 relative
+(max-norm, both mean-free: the periodic problem is singular), and the mixed
+solve (FP32 smoothing, FP64 outer FCG) within 1e-6 relative (L2) of the
+oracle's FP64 solution, in at most three more iterations.  Each oracle solve
+takes tens of seconds on the host threads; the oracle solution of a size is
+shared by the tests of that size.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfg(lx):
+    from neko_b200 import workloads
+    c = dict(workloads.CONFIG2)
+    c["lx"] = lx
+    return c
+
+
+class _Case:
+    """Device problem, right-hand side and oracle problem of one size."""
+
+    def __init__(self, nb, oracle, lx):
+        c = _cfg(lx)
+        self.cfg = c
+        self.P = nb.Problem(c["nel"], lx, lo=c["lo"], hi=c["hi"], periodic=c["periodic"],
+                            deform=c["deform"], dirichlet=c["dirichlet"])
+        from neko_b200 import workloads
+        P = self.P
+        b = workloads.config2_rhs_local(P.field("x"), P.field("y"), P.field("z"), P.field("B"),
+                                        2024).contiguous()
+        P.gs.op(b, P.n)
+        torch.cuda.synchronize()
+        self.b = b
+        self.r0 = math.sqrt(float((b * P.field("mult") * b).sum()) / P.volume)
+        self.tol = c["rel_tol"] * self.r0
+        O = oracle.OracleProblem.box(c["nel"], lx, lo=c["lo"], hi=c["hi"], periodic=c["periodic"])
+        O.deform_sine(c["deform"])
+        O.coef()
+        self.O = O
+        self.oracle = oracle
+        self._sol = {}
+
+    def oracle_solution(self, coarse_tol):
+        if coarse_tol not in self._sol:
+            H = self.oracle.OracleHsmg(self.O, coarse_tol=coarse_tol)
+            xo, it, _, _ = H.cg(self.b.cpu().numpy(), self.cfg["max_iter"], self.tol,
+                                flexible=True)
+            H.close()
+            self._sol[coarse_tol] = (xo, it)
+        return self._sol[coarse_tol]
+
+    def gpu_solve(self, nb, coarse_tol, mixed):
+        x = self.P.zeros()
+        mon = nb.FCG(max_iter=self.cfg["max_iter"], abs_tol=self.tol,
+                     M=nb.Hsmg(coarse_tol=coarse_tol, mixed=mixed)).solve(
+            nb.AxHelm(), x, self.b, self.P.n, self.P)
+        torch.cuda.synchronize()
+        return x.cpu().numpy(), mon
+
+
+def _mean_free(v):
+    return v - v.mean()
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import neko_b200
+    neko_b200.load()
+    return neko_b200
+
+
+@pytest.fixture(scope="module")
+def case8(nb, oracle):
+    return _Case(nb, oracle, 8)
+
+
+@pytest.fixture(scope="module")
+def case10(nb, oracle):
+    return _Case(nb, oracle, 10)
+
+
+@pytest.mark.parametrize("coarse_tol", [1e-9, 1e-4])
+def test_config2_fp64_solve_matches_oracle(nb, case8, coarse_tol):
+    """32^3 x lx 8: the reference's coarse solve (10 Jacobi-CG iterations at
+    abs tol 1e-9) and the 1e-4 variant."""
+    xo, it_o = case8.oracle_solution(coarse_tol)
+    x, mon = case8.gpu_solve(nb, coarse_tol, mixed=False)
+    assert mon.converged
+    assert abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    a, r = _mean_free(x), _mean_free(xo)
+    assert np.abs(a - r).max() / np.abs(r).max() < 1e-7
+
+
+def test_config3_lx8_mixed_vs_oracle(nb, case8):
+    xo, it_o = case8.oracle_solution(1e-9)
+    x, mon = case8.gpu_solve(nb, 1e-9, mixed=True)
+    assert mon.converged and mon.res_final < case8.tol
+    assert mon.iter <= it_o + 3, (mon.iter, it_o)
+    a, r = _mean_free(x), _mean_free(xo)
+    err = np.linalg.norm(a - r) / np.linalg.norm(r)
+    assert err < 1e-6, err
+
+
+def test_config3_lx10_fp64_and_mixed_vs_oracle(nb, case10):
+    """lx = 10 (32.8 M points): the FP64 solve within +-1 iteration and 1e-7
+    of the oracle, the mixed solve within 1e-6 of the oracle's solution."""
+    xo, it_o = case10.oracle_solution(1e-9)
+    r = _mean_free(xo)
+    x, mon = case10.gpu_solve(nb, 1e-9, mixed=False)
+    assert mon.converged
+    assert abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    assert np.abs(_mean_free(x) - r).max() / np.abs(r).max() < 1e-7
+    xm, mon_m = case10.gpu_solve(nb, 1e-9, mixed=True)
+    assert mon_m.converged and mon_m.iter <= it_o + 3, (mon_m.iter, it_o)
+    err = np.linalg.norm(_mean_free(xm) - r) / np.linalg.norm(r)
+    assert err < 1e-6, err

@@ -37,19 +37,23 @@ CASES = [((4, 4, 4), 8, (False,) * 3, 0.0, 1.0),
          ((3, 3, 3), 4, (False,) * 3, 0.0, 1.0)]
 
 
-def _residual(O, rng, per):
-    """A masked, assembled residual B xi.  For a fully periodic (singular)
-    problem the local values are de-meaned before the gather-scatter, so the
-    assembled vector sums to zero over the global points: a consistent
-    right-hand side, as the solver's residuals are."""
+def _residual(O, rng, singular):
+    """A masked, assembled residual B xi.  For a singular problem (fully
+    periodic, or no Dirichlet face) the local values are de-meaned before
+    the gather-scatter, so the assembled vector sums to zero over the global
+    points: a consistent right-hand side, as the solver's residuals are."""
     rl = O.f64("B") * rng.standard_normal(O.f64("B").size)
-    if all(per):
+    if singular:
         rl -= rl.sum() / rl.size
     return O.bc_apply(O.gs_add(rl))
 
 
-def _pair(nb, oracle, nel, lx, per, amp, hi):
-    dirichlet = not all(per)
+def _pair(nb, oracle, nel, lx, per, amp, hi, dirichlet=None):
+    """Device problem and oracle problem of one box.  By default every face
+    without a neighbour is zero-Dirichlet; dirichlet=False leaves them
+    natural (Neumann), which makes the problem singular."""
+    if dirichlet is None:
+        dirichlet = not all(per)
     P = nb.Problem(nel, lx, hi=(hi,) * 3, periodic=per, deform=amp, dirichlet=dirichlet)
     O = oracle.OracleProblem.box(nel, lx, hi=(hi,) * 3, periodic=per)
     if amp:
@@ -60,26 +64,34 @@ def _pair(nb, oracle, nel, lx, per, amp, hi):
     return P, O
 
 
+# Boxes whose boundary faces are natural (no Dirichlet mask): the fine
+# level then takes the merged gather-scatter path (no masked point) on a
+# non-periodic mesh, and the FDM sees unlabeled boundary faces.
+NEUMANN_CASES = [((4, 3, 4), 8, (False,) * 3, 0.05, 1.0),
+                 ((3, 4, 3), 6, (True, False, False), 0.0, 1.0)]
+
+
 @pytest.mark.parametrize("nel,lx,per,amp,hi", CASES)
-def test_hsmg_apply_matches_oracle(nb, oracle, nel, lx, per, amp, hi):
-    P, O = _pair(nb, oracle, nel, lx, per, amp, hi)
+def test_hsmg_apply_matches_oracle(nb, oracle, nel, lx, per, amp, hi, dirichlet=None):
+    P, O = _pair(nb, oracle, nel, lx, per, amp, hi, dirichlet)
+    singular = all(per) or dirichlet is False
     H = oracle.OracleHsmg(O)
     rng = np.random.default_rng(lx)
-    r = _residual(O, rng, per)
+    r = _residual(O, rng, singular)
     mult = O.f64("mult")
 
     def modc(v):
-        # Fully periodic problems are singular: the coarse solve fixes the
-        # constant mode of z arbitrarily, and the flexible CG that uses z is
-        # blind to it (r is orthogonal to constants), so compare modulo it.
-        return v - np.sum(mult * v) / np.sum(mult) if all(per) else v
+        # Singular problems: the coarse solve fixes the constant mode of z
+        # arbitrarily, and the flexible CG that uses z is blind to it (r is
+        # orthogonal to constants), so compare modulo it.
+        return v - np.sum(mult * v) / np.sum(mult) if singular else v
 
     ref = modc(H.apply(r))
     # On very small periodic meshes the ten coarse CG iterations also
     # amplify rounding in the other modes; the bound is then ten times the
     # oracle's own change under a 1e-15 relative perturbation of r.
     tol = 1e-10
-    if all(per):
+    if singular:
         rp = r * (1 + 1e-15 * rng.standard_normal(r.size))
         sens = np.abs(modc(H.apply(rp)) - ref).max() / np.abs(ref).max()
         tol = max(tol, 10 * sens)
@@ -112,12 +124,16 @@ def test_hsmg_other_line_lengths(nb, oracle, nel, lx, per, amp, hi):
 
 
 @pytest.mark.parametrize("nel,lx,per,amp,hi", CASES[:4])
-def test_fcg_hsmg_matches_oracle(nb, oracle, nel, lx, per, amp, hi):
+def test_fcg_hsmg_matches_oracle(nb, oracle, nel, lx, per, amp, hi, dirichlet=None):
     from neko_b200 import workloads
-    P, O = _pair(nb, oracle, nel, lx, per, amp, hi)
+    P, O = _pair(nb, oracle, nel, lx, per, amp, hi, dirichlet)
+    singular = all(per) or dirichlet is False
     H = oracle.OracleHsmg(O)
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
-    b = O.gs_add(workloads.config2_rhs_local(x, y, z, B, 3))
+    rl = workloads.config2_rhs_local(x, y, z, B, 3)
+    if singular:  # consistent right-hand side: zero sum over the global points
+        rl = rl - rl.sum() / rl.size
+    b = O.gs_add(rl)
     b = O.bc_apply(b)
     mult = O.f64("mult")
     r0 = np.sqrt(np.sum(b * mult * b) / O.volume)
@@ -128,9 +144,17 @@ def test_fcg_hsmg_matches_oracle(nb, oracle, nel, lx, per, amp, hi):
     assert mon.converged
     assert abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
     xdn = _np(xd)
-    if all(per):  # solutions of the singular problem agree up to a constant
+    if singular:  # solutions of the singular problem agree up to a constant
         xdn, xo = xdn - xdn.mean(), xo - xo.mean()
     assert np.abs(xdn - xo).max() / np.abs(xo).max() < 1e-7
+
+
+@pytest.mark.parametrize("nel,lx,per,amp,hi", NEUMANN_CASES)
+def test_hsmg_neumann_box_matches_oracle(nb, oracle, nel, lx, per, amp, hi):
+    """Non-periodic boxes without a Dirichlet mask: one application and the
+    flexible-CG solve against the oracle, modulo the constant mode."""
+    test_hsmg_apply_matches_oracle(nb, oracle, nel, lx, per, amp, hi, dirichlet=False)
+    test_fcg_hsmg_matches_oracle(nb, oracle, nel, lx, per, amp, hi, dirichlet=False)
 
 
 def test_hsmg_rejects_bad_lx(nb):
@@ -147,7 +171,7 @@ def test_hsmg_mixed_apply_close_to_fp64(nb, oracle, nel, lx, per, amp, hi):
     P, O = _pair(nb, oracle, nel, lx, per, amp, hi)
     H = oracle.OracleHsmg(O)
     rng = np.random.default_rng(11)
-    r = _residual(O, rng, per)
+    r = _residual(O, rng, all(per))
     mult = O.f64("mult")
 
     def modc(v):  # constant mode of the singular periodic problem, as above

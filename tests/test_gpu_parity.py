@@ -291,3 +291,29 @@ def test_solve_errors_are_returned(nb):
     nanf = torch.full((P.n,), float("nan"), dtype=torch.float64, device="cuda")
     with pytest.raises(nb.NekoB200Error):
         nb.CG(max_iter=5, abs_tol=1e-9).solve(nb.AxHelm(), x, nanf, P.n, P)
+
+
+@pytest.mark.parametrize("nel,lx,per,deform,dirichlet", [
+    ((4, 4, 4), 8, (True,) * 3, 0.05, False),    # one fused launch
+    ((3, 4, 3), 10, (True,) * 3, 0.05, False),   # one fused launch
+    ((3, 3, 3), 7, (True,) * 3, 0.05, False),    # separate passes (odd lx)
+    ((3, 3, 4), 8, (False,) * 3, 0.0, True)])    # separate passes (mask)
+def test_ax_update_p_matches_oracle(nb, oracle, nel, lx, per, deform, dirichlet):
+    """nb_ax_update_p: p = z + beta p, w = A p and sum(p w) against the
+    oracle's ax_helm of the same updated direction."""
+    hi = 2 * np.pi if all(per) else 1.0
+    P, O = _pair(nb, oracle, nel, lx, periodic=per, deform=deform, hi=hi, dirichlet=dirichlet)
+    rng = np.random.default_rng(lx)
+    z_h, p_h = rng.standard_normal(P.n), rng.standard_normal(P.n)
+    beta = 0.625
+    z, p = _cuda(z_h), _cuda(p_h)
+    w = P.zeros()
+    pap = torch.zeros(1, dtype=torch.float64, device="cuda")
+    nb.AxHelm().update_p_compute(w, p, z, beta, P, pap=pap)
+    torch.cuda.synchronize()
+    pn = z_h + beta * p_h
+    assert np.abs(_np(p) - pn).max() <= 4e-15 * np.abs(pn).max()
+    ref = O.ax_helm(pn)
+    assert rel_err(_np(w), ref) < ax_rtol(lx)
+    ref_pap = float(np.sum(pn * ref))
+    assert abs(float(pap.item()) - ref_pap) <= 1e-12 * float(np.sum(np.abs(pn * ref)))
