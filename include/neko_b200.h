@@ -44,6 +44,22 @@ void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, void *dxt,
                   void *g33, void *g12, void *g13, void *g23, int *nelv,
                   int *lx);
 
+/* (au, av, aw) = A (u, v, w), the h1 part of the operator for the three
+ * velocity components with one set of geometric factors.  Replaces
+ * cuda_ax_helm_vector (src/math/bcknd/device/cuda/ax_helm.cu:184), called
+ * from ax_helm_device_compute_vector (src/math/bcknd/device/
+ * ax_helm_device.F90).  Launches on glb_cmd_queue (see the stream rule
+ * above). */
+void cuda_ax_helm_vector(void *au, void *av, void *aw, void *u, void *v, void *w,
+                         void *dx, void *dy, void *dz, void *dxt, void *dyt, void *dzt,
+                         void *h1, void *g11, void *g22, void *g33, void *g12, void *g13,
+                         void *g23, int *nelv, int *lx);
+/* au += h2 B u, av += h2 B v, aw += h2 B w over n points.  Replaces
+ * cuda_ax_helm_vector_part2 (src/math/bcknd/device/cuda/ax_helm.cu:254);
+ * launches on glb_cmd_queue. */
+void cuda_ax_helm_vector_part2(void *au, void *av, void *aw, void *u, void *v, void *w,
+                               void *h2, void *B, int *n);
+
 /* au += h2 B u for one component.  Replaces the addcol4 used for the h2
  * term of the scalar Ax (ax_helm_device.F90:253-255 ->
  * src/math/bcknd/device/cuda/math.cu:641). */
@@ -214,6 +230,12 @@ nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1,
  * in the problem's error word and reported by the next nb_problem_sync or
  * nb_solve on the same problem. */
 nb_status nb_ax(nb_problem *p, double *w, const double *u, void *stream);
+/* (au, av, aw) = A (u, v, w) for the three components of a vector field
+ * (the velocity Helmholtz operator, incl. the h2 term when enabled), one
+ * pass over the coefficients for the three.  ax_helm_t%compute_vector
+ * (src/math/ax_helm.f90).  Asynchronous on `stream`. */
+nb_status nb_ax_vector(nb_problem *p, double *au, double *av, double *aw, const double *u,
+                       const double *v, const double *w, void *stream);
 /* Synchronises `stream` and reports (then clears) the problem's error word:
  * NB_ERR_TIMEOUT when an earlier asynchronous call on this problem had a
  * bounded device wait expire.  No counterpart in the reference, whose
@@ -252,7 +274,16 @@ typedef struct {
   int coarse_iter;     /* hsmg coarse CG iterations (reference default 10) */
   double coarse_tol;   /* hsmg coarse CG absolute tolerance (default 1e-9) */
   int flexible;        /* 1: flexible CG (Polak-Ribiere beta) with a pc */
+  int ksp;             /* NB_KSP_CG (default) or NB_KSP_GMRES */
+  int m_restart;       /* GMRES vectors per restart cycle (<= 0: 30, the
+                          reference's default; at most 64) */
 } nb_solve_opts;
+
+typedef enum {
+  NB_KSP_CG = 0,     /* cg_device_solve (flexible when opts.flexible) */
+  NB_KSP_GMRES = 1   /* gmres_device_solve: restarted flexible GMRES,
+                        src/krylov/bcknd/device/gmres_device.F90:319-487 */
+} nb_ksp_type;
 
 typedef struct {
   int iter;
@@ -277,9 +308,10 @@ nb_status nb_hsmg_init(nb_problem *p, int mixed, int coarse_iter, double coarse_
 nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r, void *stream);
 
 /* Solves A x = f (f already assembled and masked) from x0 = 0 with
- * preconditioned CG, entirely on the device.  Follows cg_device_solve
- * (src/krylov/bcknd/device/cg_device.f90:162-238) with device-resident
- * scalars.  x and f are device arrays of n doubles. */
+ * preconditioned CG (opts.ksp = NB_KSP_CG; cg_device_solve,
+ * src/krylov/bcknd/device/cg_device.f90:162-238) or restarted flexible
+ * GMRES (NB_KSP_GMRES; gmres_device_solve), entirely on the device with
+ * device-resident scalars.  x and f are device arrays of n doubles. */
 nb_status nb_solve(nb_problem *p, double *x, const double *f,
                    const nb_solve_opts *opts, nb_solve_result *res,
                    void *stream);

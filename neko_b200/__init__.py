@@ -27,7 +27,7 @@ from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpt
 
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
-__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "KspMonitor",
+__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "KspMonitor",
            "Jacobi", "Hsmg", "Batch", "GS_OP_ADD", "NekoB200Error", "load", "version"]
 
 
@@ -143,6 +143,12 @@ class AxHelm:
     def compute(self, w, u, coef, msh=None, Xh=None, stream=None):
         check(load().nb_ax(coef.handle, _ptr(w), _ptr(u), _stream_handle(stream)))
 
+    def compute_vector(self, au, av, aw, u, v, w, coef, msh=None, Xh=None, stream=None):
+        """ax_t%compute_vector: the operator on the three components of a
+        vector field with one pass over the coefficients (nb_ax_vector)."""
+        check(load().nb_ax_vector(coef.handle, _ptr(au), _ptr(av), _ptr(aw), _ptr(u), _ptr(v),
+                                  _ptr(w), _stream_handle(stream)))
+
     def update_p_compute(self, w, p, z, beta, coef, pap=None, stream=None):
         """p = z + beta p, then w = A p in one streaming pass; pap (a
         one-element float64 CUDA tensor, optional) receives sum(p * w) over
@@ -217,6 +223,8 @@ class CG:
     flexible=True uses the Polak-Ribiere beta of flexible CG, which keeps
     converging with a non-symmetric preconditioner such as hsmg."""
 
+    ksp = _lib.NB_KSP_CG
+
     def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False,
                  flexible=False):
         self.max_iter, self.abs_tol, self.mixed = max_iter, abs_tol, mixed
@@ -233,6 +241,8 @@ class CG:
         o.coarse_iter = getattr(self.M, "coarse_iter", 10)
         o.coarse_tol = getattr(self.M, "coarse_tol", 1e-9)
         o.flexible = int(self.flexible)
+        o.ksp = self.ksp
+        o.m_restart = getattr(self, "m_restart", 0)
         r = SolveResult()
         check(load().nb_solve(coef.handle, _ptr(x), _ptr(f), ctypes.byref(o), ctypes.byref(r),
                               _stream_handle(stream)))
@@ -244,6 +254,18 @@ class FCG(CG):
 
     def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False):
         super().__init__(n, max_iter, M, abs_tol, mixed, flexible=True)
+
+
+class GMRES(CG):
+    """ksp_t of type 'gmres': restarted flexible GMRES with m_restart
+    vectors a cycle (gmres_device_t, src/krylov/bcknd/device/gmres_device.F90;
+    the reference's default m_restart is 30)."""
+    ksp = _lib.NB_KSP_GMRES
+
+    def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False,
+                 m_restart=30):
+        super().__init__(n, max_iter, M, abs_tol, mixed)
+        self.m_restart = m_restart
 
 
 class Batch:

@@ -21,6 +21,7 @@ STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR
                 7: "NB_ERR_TIMEOUT"}
 
 NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED = 0, 1, 2, 3
+NB_KSP_CG, NB_KSP_GMRES = 0, 1
 NB_OK, NB_ERR_ARG, NB_ERR_UNSUPPORTED, NB_ERR_OOM, NB_ERR_CUDA = 0, 1, 2, 3, 4
 NB_ERR_NOT_CONVERGED, NB_ERR_NAN, NB_ERR_TIMEOUT = 5, 6, 7
 
@@ -29,7 +30,7 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("abs_tol", ctypes.c_double),
                 ("pc", ctypes.c_int), ("mixed", ctypes.c_int),
                 ("coarse_iter", ctypes.c_int), ("coarse_tol", ctypes.c_double),
-                ("flexible", ctypes.c_int)]
+                ("flexible", ctypes.c_int), ("ksp", ctypes.c_int), ("m_restart", ctypes.c_int)]
 
 
 class SolveResult(ctypes.Structure):
@@ -49,6 +50,8 @@ SIGNATURES = {
     # drop-in cuda_* entry points
     "cuda_ax_helm": (None, [_P] * 15 + [_IP, _IP]),
     "cuda_addcol4": (None, [_P, _P, _P, _P, _IP, _P]),
+    "cuda_ax_helm_vector": (None, [_P] * 19 + [_IP, _IP]),
+    "cuda_ax_helm_vector_part2": (None, [_P] * 8 + [_IP]),
     "cuda_gather_kernel": (None, [_P, _IP, _IP, _P, _P, _IP, _P, _IP, _P, _P, _IP, _P]),
     "cuda_scatter_kernel": (None, [_P, _IP, _P, _P, _IP, _P, _IP, _P, _P, _P]),
     "cuda_glsc3": (ctypes.c_double, [_P, _P, _P, _IP, _P]),
@@ -88,6 +91,7 @@ SIGNATURES = {
     "nb_problem_set_coefficients": (_I, [_P, _P, _P, _I]),
     "nb_ax": (_I, [_P, _P, _P, _P]),
     "nb_problem_sync": (_I, [_P, _P]),
+    "nb_ax_vector": (_I, [_P] * 8),
     "nb_ax_update_p": (_I, [_P, _P, _P, _P, ctypes.c_double, _P, _P]),
     "nb_gs_add": (_I, [_P, _P, _P]),
     "nb_bc_apply": (_I, [_P, _P, _P]),

@@ -519,6 +519,18 @@ cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, 
   }
 }
 
+int *dropin_error_word() {
+  static int *cache[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!cache[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, nb_dropin_error) != cudaSuccess) return nullptr;
+    cache[dev] = (int *)p;
+  }
+  return cache[dev];
+}
+
 int take_dropin_error() {
   int v = 0, zero = 0;
   if (cudaMemcpyFromSymbol(&v, nb_dropin_error, sizeof(int)) != cudaSuccess) return -1;

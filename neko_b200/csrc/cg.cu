@@ -353,6 +353,7 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
 using namespace nb;
 
 void nb_problem::invalidate_solver_cache() {
+  gmres_invalidate(this);
   if (solver_ws) {
     CgWorkspace *W = (CgWorkspace *)solver_ws;
     if (W->graph_exec) {
@@ -467,6 +468,12 @@ extern "C" nb_status nb_solve(nb_problem *p, double *x, const double *f,
     if (st != NB_OK) return st;
   } else if (opts->pc != NB_PC_JACOBI && opts->pc != NB_PC_NONE) {
     set_error("unknown preconditioner");
+    return NB_ERR_ARG;
+  }
+  if (opts->ksp == NB_KSP_GMRES)
+    return gmres_solve(p, x, f, *opts, pc, res, (cudaStream_t)stream);
+  if (opts->ksp != NB_KSP_CG) {
+    set_error("unknown Krylov method");
     return NB_ERR_ARG;
   }
   return cg_solve(p, x, f, *opts, pc, res, (cudaStream_t)stream);

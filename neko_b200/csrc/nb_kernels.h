@@ -31,6 +31,17 @@ cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h
 // Reads and clears the error word of the drop-in cuda_ax_helm (0 = no
 // error); kernels given a null error word record their timeouts there.
 int take_dropin_error();
+// Device address of that word on the current device (looked up once).
+int *dropin_error_word();
+
+// (au, av, aw) = A (u, v, w), h1 part, one set of coefficients
+// (ax_vector.cu).
+cudaError_t ax_helm_vector(double *au, double *av, double *aw, const double *u,
+                           const double *v, const double *w, const double *D,
+                           const double *Dt, const double *h1, const double *g11,
+                           const double *g22, const double *g33, const double *g12,
+                           const double *g13, const double *g23, int nelv, int lx,
+                           cudaStream_t s, int *err);
 
 struct CgState;
 // p = z + beta p, w = A p (no gather-scatter) and pap = sum p * w in one

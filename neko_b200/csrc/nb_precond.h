@@ -67,6 +67,9 @@ __global__ void cg_update_xr_kernel(double *x, double *r, const double *p, const
 
 nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
                    Precond *pc, nb_solve_result *res, cudaStream_t s);
+// Restarted flexible GMRES (gmres.cu).
+nb_status gmres_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
+                      Precond *pc, nb_solve_result *res, cudaStream_t s);
 
 // Operands of the persistent coarse-level launch of hsmg (hsmg_coarse.cu).
 // T is the precision of the middle level; the coarse level is FP64.

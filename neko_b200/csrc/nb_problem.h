@@ -54,8 +54,9 @@ struct nb_problem {
   // bulk-copy wait expired); read and cleared by take_error().
   int *err = nullptr;
   int take_error();
-  // Krylov workspace (allocated on first solve)
+  // Krylov workspaces (allocated on first solve)
   void *solver_ws = nullptr;
+  void *gmres_ws = nullptr;
   size_t solver_ws_bytes = 0;
   nb::HsmgState *hsmg[2] = {nullptr, nullptr};  // hsmg: [0] FP64, [1] mixed
 
@@ -69,6 +70,8 @@ struct nb_problem {
 
 namespace nb {
 void hsmg_free(nb_problem *p);
+void gmres_free(nb_problem *p);
+void gmres_invalidate(nb_problem *p);
 // After new h1: the coarse levels take the new h1 (hsmg_set_h).
 cudaError_t hsmg_refresh_coefficients(nb_problem *p);
 

@@ -182,6 +182,7 @@ static nb_status fail(nb_status s, const std::string &msg) {
 nb_problem::~nb_problem() {
   if (arena) cudaFree(arena);
   if (solver_ws) delete (nb::CgWorkspace *)solver_ws;
+  gmres_free(this);
   hsmg_free(this);
 }
 

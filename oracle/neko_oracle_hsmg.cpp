@@ -21,6 +21,10 @@
 #include "neko_oracle.h"
 
 extern "C" void or_destroy(OrProblem *P);
+int or_gmres_solve_impl(const OrProblem &P, double *x, const double *f, int max_iter,
+                        double abs_tol, int m,
+                        const std::function<void(double *, const double *)> &M,
+                        double *res_start, double *res_final);
 int or_fcg_solve_impl(const OrProblem &P, double *x, const double *f, int max_iter,
                       double abs_tol, const std::function<void(double *, const double *)> &M,
                       double *res_start, double *res_final);
@@ -693,6 +697,13 @@ int or_cg_hsmg(OrProblem *P, OrHsmg *H, double *x, const double *f, int max_iter
                double abs_tol, double *res_start, double *res_final) {
   auto M = [&](double *z, const double *r) { or_hsmg_apply(H, z, r); };
   return or_cg_solve_impl(*P, x, f, max_iter, abs_tol, M, res_start, res_final);
+}
+
+// Restarted flexible GMRES with hsmg (gmres_device_solve, M = hsmg).
+int or_gmres_hsmg(OrProblem *P, OrHsmg *H, double *x, const double *f, int max_iter,
+                  double abs_tol, int m, double *res_start, double *res_final) {
+  auto M = [&](double *z, const double *r) { or_hsmg_apply(H, z, r); };
+  return or_gmres_solve_impl(*P, x, f, max_iter, abs_tol, m, M, res_start, res_final);
 }
 
 // Flexible CG with hsmg.

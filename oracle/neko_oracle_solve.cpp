@@ -263,6 +263,108 @@ int or_fcg_solve_impl(const OrProblem &P, double *x, const double *f, int max_it
   return iter > max_iter ? max_iter : iter;
 }
 
+// Restarted flexible GMRES of gmres_device_solve
+// (src/krylov/bcknd/device/gmres_device.F90:319-487), m_restart vectors a
+// cycle (default 30, :63): classical Gram-Schmidt -- all h(i,j) from one
+// pass (device_glsc3_many, math_kernel.h glsc3_many_kernel), then
+// gmres_part2 (cuda/gmres_kernel.h: w -= sum_k h(k,j) v_k with the sum
+// formed first, alpha2 = (w, mult w)) -- Givens rotations on the host
+// scalars, back substitution into c and x += sum_i c(i) z_i
+// (add2s2_many_kernel: the sum formed first).
+int or_gmres_solve_impl(const OrProblem &P, double *x, const double *f, int max_iter,
+                        double abs_tol, int m,
+                        const std::function<void(double *, const double *)> &M,
+                        double *res_start, double *res_final) {
+  const long n = P.n;
+  std::vector<double> w(n), r(n), z((size_t)n * m), v((size_t)n * m), h((size_t)m * m, 0.0);
+  std::vector<double> c(m, 1.0), s(m, 1.0), gam(m + 1, 0.0);
+  auto H = [&](int i, int j) -> double & { return h[(size_t)(i - 1) + (size_t)m * (j - 1)]; };
+  auto V = [&](int i) { return &v[(size_t)(i - 1) * n]; };
+  auto Z = [&](int i) { return &z[(size_t)(i - 1) * n]; };
+  const double norm_fac = 1.0 / std::sqrt(P.volume);
+  for (long q = 0; q < n; q++) x[q] = 0.0;
+  int iter = 0;
+  double rnorm = 0.0;
+  bool conv = false;
+  *res_start = 0.0;
+  while (!conv && iter < max_iter) {
+    for (long q = 0; q < n; q++) r[q] = f[q];
+    if (iter != 0) {
+      ax_helm(P, w.data(), x);
+      or_gs_add_impl(P, w.data());
+      bc_apply(P, w.data());
+      for (long q = 0; q < n; q++) r[q] = r[q] - w[q];
+    }
+    gam[0] = std::sqrt(glsc3(r.data(), r.data(), P.mult.data(), n));
+    if (iter == 0) *res_start = gam[0] * norm_fac;
+    if (gam[0] == 0.0) break;
+    rnorm = 0.0;
+    double temp = 1.0 / gam[0];
+    for (long q = 0; q < n; q++) V(1)[q] = r[q] * temp;
+    int j;
+    for (j = 1; j <= m; j++) {
+      iter = iter + 1;
+      M(Z(j), V(j));
+      ax_helm(P, w.data(), Z(j));
+      or_gs_add_impl(P, w.data());
+      bc_apply(P, w.data());
+      for (int i = 1; i <= j; i++) {
+        double t = 0.0;
+        for (long q = 0; q < n; q++) t = t + w[q] * V(i)[q] * P.mult[q];
+        H(i, j) = t;
+      }
+      double alpha2 = 0.0;
+      for (long q = 0; q < n; q++) {
+        double t = 0.0;
+        for (int k = 1; k <= j; k++) t = t + (-H(k, j)) * V(k)[q];
+        w[q] = w[q] + t;
+        alpha2 = alpha2 + w[q] * w[q] * P.mult[q];
+      }
+      const double alpha = std::sqrt(alpha2);
+      for (int i = 1; i <= j - 1; i++) {
+        temp = H(i, j);
+        H(i, j) = c[i - 1] * temp + s[i - 1] * H(i + 1, j);
+        H(i + 1, j) = -s[i - 1] * temp + c[i - 1] * H(i + 1, j);
+      }
+      rnorm = 0.0;
+      if (alpha == 0.0) {
+        conv = true;
+        break;
+      }
+      const double lr = std::sqrt(H(j, j) * H(j, j) + alpha2);
+      temp = 1.0 / lr;
+      c[j - 1] = H(j, j) * temp;
+      s[j - 1] = alpha * temp;
+      H(j, j) = lr;
+      gam[j] = -s[j - 1] * gam[j - 1];
+      gam[j - 1] = c[j - 1] * gam[j - 1];
+      rnorm = std::fabs(gam[j]) * norm_fac;
+      if (rnorm < abs_tol) {
+        conv = true;
+        break;
+      }
+      if (iter + 1 > max_iter) break;
+      if (j < m) {
+        temp = 1.0 / alpha;
+        for (long q = 0; q < n; q++) V(j + 1)[q] = w[q] * temp;
+      }
+    }
+    j = std::min(j, m);
+    for (int k = j; k >= 1; k--) {
+      temp = gam[k - 1];
+      for (int i = j; i >= k + 1; i--) temp = temp - H(k, i) * c[i - 1];
+      c[k - 1] = temp / H(k, k);
+    }
+    for (long q = 0; q < n; q++) {
+      double t = 0.0;
+      for (int i = 1; i <= j; i++) t = t + Z(i)[q] * c[i - 1];
+      x[q] = x[q] + t;
+    }
+  }
+  *res_final = rnorm;
+  return iter;
+}
+
 extern "C" {
 
 void or_ax_helm(OrProblem *P, double *w, const double *u) { ax_helm(*P, w, u); }
@@ -285,6 +387,17 @@ int or_cg_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double 
     for (long i = 0; i < P->n; i++) z[i] = r[i] * d[i];  // col3 (pc_jacobi.f90:86-92)
   };
   return or_cg_solve_impl(*P, x, f, max_iter, abs_tol, M, res_start, res_final);
+}
+
+// Jacobi-preconditioned restarted GMRES (m vectors a cycle).
+int or_gmres_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double abs_tol,
+                    int m, double *res_start, double *res_final) {
+  std::vector<double> d;
+  jacobi_update(*P, d);
+  auto M = [&](double *z, const double *r) {
+    for (long i = 0; i < P->n; i++) z[i] = d[i] * r[i];
+  };
+  return or_gmres_solve_impl(*P, x, f, max_iter, abs_tol, m, M, res_start, res_final);
 }
 
 }  // extern "C"

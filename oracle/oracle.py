@@ -80,6 +80,10 @@ def lib():
             "or_schwarz_toreg3d": (None, [_D, _D, ctypes.c_int, ctypes.c_int]),
             "or_cg_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
             "or_fcg_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
+            "or_gmres_hsmg": (ctypes.c_int, [_P, _P, _D, _D, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_int, _D, _D]),
+            "or_gmres_jacobi": (ctypes.c_int, [_P, _D, _D, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_int, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -235,6 +239,16 @@ class OracleProblem:
                                 ctypes.byref(r0), ctypes.byref(r1))
         return x, it, r0.value, r1.value
 
+    def gmres_jacobi(self, f, max_iter, abs_tol, m_restart=30):
+        """Jacobi-preconditioned restarted GMRES (gmres_device_solve)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        x = np.zeros_like(f)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        it = lib().or_gmres_jacobi(self.h, _dp(x), _dp(f), max_iter, abs_tol, m_restart,
+                                   ctypes.byref(r0), ctypes.byref(r1))
+        return x, it, r0.value, r1.value
+
 
 class OracleHsmg:
     """hsmg_t of an OracleProblem (coef and bc must be set up first)."""
@@ -267,6 +281,17 @@ class OracleHsmg:
         fn = lib().or_fcg_hsmg if flexible else lib().or_cg_hsmg
         it = fn(self.P.h, self.h, _dp(x), _dp(f), max_iter, abs_tol,
                 ctypes.byref(r0), ctypes.byref(r1))
+        return x, it, r0.value, r1.value
+
+    def gmres(self, f, max_iter, abs_tol, m_restart=30):
+        """Restarted flexible GMRES preconditioned by this hsmg
+        (gmres_device_solve)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        x = np.zeros_like(f)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        it = lib().or_gmres_hsmg(self.P.h, self.h, _dp(x), _dp(f), max_iter, abs_tol,
+                                 m_restart, ctypes.byref(r0), ctypes.byref(r1))
         return x, it, r0.value, r1.value
 
     def close(self):

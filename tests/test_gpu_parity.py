@@ -317,3 +317,48 @@ def test_ax_update_p_matches_oracle(nb, oracle, nel, lx, per, deform, dirichlet)
     assert rel_err(_np(w), ref) < ax_rtol(lx)
     ref_pap = float(np.sum(pn * ref))
     assert abs(float(pap.item()) - ref_pap) <= 1e-12 * float(np.sum(np.abs(pn * ref)))
+
+
+@pytest.mark.parametrize("nel,lx,per,deform", [((4, 4, 4), 8, (True,) * 3, 0.05),
+                                               ((3, 4, 3), 10, (False,) * 3, 0.05),
+                                               ((3, 3, 3), 6, (True, False, True), 0.0),
+                                               ((3, 2, 3), 7, (False,) * 3, 0.05)])
+def test_ax_vector_matches_oracle(nb, oracle, nel, lx, per, deform):
+    """Three-component operator (nb_ax_vector, h1 and h2 parts) and the
+    drop-ins cuda_ax_helm_vector / cuda_ax_helm_vector_part2: each component
+    against the oracle's scalar ax_helm (compute_vector applies the scalar
+    operator to each component, ax_helm_cpu.f90)."""
+    hi = 2 * np.pi if any(per) else 1.0
+    P, O = _pair(nb, oracle, nel, lx, periodic=per, deform=deform, hi=hi, dirichlet=False)
+    rng = np.random.default_rng(31 + lx)
+    comps = [rng.uniform(-1, 1, P.n) for _ in range(3)]
+    h1 = rng.uniform(0.5, 2.0, P.n)
+    h2 = rng.uniform(0.0, 10.0, P.n)
+    P.set_coefficients(_cuda(h1), _cuda(h2))
+    O.set_f64("h1", h1)
+    O.set_f64("h2", h2)
+    O.set_ifh2(True)
+    refs = [O.ax_helm(c) for c in comps]
+    ins = [_cuda(c) for c in comps]
+    outs = [P.zeros() for _ in range(3)]
+    nb.AxHelm().compute_vector(*outs, *ins, P)
+    torch.cuda.synchronize()
+    for o, r in zip(outs, refs):
+        assert rel_err(_np(o), r) < ax_rtol(lx)
+    # drop-ins: h1 part, then the h2 B term
+    vp = ctypes.c_void_p
+    L = nb.load()
+    f = {k: P.field(k) for k in ("dx", "dxt", "h1", "h2", "B", "g11", "g22", "g33", "g12",
+                                 "g13", "g23")}
+    d = [P.zeros() for _ in range(3)]
+    p = lambda t: vp(t.data_ptr())
+    L.cuda_ax_helm_vector(*(p(t) for t in d), *(p(t) for t in ins), p(f["dx"]), p(f["dx"]),
+                          p(f["dx"]), p(f["dxt"]), p(f["dxt"]), p(f["dxt"]), p(f["h1"]),
+                          p(f["g11"]), p(f["g22"]), p(f["g33"]), p(f["g12"]), p(f["g13"]),
+                          p(f["g23"]), ctypes.byref(ctypes.c_int(P.nelv)),
+                          ctypes.byref(ctypes.c_int(lx)))
+    L.cuda_ax_helm_vector_part2(*(p(t) for t in d), *(p(t) for t in ins), p(f["h2"]), p(f["B"]),
+                                ctypes.byref(ctypes.c_int(P.n)))
+    torch.cuda.synchronize()
+    for o, r in zip(d, refs):
+        assert rel_err(_np(o), r) < ax_rtol(lx)
