@@ -316,6 +316,37 @@ nb_status nb_solve(nb_problem *p, double *x, const double *f,
                    const nb_solve_opts *opts, nb_solve_result *res,
                    void *stream);
 
+/* Projection of the right-hand side onto earlier solutions, the step around
+ * the pressure solve of a time step (projection_t,
+ * src/common/projection.f90): a basis X of up to L earlier solutions and
+ * B = A X, A-orthonormal in the mult-weighted inner product.  Every call is
+ * asynchronous on `stream` (the basis size and coefficients stay on the
+ * device) except nb_projection_info and nb_projection_reorthogonalize.
+ *   project_on:  b -= B (X^T b) twice, xbar = X (X^T b) (device_project_on,
+ *                :553-622); call it on the assembled, masked right-hand side.
+ *   project_back: x += xbar; x enters the basis (bcknd_project_back and
+ *                device_proj_ortho, :317-358, :638-714), dropped when it is
+ *                not independent to 1e-7.
+ *   reorthogonalize: B = A X with the current coefficients, then modified
+ *                Gram-Schmidt (device_reorthogonalize_basis, :426-473).
+ *   clear: empty basis (bcknd_clear).  The activation step and time-step
+ *   control of pre_solving/post_solving stay with the caller. */
+typedef struct nb_projection nb_projection;
+nb_status nb_projection_create(nb_problem *p, int L, nb_projection **out);
+nb_status nb_projection_destroy(nb_projection *j);
+nb_status nb_projection_clear(nb_projection *j, void *stream);
+nb_status nb_projection_project_on(nb_projection *j, double *b, void *stream);
+nb_status nb_projection_project_back(nb_projection *j, double *x, void *stream);
+nb_status nb_projection_reorthogonalize(nb_projection *j, void *stream);
+nb_status nb_projection_info(nb_projection *j, int *m, int *proj_m, double *proj_res,
+                             void *stream);
+
+/* x -= sum(x) / n over the n local points: the mean removal of a singular
+ * (all-Neumann or periodic) pressure problem, device_ortho
+ * (src/math/operators.f90:349-368 with glb_n_points = n), with the mean kept
+ * on the device.  Asynchronous on `stream`. */
+nb_status nb_ortho(nb_problem *p, double *x, void *stream);
+
 /* Batched solves.  A batch advances many independent Jacobi-PCG solves
  * (same iteration as nb_solve with NB_PC_JACOBI) together: one iteration
  * of every active solve is one persistent Ax launch over a work queue of

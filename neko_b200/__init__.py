@@ -28,7 +28,8 @@ from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpt
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
 __all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "KspMonitor",
-           "Jacobi", "Hsmg", "Batch", "GS_OP_ADD", "NekoB200Error", "load", "version"]
+           "Jacobi", "Hsmg", "Batch", "Projection", "ortho", "GS_OP_ADD", "NekoB200Error",
+           "load", "version"]
 
 
 def version():
@@ -266,6 +267,61 @@ class GMRES(CG):
                  m_restart=30):
         super().__init__(n, max_iter, M, abs_tol, mixed)
         self.m_restart = m_restart
+
+
+class Projection:
+    """projection_t (src/common/projection.f90): projects the pressure
+    right-hand side onto up to L earlier solutions before the solve and adds
+    the projected part back after it.  pre_solving / post_solving act from
+    time step activ_step + 1 on, as the reference's fixed-step path does."""
+
+    def __init__(self, coef, L=20, activ_step=5):
+        h = ctypes.c_void_p()
+        check(load().nb_projection_create(coef.handle, int(L), ctypes.byref(h)))
+        self._h, self.coef, self.L, self.activ_step = h, coef, L, activ_step
+
+    def pre_solving(self, b, tstep, stream=None):
+        if tstep > self.activ_step and self.L > 0:
+            self.project_on(b, stream)
+
+    def post_solving(self, x, tstep, stream=None):
+        if tstep > self.activ_step and self.L > 0:
+            self.project_back(x, stream)
+
+    def project_on(self, b, stream=None):
+        check(load().nb_projection_project_on(self._h, _ptr(b), _stream_handle(stream)))
+
+    def project_back(self, x, stream=None):
+        check(load().nb_projection_project_back(self._h, _ptr(x), _stream_handle(stream)))
+
+    def reortho_basis(self, stream=None):
+        check(load().nb_projection_reorthogonalize(self._h, _stream_handle(stream)))
+
+    def clear(self, stream=None):
+        check(load().nb_projection_clear(self._h, _stream_handle(stream)))
+
+    def info(self, stream=None):
+        """(basis size, basis size at the last projection, its residual)."""
+        m, pm, pr = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(load().nb_projection_info(self._h, ctypes.byref(m), ctypes.byref(pm),
+                                        ctypes.byref(pr), _stream_handle(stream)))
+        return m.value, pm.value, pr.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            load().nb_projection_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ortho(x, coef, stream=None):
+    """device_ortho: x -= mean of x over the local points (nb_ortho)."""
+    check(load().nb_ortho(coef.handle, _ptr(x), _stream_handle(stream)))
 
 
 class Batch:

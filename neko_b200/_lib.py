@@ -99,6 +99,14 @@ SIGNATURES = {
     "nb_glsc3_noalloc": (_I, [_P, _P, _P, _I, _DP, _P]),
     "nb_pc_apply": (_I, [_P, _I, _P, _P, _P]),
     "nb_hsmg_init": (_I, [_P, _I, _I, ctypes.c_double]),
+    "nb_projection_create": (_I, [_P, _I, _P]),
+    "nb_projection_destroy": (_I, [_P]),
+    "nb_projection_clear": (_I, [_P, _P]),
+    "nb_projection_project_on": (_I, [_P, _P, _P]),
+    "nb_projection_project_back": (_I, [_P, _P, _P]),
+    "nb_projection_reorthogonalize": (_I, [_P, _P]),
+    "nb_projection_info": (_I, [_P, _IP, _IP, _DP, _P]),
+    "nb_ortho": (_I, [_P, _P, _P]),
     "nb_batch_create": (_I, [ctypes.c_int64, _P]),
     "nb_batch_destroy": (None, [_P]),
     "nb_batch_submit": (_I, [_P, _P, _P, _P, ctypes.c_double, _I, _IP]),

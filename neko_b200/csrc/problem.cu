@@ -545,6 +545,24 @@ extern "C" nb_status nb_ax_update_p(nb_problem *p, double *w, double *pdir, cons
   return NB_OK;
 }
 
+// x -= red_out / n, the mean kept on the device
+__global__ void k_sub_mean(double *__restrict__ x, const double *__restrict__ sum, long n) {
+  const double c = *sum / (double)n;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    x[i] = x[i] + (-c);
+}
+
+extern "C" nb_status nb_ortho(nb_problem *p, double *x, void *stream) {
+  if (!p || !x) return fail(NB_ERR_ARG, "null argument");
+  const cudaStream_t s = (cudaStream_t)stream;
+  NB_TRY(reduce_to<1, double>(x, nullptr, nullptr, p->n, p->red_partials, p->red_counter,
+                              p->red_out, s));
+  k_sub_mean<<<stream_grid(p->n, 256), 256, 0, s>>>(x, p->red_out, p->n);
+  NB_TRY(cudaGetLastError());
+  return NB_OK;
+}
+
 extern "C" nb_status nb_gs_add(nb_problem *p, double *u, void *stream) {
   if (!p || !u) return fail(NB_ERR_ARG, "null argument");
   NB_TRY(gs_add_fused<double>(p->gsd, u, false, (cudaStream_t)stream));

@@ -365,6 +365,77 @@ int or_gmres_solve_impl(const OrProblem &P, double *x, const double *f, int max_
   return iter;
 }
 
+// projection_t with the device forms of its steps (src/common/projection.f90):
+// device_project_on (:553-622), bcknd_project_back (:317-358) and
+// device_proj_ortho (:638-714); tol = 1e-7 (:101).  Inner products are
+// glsc3 with mult; the many-vector updates form sum_k c_k v_k first
+// (add2s2_many_kernel).
+struct OrProjection {
+  const OrProblem *P;
+  int L, m = 0;
+  double tol = 1e-7, proj_res = 0.0;
+  std::vector<double> xx, bb, xbar;
+};
+
+static void proj_add_many(double *x, const double *V, const double *c, int cnt, long n) {
+  for (long q = 0; q < n; q++) {
+    double t = 0.0;
+    for (int k = 0; k < cnt; k++) t = t + V[(size_t)k * n + q] * c[k];
+    x[q] = x[q] + t;
+  }
+}
+
+static void proj_project_on(OrProjection &J, double *b) {
+  const OrProblem &P = *J.P;
+  const long n = P.n;
+  if (J.m <= 0) return;
+  J.proj_res = std::sqrt(glsc3(b, b, P.mult.data(), n) / P.volume);
+  std::vector<double> alpha(J.m);
+  for (int i = 0; i < J.m; i++) alpha[i] = glsc3(b, &J.xx[(size_t)i * n], P.mult.data(), n);
+  for (long q = 0; q < n; q++) J.xbar[q] = 0.0;
+  proj_add_many(J.xbar.data(), J.xx.data(), alpha.data(), J.m, n);
+  for (int i = 0; i < J.m; i++) alpha[i] = -alpha[i];
+  proj_add_many(b, J.bb.data(), alpha.data(), J.m, n);
+  for (int i = 0; i < J.m; i++) alpha[i] = glsc3(b, &J.xx[(size_t)i * n], P.mult.data(), n);
+  proj_add_many(J.xbar.data(), J.xx.data(), alpha.data(), J.m, n);
+  for (int i = 0; i < J.m; i++) alpha[i] = -alpha[i];
+  proj_add_many(b, J.bb.data(), alpha.data(), J.m, n);
+}
+
+static void proj_project_back(OrProjection &J, double *x) {
+  const OrProblem &P = *J.P;
+  const long n = P.n;
+  if (J.m > 0)
+    for (long q = 0; q < n; q++) x[q] = x[q] + J.xbar[q];
+  J.m = J.m == J.L ? 1 : std::min(J.m + 1, J.L);
+  const int m = J.m;
+  double *xm = &J.xx[(size_t)(m - 1) * n], *bm = &J.bb[(size_t)(m - 1) * n];
+  for (long q = 0; q < n; q++) xm[q] = x[q];
+  ax_helm(P, bm, xm);
+  or_gs_add_impl(P, bm);
+  bc_apply(P, bm);
+  // device_proj_ortho
+  std::vector<double> alpha(m);
+  for (int i = 0; i < m; i++) alpha[i] = glsc3(bm, &J.xx[(size_t)i * n], P.mult.data(), n);
+  const double nrm = std::sqrt(alpha[m - 1]);
+  for (int pass = 0; pass < 2; pass++) {
+    for (int i = 0; i < m; i++) alpha[i] = -alpha[i];
+    proj_add_many(xm, J.xx.data(), alpha.data(), m - 1, n);
+    proj_add_many(bm, J.bb.data(), alpha.data(), m - 1, n);
+    for (int i = 0; i < m; i++) alpha[i] = glsc3(bm, &J.xx[(size_t)i * n], P.mult.data(), n);
+  }
+  const double am = std::sqrt(glsc3(xm, P.mult.data(), bm, n));
+  if (am > J.tol * nrm) {
+    const double scl = 1.0 / am;
+    for (long q = 0; q < n; q++) {
+      xm[q] = xm[q] * scl;
+      bm[q] = bm[q] * scl;
+    }
+  } else {
+    J.m = m - 1;
+  }
+}
+
 extern "C" {
 
 void or_ax_helm(OrProblem *P, double *w, const double *u) { ax_helm(*P, w, u); }
@@ -388,6 +459,20 @@ int or_cg_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double 
   };
   return or_cg_solve_impl(*P, x, f, max_iter, abs_tol, M, res_start, res_final);
 }
+
+OrProjection *or_projection_create(OrProblem *P, int L) {
+  OrProjection *J = new OrProjection();
+  J->P = P;
+  J->L = L;
+  J->xx.assign((size_t)L * P->n, 0.0);
+  J->bb.assign((size_t)L * P->n, 0.0);
+  J->xbar.assign(P->n, 0.0);
+  return J;
+}
+void or_projection_destroy(OrProjection *J) { delete J; }
+void or_projection_project_on(OrProjection *J, double *b) { proj_project_on(*J, b); }
+void or_projection_project_back(OrProjection *J, double *x) { proj_project_back(*J, x); }
+int or_projection_m(OrProjection *J) { return J->m; }
 
 // Jacobi-preconditioned restarted GMRES (m vectors a cycle).
 int or_gmres_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double abs_tol,

@@ -84,6 +84,11 @@ def lib():
                                              ctypes.c_int, _D, _D]),
             "or_gmres_jacobi": (ctypes.c_int, [_P, _D, _D, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, _D, _D]),
+            "or_projection_create": (_P, [_P, ctypes.c_int]),
+            "or_projection_destroy": (None, [_P]),
+            "or_projection_project_on": (None, [_P, _D]),
+            "or_projection_project_back": (None, [_P, _D]),
+            "or_projection_m": (ctypes.c_int, [_P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -248,6 +253,39 @@ class OracleProblem:
         it = lib().or_gmres_jacobi(self.h, _dp(x), _dp(f), max_iter, abs_tol, m_restart,
                                    ctypes.byref(r0), ctypes.byref(r1))
         return x, it, r0.value, r1.value
+
+
+class OracleProjection:
+    """projection_t of an OracleProblem (device forms of its steps)."""
+
+    def __init__(self, P, L):
+        self.P = P
+        self.h = lib().or_projection_create(P.h, int(L))
+
+    def project_on(self, b):
+        b = np.array(b, dtype=np.float64, copy=True)
+        lib().or_projection_project_on(self.h, _dp(b))
+        return b
+
+    def project_back(self, x):
+        x = np.array(x, dtype=np.float64, copy=True)
+        lib().or_projection_project_back(self.h, _dp(x))
+        return x
+
+    @property
+    def m(self):
+        return lib().or_projection_m(self.h)
+
+    def close(self):
+        if self.h:
+            lib().or_projection_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class OracleHsmg:
