@@ -89,9 +89,9 @@ def test_projection_reorthogonalize_and_clear(nb):
         f.copy_(_cuda(rng.standard_normal(P.n)))
         P.gs.op(f)
         P.bclst.apply(f)
+        J.project_on(f)
         x = P.zeros()
         nb.CG(max_iter=2000, abs_tol=1e-12, M=nb.Jacobi()).solve(nb.AxHelm(), x, f, P.n, P)
-        J.project_on(f)
         J.project_back(x)
         xs.append(x.clone())
     P.set_coefficients(torch.full((P.n,), 2.0, dtype=torch.float64, device="cuda"))
