@@ -109,6 +109,24 @@ void cuda_fusedcg_update_x(void *x, void *p, void *alpha, int *p_cur, int *n);
 double cuda_fusedcg_part2(void *a, void *b, void *c, void *alpha_d, double *alpha,
                           int *p_cur, int *n);
 
+/* Point-wise parts of the Pn-Pn pressure and velocity residuals, the
+ * caller of the pressure solve (pnpn_prs_res_device_compute /
+ * pnpn_vel_res_device_compute, src/fluid/bcknd/device/pnpn_res_device.F90).
+ * Replace src/fluid/bcknd/device/cuda/pnpn_res.cu:43-107; launched on
+ * glb_cmd_queue.
+ *   part1: h1 = 1/rho; ta_i = f_i / rho - (wa_i (mu / rho)) B
+ *   part2: p_res = -p_res + (wa1 + wa2 + wa3)
+ *   part3: p_res = p_res - dtbd (ta1 + ta2 + ta3)
+ *   vel_res_update: res_i = -res_i - ta_i + f_i */
+void pnpn_prs_res_part1_cuda(void *ta1, void *ta2, void *ta3, void *wa1, void *wa2, void *wa3,
+                             void *f_u, void *f_v, void *f_w, void *B, void *h1, double *mu,
+                             double *rho, int *n);
+void pnpn_prs_res_part2_cuda(void *p_res, void *wa1, void *wa2, void *wa3, int *n);
+void pnpn_prs_res_part3_cuda(void *p_res, void *ta1, void *ta2, void *ta3, double *dtbd,
+                             int *n);
+void pnpn_vel_res_update_cuda(void *u_res, void *v_res, void *w_res, void *ta1, void *ta2,
+                              void *ta3, void *f_u, void *f_v, void *f_w, int *n);
+
 /* Stream for the Part-1 entry points that take none, overriding
  * glb_cmd_queue (NULL selects the legacy default stream).  No counterpart in
  * the reference, where Neko's device layer owns glb_cmd_queue. */

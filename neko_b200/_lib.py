@@ -77,6 +77,10 @@ SIGNATURES = {
     "cuda_fusedcg_update_x": (None, [_P, _P, _P, _IP, _IP]),
     "cuda_fusedcg_part2": (ctypes.c_double, [_P, _P, _P, _P, _DP, _IP, _IP]),
     "nb_set_default_stream": (None, [_P]),
+    "pnpn_prs_res_part1_cuda": (None, [_P] * 11 + [_DP, _DP, _IP]),
+    "pnpn_prs_res_part2_cuda": (None, [_P] * 4 + [_IP]),
+    "pnpn_prs_res_part3_cuda": (None, [_P] * 4 + [_DP, _IP]),
+    "pnpn_vel_res_update_cuda": (None, [_P] * 9 + [_IP]),
     # native API
     "nb_last_error": (ctypes.c_char_p, []),
     "nb_version": (ctypes.c_char_p, []),

@@ -235,3 +235,41 @@ def test_error_word_reported_by_its_problem(nblib):
                                                                P1.n, P1)
     assert ei.value.status == 7
     assert int(word.item()) == 0
+
+
+def test_pnpn_residual_parts(nblib):
+    """The point-wise parts of the pressure and velocity residuals against
+    numpy forms of src/fluid/bcknd/device/cuda/prs_res_kernel.h and
+    vel_res_update_kernel.h."""
+    rng = np.random.default_rng(9)
+    n = 200_003
+    H = {k: rng.standard_normal(n) for k in ("ta1", "ta2", "ta3", "wa1", "wa2", "wa3", "fu",
+                                             "fv", "fw", "B", "p", "ur", "vr", "wr")}
+    D = {k: torch.as_tensor(v, device="cuda") for k, v in H.items()}
+    h1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    nn = ctypes.byref(ctypes.c_int(n))
+    mu, rho, dtbd = 0.013, 1.7, 3.25
+    nblib.pnpn_prs_res_part1_cuda(*(_ptr(D[k]) for k in ("ta1", "ta2", "ta3", "wa1", "wa2",
+                                                         "wa3", "fu", "fv", "fw", "B")),
+                                  _ptr(h1), ctypes.byref(ctypes.c_double(mu)),
+                                  ctypes.byref(ctypes.c_double(rho)), nn)
+    torch.cuda.synchronize()
+    for t, w, f in (("ta1", "wa1", "fu"), ("ta2", "wa2", "fv"), ("ta3", "wa3", "fw")):
+        _close(D[t].cpu().numpy(), H[f] / rho - (H[w] * (mu / rho)) * H["B"])
+    assert np.all(h1.cpu().numpy() == 1.0 / rho)
+    nblib.pnpn_prs_res_part2_cuda(_ptr(D["p"]), _ptr(D["wa1"]), _ptr(D["wa2"]), _ptr(D["wa3"]),
+                                  nn)
+    torch.cuda.synchronize()
+    p1 = -H["p"] + (H["wa1"] + H["wa2"] + H["wa3"])
+    _close(D["p"].cpu().numpy(), p1)
+    ta = [D[k].cpu().numpy() for k in ("ta1", "ta2", "ta3")]
+    nblib.pnpn_prs_res_part3_cuda(_ptr(D["p"]), _ptr(D["ta1"]), _ptr(D["ta2"]), _ptr(D["ta3"]),
+                                  ctypes.byref(ctypes.c_double(dtbd)), nn)
+    torch.cuda.synchronize()
+    _close(D["p"].cpu().numpy(), p1 - dtbd * (ta[0] + ta[1] + ta[2]))
+    nblib.pnpn_vel_res_update_cuda(*(_ptr(D[k]) for k in ("ur", "vr", "wr")),
+                                   *(_ptr(D[k]) for k in ("ta1", "ta2", "ta3")),
+                                   *(_ptr(D[k]) for k in ("fu", "fv", "fw")), nn)
+    torch.cuda.synchronize()
+    for r, t, f in (("ur", 0, "fu"), ("vr", 1, "fv"), ("wr", 2, "fw")):
+        _close(D[r].cpu().numpy(), (-H[r]) - ta[t] + H[f])
