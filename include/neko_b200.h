@@ -205,6 +205,14 @@ nb_status nb_box_gs_maps(const int nel[3], const int periodic[3], int lx,
                          int *nlocal, int *facet_offset, int *nblocks,
                          int *dof_gs, int *gs_dof, int *blk_len, int *blk_off);
 
+/* Gather-scatter maps (and the neighbour per face, 6 per element, 1-based,
+ * 0 on the boundary) of the unstructured mesh that nb_problem_create_mesh
+ * takes, in the reference layout of gs_init_mapping.  Host only; call once
+ * with NULL arrays to get the sizes. */
+nb_status nb_mesh_gs_maps(int nelv, const int *vertex_ids, int lx, int *nlocal,
+                          int *facet_offset, int *nblocks, int *facet_neigh, int *dof_gs,
+                          int *gs_dof, int *blk_len, int *blk_off);
+
 /* Builds a structured box problem on the current device: nel[3] hexahedra
  * on [lo,hi]^3 (x fastest), optional periodicity, polynomial size lx
  * (2..16), and an optional smooth deformation of the GLL points
@@ -218,6 +226,22 @@ nb_status nb_problem_create_box(const int nel[3], const double lo[3],
                                 const double hi[3], const int periodic[3],
                                 int lx, double deform_amp,
                                 int dirichlet_boundary, nb_problem **out);
+/* Builds a problem on the current device from a caller's unstructured
+ * hexahedral mesh: nelv elements, each with 8 positive global vertex ids
+ * (vertex_ids[8 e + v]) and coordinates (vertex_xyz[24 e + 3 v + d]) in the
+ * reference's symmetric vertex order (src/mesh/hex.f90:40-57); vertices that
+ * a periodic boundary identifies carry one id.  Faces, edges and neighbours
+ * come from the ids (mesh_generate_conn, src/mesh/mesh.f90:476-687), the
+ * GLL points by trilinear interpolation of the vertices (dofmap_xyzlin) and
+ * the optional sine deformation of nb_problem_create_box, the gather-scatter
+ * maps follow gs_init_mapping entry for entry for any relative rotation of
+ * neighbouring elements.  Faces with no neighbour become zero-Dirichlet when
+ * dirichlet_boundary is non-zero.  Jacobi-preconditioned solves accept any
+ * conforming mesh; hsmg needs neighbours that meet through opposite faces
+ * with the same orientation (NB_ERR_UNSUPPORTED otherwise). */
+nb_status nb_problem_create_mesh(int nelv, const int *vertex_ids, const double *vertex_xyz,
+                                 int lx, double deform_amp, int dirichlet_boundary,
+                                 nb_problem **out);
 nb_status nb_problem_destroy(nb_problem *p);
 
 /* Sizes: n = lx^3 * nelv local dofs. */

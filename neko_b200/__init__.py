@@ -71,6 +71,33 @@ class Problem:
         torch.cuda.init()
         check(L.nb_problem_create_box(ne, lo_, hi_, per, lx, float(deform), int(bool(dirichlet)),
                                       ctypes.byref(h)))
+        self._adopt(h)
+        self.nel, self.periodic, self.deform = tuple(nel), tuple(periodic), deform
+
+    @classmethod
+    def from_mesh(cls, vertex_ids, vertex_xyz, lx, deform=0.0, dirichlet=True):
+        """Problem on an unstructured hex mesh: vertex_ids (nelv, 8) positive
+        global ids, vertex_xyz (nelv, 8, 3), symmetric vertex order
+        (nb_problem_create_mesh)."""
+        import numpy as np
+        ids = np.ascontiguousarray(vertex_ids, dtype=np.int32)
+        xyz = np.ascontiguousarray(vertex_xyz, dtype=np.float64)
+        nelv = ids.shape[0]
+        if ids.shape != (nelv, 8) or xyz.shape != (nelv, 8, 3):
+            raise ValueError("vertex_ids must be (nelv, 8) and vertex_xyz (nelv, 8, 3)")
+        self = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        torch.cuda.init()
+        check(load().nb_problem_create_mesh(
+            nelv, ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            xyz.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(lx), float(deform),
+            int(bool(dirichlet)), ctypes.byref(h)))
+        self._adopt(h)
+        self.nel, self.periodic, self.deform = (nelv,), (False, False, False), deform
+        return self
+
+    def _adopt(self, h):
+        L = load()
         self._h = h
         n = ctypes.c_int64()
         nelv, lxo, nloc, nblk, nmsk = (ctypes.c_int() for _ in range(5))
@@ -81,7 +108,6 @@ class Problem:
         vol = ctypes.c_double()
         check(L.nb_problem_volume(h, ctypes.byref(vol)))
         self.volume = vol.value
-        self.nel, self.periodic, self.deform = tuple(nel), tuple(periodic), deform
         self.gs = GatherScatter(self)
         self.bclst = BcList(self)
 

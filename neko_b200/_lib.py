@@ -86,8 +86,10 @@ SIGNATURES = {
     "nb_version": (ctypes.c_char_p, []),
     "nb_gll": (_I, [_I, _DP, _DP, _DP]),
     "nb_box_gs_maps": (_I, [_IP, _IP, _I, _IP, _IP, _IP, _IP, _IP, _IP, _IP]),
+    "nb_mesh_gs_maps": (_I, [_I, _IP, _I, _IP, _IP, _IP, _IP, _IP, _IP, _IP, _IP]),
     "nb_problem_create_box": (_I, [_IP, _DP, _DP, _IP, _I, ctypes.c_double, _I,
                                    ctypes.POINTER(_P)]),
+    "nb_problem_create_mesh": (_I, [_I, _IP, _DP, _I, ctypes.c_double, _I, ctypes.POINTER(_P)]),
     "nb_problem_destroy": (_I, [_P]),
     "nb_problem_sizes": (_I, [_P, ctypes.POINTER(ctypes.c_int64), _IP, _IP, _IP, _IP, _IP]),
     "nb_problem_field": (_I, [_P, ctypes.c_char_p, ctypes.POINTER(_P)]),

@@ -64,6 +64,23 @@ void box_vertices(const BoxSpec &b, std::vector<double> &xyz8);
 void box_facet_neigh(const BoxSpec &b, std::vector<int> &fn);
 // Gather-scatter maps of the box at polynomial size lx.
 int box_gs_maps(const BoxSpec &b, int lx, const std::vector<int> &facet_neigh, GsMaps &g);
+// Connectivity of an unstructured hex mesh (8 positive global vertex ids per
+// element, symmetric order): faces and edges numbered in first-appearance
+// order, neighbour per face (1-based, 0 on the boundary).  Returns non-zero
+// with a message for an invalid mesh.
+struct MeshConn {
+  std::vector<int> fn, face_gid, edge_gid;
+  int nfaces = 0, nedges = 0, max_vid = 0;
+};
+int mesh_connectivity(long nelv, const int *ids, MeshConn &c, std::string &err);
+// Gather-scatter maps of the mesh at polynomial size lx (reference layout).
+int mesh_gs_maps(long nelv, const int *ids, const MeshConn &c, int lx, GsMaps &g);
+// Zero-Dirichlet mask of the mesh's faces without a neighbour.
+void mesh_boundary_mask(long nelv, int lx, const std::vector<int> &fn, std::vector<int> &msk);
+// Every face neighbour meets the element through the opposite face with the
+// same orientation (what the direct Schwarz ghost exchange needs).
+bool mesh_faces_aligned(long nelv, const int *ids, const std::vector<int> &fn);
+
 // Zero-Dirichlet mask (1-based, ascending) of all faces with facet_neigh == 0.
 void box_boundary_mask(const BoxSpec &b, int lx, const std::vector<int> &facet_neigh,
                        std::vector<int> &msk);

@@ -30,7 +30,13 @@ __global__ void addcol4_kernel(double *w, const double *h2, const double *B, con
 }  // namespace nb
 
 struct nb_problem {
-  nb::BoxSpec box{};
+  nb::BoxSpec box{};               // structured box (when !from_mesh)
+  bool from_mesh = false;          // built from a caller's unstructured mesh
+  bool dirichlet = false;          // faces without a neighbour are zero-Dirichlet
+  bool faces_aligned = false;      // every neighbour meets through the opposite face
+  std::vector<int> mesh_ids;       // 8 vertex ids per element (from_mesh)
+  std::vector<double> mesh_xyz8;   // 8 vertex coordinates per element (from_mesh)
+  std::vector<int> fn;             // neighbour per face, 1-based, 0 on the boundary
   int lx = 0, nelv = 0, nmask = 0;
   long n = 0;
   double deform_amp = 0.0, volume = 0.0;

@@ -71,7 +71,16 @@ struct FdmCfg {
   static constexpr int G = NL == 8 ? 2 : NL == 12 ? 3 : 4;
   static constexpr int C = (NL % 2 == 0 && NL != 16) ? 1 : 0;
   static constexpr int BUF = (NLP * (N2 - 1) + ((N2 - 1) >> G) * C + NL + 1) / 2 * 2;
-  static constexpr int STR0 = 2 * BUF + 3 * N2 + 3 * NL + 1;
+  // One element a block: the matrices are kept twice, each row l of the
+  // forward (S(l, .)) and backward (S(., l)) forms contiguous with a pitch of
+  // whole 16-byte vectors, so a lane reads a row with NL*sizeof(T)/16 vector
+  // loads instead of NL scalar ones.
+  static constexpr bool VEC = EPW == 1;
+  static constexpr int VW = 16 / (int)sizeof(T);            // values per vector
+  static constexpr int NLR = (NL + VW - 1) / VW * VW;        // row pitch
+  static constexpr int OFFM = (2 * BUF + VW - 1) / VW * VW;  // matrices, aligned
+  static constexpr int MAT = VEC ? 6 * NL * NLR : 3 * N2;
+  static constexpr int STR0 = VEC ? OFFM + MAT + 3 * NL + 1 : 2 * BUF + 3 * N2 + 3 * NL + 1;
   // per-element stride; with several elements in a warp it is 9 mod 16
   // values, which keeps the line reads of neighbouring elements in distinct banks
   static constexpr int STR = EPW > 1 ? STR0 + ((9 - STR0 % 16) + 16) % 16 : STR0;
@@ -148,11 +157,25 @@ __device__ __forceinline__ void fdm_pass(const T *__restrict__ src, T *__restric
         x[j] = x[j] * (d > ep ? T(1) / d : T(0));
       }
     }
+    if constexpr (C::VEC) {
+      // row l of the pass's matrix in 16-byte vector loads (broadcast)
+      T mr[C::NLR];
+      using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+      const V *row = reinterpret_cast<const V *>(Sd + C::NLR * l);
 #pragma unroll
-    for (int i = 0; i < NL; i++) {
-      const T mv = Sd[FWD ? l + NL * i : i + NL * l];
+      for (int q = 0; q < C::NLR / C::VW; q++) reinterpret_cast<V *>(mr)[q] = row[q];
 #pragma unroll
-      for (int j = 0; j < M; j++) o[j][i] += mv * x[j];
+      for (int i = 0; i < NL; i++) {
+#pragma unroll
+        for (int j = 0; j < M; j++) o[j][i] += mr[i] * x[j];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NL; i++) {
+        const T mv = Sd[FWD ? l + NL * i : i + NL * l];
+#pragma unroll
+        for (int j = 0; j < M; j++) o[j][i] += mv * x[j];
+      }
     }
   }
 #pragma unroll
@@ -181,8 +204,12 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
   extern __shared__ __align__(16) unsigned char fdm_smem[];
   const int es = threadIdx.x / C::LPE, ul = threadIdx.x - es * C::LPE;
   T *b0 = reinterpret_cast<T *>(fdm_smem) + es * C::STR, *b1 = b0 + C::BUF;
-  T *sS = b1 + C::BUF;  // S_x, S_y, S_z: S(l,i) at l + NL*i
-  T *sL = sS + 3 * N2;  // spectra + eps
+  // scalar form: S_x, S_y, S_z with S(l,i) at l + NL*i; vector form: the
+  // forward rows (S(l, i) at i + NLR*l) then the backward rows (S(i, l) at
+  // i + NLR*l), the factors staged in b1 first
+  T *sS = C::VEC ? b0 + C::OFFM : b1 + C::BUF;
+  T *sL = sS + C::MAT;  // spectra + eps
+  T *stage = C::VEC ? b1 : sS;
   const long e = (long)blockIdx.x * C::EPW + es;
   if ((long)blockIdx.x * C::EPW >= nelv) return;
   const bool active = e < nelv;
@@ -225,24 +252,37 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
       }
       b0[C::pos(b + NL * c, a)] = T(0);
     }
-    for (int q = u; q < 3 * N2; q += LPE) cp_async_elem<T>(sS + q, S + e * 3 * N2 + q, true);
+    for (int q = u; q < 3 * N2; q += LPE) cp_async_elem<T>(stage + q, S + e * 3 * N2 + q, true);
     for (int q = u; q < 3 * NL; q += LPE) cp_async_elem<T>(sL + q, lam + e * 3 * NL + q, true);
     if (u == 0) cp_async_elem<T>(sL + 3 * NL, eps + e, true);
   }
   cp_async_wait_all();
   __syncthreads();
+  // matrix of direction d for the forward / backward passes
+  constexpr int MS = C::VEC ? NL * C::NLR : N2;
+  T *fwd = sS, *bwd = C::VEC ? sS + 3 * MS : sS;
+  if constexpr (C::VEC) {
+    if (active)
+      for (int q = u; q < 3 * N2; q += LPE) {
+        const int d = q / N2, r = q - d * N2, a = r % NL, b = r / NL;
+        const T v = stage[q];  // S_d(a, b)
+        fwd[d * MS + b + C::NLR * a] = v;
+        bwd[d * MS + a + C::NLR * b] = v;
+      }
+    __syncthreads();
+  }
   // forward: b0 -> b1 -> b0 -> b1; backward (D^-1 on the first read): b1 -> b0 -> b1 -> out
-  fdm_pass<T, NL, true, false>(b0, b1, sS, sL, nullptr, u);
+  fdm_pass<T, NL, true, false>(b0, b1, fwd, sL, nullptr, u);
   __syncthreads();
-  fdm_pass<T, NL, true, false>(b1, b0, sS + N2, sL, nullptr, u);
+  fdm_pass<T, NL, true, false>(b1, b0, fwd + MS, sL, nullptr, u);
   __syncthreads();
-  fdm_pass<T, NL, true, false>(b0, b1, sS + 2 * N2, sL, nullptr, u);
+  fdm_pass<T, NL, true, false>(b0, b1, fwd + 2 * MS, sL, nullptr, u);
   __syncthreads();
-  fdm_pass<T, NL, false, true>(b1, b0, sS, sL, nullptr, u);
+  fdm_pass<T, NL, false, true>(b1, b0, bwd, sL, nullptr, u);
   __syncthreads();
-  fdm_pass<T, NL, false, false>(b0, b1, sS + N2, sL, nullptr, u);
+  fdm_pass<T, NL, false, false>(b0, b1, bwd + MS, sL, nullptr, u);
   __syncthreads();
-  fdm_pass<T, NL, false, false>(b1, nullptr, sS + 2 * N2, sL, out + e * N3, u);
+  fdm_pass<T, NL, false, false>(b1, nullptr, bwd + 2 * MS, sL, out + e * N3, u);
 }
 
 // e(i,j,k) = ext interior + neighbours' ghost results on the first interior
@@ -658,7 +698,7 @@ static nb_status build_schwarz_host(nb_problem *L, bool dirichlet, SchwarzHost &
       cudaMemcpy(y.data(), L->y, L->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
       cudaMemcpy(z.data(), L->z, L->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
     return hfail(NB_ERR_CUDA, "hsmg: coordinate copy failed");
-  box_facet_neigh(L->box, H.fn);
+  H.fn = L->fn;
   std::vector<int> ft;
   facet_types(H.fn, dirichlet, ft);
   FdmHost F;
@@ -793,6 +833,11 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   }
   const int lx = P->lx;
   if (lx < 3 || lx > 14) return hfail(NB_ERR_UNSUPPORTED, "hsmg supports lx 3..14");
+  if (!P->faces_aligned)
+    return hfail(NB_ERR_UNSUPPORTED,
+                 "hsmg needs every face neighbour to meet through the opposite face with the "
+                 "same orientation (the direct Schwarz ghost exchange); this mesh has rotated "
+                 "neighbours");
   const int lx_mid = lx < 5 ? std::max(lx - 1, 3) : 4, lx_crs = 2;
   HsmgState *H = mixed ? (HsmgState *)new HsmgImpl<float>() : (HsmgState *)new HsmgImpl<double>();
   H->fine = P;
@@ -800,11 +845,17 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   H->tol = tol;
   H->mixed = mixed;
   const bool dirichlet = P->nmask > 0;
-  nb_status st = nb_problem_create_box(P->box.nel, P->box.lo, P->box.hi, P->box.periodic,
-                                       lx_mid, P->deform_amp, dirichlet, &H->mid);
-  if (st == NB_OK)
-    st = nb_problem_create_box(P->box.nel, P->box.lo, P->box.hi, P->box.periodic, lx_crs,
-                               P->deform_amp, dirichlet, &H->crs);
+  // the coarser levels are the same mesh at lx_mid and lx_crs points a side
+  auto level = [&](int lxl, nb_problem **q) {
+    return P->from_mesh ? nb_problem_create_mesh(P->nelv, P->mesh_ids.data(),
+                                                 P->mesh_xyz8.data(), lxl, P->deform_amp,
+                                                 dirichlet, q)
+                        : nb_problem_create_box(P->box.nel, P->box.lo, P->box.hi,
+                                                P->box.periodic, lxl, P->deform_amp, dirichlet,
+                                                q);
+  };
+  nb_status st = level(lx_mid, &H->mid);
+  if (st == NB_OK) st = level(lx_crs, &H->crs);
   if (st != NB_OK) {
     delete H;
     return st;

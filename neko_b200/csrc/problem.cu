@@ -186,6 +186,9 @@ nb_problem::~nb_problem() {
   hsmg_free(this);
 }
 
+static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
+                                const std::vector<int> &msk, nb_problem **out);
+
 extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
                                            const double hi[3], const int periodic[3], int lx,
                                            double deform_amp, int dirichlet_boundary,
@@ -216,22 +219,66 @@ extern "C" nb_status nb_problem_create_box(const int nel[3], const double lo[3],
   P->nelv = (int)nelv;
   P->n = n;
   P->deform_amp = deform_amp;
-  if (const char *k = getenv("NB_AX_KERNEL")) P->use_stream_ax = strcmp(k, "classic") != 0;
+  // host setup: vertices, neighbours, maps, mask of the structured box
+  std::vector<double> xyz8;
+  box_vertices(b, xyz8);
+  box_facet_neigh(b, P->fn);
+  box_gs_maps(b, lx, P->fn, P->maps);
+  std::vector<int> msk;
+  P->dirichlet = dirichlet_boundary != 0;
+  if (dirichlet_boundary) box_boundary_mask(b, lx, P->fn, msk);
+  P->faces_aligned = true;
+  return finish_problem(P, xyz8, msk, out);
+}
 
-  // host setup: space, vertices, neighbours, maps, mask
+extern "C" nb_status nb_problem_create_mesh(int nelv, const int *vertex_ids,
+                                            const double *vertex_xyz, int lx, double deform_amp,
+                                            int dirichlet_boundary, nb_problem **out) {
+  if (!vertex_ids || !vertex_xyz || !out) return fail(NB_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (lx < 2 || lx > 16) return fail(NB_ERR_UNSUPPORTED, "lx must be in 2..16");
+  if (nelv < 1) return fail(NB_ERR_ARG, "nelv must be positive");
+  const long n = (long)nelv * lx * lx * lx;
+  if (n > 0x7fffffffL) return fail(NB_ERR_UNSUPPORTED, "more than 2^31-1 points");
+  nb_problem *P = new (std::nothrow) nb_problem();
+  if (!P) return fail(NB_ERR_OOM, "host allocation");
+  P->lx = lx;
+  P->nelv = nelv;
+  P->n = n;
+  P->deform_amp = deform_amp;
+  P->from_mesh = true;
+  P->dirichlet = dirichlet_boundary != 0;
+  P->mesh_ids.assign(vertex_ids, vertex_ids + (size_t)nelv * 8);
+  std::vector<double> xyz8(vertex_xyz, vertex_xyz + (size_t)nelv * 24);
+  P->mesh_xyz8 = xyz8;
+  MeshConn c;
+  std::string err;
+  if (mesh_connectivity(nelv, vertex_ids, c, err)) {
+    delete P;
+    return fail(NB_ERR_ARG, "mesh: " + err);
+  }
+  P->fn = c.fn;
+  mesh_gs_maps(nelv, vertex_ids, c, lx, P->maps);
+  std::vector<int> msk;
+  if (dirichlet_boundary) mesh_boundary_mask(nelv, lx, P->fn, msk);
+  P->faces_aligned = mesh_faces_aligned(nelv, vertex_ids, P->fn);
+  return finish_problem(P, xyz8, msk, out);
+}
+
+// The part of problem creation shared by the box and the unstructured mesh:
+// device arena, uploads, geometry, mult, Jacobi diagonal.
+static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
+                                const std::vector<int> &msk, nb_problem **out) {
+  const int lx = P->lx;
+  const long nelv = P->nelv, n = P->n;
+  if (const char *k = getenv("NB_AX_KERNEL")) P->use_stream_ax = strcmp(k, "classic") != 0;
   std::vector<double> zg, wx, D, Dt;
   gll_space(lx, zg, wx, D, Dt);
   std::vector<double> w3((size_t)lx * lx * lx);
   for (int k = 0; k < lx; k++)
     for (int j = 0; j < lx; j++)
       for (int i = 0; i < lx; i++) w3[i + lx * (j + lx * k)] = wx[i] * wx[j] * wx[k];
-  std::vector<double> xyz8;
-  box_vertices(b, xyz8);
-  std::vector<int> fn;
-  box_facet_neigh(b, fn);
-  box_gs_maps(b, lx, fn, P->maps);
-  std::vector<int> msk;
-  if (dirichlet_boundary) box_boundary_mask(b, lx, fn, msk);
+  const double deform_amp = P->deform_amp;
   P->nmask = (int)msk.size();
   if (!gs_pairs_regular(P->maps)) {
     delete P;

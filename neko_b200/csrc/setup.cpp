@@ -16,8 +16,11 @@
 // reference gives them the same global dof, so the ids -- and therefore the
 // maps -- coincide, while the lookup is a dense array instead of a hash.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <string>
+#include <unordered_map>
 #include <utility>
 
 #include "nb_internal.h"
@@ -187,10 +190,12 @@ inline long lin(int i, int j, int k, long e, int lx) {
 
 }  // namespace
 
-int box_gs_maps(const BoxSpec &b, int lx, const std::vector<int> &fn, GsMaps &g) {
-  const long nelv = (long)b.nel[0] * b.nel[1] * b.nel[2];
-  Lattice L(b, lx);
-  const long nkeys = L.G[0] * L.G[1] * L.G[2];
+// The gather-scatter maps of gs_init_mapping from a key per shared local
+// point: two local points share a key exactly when the reference gives them
+// the same global dof.  key(i, j, k, e) in [0, nkeys), 1-based (i,j,k).
+template <class KeyFn>
+static void gs_maps_from_keys(long nelv, int lx, const std::vector<int> &fn, long nkeys,
+                              KeyFn key, GsMaps &g) {
   std::vector<int> idmap(nkeys, 0);
   int max_id = 0;
   std::vector<int> &dg = g.dof_gs;
@@ -202,7 +207,7 @@ int box_gs_maps(const BoxSpec &b, int lx, const std::vector<int> &fn, GsMaps &g)
   dg.reserve(nv + ne + nf);
   gd.reserve(nv + ne + nf);
   auto push = [&](int i, int j, int k, long e) {
-    int &id = idmap[L.key(i, j, k, e)];
+    int &id = idmap[key(i, j, k, e)];
     if (id == 0) id = ++max_id;
     dg.push_back(id);
     gd.push_back((int)(lin(i, j, k, e, lx) + 1));
@@ -281,6 +286,13 @@ int box_gs_maps(const BoxSpec &b, int lx, const std::vector<int> &fn, GsMaps &g)
   }
   g.blk_off.assign(g.blk_len.size(), 0);
   for (size_t k = 1; k < g.blk_len.size(); k++) g.blk_off[k] = g.blk_off[k - 1] + g.blk_len[k - 1];
+}
+
+int box_gs_maps(const BoxSpec &b, int lx, const std::vector<int> &fn, GsMaps &g) {
+  const long nelv = (long)b.nel[0] * b.nel[1] * b.nel[2];
+  Lattice L(b, lx);
+  gs_maps_from_keys(nelv, lx, fn, L.G[0] * L.G[1] * L.G[2],
+                    [&](int i, int j, int k, long e) { return L.key(i, j, k, e); }, g);
   return 0;
 }
 
@@ -308,6 +320,220 @@ void box_boundary_mask(const BoxSpec &b, int lx, const std::vector<int> &fn,
           if (on) msk.push_back((int)(lin(i, j, k, e, lx) + 1));
         }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Unstructured hexahedral meshes given by the caller: eight global vertex
+// ids per element (periodic partners already sharing ids) in the reference's
+// symmetric vertex order.
+// ---------------------------------------------------------------------------
+
+// Vertices of each face and each edge of the reference hex
+// (face_nodes / edge_nodes, src/mesh/hex.f90:93-106, 113-127), 1-based.
+static const int kHexFaceNodes[6][4] = {{1, 5, 7, 3}, {2, 6, 8, 4}, {1, 2, 6, 5},
+                                        {3, 4, 8, 7}, {1, 2, 4, 3}, {5, 6, 8, 7}};
+static const int kHexEdgeNodes[12][2] = {{1, 2}, {3, 4}, {5, 6}, {7, 8}, {1, 3}, {2, 4},
+                                         {5, 7}, {6, 8}, {1, 5}, {2, 6}, {3, 7}, {4, 8}};
+
+namespace {
+struct ArrHash4 {
+  size_t operator()(const std::array<int, 4> &a) const {
+    size_t h = 1469598103934665603ull;
+    for (int v : a) h = (h ^ (size_t)(unsigned)v) * 1099511628211ull;
+    return h;
+  }
+};
+struct PairHash {
+  size_t operator()(const std::pair<int, int> &p) const {
+    return ((size_t)(unsigned)p.first << 32) ^ (size_t)(unsigned)p.second;
+  }
+};
+// vertex (1-based, symmetric order) at corner (i,j,k) of an lx^3 element
+inline int corner_vertex(int i, int j, int k, int lx) {
+  return 1 + (i == lx ? 1 : 0) + (j == lx ? 2 : 0) + (k == lx ? 4 : 0);
+}
+}  // namespace
+
+int mesh_connectivity(long nelv, const int *ids, MeshConn &c, std::string &err) {
+  c.fn.assign(nelv * 6, 0);
+  c.face_gid.assign(nelv * 6, 0);
+  c.edge_gid.assign(nelv * 12, 0);
+  c.max_vid = 0;
+  for (long q = 0; q < nelv * 8; q++) {
+    if (ids[q] <= 0) {
+      err = "vertex ids must be positive";
+      return 1;
+    }
+    c.max_vid = std::max(c.max_vid, ids[q]);
+  }
+  for (long e = 0; e < nelv; e++)
+    for (int a = 0; a < 8; a++)
+      for (int b = a + 1; b < 8; b++)
+        if (ids[e * 8 + a] == ids[e * 8 + b]) {
+          err = "element " + std::to_string(e + 1) + " repeats a vertex id";
+          return 1;
+        }
+  // faces and edges numbered in order of first appearance
+  // (mesh_generate_conn, src/mesh/mesh.f90:476-687); a face key is its four
+  // sorted vertex ids, an edge key its two.
+  std::unordered_map<std::array<int, 4>, std::array<long, 3>, ArrHash4> faces;  // id, e1, e2
+  std::unordered_map<std::pair<int, int>, int, PairHash> edges;
+  int nf = 0, ne = 0;
+  for (long e = 0; e < nelv; e++) {
+    for (int f = 0; f < 6; f++) {
+      std::array<int, 4> k;
+      for (int v = 0; v < 4; v++) k[v] = ids[e * 8 + kHexFaceNodes[f][v] - 1];
+      std::sort(k.begin(), k.end());
+      auto it = faces.find(k);
+      if (it == faces.end()) {
+        faces.emplace(k, std::array<long, 3>{nf, e + 1, 0});
+        c.face_gid[e * 6 + f] = nf++;
+      } else {
+        if (it->second[2] != 0 || it->second[1] == e + 1) {
+          err = "a face is shared by more than two element faces";
+          return 1;
+        }
+        it->second[2] = e + 1;
+        c.face_gid[e * 6 + f] = (int)it->second[0];
+      }
+    }
+    for (int q = 0; q < 12; q++) {
+      int a = ids[e * 8 + kHexEdgeNodes[q][0] - 1], b = ids[e * 8 + kHexEdgeNodes[q][1] - 1];
+      std::pair<int, int> k = a < b ? std::make_pair(a, b) : std::make_pair(b, a);
+      auto it = edges.find(k);
+      if (it == edges.end()) {
+        edges.emplace(k, ne);
+        c.edge_gid[e * 12 + q] = ne++;
+      } else {
+        c.edge_gid[e * 12 + q] = it->second;
+      }
+    }
+  }
+  c.nfaces = nf;
+  c.nedges = ne;
+  // neighbour across each face: the other element holding the same face
+  for (long e = 0; e < nelv; e++)
+    for (int f = 0; f < 6; f++) {
+      std::array<int, 4> k;
+      for (int v = 0; v < 4; v++) k[v] = ids[e * 8 + kHexFaceNodes[f][v] - 1];
+      std::sort(k.begin(), k.end());
+      const std::array<long, 3> &r = faces.at(k);
+      c.fn[e * 6 + f] = (int)(r[1] == e + 1 ? r[2] : r[1]);
+    }
+  return 0;
+}
+
+// Key of a shared local point: vertices by id, edge interiors by edge and
+// position from the lower-id end, face interiors by face and position in a
+// frame fixed by the face's vertex ids (origin at the lowest id, first axis
+// towards its lower-id neighbour corner), the same position from either
+// element whatever the relative rotation or mirroring of the two faces.
+// Equal keys are exactly the local points the reference's dofmap numbering
+// (src/sem/dofmap.f90:264-771) gives one global dof.
+struct MeshKeys {
+  const int *ids;
+  const MeshConn *c;
+  int lx;
+  long off_e, off_f, nkeys;
+  MeshKeys(const int *ids_, const MeshConn &c_, int lx_) : ids(ids_), c(&c_), lx(lx_) {
+    const long m = lx - 2;
+    off_e = (long)c_.max_vid + 1;
+    off_f = off_e + (long)c_.nedges * m;
+    nkeys = off_f + (long)c_.nfaces * m * m;
+  }
+  int vid(long e, int v) const { return ids[e * 8 + v - 1]; }
+  long operator()(int i, int j, int k, long e) const {
+    const int L = lx;
+    const int loc[3] = {i, j, k};
+    int nb = 0;
+    for (int d = 0; d < 3; d++) nb += (loc[d] == 1 || loc[d] == L);
+    if (nb == 3) return vid(e, corner_vertex(i, j, k, L));
+    if (nb == 2) {
+      int d = 0;
+      while (loc[d] == 1 || loc[d] == L) d++;  // the free direction
+      int a[3] = {i, j, k}, b[3] = {i, j, k};
+      a[d] = 1;
+      b[d] = L;
+      const int va = corner_vertex(a[0], a[1], a[2], L), vb = corner_vertex(b[0], b[1], b[2], L);
+      int q = 0;
+      while (!((kHexEdgeNodes[q][0] == va && kHexEdgeNodes[q][1] == vb) ||
+               (kHexEdgeNodes[q][0] == vb && kHexEdgeNodes[q][1] == va)))
+        q++;
+      const int t = loc[d];
+      const long p = vid(e, va) < vid(e, vb) ? t - 2 : L - 1 - t;
+      return off_e + (long)c->edge_gid[e * 12 + q] * (L - 2) + p;
+    }
+    // face interior: fixed direction d, free directions u < v
+    int d = 0;
+    while (!(loc[d] == 1 || loc[d] == L)) d++;
+    const int side = 2 * d + (loc[d] == L ? 1 : 0);
+    const int u = d == 0 ? 1 : 0, v = d == 2 ? 1 : 2;
+    auto cv = [&](int cu, int cvv) {
+      int p[3] = {i, j, k};
+      p[u] = cu;
+      p[v] = cvv;
+      return vid(e, corner_vertex(p[0], p[1], p[2], L));
+    };
+    // corners (u, v) in {1, L}^2 and the one with the lowest id
+    const int cu[4] = {1, L, 1, L}, cw[4] = {1, 1, L, L};
+    int o = 0;
+    for (int q = 1; q < 4; q++)
+      if (cv(cu[q], cw[q]) < cv(cu[o], cw[o])) o = q;
+    const int ou = cu[o], ow = cw[o];
+    const int nu = cv(ou == 1 ? L : 1, ow), nw = cv(ou, ow == 1 ? L : 1);
+    const long du = ou == 1 ? loc[u] - 2 : L - 1 - loc[u];
+    const long dw = ow == 1 ? loc[v] - 2 : L - 1 - loc[v];
+    const long m = L - 2;
+    const long pq = nu < nw ? du * m + dw : dw * m + du;
+    return off_f + (long)c->face_gid[e * 6 + side] * m * m + pq;
+  }
+};
+
+int mesh_gs_maps(long nelv, const int *ids, const MeshConn &c, int lx, GsMaps &g) {
+  MeshKeys K(ids, c, lx);
+  gs_maps_from_keys(nelv, lx, c.fn, K.nkeys, K, g);
+  return 0;
+}
+
+// Local points on faces without a neighbour, ascending (1-based).
+void mesh_boundary_mask(long nelv, int lx, const std::vector<int> &fn, std::vector<int> &msk) {
+  const long L3 = (long)lx * lx * lx;
+  std::vector<unsigned char> mark(nelv * L3, 0);
+  for (long e = 0; e < nelv; e++)
+    for (int side = 0; side < 6; side++) {
+      if (fn[e * 6 + side]) continue;
+      const int d = side >> 1, fix = (side & 1) ? lx : 1;
+      for (int a = 1; a <= lx; a++)
+        for (int b = 1; b <= lx; b++) {
+          int p[3];
+          p[d] = fix;
+          p[d == 0 ? 1 : 0] = a;
+          p[d == 2 ? 1 : 2] = b;
+          mark[lin(p[0], p[1], p[2], e, lx)] = 1;
+        }
+    }
+  msk.clear();
+  for (long q = 0; q < nelv * L3; q++)
+    if (mark[q]) msk.push_back((int)(q + 1));
+}
+
+// True when every neighbour across face f is reached through its opposite
+// face f^1 with the same vertex ids at the same face positions, so the
+// element's and its neighbour's face parametrisations coincide (a
+// structured-type mesh without rotated elements).
+bool mesh_faces_aligned(long nelv, const int *ids, const std::vector<int> &fn) {
+  for (long e = 0; e < nelv; e++)
+    for (int f = 0; f < 6; f++) {
+      const int nb = fn[e * 6 + f];
+      if (!nb) continue;
+      const long n = nb - 1;
+      const int g = f ^ 1;
+      if (fn[n * 6 + g] != e + 1) return false;
+      for (int v = 0; v < 4; v++)
+        if (ids[e * 8 + kHexFaceNodes[f][v] - 1] != ids[n * 8 + kHexFaceNodes[g][v] - 1])
+          return false;
+    }
+  return true;
 }
 
 }  // namespace nb

@@ -98,3 +98,57 @@ def uneven_rhs(P, rhs_seed, kmax=3):
     P.gs.op(f)
     P.bclst.apply(f)
     return f
+
+
+# --- unstructured hexahedral meshes -------------------------------------------
+def cube_rotations():
+    """The 24 proper rotations of the reference cube as (axis permutation,
+    flips): local corner c' of the rotated element is corner
+    (c'[perm[d]] ^ flips[d])_d of the original."""
+    import itertools
+    out = []
+    for perm in itertools.permutations(range(3)):
+        inv = sum(1 for a in range(3) for b in range(a + 1, 3) if perm[a] > perm[b])
+        for flips in itertools.product((0, 1), repeat=3):
+            if (inv + sum(flips)) % 2 == 0:
+                out.append((perm, flips))
+    return out
+
+
+def box_mesh(nel, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), periodic=(False, False, False),
+             rotate_seed=None):
+    """An nel[0] x nel[1] x nel[2] box as an unstructured mesh: vertex ids
+    (nelv, 8) and coordinates (nelv, 8, 3) in symmetric vertex order, x
+    fastest; in periodic directions the last grid plane takes the ids of the
+    first.  With rotate_seed each element's local frame is turned by a
+    random proper rotation of the cube (same hexahedron, rotated numbering),
+    so neighbouring elements meet with arbitrary relative orientation."""
+    nx, ny, nz = nel
+    G = [n + (0 if p else 1) for n, p in zip(nel, periodic)]
+    h = [(hi[d] - lo[d]) / nel[d] for d in range(3)]
+    rots = cube_rotations()
+    rng = np.random.default_rng(rotate_seed) if rotate_seed is not None else None
+    ids, xyz = [], []
+    for ez in range(nz):
+        for ey in range(ny):
+            for ex in range(nx):
+                base = (ex, ey, ez)
+                vid, vx = [], []
+                for v in range(8):
+                    c = (v & 1, (v >> 1) & 1, v >> 2)
+                    g = [base[d] + c[d] for d in range(3)]
+                    w = [g[d] % G[d] if periodic[d] else g[d] for d in range(3)]
+                    vid.append(1 + w[0] + G[0] * (w[1] + G[1] * w[2]))
+                    vx.append([lo[d] + h[d] * g[d] for d in range(3)])
+                if rng is not None:
+                    perm, flips = rots[rng.integers(len(rots))]
+                    order = []
+                    for v in range(8):
+                        c = (v & 1, (v >> 1) & 1, v >> 2)
+                        o = [c[perm[d]] ^ flips[d] for d in range(3)]
+                        order.append(o[0] + 2 * o[1] + 4 * o[2])
+                    vid = [vid[q] for q in order]
+                    vx = [vx[q] for q in order]
+                ids.append(vid)
+                xyz.append(vx)
+    return np.array(ids, dtype=np.int32), np.array(xyz, dtype=np.float64)

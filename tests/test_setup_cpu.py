@@ -63,3 +63,79 @@ def test_periodic_needs_three(nblib):
     st = nblib.nb_box_gs_maps(ne, pe, 4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
                               None, None, None, None)
     assert st == 2 and b"at least 3" in nblib.nb_last_error() or b">= 3" in nblib.nb_last_error()
+
+
+# --- unstructured meshes (nb_mesh_gs_maps) ------------------------------------
+def nb_mesh_maps(nblib, ids, lx):
+    IP = ctypes.POINTER(ctypes.c_int)
+    ids = np.ascontiguousarray(ids, dtype=np.int32)
+    nelv = ids.shape[0]
+    nl, fo, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    args = (nelv, ids.ctypes.data_as(IP), lx, ctypes.byref(nl), ctypes.byref(fo),
+            ctypes.byref(nb))
+    assert nblib.nb_mesh_gs_maps(*args, None, None, None, None, None) == 0, \
+        nblib.nb_last_error()
+    fn = np.zeros(nelv * 6, np.int32)
+    dg, gd = np.zeros(nl.value, np.int32), np.zeros(nl.value, np.int32)
+    bl, bo = np.zeros(nb.value, np.int32), np.zeros(nb.value, np.int32)
+    assert nblib.nb_mesh_gs_maps(*args, *(a.ctypes.data_as(IP) for a in (fn, dg, gd, bl, bo))) == 0
+    return fo.value, fn, dg, gd, bl, bo
+
+
+MESH_CASES = [((3, 2, 4), 5, 1, (False,) * 3), ((4, 4, 4), 6, 2, (False,) * 3),
+              ((2, 3, 3), 8, 3, (False,) * 3), ((3, 3, 3), 4, None, (False,) * 3),
+              ((3, 4, 3), 6, 5, (True, False, True)), ((3, 3, 3), 7, 6, (True,) * 3)]
+
+
+@pytest.mark.parametrize("nel,lx,seed,periodic", MESH_CASES)
+def test_mesh_gs_maps_bit_exact(nblib, oracle, nel, lx, seed, periodic):
+    """Maps of a box meshed as unstructured elements, with every element's
+    local frame turned by a random cube rotation (neighbours meet with any
+    relative orientation), against the oracle's dofmap + gs_init_mapping."""
+    from neko_b200 import workloads
+    ids, xyz = workloads.box_mesh(nel, periodic=periodic, rotate_seed=seed)
+    P = oracle.OracleProblem.from_elements(ids, xyz, lx)
+    fo, fn, dg, gd, bl, bo = nb_mesh_maps(nblib, ids, lx)
+    assert fo == P.local_facet_offset
+    np.testing.assert_array_equal(dg, P.i32("dof_gs"))
+    np.testing.assert_array_equal(gd, P.i32("gs_dof"))
+    np.testing.assert_array_equal(bl, P.i32("blk_len"))
+    np.testing.assert_array_equal(bo, P.i32("blk_off"))
+
+
+@pytest.mark.parametrize("nel,periodic,lx", CASES[:7])
+def test_unrotated_mesh_maps_equal_box_maps(nblib, nel, periodic, lx):
+    from neko_b200 import workloads
+    ids, _ = workloads.box_mesh(nel, periodic=[bool(p) for p in periodic])
+    fo, fn, dg, gd, bl, bo = nb_mesh_maps(nblib, ids, lx)
+    fo2, dg2, gd2, bl2, bo2 = nb_maps(nblib, nel, periodic, lx)
+    assert fo == fo2
+    for a, b in ((dg, dg2), (gd, gd2), (bl, bl2), (bo, bo2)):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_mesh_maps_on_reference_face_fixtures(nblib, oracle):
+    """The reference's seven two-element face-orientation meshes."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "gs_face_fixtures.json")) as f:
+        fixtures = json.load(f)
+    for t in fixtures:
+        pts = t["points"]
+        ids = np.array([[pts[str(r)]["id"] for r in el] for el in t["elements"]], np.int32)
+        xyz = np.array([[pts[str(r)]["xyz"] for r in el] for el in t["elements"]])
+        P = oracle.OracleProblem.from_elements(ids, xyz, t["lx"])
+        fo, fn, dg, gd, bl, bo = nb_mesh_maps(nblib, ids, t["lx"])
+        assert fo == P.local_facet_offset, t["name"]
+        np.testing.assert_array_equal(dg, P.i32("dof_gs"))
+        np.testing.assert_array_equal(gd, P.i32("gs_dof"))
+        assert list(fn) == [0] * 6 + [0] * 6 or fn.max() == 2
+
+
+def test_mesh_rejects_bad_input(nblib):
+    IP = ctypes.POINTER(ctypes.c_int)
+    ids = np.array([[1, 2, 3, 4, 5, 6, 7, 7]], np.int32)  # repeated vertex
+    a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = nblib.nb_mesh_gs_maps(1, ids.ctypes.data_as(IP), 4, ctypes.byref(a), ctypes.byref(b),
+                               ctypes.byref(c), None, None, None, None, None)
+    assert st == 1 and b"repeats a vertex" in nblib.nb_last_error()
