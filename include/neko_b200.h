@@ -205,6 +205,21 @@ nb_status nb_box_gs_maps(const int nel[3], const int periodic[3], int lx,
                          int *nlocal, int *facet_offset, int *nblocks,
                          int *dof_gs, int *gs_dof, int *blk_len, int *blk_off);
 
+/* Reads a 3-D Neko mesh file (.nmsh; nmsh_file_read,
+ * src/io/nmsh_file.f90:70-207) into the arrays nb_problem_create_mesh
+ * takes: vertex ids with the periodic zones applied (the ids of periodic
+ * faces replaced by their partners', mesh_apply_periodic_facet) and
+ * coordinates, both in symmetric vertex order.  Call once with NULL arrays
+ * to get nelv.  *nperiodic / *nlabeled (may be NULL) receive the number of
+ * periodic and labeled-boundary zones.  Host only. */
+nb_status nb_mesh_read_nmsh(const char *path, int *nelv, int *vertex_ids, double *vertex_xyz,
+                            int *nperiodic, int *nlabeled);
+/* Writes such a mesh as a .nmsh file (element ids 1..nelv, no zones, no
+ * curved edges; periodic identification stays in the vertex ids).  Host
+ * only. */
+nb_status nb_mesh_write_nmsh(const char *path, int nelv, const int *vertex_ids,
+                             const double *vertex_xyz);
+
 /* Gather-scatter maps (and the neighbour per face, 6 per element, 1-based,
  * 0 on the boundary) of the unstructured mesh that nb_problem_create_mesh
  * takes, in the reference layout of gs_init_mapping.  Host only; call once

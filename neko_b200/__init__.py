@@ -28,7 +28,8 @@ from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpt
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
 __all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "KspMonitor",
-           "Jacobi", "Hsmg", "Batch", "Projection", "ortho", "GS_OP_ADD", "NekoB200Error",
+           "Jacobi", "Hsmg", "Batch", "Projection", "ortho", "read_nmsh", "write_nmsh",
+           "GS_OP_ADD", "NekoB200Error",
            "load", "version"]
 
 
@@ -343,6 +344,32 @@ class Projection:
             self.close()
         except Exception:
             pass
+
+
+def read_nmsh(path):
+    """Reads a 3-D .nmsh mesh (nb_mesh_read_nmsh): (vertex ids (nelv, 8),
+    coordinates (nelv, 8, 3)) with the periodic zones applied, ready for
+    Problem.from_mesh."""
+    import numpy as np
+    L = load()
+    ne = ctypes.c_int()
+    check(L.nb_mesh_read_nmsh(str(path).encode(), ctypes.byref(ne), None, None, None, None))
+    ids = np.zeros((ne.value, 8), np.int32)
+    xyz = np.zeros((ne.value, 8, 3))
+    check(L.nb_mesh_read_nmsh(str(path).encode(), ctypes.byref(ne),
+                              ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                              xyz.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None, None))
+    return ids, xyz
+
+
+def write_nmsh(path, vertex_ids, vertex_xyz):
+    """Writes a mesh as a .nmsh file (nb_mesh_write_nmsh)."""
+    import numpy as np
+    ids = np.ascontiguousarray(vertex_ids, dtype=np.int32)
+    xyz = np.ascontiguousarray(vertex_xyz, dtype=np.float64)
+    check(load().nb_mesh_write_nmsh(str(path).encode(), ids.shape[0],
+                                    ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    xyz.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
 
 
 def ortho(x, coef, stream=None):

@@ -1212,6 +1212,41 @@ OrProblem *or_box_create(int nelx, int nely, int nelz, double x0, double x1,
   return build_common(P, lx);
 }
 
+// genmeshbox followed by nmsh_file_write into `path` in the file layout of
+// nmsh_file_write (src/io/nmsh_file.f90:650-760, packed MPI-IO records of
+// src/comm/mpi_types.f90:120-200): header, element records (el_idx, 8 x
+// (v_idx, xyz) in cyclic order), zone records, zero curves.  Returns 0.
+int or_genmeshbox_nmsh(const char *path, int nelx, int nely, int nelz, double x0, double x1,
+                       double y0, double y1, double z0, double z1, int px, int py, int pz) {
+  std::vector<ElemRecord> elems;
+  std::vector<ZoneRecord> zones;
+  genmeshbox(x0, x1, y0, y1, z0, z1, nelx, nely, nelz, px, py, pz, elems, zones);
+  FILE *f = fopen(path, "wb");
+  if (!f) return 1;
+  int32_t hdr[2] = {(int32_t)elems.size(), 3};
+  fwrite(hdr, 4, 2, f);
+  for (auto &r : elems) {
+    int32_t id = r.el_idx;
+    fwrite(&id, 4, 1, f);
+    for (int j = 0; j < 8; j++) {
+      int32_t v = r.v[j].id;
+      fwrite(&v, 4, 1, f);
+      fwrite(r.v[j].x, 8, 3, f);
+    }
+  }
+  int32_t nz = (int32_t)zones.size();
+  fwrite(&nz, 4, 1, f);
+  for (auto &z : zones) {
+    int32_t rec[9] = {z.e, z.f, z.p_e, z.p_f, z.glb_pt_ids[0], z.glb_pt_ids[1],
+                      z.glb_pt_ids[2], z.glb_pt_ids[3], z.type};
+    fwrite(rec, 4, 9, f);
+  }
+  int32_t nc = 0;
+  fwrite(&nc, 4, 1, f);
+  fclose(f);
+  return 0;
+}
+
 // Two-element style meshes of the gs unit tests: point ids and coordinates
 // given per element in symmetric vertex order, then mesh_generate_conn.
 OrProblem *or_elements_create(int nelv, const int *ids, const double *xyz, int lx) {

@@ -85,6 +85,8 @@ def lib():
             "or_gmres_jacobi": (ctypes.c_int, [_P, _D, _D, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, _D, _D]),
             "or_projection_create": (_P, [_P, ctypes.c_int]),
+            "or_genmeshbox_nmsh": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int] * 3 +
+                                   [ctypes.c_double] * 6 + [ctypes.c_int] * 3),
             "or_projection_destroy": (None, [_P]),
             "or_projection_project_on": (None, [_P, _D]),
             "or_projection_project_back": (None, [_P, _D]),
@@ -342,6 +344,16 @@ class OracleHsmg:
             self.close()
         except Exception:
             pass
+
+
+def genmeshbox_nmsh(path, nel, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+                    periodic=(False, False, False)):
+    """Writes the genmeshbox mesh of the box as an .nmsh file (the
+    reference's file layout, periodic zones included)."""
+    rc = lib().or_genmeshbox_nmsh(str(path).encode(), nel[0], nel[1], nel[2], lo[0], hi[0],
+                                  lo[1], hi[1], lo[2], hi[2], int(periodic[0]),
+                                  int(periodic[1]), int(periodic[2]))
+    assert rc == 0
 
 
 def fd_weights_full(xi, x, m):

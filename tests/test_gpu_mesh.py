@@ -114,3 +114,30 @@ def test_unrotated_mesh_solves_like_box(nb, nel, lx, periodic):
     if all(periodic):
         a, b = a - a.mean(), b - b.mean()
     assert np.abs(a - b).max() / np.abs(b).max() < 1e-10
+
+
+def test_problem_from_nmsh_file(nb, oracle, tmp_path):
+    """An .nmsh file in the reference's layout (genmeshbox with periodic
+    zones) read by the product and solved with hsmg-FCG: the same iteration
+    count and solution (1e-7) as the oracle's box problem."""
+    from neko_b200 import workloads
+    nel, lx, hi = (4, 4, 3), 6, (2 * np.pi,) * 3
+    path = tmp_path / "box.nmsh"
+    oracle.genmeshbox_nmsh(path, nel, hi=hi, periodic=(True, True, True))
+    ids, xyz = nb.read_nmsh(path)
+    P = nb.Problem.from_mesh(ids, xyz, lx, deform=0.05, dirichlet=False)
+    O = oracle.OracleProblem.box(nel, lx, hi=hi, periodic=(True,) * 3)
+    O.deform_sine(0.05)
+    O.coef()
+    x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
+    b = O.gs_add(workloads.config2_rhs_local(x, y, z, B, 4))
+    r0 = np.sqrt(np.sum(b * O.f64("mult") * b) / O.volume)
+    H = oracle.OracleHsmg(O)
+    xo, it_o, _, _ = H.cg(b, 200, 1e-8 * r0, flexible=True)
+    xd = P.zeros()
+    mon = nb.FCG(max_iter=200, abs_tol=1e-8 * r0, M=nb.Hsmg()).solve(nb.AxHelm(), xd, _cuda(b),
+                                                                     P.n, P)
+    assert mon.converged and abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    a = _np(xd)
+    a, r = a - a.mean(), xo - xo.mean()
+    assert np.abs(a - r).max() / np.abs(r).max() < 1e-7

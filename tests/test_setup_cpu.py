@@ -139,3 +139,55 @@ def test_mesh_rejects_bad_input(nblib):
     st = nblib.nb_mesh_gs_maps(1, ids.ctypes.data_as(IP), 4, ctypes.byref(a), ctypes.byref(b),
                                ctypes.byref(c), None, None, None, None, None)
     assert st == 1 and b"repeats a vertex" in nblib.nb_last_error()
+
+
+def _read_nmsh(nblib, path):
+    IP, DP = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    ne = ctypes.c_int()
+    assert nblib.nb_mesh_read_nmsh(str(path).encode(), ctypes.byref(ne), None, None, None,
+                                   None) == 0, nblib.nb_last_error()
+    ids = np.zeros((ne.value, 8), np.int32)
+    xyz = np.zeros((ne.value, 8, 3))
+    npz, nlz = ctypes.c_int(), ctypes.c_int()
+    assert nblib.nb_mesh_read_nmsh(str(path).encode(), ctypes.byref(ne), ids.ctypes.data_as(IP),
+                                   xyz.ctypes.data_as(DP), ctypes.byref(npz),
+                                   ctypes.byref(nlz)) == 0
+    return ids, xyz, npz.value
+
+
+@pytest.mark.parametrize("nel,periodic,lx", [((3, 2, 4), (0, 0, 0), 5), ((4, 3, 5), (1, 0, 1), 6),
+                                             ((3, 3, 3), (1, 1, 1), 4)])
+def test_nmsh_read_of_genmeshbox_file(nblib, oracle, tmp_path, nel, periodic, lx):
+    """A genmeshbox mesh written in the reference's nmsh layout (periodic
+    zones included) and read by the product: the gs maps equal the oracle's
+    box maps (the oracle builds them from the same records)."""
+    path = tmp_path / "box.nmsh"
+    oracle.genmeshbox_nmsh(path, nel, hi=(2.0, 3.0, 1.5), periodic=[bool(p) for p in periodic])
+    ids, xyz, npz = _read_nmsh(nblib, path)
+    assert npz == 2 * sum(int(p) * nel[(d + 1) % 3] * nel[(d + 2) % 3] for d, p in
+                          enumerate(periodic))
+    P = oracle.OracleProblem.box(nel, lx, hi=(2.0, 3.0, 1.5), periodic=[bool(p) for p in periodic])
+    fo, fn, dg, gd, bl, bo = nb_mesh_maps(nblib, ids, lx)
+    assert fo == P.local_facet_offset
+    np.testing.assert_array_equal(dg, P.i32("dof_gs"))
+    np.testing.assert_array_equal(gd, P.i32("gs_dof"))
+    np.testing.assert_array_equal(bl, P.i32("blk_len"))
+    np.testing.assert_array_equal(bo, P.i32("blk_off"))
+    # element coordinates: the box's grid (x fastest)
+    h = np.array([2.0, 3.0, 1.5]) / np.array(nel)
+    e = nel[0] * nel[1] * nel[2] - 1
+    assert np.allclose(xyz[e, 7], [nel[0] * h[0], nel[1] * h[1], nel[2] * h[2]])
+
+
+def test_nmsh_write_read_roundtrip(nblib, tmp_path):
+    from neko_b200 import workloads
+    IP, DP = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    ids, xyz = workloads.box_mesh((3, 2, 2), periodic=(True, False, False), rotate_seed=9)
+    path = tmp_path / "m.nmsh"
+    assert nblib.nb_mesh_write_nmsh(str(path).encode(), ids.shape[0], ids.ctypes.data_as(IP),
+                                    xyz.ctypes.data_as(DP)) == 0
+    assert path.stat().st_size == 8 + ids.shape[0] * 228 + 8
+    ids2, xyz2, npz = _read_nmsh(nblib, path)
+    assert npz == 0
+    np.testing.assert_array_equal(ids2, ids)
+    np.testing.assert_array_equal(xyz2, xyz)
