@@ -282,6 +282,14 @@ nb_status nb_problem_volume(const nb_problem *p, double *vol);
 nb_status nb_problem_set_coefficients(nb_problem *p, const double *h1,
                                       const double *h2, int ifh2);
 
+/* Constant coefficients h1 > 0 and h2 >= 0 (h2 = 0 turns the h2 B u term
+ * off), set asynchronously on `stream`: the h1/h2 fields, the Jacobi
+ * diagonal and the coarse levels of the problem's hsmg preconditioners are
+ * rewritten by kernels on that stream, with no device synchronisation (the
+ * form a serving loop uses between the solves of one problem instance).
+ * The same coefficients as nb_problem_set_coefficients with filled arrays. */
+nb_status nb_problem_set_coefficients_const(nb_problem *p, double h1, double h2, void *stream);
+
 /* w = A u (ax_helm incl. h2 term when enabled), element-local.
  * Asynchronous on `stream`; a bounded device wait that expires is recorded
  * in the problem's error word and reported by the next nb_problem_sync or
@@ -429,6 +437,18 @@ nb_status nb_batch_submit(nb_batch *b, nb_problem *p, const double *f, double *x
  * coefficients. */
 nb_status nb_batch_submit_coef(nb_batch *b, nb_problem *p, const double *f, double *x,
                                double abs_tol, int max_iter, double h1, double h2, int *slot);
+/* Adds a solve of problem instance p run as its own Krylov solve inside the
+ * batch's run loop, concurrently with the other slots on a pool of streams:
+ * opts chooses CG or flexible CG, Jacobi or hsmg, FP64 or mixed precision
+ * (opts->ksp must be NB_KSP_CG).  The constant coefficients h1 > 0, h2 >= 0
+ * are set on p when the slot starts (nb_problem_set_coefficients_const).  p
+ * belongs to the slot until it is released: give concurrent slots of one
+ * mesh distinct problem instances.  The slot's Krylov vectors (4 n doubles)
+ * are charged against the budget; its result is bit-identical to nb_solve
+ * of the same problem with the same options.  Slot ids of these solves
+ * start at 2^24. */
+nb_status nb_batch_submit_solve(nb_batch *b, nb_problem *p, const double *f, double *x,
+                                const nb_solve_opts *opts, double h1, double h2, int *slot);
 /* Frees a slot (finished or not) and its budget. */
 nb_status nb_batch_release(nb_batch *b, int slot);
 /* Runs up to max_chunks graph replays (<= 0: until every solve finished);

@@ -143,6 +143,12 @@ class Problem:
                                                  _ptr(h2c) if h2c is not None else None,
                                                  int(h2 is not None)))
 
+    def set_coefficients_const(self, h1, h2=0.0, stream=None):
+        """Constant h1 > 0, h2 >= 0 set asynchronously on `stream` (h2 = 0:
+        no h2 term) -- nb_problem_set_coefficients_const."""
+        check(load().nb_problem_set_coefficients_const(self.handle, float(h1), float(h2),
+                                                       _stream_handle(stream)))
+
     def zeros(self):
         return torch.zeros(self.n, dtype=torch.float64, device="cuda")
 
@@ -400,6 +406,26 @@ class Batch:
             check(load().nb_batch_submit_coef(self._h, problem.handle, _ptr(f), _ptr(x),
                                               float(abs_tol), int(max_iter), float(h1),
                                               float(h2), ctypes.byref(slot)))
+        self._keep[slot.value] = (problem, f, x)
+        return slot.value
+
+    def submit_solve(self, problem, f, x, abs_tol, max_iter=1000, h1=1.0, h2=0.0, pc="hsmg",
+                     mixed=False, flexible=None, coarse_iter=10, coarse_tol=1e-9):
+        """Adds a per-problem Krylov solve of the problem instance (which the
+        slot owns until release) run concurrently with the other slots:
+        pc "hsmg" (flexible CG, FP64 or mixed) or "jacobi" (CG), constant
+        coefficients h1, h2 (nb_batch_submit_solve)."""
+        o = SolveOpts()
+        o.max_iter, o.abs_tol = int(max_iter), float(abs_tol)
+        o.pc = {"hsmg": NB_PC_HSMG, "jacobi": NB_PC_JACOBI, "none": NB_PC_NONE}[pc]
+        o.mixed = int(bool(mixed))
+        o.coarse_iter, o.coarse_tol = int(coarse_iter), float(coarse_tol)
+        o.flexible = int(pc == "hsmg" if flexible is None else flexible)
+        o.ksp, o.m_restart = _lib.NB_KSP_CG, 0
+        slot = ctypes.c_int()
+        check(load().nb_batch_submit_solve(self._h, problem.handle, _ptr(f), _ptr(x),
+                                           ctypes.byref(o), float(h1), float(h2),
+                                           ctypes.byref(slot)))
         self._keep[slot.value] = (problem, f, x)
         return slot.value
 

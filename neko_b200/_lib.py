@@ -97,6 +97,7 @@ SIGNATURES = {
     "nb_problem_field": (_I, [_P, ctypes.c_char_p, ctypes.POINTER(_P)]),
     "nb_problem_volume": (_I, [_P, _DP]),
     "nb_problem_set_coefficients": (_I, [_P, _P, _P, _I]),
+    "nb_problem_set_coefficients_const": (_I, [_P, ctypes.c_double, ctypes.c_double, _P]),
     "nb_ax": (_I, [_P, _P, _P, _P]),
     "nb_problem_sync": (_I, [_P, _P]),
     "nb_ax_vector": (_I, [_P] * 8),
@@ -120,6 +121,8 @@ SIGNATURES = {
     "nb_batch_submit": (_I, [_P, _P, _P, _P, ctypes.c_double, _I, _IP]),
     "nb_batch_submit_coef": (_I, [_P, _P, _P, _P, ctypes.c_double, _I, ctypes.c_double,
                                   ctypes.c_double, _IP]),
+    "nb_batch_submit_solve": (_I, [_P, _P, _P, _P, ctypes.POINTER(SolveOpts), ctypes.c_double,
+                                   ctypes.c_double, _IP]),
     "nb_batch_release": (_I, [_P, _I]),
     "nb_batch_run": (_I, [_P, _I, _IP, _P]),
     "nb_batch_result": (_I, [_P, _I, _IP, _P]),

@@ -37,6 +37,7 @@
 
 #include "nb_gs_dev.cuh"
 #include "nb_kernels.h"
+#include "nb_precond.h"
 #include "nb_problem.h"
 #include "nb_reduce.cuh"
 #include "nb_tma.cuh"
@@ -414,11 +415,37 @@ struct SlotHost {
   double h1c = 1.0, h2c = 0.0;
 };
 
+// A solve of its own problem instance run inside the batch's run loop: the
+// per-problem Krylov iteration (CG/flexible CG, Jacobi or hsmg, FP64 or
+// mixed) launched chunk by chunk on one of the batch's streams, concurrently
+// with the other slots.
+struct KspSlot {
+  bool used = false, started = false, finished = false;
+  nb_problem *P = nullptr;
+  const double *f = nullptr;
+  double *x = nullptr;
+  nb_solve_opts o{};
+  double h1 = 1.0, h2 = 0.0;
+  size_t bytes = 0;
+  CgRun run;
+  nb_solve_result res{};
+  nb_status status = NB_OK;
+};
+
+// Slot ids of the per-problem solves start here (the batched Jacobi slots
+// are numbered from 0).
+constexpr int kKspBase = 1 << 24;
+constexpr int kKspStreams = 8;
+
 }  // namespace
 
 struct nb_batch {
   size_t budget = 0, used = 0;
   std::vector<SlotHost> slots;
+  std::vector<KspSlot> kslots;
+  std::vector<cudaStream_t> kstreams;
+  int next_stream = 0;
+  cudaEvent_t ev_jacobi = nullptr;
   // device tables
   BSlot *d_slots = nullptr;
   AxItem *d_items = nullptr;
@@ -459,6 +486,9 @@ static nb_status bfail(nb_status s, const std::string &m) {
   } while (0)
 
 nb_batch::~nb_batch() {
+  cudaDeviceSynchronize();  // per-problem solves still running finish first
+  for (auto st : kstreams) cudaStreamDestroy(st);
+  if (ev_jacobi) cudaEventDestroy(ev_jacobi);
   if (graph) cudaGraphExecDestroy(graph);
   for (auto &s : slots)
     if (s.vec) cudaFree(s.vec);
@@ -854,7 +884,116 @@ extern "C" nb_status nb_batch_submit_coef(nb_batch *b, nb_problem *p, const doub
   return submit(b, p, f, x, abs_tol, max_iter, true, h1, h2, slot);
 }
 
+extern "C" nb_status nb_batch_submit_solve(nb_batch *b, nb_problem *p, const double *f,
+                                           double *x, const nb_solve_opts *opts, double h1,
+                                           double h2, int *slot) {
+  if (!b || !p || !f || !x || !opts || !slot) return bfail(NB_ERR_ARG, "null argument");
+  if (opts->max_iter < 1) return bfail(NB_ERR_ARG, "max_iter must be >= 1");
+  if (!(h1 > 0.0 && h2 >= 0.0)) return bfail(NB_ERR_ARG, "need h1 > 0, h2 >= 0");
+  if (opts->ksp != NB_KSP_CG) return bfail(NB_ERR_UNSUPPORTED, "batch solves use CG / flexible CG");
+  if (opts->pc != NB_PC_JACOBI && opts->pc != NB_PC_HSMG && opts->pc != NB_PC_NONE)
+    return bfail(NB_ERR_ARG, "unknown preconditioner");
+  for (auto &k : b->kslots)
+    if (k.used && k.P == p) return bfail(NB_ERR_ARG, "the problem is already in use by a slot");
+  // the instance's Krylov vectors (r, z, p, w)
+  const size_t bytes = 4 * (size_t)p->n * sizeof(double);
+  if (b->used + bytes > b->budget) return bfail(NB_ERR_OOM, "batch: over the HBM budget");
+  KspSlot k;
+  k.used = true;
+  k.P = p;
+  k.f = f;
+  k.x = x;
+  k.o = *opts;
+  k.h1 = h1;
+  k.h2 = h2;
+  k.bytes = bytes;
+  if (k.o.pc == NB_PC_HSMG) {  // build the preconditioner now (synchronous set-up)
+    Precond *pc = nullptr;
+    nb_status st = hsmg_get(p, k.o, &pc);
+    if (st != NB_OK) return st;
+  }
+  int q = -1;
+  for (size_t i = 0; i < b->kslots.size(); i++)
+    if (!b->kslots[i].used) {
+      q = (int)i;
+      break;
+    }
+  if (q < 0) {
+    q = (int)b->kslots.size();
+    b->kslots.push_back(k);
+  } else {
+    b->kslots[q] = k;
+  }
+  b->used += bytes;
+  *slot = kKspBase + q;
+  return NB_OK;
+}
+
+static KspSlot *ksp_slot(nb_batch *b, int slot) {
+  const int q = slot - kKspBase;
+  if (q < 0 || q >= (int)b->kslots.size() || !b->kslots[q].used) return nullptr;
+  return &b->kslots[q];
+}
+
+// Starts the slots not yet started and follows the running ones without
+// blocking; returns the number still running.
+static nb_status ksp_advance(nb_batch *b, int *left) {
+  *left = 0;
+  for (auto &k : b->kslots) {
+    if (!k.used || k.finished) continue;
+    if (!k.started) {
+      if ((int)b->kstreams.size() < kKspStreams) {
+        cudaStream_t st;
+        NB_BTRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        b->kstreams.push_back(st);
+      }
+      const cudaStream_t s = b->kstreams[b->next_stream++ % b->kstreams.size()];
+      NB_BTRY(set_coefficients_const(k.P, k.h1, k.h2, s));
+      Precond *pc = nullptr;
+      if (k.o.pc == NB_PC_HSMG) {
+        nb_status st = hsmg_get(k.P, k.o, &pc);
+        if (st != NB_OK) return st;
+      }
+      k.run = CgRun{};
+      k.run.P = k.P;
+      k.run.x = k.x;
+      k.run.f = k.f;
+      k.run.o = k.o;
+      k.run.pc = pc;
+      k.run.s = s;
+      k.started = true;
+      k.status = cg_start(k.run);
+      if (k.status != NB_OK) {
+        k.finished = true;
+        continue;
+      }
+    }
+    if (cg_poll(k.run, false, &k.res, &k.status))
+      k.finished = true;
+    else
+      (*left)++;
+  }
+  return NB_OK;
+}
+
+// Blocks until the first running per-problem solve has finished its chunk.
+static void ksp_wait_one(nb_batch *b) {
+  for (auto &k : b->kslots)
+    if (k.used && k.started && !k.finished) {
+      if (cg_poll(k.run, true, &k.res, &k.status)) k.finished = true;
+      return;
+    }
+}
+
 extern "C" nb_status nb_batch_release(nb_batch *b, int slot) {
+  if (b && slot >= kKspBase) {
+    KspSlot *k = ksp_slot(b, slot);
+    if (!k) return bfail(NB_ERR_ARG, "no such slot");
+    if (k->started && !k->finished) NB_BTRY(cudaStreamSynchronize(k->run.s));
+    b->used -= k->bytes;
+    *k = KspSlot{};
+    return NB_OK;
+  }
   if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
     return bfail(NB_ERR_ARG, "no such slot");
   SlotHost &h = b->slots[slot];
@@ -884,20 +1023,37 @@ extern "C" nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void
   cudaStream_t s = (cudaStream_t)stream;
   nb_status st = prepare(b, s);
   if (st != NB_OK) return st;
+  if (!b->ev_jacobi) NB_BTRY(cudaEventCreateWithFlags(&b->ev_jacobi, cudaEventDisableTiming));
   const int ns = (int)b->slots.size();
   std::vector<BSlot> &hs = b->mirror;
   hs.resize(ns);
   b->mirror_valid = false;
-  int left = 0;
+  int left = 0, jleft = 0;
+  for (int q = 0; q < ns; q++) jleft += b->slots[q].used ? 1 : 0;
   for (int c = 0; max_chunks <= 0 || c < max_chunks; c++) {
-    if (ns == 0) break;
-    NB_BTRY(cudaGraphLaunch(b->graph, s));
-    NB_BTRY(cudaMemcpyAsync(hs.data(), b->d_slots, ns * sizeof(BSlot), cudaMemcpyDeviceToHost, s));
-    NB_BTRY(cudaStreamSynchronize(s));
-    b->mirror_valid = true;
-    left = 0;
-    for (int q = 0; q < ns; q++)
-      if (b->slots[q].used && !hs[q].done) left++;
+    // one chunk of the batched Jacobi solves on s, the per-problem solves
+    // advanced on their streams meanwhile
+    const bool jac = ns > 0 && jleft > 0;
+    if (jac) {
+      NB_BTRY(cudaGraphLaunch(b->graph, s));
+      NB_BTRY(cudaMemcpyAsync(hs.data(), b->d_slots, ns * sizeof(BSlot), cudaMemcpyDeviceToHost, s));
+      NB_BTRY(cudaEventRecord(b->ev_jacobi, s));
+    }
+    int kleft = 0;
+    st = ksp_advance(b, &kleft);
+    if (st != NB_OK) return st;
+    if (jac) {
+      NB_BTRY(cudaEventSynchronize(b->ev_jacobi));
+      b->mirror_valid = true;
+      jleft = 0;
+      for (int q = 0; q < ns; q++)
+        if (b->slots[q].used && !hs[q].done) jleft++;
+    } else if (kleft) {
+      ksp_wait_one(b);
+      st = ksp_advance(b, &kleft);
+      if (st != NB_OK) return st;
+    }
+    left = (ns > 0 ? jleft : 0) + kleft;
     if (!left) break;
   }
   if (active) *active = left;
@@ -908,10 +1064,21 @@ extern "C" nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void
     cudaDeviceSynchronize();
     return bfail(NB_ERR_TIMEOUT, "batch: a bounded bulk-copy wait expired");
   }
+  for (auto &k : b->kslots)
+    if (k.used && k.finished && k.status == NB_ERR_TIMEOUT)
+      return bfail(NB_ERR_TIMEOUT, "batch: a bounded device wait of a solve expired");
   return NB_OK;
 }
 
 extern "C" nb_status nb_batch_result(nb_batch *b, int slot, int *done, nb_solve_result *res) {
+  if (b && slot >= kKspBase) {
+    KspSlot *k = ksp_slot(b, slot);
+    if (!k) return bfail(NB_ERR_ARG, "no such slot");
+    if (done) *done = k->finished ? 1 : 0;
+    if (res) *res = k->finished ? k->res : nb_solve_result{};
+    if (k->finished && k->status != NB_OK && k->status != NB_ERR_NAN) return k->status;
+    return NB_OK;
+  }
   if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
     return bfail(NB_ERR_ARG, "no such slot");
   if (!b->slots[slot].started) {  // submitted, not yet initialised

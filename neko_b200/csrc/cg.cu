@@ -254,6 +254,7 @@ static nb_status ws_fail(nb_status s, const std::string &m) {
 }
 
 CgWorkspace::~CgWorkspace() {
+  if (ev) cudaEventDestroy(ev);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (base) cudaFree(base);
   if (host_state) cudaFreeHost(host_state);
@@ -367,14 +368,22 @@ namespace nb {
 
 // Runs the whole solve on stream s.  Iterations are replayed from a graph
 // holding `chunk` iterations; the host reads the state once per chunk.
-nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
-                   Precond *pc, nb_solve_result *res, cudaStream_t s) {
+// Starts a solve on stream s: state, init kernel, the iteration graph
+// (captured again when the operands changed), the first chunk of
+// iterations, an asynchronous copy of the state to the host and an event
+// behind it.  cg_poll then follows the solve without blocking.
+nb_status cg_start(CgRun &R) {
+  nb_problem *P = R.P;
+  const nb_solve_opts &o = R.o;
   if (!P->solver_ws) P->solver_ws = new CgWorkspace();
   CgWorkspace &W = *(CgWorkspace *)P->solver_ws;
   cudaError_t e = W.ensure(P->n);
   if (e != cudaSuccess)
     return ws_fail(e == cudaErrorMemoryAllocation ? NB_ERR_OOM : NB_ERR_CUDA,
                    std::string("CG workspace: ") + cudaGetErrorString(e));
+  if (!W.ev) NB_CUDA_TRY(cudaEventCreateWithFlags(&W.ev, cudaEventDisableTiming));
+  Precond *pc = R.pc;
+  const cudaStream_t s = R.s;
   W.use_jacobi = o.pc == NB_PC_JACOBI;
   W.flexible = (o.flexible != 0 || o.mixed != 0) && pc != nullptr;
   W.recompute_every = o.mixed ? 50 : 0;
@@ -386,16 +395,16 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
   init.skip_rc = 1;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const long n = P->n;
-  cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(x, W.p, W.r, f, P->mult, P->multf, n, W.st,
-                                                        W.partials, W.counter, nullptr);
+  cg_init_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(R.x, W.p, W.r, R.f, P->mult, P->multf, n,
+                                                        W.st, W.partials, W.counter, nullptr);
   NB_CUDA_TRY(cudaGetLastError());
   // (Re)capture the iteration graph when the operands changed.
-  const void *key[5] = {x, f, pc,
+  const void *key[5] = {R.x, R.f, pc,
                         (const void *)(intptr_t)(W.use_jacobi | (W.flexible << 1) |
                                                  ((W.recompute_every > 0) << 2)),
                         (const void *)(intptr_t)P->ifh2};
   bool same = W.graph_exec && !memcmp(key, W.graph_key, sizeof(key));
-  const int chunk = n > (1 << 22) ? 4 : 16;
+  R.chunk = n > (1 << 22) ? 4 : 16;
   if (!same) {
     if (W.graph_exec) {
       cudaGraphExecDestroy(W.graph_exec);
@@ -406,7 +415,8 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     cudaGraph_t g;
     NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t ce = cudaSuccess;
-    for (int k = 0; k < chunk && ce == cudaSuccess; k++) ce = cg_iteration(P, W, pc, x, f, cs);
+    for (int k = 0; k < R.chunk && ce == cudaSuccess; k++)
+      ce = cg_iteration(P, W, pc, R.x, R.f, cs);
     W.launches_per_iter = (W.fused ? 4 : 6 + (P->ifh2 ? 1 : 0)) + (pc ? pc->launches() : 0) +
                           (W.recompute_every > 0 ? 3 + (P->ifh2 ? 1 : 0) : 0);
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
@@ -421,33 +431,80 @@ nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opt
     NB_CUDA_TRY(ee);
     memcpy(W.graph_key, key, sizeof(key));
   }
-  CgState *hs = (CgState *)W.host_state;
-  int launches = 1;
-  for (;;) {
-    NB_CUDA_TRY(cudaGraphLaunch(W.graph_exec, s));
-    launches += chunk * W.launches_per_iter;
-    NB_CUDA_TRY(cudaMemcpyAsync(hs, W.st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
-    NB_CUDA_TRY(cudaStreamSynchronize(s));
-    if (hs->done) break;
+  R.launches = 1;
+  R.active = true;
+  return cg_next_chunk(R);
+}
+
+// One more chunk of iterations, the state copy and the event behind them.
+nb_status cg_next_chunk(CgRun &R) {
+  CgWorkspace &W = *(CgWorkspace *)R.P->solver_ws;
+  NB_CUDA_TRY(cudaGraphLaunch(W.graph_exec, R.s));
+  R.launches += R.chunk * W.launches_per_iter;
+  NB_CUDA_TRY(cudaMemcpyAsync(W.host_state, W.st, sizeof(CgState), cudaMemcpyDeviceToHost, R.s));
+  NB_CUDA_TRY(cudaEventRecord(W.ev, R.s));
+  return NB_OK;
+}
+
+// Follows a started solve: 0 while it runs (the next chunk is launched once
+// the previous one has finished), 1 when it has finished, with *res and
+// *status set.  wait = true blocks until the current chunk has finished.
+int cg_poll(CgRun &R, bool wait, nb_solve_result *res, nb_status *status) {
+  nb_problem *P = R.P;
+  CgWorkspace &W = *(CgWorkspace *)P->solver_ws;
+  cudaError_t e = wait ? cudaEventSynchronize(W.ev) : cudaEventQuery(W.ev);
+  if (e == cudaErrorNotReady) return 0;
+  if (e != cudaSuccess) {
+    *status = ws_fail(NB_ERR_CUDA, std::string("solve: ") + cudaGetErrorString(e));
+    R.active = false;
+    return 1;
   }
+  const CgState *hs = (const CgState *)W.host_state;
+  if (!hs->done) {
+    *status = cg_next_chunk(R);
+    if (*status == NB_OK) return 0;
+    R.active = false;
+    return 1;
+  }
+  R.active = false;
   if (res) {
     res->iter = hs->iter;
     res->res_start = hs->res_start;
     res->res_final = hs->iter ? hs->rnorm : hs->res_start;
-    res->converged = !hs->nan && (hs->iter == 0 || hs->rnorm < o.abs_tol);
-    res->launches = launches;
+    res->converged = !hs->nan && (hs->iter == 0 || hs->rnorm < R.o.abs_tol);
+    res->launches = R.launches;
     // krylov_is_converged (src/krylov/krylov.f90:411-421) also fails a solve
     // that used the whole iteration budget.
-    if (hs->iter >= o.max_iter) res->converged = 0;
+    if (hs->iter >= R.o.max_iter) res->converged = 0;
   }
+  *status = NB_OK;
   // the problem's own error word: this solve's operator launches, or an
   // earlier asynchronous nb_ax on the same problem not yet reported
   if (P->take_error())
-    return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (bulk copy never completed)");
-  if (pc && pc->take_error())
-    return ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (coarse-level grid barrier)");
-  if (hs->nan) return ws_fail(NB_ERR_NAN, "residual became NaN or Inf");
-  return NB_OK;
+    *status = ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (bulk copy never completed)");
+  else if (R.pc && R.pc->take_error())
+    *status = ws_fail(NB_ERR_TIMEOUT, "a bounded device wait expired (coarse-level grid barrier)");
+  else if (hs->nan)
+    *status = ws_fail(NB_ERR_NAN, "residual became NaN or Inf");
+  return 1;
+}
+
+// Runs the whole solve on stream s: iterations are replayed from a graph
+// holding a chunk of them; the host reads the state once per chunk.
+nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
+                   Precond *pc, nb_solve_result *res, cudaStream_t s) {
+  CgRun R;
+  R.P = P;
+  R.x = x;
+  R.f = f;
+  R.o = o;
+  R.pc = pc;
+  R.s = s;
+  nb_status st = cg_start(R);
+  if (st != NB_OK) return st;
+  while (!cg_poll(R, true, res, &st)) {
+  }
+  return st;
 }
 
 }  // namespace nb

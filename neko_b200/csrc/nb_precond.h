@@ -46,6 +46,7 @@ struct CgWorkspace {
   int recompute_every = 0;
   int launches_per_iter = 6;
   cudaGraphExec_t graph_exec = nullptr;
+  cudaEvent_t ev = nullptr;  // behind the state copy of the last chunk
   const void *graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   ~CgWorkspace();
   cudaError_t ensure(long n);
@@ -67,6 +68,21 @@ __global__ void cg_update_xr_kernel(double *x, double *r, const double *p, const
 
 nb_status cg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
                    Precond *pc, nb_solve_result *res, cudaStream_t s);
+
+// A CG solve followed without blocking (the batch's concurrent solves).
+struct CgRun {
+  nb_problem *P = nullptr;
+  double *x = nullptr;
+  const double *f = nullptr;
+  nb_solve_opts o{};
+  Precond *pc = nullptr;
+  cudaStream_t s = nullptr;
+  int chunk = 0, launches = 0;
+  bool active = false;
+};
+nb_status cg_start(CgRun &R);
+nb_status cg_next_chunk(CgRun &R);
+int cg_poll(CgRun &R, bool wait, nb_solve_result *res, nb_status *status);
 // Restarted flexible GMRES (gmres.cu).
 nb_status gmres_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
                       Precond *pc, nb_solve_result *res, cudaStream_t s);

@@ -80,6 +80,13 @@ void gmres_free(nb_problem *p);
 void gmres_invalidate(nb_problem *p);
 // After new h1: the coarse levels take the new h1 (hsmg_set_h).
 cudaError_t hsmg_refresh_coefficients(nb_problem *p);
+// The same for constant coefficients, asynchronously on stream s.
+cudaError_t hsmg_set_h_const(nb_problem *p, double h1, cudaStream_t s);
+// a[0..n) = v on stream s
+cudaError_t fill_const(double *a, double v, long n, cudaStream_t s);
+// Constant h1 > 0, h2 >= 0 (h2 = 0: no h2 term) set on stream s without
+// waiting for the device: fields, Jacobi diagonal, hsmg coarse levels.
+cudaError_t set_coefficients_const(nb_problem *p, double h1, double h2, cudaStream_t s);
 
 // Deletes a half-built problem on early return.
 struct nb_problem_guard {

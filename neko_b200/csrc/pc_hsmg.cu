@@ -665,6 +665,19 @@ static cudaError_t hsmg_set_h(nb_problem *P, nb_problem *C) {
   return C->update_jacobi(nullptr);
 }
 
+// Constant h1 on the coarse levels of p's preconditioners, on stream s
+// (hsmg_set_h with a constant fine h1: every coarse value is h1).
+cudaError_t hsmg_set_h_const(nb_problem *p, double h1, cudaStream_t s) {
+  for (auto *h : p->hsmg) {
+    if (!h) continue;
+    nb_problem *C = h->crs;
+    cudaError_t e = fill_const(C->h1, h1, C->n, s);
+    if (e != cudaSuccess) return e;
+    if ((e = C->update_jacobi(s)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t hsmg_refresh_coefficients(nb_problem *p) {
   for (auto *h : p->hsmg) {
     if (!h) continue;

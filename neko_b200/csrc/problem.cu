@@ -552,6 +552,34 @@ int nb_problem::take_error() {
   return v;
 }
 
+namespace nb {
+cudaError_t fill_const(double *a, double v, long n, cudaStream_t s) {
+  k_fill<<<stream_grid(n, 256), 256, 0, s>>>(a, v, n);
+  return cudaGetLastError();
+}
+
+cudaError_t set_coefficients_const(nb_problem *p, double h1, double h2, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = fill_const(p->h1, h1, p->n, s)) != cudaSuccess) return e;
+  if ((e = fill_const(p->h2, h2, p->n, s)) != cudaSuccess) return e;
+  const bool ifh2 = h2 != 0.0;
+  if (ifh2 != p->ifh2) {
+    p->ifh2 = ifh2;
+    p->invalidate_solver_cache();
+  }
+  if ((e = p->update_jacobi(s)) != cudaSuccess) return e;
+  return hsmg_set_h_const(p, h1, s);
+}
+}  // namespace nb
+
+extern "C" nb_status nb_problem_set_coefficients_const(nb_problem *p, double h1, double h2,
+                                                       void *stream) {
+  if (!p) return fail(NB_ERR_ARG, "null argument");
+  if (!(h1 > 0.0) || !(h2 >= 0.0)) return fail(NB_ERR_ARG, "need h1 > 0 and h2 >= 0");
+  NB_TRY(set_coefficients_const(p, h1, h2, (cudaStream_t)stream));
+  return NB_OK;
+}
+
 extern "C" nb_status nb_problem_sync(nb_problem *p, void *stream) {
   if (!p) return fail(NB_ERR_ARG, "null problem");
   NB_TRY(cudaStreamSynchronize((cudaStream_t)stream));

@@ -20,7 +20,7 @@ import time
 import numpy as np
 import torch
 
-from . import AxHelm, Batch, CG, Jacobi, NekoB200Error, Problem
+from . import AxHelm, Batch, CG, FCG, Hsmg, Jacobi, NekoB200Error, Problem
 from . import workloads
 from ._lib import NB_ERR_OOM, NB_ERR_TIMEOUT
 
@@ -56,6 +56,54 @@ class GeometryCache:
         for P in self.problems.values():
             P.close()
         self.problems.clear()
+
+
+class InstancePool:
+    """Problem instances for the per-problem solves (hsmg slots): a slot owns
+    its instance until it is released, so concurrent requests of one shape
+    get distinct instances.  The first instance of a shape is the
+    GeometryCache's problem; the others are created on demand and kept.
+    Every instance has its hsmg preconditioners (the `variants`: False for
+    FP64, True for mixed precision) built when it is created."""
+
+    def __init__(self, cache, variants=(False,)):
+        self.cache, self.variants = cache, tuple(variants)
+        self.free, self.count, self.setup_s = {}, {}, 0.0
+        self.extra = []
+
+    def acquire(self, spec):
+        k = self.cache.key(spec)
+        fl = self.free.setdefault(k, [])
+        if fl:
+            return fl.pop()
+        t0 = time.perf_counter()
+        if self.count.get(k, 0) == 0:
+            P = self.cache.get(spec)
+        else:
+            P = Problem((spec["n"],) * 3, spec["lx"],
+                        deform=workloads.deform_amplitude(spec["dseed"]), dirichlet=True)
+            self.extra.append(P)
+        for m in self.variants:
+            Hsmg(mixed=m).init(P)
+        self.count[k] = self.count.get(k, 0) + 1
+        self.setup_s += time.perf_counter() - t0
+        return P
+
+    def release(self, spec, P):
+        self.free.setdefault(self.cache.key(spec), []).append(P)
+
+    def instances(self):
+        return sum(self.count.values())
+
+    def device_bytes(self):
+        """Approximate HBM of the extra instances (their hsmg levels
+        included: about 30 arrays of n)."""
+        return sum(P.n * 8 * 30 for P in self.extra)
+
+    def close(self):
+        for P in self.extra:
+            P.close()
+        self.extra.clear()
 
 
 class RhsPool:
@@ -95,10 +143,19 @@ OK, NOT_CONVERGED, NAN, OOM_REJECTED, TIMEOUT, CANCELLED = (
 
 
 def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000, chunk_runs=1,
-                  batch=None, stream=None, cancel=None, status=None):
+                  batch=None, stream=None, cancel=None, status=None, mode="jacobi",
+                  instances=None, max_solves=64):
     """Continuous-batching server.  Returns per-request latency (s),
     iterations, convergence flags, the span of the run (s) and the solutions
     (request index -> device tensor).
+
+    mode "jacobi": every request is a Jacobi-PCG slot of the batched engine
+    (one persistent Ax launch over all of them).  mode "fp64" / "mixed":
+    requests whose spec says pc "jacobi" stay batched Jacobi slots, those
+    with pc "hsmg" run as per-problem hsmg flexible-CG solves (FP64, or FP32
+    smoothing with FP64 outer iteration for "mixed") on instances of
+    `instances` (an InstancePool), at most `max_solves` at a time, all
+    advanced together by the same run loop.
 
     A request may set "max_iter" in its spec.  `cancel` maps request index ->
     time (s after the start) at which the client withdraws it; a withdrawn
@@ -116,10 +173,11 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
     if len(st) < n:
         st.extend([None] * (n - len(st)))
     cancel = dict(cancel or {})
-    xs, active = {}, {}
+    xs, active, owned = {}, {}, {}
     waiting = collections.deque()
     nxt, done_count = 0, 0
     t0 = time.perf_counter()
+    per_problem = mode in ("fp64", "mixed")
 
     def finish(i, outcome, now, mon=None):
         nonlocal done_count
@@ -128,6 +186,13 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
         if mon is not None:
             iters[i], conv[i] = mon.iter, mon.converged
         done_count += 1
+
+    def release(slot):
+        B.release(slot)
+        i = active.pop(slot)
+        if slot in owned:
+            instances.release(specs[i], owned.pop(slot))
+        return i
 
     while done_count < n:
         now = time.perf_counter() - t0
@@ -140,12 +205,23 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
         while waiting:  # admission in arrival order while the budget allows
             i = waiting[0]
             sp = specs[i]
+            solo = per_problem and sp.get("pc", "jacobi") == "hsmg"
+            if solo and len(owned) >= max_solves:
+                break
             P, f, r0 = pool.get(sp)
             x = torch.empty(P.n, dtype=torch.float64, device="cuda")
+            Pi = instances.acquire(sp) if solo else None
             try:
-                slot = B.submit(P, f, x, rel_tol * r0, sp.get("max_iter", max_iter),
-                                h1=sp["h1"], h2=sp["h2"])
+                if solo:
+                    slot = B.submit_solve(Pi, f, x, rel_tol * r0, sp.get("max_iter", max_iter),
+                                          h1=sp["h1"], h2=sp["h2"], pc="hsmg",
+                                          mixed=mode == "mixed")
+                else:
+                    slot = B.submit(P, f, x, rel_tol * r0, sp.get("max_iter", max_iter),
+                                    h1=sp["h1"], h2=sp["h2"])
             except NekoB200Error as e:
+                if Pi is not None:
+                    instances.release(sp, Pi)
                 if e.status != NB_ERR_OOM:
                     raise
                 if active:  # over budget for now: wait for slots to free
@@ -155,6 +231,8 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
                 continue
             waiting.popleft()
             active[slot] = i
+            if Pi is not None:
+                owned[slot] = Pi
             xs[i] = x
         if not active:
             if nxt < n and not waiting:
@@ -170,20 +248,17 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
         now = time.perf_counter() - t0
         for slot, i in list(active.items()):
             if failed is not None:
-                B.release(slot)
-                del active[slot]
+                release(slot)
                 finish(i, failed, now)
                 continue
             done, mon = B.result(slot)
             if i in cancel and cancel[i] <= now and not done:
-                B.release(slot)
-                del active[slot]
+                release(slot)
                 finish(i, CANCELLED, now, mon)
             elif done:
                 outcome = OK if mon.converged else (
                     NAN if not math.isfinite(mon.res_final) else NOT_CONVERGED)
-                B.release(slot)
-                del active[slot]
+                release(slot)
                 finish(i, outcome, now, mon)
     span = time.perf_counter() - t0
     if own:
@@ -191,8 +266,10 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
     return lat, iters, conv, span, xs
 
 
-def serve_sequential(specs, t_arr, pool, rel_tol=1e-8, max_iter=5000):
-    """One request at a time with nb_solve, in arrival order."""
+def serve_sequential(specs, t_arr, pool, rel_tol=1e-8, max_iter=5000, mode="jacobi"):
+    """One request at a time with nb_solve, in arrival order, on the plain
+    FP64 path: Jacobi-PCG (mode "jacobi", or a spec with pc "jacobi") or
+    hsmg flexible CG."""
     n = len(specs)
     lat, iters, conv = [None] * n, [0] * n, [False] * n
     t0 = time.perf_counter()
@@ -201,11 +278,13 @@ def serve_sequential(specs, t_arr, pool, rel_tol=1e-8, max_iter=5000):
         if t_arr[i] > now:
             time.sleep(t_arr[i] - now)
         P, f, r0 = pool.get(sp)
-        h1 = torch.full((P.n,), sp["h1"], dtype=torch.float64, device="cuda")
-        P.set_coefficients(h1, torch.full_like(h1, sp["h2"]))
+        P.set_coefficients_const(sp["h1"], sp["h2"])
         x = P.zeros()
-        mon = CG(max_iter=max_iter, abs_tol=rel_tol * r0, M=Jacobi()).solve(AxHelm(), x, f,
-                                                                           P.n, P)
+        if mode != "jacobi" and sp.get("pc", "jacobi") == "hsmg":
+            solver = FCG(max_iter=max_iter, abs_tol=rel_tol * r0, M=Hsmg())
+        else:
+            solver = CG(max_iter=max_iter, abs_tol=rel_tol * r0, M=Jacobi())
+        mon = solver.solve(AxHelm(), x, f, P.n, P)
         torch.cuda.synchronize()
         lat[i] = time.perf_counter() - t0 - t_arr[i]
         iters[i], conv[i] = mon.iter, mon.converged

@@ -78,13 +78,17 @@ def uneven_specs(count=512, seed=4):
     """Problem descriptions of the batched / served workloads: a box of n^3
     elements with n ~ U{2..16}, N ~ {5, 7, 9} (lx = N + 1), h1 ~ U[0.5, 2],
     h2 ~ U[0, 100], a deformation seed (8 seeds, amplitude U[0, 0.1] each),
-    zero Dirichlet on the box faces and a Fourier-mode right-hand side."""
+    zero Dirichlet on the box faces and a Fourier-mode right-hand side.
+    The preconditioner per problem ("pc"): Jacobi for the boxes of at most
+    3^3 elements, where the multigrid's fixed cost per iteration outweighs
+    its savings, hsmg for the others."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
         out.append(dict(n=int(rng.integers(2, 17)), lx=int(rng.choice([5, 7, 9])) + 1,
                         h1=float(rng.uniform(0.5, 2.0)), h2=float(rng.uniform(0.0, 100.0)),
                         dseed=int(rng.integers(0, N_DEFORM_SEEDS)), rhs_seed=int(seed * 100003 + i)))
+        out[-1]["pc"] = "jacobi" if out[-1]["n"] <= 3 else "hsmg"
     return out
 
 
