@@ -324,109 +324,98 @@ def kernel_only(args, cfg):
 
 def run_batch(args):
     """Batched uneven Helmholtz solves: `--batch-count` problems of
-    workloads.uneven_specs, Jacobi-PCG to 1e-8 relative, FP64, advanced
-    together by nb_batch (one persistent Ax launch over every solve's
-    elements per iteration, graph replay, per-lx autotuned k-split), timed
-    against the same solves run one by one through nb_solve."""
+    workloads.uneven_specs (Jacobi for boxes of at most 3^3 elements, hsmg
+    for the others), to 1e-8 relative, all present at once, served by one
+    Batch: the Jacobi problems as slots of the persistent batched engine
+    (one Ax launch over every such solve's elements per iteration, graph
+    replay, per-lx autotuned k-split), the hsmg problems as per-problem
+    flexible-CG solves advanced concurrently on a stream pool by the same run
+    loop, in mixed precision (FP32 smoothing, FP64 outer iteration) and in
+    FP64; timed against the same solves run one by one on the plain FP64
+    path (nb_solve).  An untimed warm-up pass of each builds the problem
+    instances, preconditioners, graphs and the autotuner's choice."""
     import torch
     import neko_b200 as nb
-    from neko_b200 import workloads
-    from neko_b200.serve import GeometryCache
+    from neko_b200 import serve, workloads
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    # replicas: each GPU solves its share of the independent problems
+    # replicas: each GPU serves its share of the independent problems
     specs = shard(workloads.uneven_specs(args.batch_count, seed=args.seed), rank, world)
-    cache = GeometryCache()
-    reqs = []
+    cache = serve.GeometryCache()
+    pool = serve.RhsPool(cache)
+    inst = serve.InstancePool(cache, variants=(False, True))
     for sp in specs:
-        P = cache.get(sp)
-        f = workloads.uneven_rhs(P, sp["rhs_seed"])
-        r0 = math.sqrt(float((f * P.field("mult") * f).sum()) / P.volume)
-        reqs.append((sp, P, f, 1e-8 * r0))
-    torch.cuda.synchronize()
+        pool.get(sp)
+    zeros = [0.0] * len(specs)
     stream = torch.cuda.Stream()
-    # autotune once per lx on a small warm-up batch (the first-use cost)
     B = nb.Batch()
-    warm = {}
-    for sp, P, f, tol in reqs:
-        warm.setdefault(sp["lx"], (sp, P, f, tol))
-    xs = []
-    for sp, P, f, tol in warm.values():
-        x = P.zeros()
-        xs.append(x)
-        B.submit(P, f, x, tol, 5000, h1=sp["h1"], h2=sp["h2"])
-    with torch.cuda.stream(stream):
-        B.run(stream=stream)
-    tuning = {lx: B.tuning(lx) for lx in sorted(warm)}
-    for q in range(len(warm)):
-        B.release(q)
-    # --- batched ---------------------------------------------------------
-    xb = [P.zeros() for _, P, _, _ in reqs]
-    torch.cuda.synchronize()
-    barrier(world)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
-    e0.record(stream)
-    slots = [B.submit(P, f, x, tol, 5000, h1=sp["h1"], h2=sp["h2"])
-             for (sp, P, f, tol), x in zip(reqs, xb)]
-    with torch.cuda.stream(stream):
-        B.run(stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    t_batch = max_over_ranks(max(e0.elapsed_time(e1) / 1e3, 1e-9), world)
-    wall_batch = time.perf_counter() - t0
-    res_b = [B.result(s)[1] for s in slots]
-    # --- one by one ------------------------------------------------------
-    xs_seq, it_seq = [], []
-    torch.cuda.synchronize()
-    barrier(world)
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t1 = time.perf_counter()
-    e2.record(stream)
-    with torch.cuda.stream(stream):
-        for sp, P, f, tol in reqs:
-            h1 = torch.full((P.n,), sp["h1"], dtype=torch.float64, device="cuda")
-            P.set_coefficients(h1, torch.full_like(h1, sp["h2"]))
-            x = P.zeros()
-            mon = nb.CG(max_iter=5000, abs_tol=tol, M=nb.Jacobi()).solve(nb.AxHelm(), x, f, P.n, P,
-                                                                         stream=stream)
-            xs_seq.append(x)
-            it_seq.append(mon.iter)
-    e3.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    t_seq = max_over_ranks(max(e2.elapsed_time(e3) / 1e3, 1e-9), world)
-    wall_seq = time.perf_counter() - t1
-    d_it = max(abs(a.iter - b) for a, b in zip(res_b, it_seq))
-    err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(xb, xs_seq))
-    conv = int(sum_over_ranks(sum(1 for r in res_b if r.converged), world))
-    d_it = int(max_over_ranks(d_it, world))
-    err = max_over_ranks(err, world)
-    ndof = sum_over_ranks(sum(P.n for _, P, _, _ in reqs), world)
+
+    def timed_run(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3, world), time.perf_counter() - t0, out
+
+    res = {}
+    for mode in ("mixed", "fp64"):
+        run = lambda: serve.serve_batched(specs, zeros, pool, 0, batch=B, mode=mode,
+                                          instances=inst, max_solves=args.max_solves,
+                                          stream=stream)
+        run()  # warm-up: instances, preconditioners, graphs, autotune
+        res[mode] = timed_run(run)
+    # one by one on the plain FP64 path (preconditioners already built)
+    seq = lambda: serve.serve_sequential(specs, zeros, pool, mode="fp64")
+    seq()
+    t_seq, wall_seq, (lat_s, it_s, conv_s, _) = timed_run(seq)
+    xs_seq = None  # the one-by-one solutions of each request
+    lat_s2, it_s2, conv_s2, _, xs_seq = serve.serve_batched(specs, zeros, pool, 0, batch=B,
+                                                            mode="fp64", instances=inst,
+                                                            max_solves=1, stream=stream)
     total = args.batch_count
+    out = {}
+    for mode, (t, wall, (lat, it, conv, span, xs)) in res.items():
+        err = max(float(torch.linalg.norm(xs[i] - xs_seq[i]) / torch.linalg.norm(xs_seq[i]))
+                  for i in range(len(specs)))
+        out[mode] = {"value": total / t, "seconds": t, "wall_s": wall,
+                     "converged": int(sum_over_ranks(sum(1 for c in conv if c), world)),
+                     "iterations": {"min": min(it), "max": max(it), "mean": sum(it) / len(it)},
+                     "max_iter_diff_vs_sequential": int(max_over_ranks(
+                         max(abs(a - b) for a, b in zip(it, it_s)), world)),
+                     "max_rel_diff_vs_sequential": max_over_ranks(err, world)}
+    ndof = sum_over_ranks(sum(cache.get(sp).n for sp in specs), world)
+    n_hsmg = int(sum_over_ranks(sum(1 for sp in specs if sp["pc"] == "hsmg"), world))
     line = {
-        "metric": "batched uneven Helmholtz solves/s to 1e-8 rel", "value": total / t_batch,
-        "unit": "solves/s", "n_gpus": world, "higher_is_better": True, "dtype": "f64",
+        "metric": "batched uneven Helmholtz solves/s to 1e-8 rel", "value": out["mixed"]["value"],
+        "unit": "solves/s", "n_gpus": world, "higher_is_better": True, "dtype": "f64+f32",
         "data": "synthetic", "vs_baseline": None, "scaling": "strong",
         "parallelism": "replicas x%d" % world,
-        "config": {"workload": f"{total} Jacobi-PCG Helmholtz solves, n^3 elements n~U{{2..16}}, "
+        "config": {"workload": f"{total} Helmholtz solves, n^3 elements n~U{{2..16}}, "
                                f"N~{{5,7,9}}, h1~U[0.5,2], h2~U[0,100], 8 deformation seeds, "
-                               f"zero Dirichlet, Fourier RHS ({ndof / 1e6:.0f}M DOF in total)",
-                   "geometries": len(cache.problems), "geometry_setup_s": cache.setup_s},
-        "batched_s": t_batch, "batched_wall_s": wall_batch,
+                               f"zero Dirichlet, Fourier RHS ({ndof / 1e6:.0f}M DOF in total); "
+                               f"{n_hsmg} hsmg flexible-CG (mixed precision), "
+                               f"{total - n_hsmg} Jacobi-PCG in the persistent batched launch",
+                   "max_concurrent_hsmg_solves": args.max_solves,
+                   "instances": inst.instances(), "geometries": len(cache.problems),
+                   "setup_s": cache.setup_s + inst.setup_s},
+        "mixed": out["mixed"], "fp64_batched": out["fp64"],
         "sequential": {"value": total / t_seq, "seconds": t_seq, "wall_s": wall_seq,
-                       "path": "nb_solve one by one (set_coefficients + Jacobi-PCG graph)"},
-        "speedup_vs_sequential": t_seq / t_batch,
-        "converged": conv, "max_iter_diff_vs_sequential": d_it,
-        "max_rel_diff_vs_sequential": err,
-        "iterations": {"min": min(r.iter for r in res_b), "max": max(r.iter for r in res_b),
-                       "mean": sum(r.iter for r in res_b) / len(res_b)},
-        "autotune": {str(lx): {"ks": t[0], "candidate_ms": t[1]} for lx, t in tuning.items()},
+                       "path": "nb_solve one by one on the plain FP64 path (hsmg flexible CG or "
+                               "Jacobi-PCG per problem, constant coefficients set per solve)"},
+        "speedup_vs_sequential": t_seq / res["mixed"][0],
+        "fp64_speedup_vs_sequential": t_seq / res["fp64"][0],
+        "autotune": {str(lx): {"ks": B.tuning(lx)[0], "candidate_ms": B.tuning(lx)[1]}
+                     for lx in (6, 8, 10) if B.tuning(lx)[0]},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     B.close()
+    inst.close()
     cache.close()
     if world > 1:
         import torch.distributed as dist
@@ -502,61 +491,81 @@ def run_axgs(args):
 
 def run_serve(args):
     """Served request stream: open-loop Poisson arrivals at each of
-    --serve-rates, --serve-requests requests per rate drawn as the batched
-    workload, answered (a) by the continuous-batching server under a
-    --serve-budget-gb HBM budget and (b) one request at a time with
-    nb_solve; latency percentiles and solves/s for both."""
+    --serve-rates (plus one rate at half the measured capacity when every
+    given rate is above it), --serve-requests requests per rate drawn as the
+    batched workload, answered by the continuous-batching server under a
+    --serve-budget-gb HBM budget in mixed precision and in FP64 (hsmg
+    problems as per-problem solves, Jacobi ones in the persistent batched
+    launch), and a bounded sample of each stream by the one-request-at-a-time
+    server on the plain FP64 path; latency percentiles and solves/s."""
     import numpy as np
     import torch
     import neko_b200 as nb
     from neko_b200 import serve, workloads
     torch.cuda.set_device(0)
-    rates = [float(r) for r in args.serve_rates.split(",")]
     cache = serve.GeometryCache()
     pool = serve.RhsPool(cache)
-    all_specs = {rate: workloads.uneven_specs(args.serve_requests, seed=args.seed + 17 * q)
-                 for q, rate in enumerate(rates)}
-    for specs in all_specs.values():  # warm the geometry cache and payloads
-        for sp in specs:
-            pool.get(sp)
-    torch.cuda.synchronize()
-    budget = int(args.serve_budget_gb * 1e9) - cache.device_bytes()
-    B = nb.Batch(hbm_budget=max(budget, 1))
-    warm = {}
-    for specs in all_specs.values():
-        for sp in specs:
-            warm.setdefault(sp["lx"], sp)
-    serve.serve_batched(list(warm.values()), np.zeros(len(warm)), pool, budget, batch=B)
+    inst = serve.InstancePool(cache, variants=(False, True))
+    stream = torch.cuda.Stream()
+    # capacity: the solves/s of a saturated mixed-precision stream
+    cap_specs = workloads.uneven_specs(min(args.serve_requests, 512), seed=args.seed + 999)
+    for sp in cap_specs:
+        pool.get(sp)
+    B = nb.Batch(hbm_budget=max(int(args.serve_budget_gb * 1e9) - cache.device_bytes(), 1))
+    zeros = np.zeros(len(cap_specs))
+    serve.serve_batched(cap_specs, zeros, pool, 0, batch=B, mode="mixed", instances=inst,
+                        max_solves=args.max_solves, stream=stream)
+    _, _, _, span, _ = serve.serve_batched(cap_specs, zeros, pool, 0, batch=B, mode="mixed",
+                                           instances=inst, max_solves=args.max_solves,
+                                           stream=stream)
+    capacity = len(cap_specs) / span
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    if min(rates) >= capacity:
+        rates.insert(0, round(0.5 * capacity, 1))
     out = {}
     for q, rate in enumerate(rates):
-        specs = all_specs[rate]
+        specs = workloads.uneven_specs(args.serve_requests, seed=args.seed + 17 * q)
+        for sp in specs:
+            pool.get(sp)
         t_arr = serve.arrivals(rate, len(specs), seed=args.seed + q)
-        lat, it, conv, span, _ = serve.serve_batched(specs, t_arr, pool, budget, batch=B)
-        lat_s, it_s, conv_s, span_s = serve.serve_sequential(specs, t_arr, pool)
-        out[str(int(rate))] = {
-            "batched": dict(serve.percentiles(lat), solves_per_s=len(specs) / span,
-                            converged=int(sum(conv)), mean_iter=float(np.mean(it))),
-            "one_by_one": dict(serve.percentiles(lat_s), solves_per_s=len(specs) / span_s,
-                               converged=int(sum(conv_s)), mean_iter=float(np.mean(it_s))),
-            "max_iter_diff": int(max(abs(a - b) for a, b in zip(it, it_s))),
-            "arrival_span_s": float(t_arr[-1]),
-        }
+        r = {}
+        for mode in ("mixed", "fp64"):
+            status = []
+            lat, it, conv, span, _ = serve.serve_batched(
+                specs, t_arr, pool, 0, batch=B, mode=mode, instances=inst,
+                max_solves=args.max_solves, stream=stream, status=status)
+            r[mode] = dict(serve.percentiles(lat), solves_per_s=len(specs) / span,
+                           requests=len(specs), converged=int(sum(conv)),
+                           mean_iter=float(np.mean(it)), span_s=span)
+        k = min(args.serve_seq_requests, len(specs))
+        lat_s, it_s, conv_s, span_s = serve.serve_sequential(specs[:k], t_arr[:k], pool,
+                                                             mode="fp64")
+        r["one_by_one_fp64"] = dict(serve.percentiles(lat_s), solves_per_s=k / span_s,
+                                    requests=k, converged=int(sum(conv_s)))
+        r["arrival_span_s"] = float(t_arr[-1])
+        out[str(rate)] = r
+    first = str(rates[0])
     line = {
         "metric": "served Helmholtz solves: p50/p95/p99 latency (ms) and solves/s",
-        "value": out[str(int(rates[0]))]["batched"]["p99_ms"],
-        "unit": "ms (p99 at the first rate)", "higher_is_better": False, "n_gpus": 1,
-        "dtype": "f64", "data": "synthetic", "vs_baseline": None,
+        "value": out[first]["mixed"]["p99_ms"],
+        "unit": f"ms (p99, mixed precision, at {rates[0]:g} req/s)", "higher_is_better": False,
+        "n_gpus": 1, "dtype": "f64+f32", "data": "synthetic", "vs_baseline": None,
         "config": {"workload": f"{args.serve_requests} requests per rate, open-loop Poisson "
                                f"arrivals, shapes/orders/coefficients as the batched workload, "
-                               f"Jacobi-PCG to 1e-8 rel, FP64, HBM budget "
-                               f"{args.serve_budget_gb:.0f} GB, geometry cached by "
-                               f"(n, lx, deformation seed)",
-                   "rates_per_s": rates, "geometries": len(cache.problems),
-                   "geometry_setup_s": cache.setup_s},
+                               f"hsmg flexible CG (boxes above 3^3 elements) or Jacobi-PCG, "
+                               f"to 1e-8 rel, HBM budget {args.serve_budget_gb:.0f} GB, "
+                               f"geometry cached by (n, lx, deformation seed)",
+                   "rates_per_s": rates, "capacity_solves_per_s": capacity,
+                   "max_concurrent_hsmg_solves": args.max_solves,
+                   "one_by_one_sample": f"first {args.serve_seq_requests} requests of each "
+                                        f"stream",
+                   "geometries": len(cache.problems), "instances": inst.instances(),
+                   "setup_s": cache.setup_s + inst.setup_s},
         "rates": out,
     }
     print(json.dumps(line), flush=True)
     B.close()
+    inst.close()
     cache.close()
 
 
@@ -580,11 +589,15 @@ def main():
                     help="solve: the hsmg-FCG config-2 line (default); batch: batched "
                          "uneven solves; serve: the served request stream")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--max-solves", type=int, default=64,
+                    help="per-problem hsmg solves running at once in the batch / server")
     ap.add_argument("--coarse-tol", type=float, default=1e-9,
                     help="hsmg coarse CG absolute tolerance (reference KSP_ABS_TOL 1e-9; "
                          "1e-4 is the config-2 variant)")
     ap.add_argument("--serve-rates", default="200,1000,5000")
-    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-requests", type=int, default=20000)
+    ap.add_argument("--serve-seq-requests", type=int, default=1000,
+                    help="requests of each stream also answered one at a time")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--nel", type=int, default=16)
     ap.add_argument("--lx", type=int, default=8)
