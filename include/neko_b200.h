@@ -220,6 +220,16 @@ nb_status nb_mesh_read_nmsh(const char *path, int *nelv, int *vertex_ids, double
 nb_status nb_mesh_write_nmsh(const char *path, int nelv, const int *vertex_ids,
                              const double *vertex_xyz);
 
+/* Writes a field file in Neko's fld format (fld_file_write,
+ * src/io/fld_file.f90:183-620; the Nek5000 layout): 132-byte header with
+ * real size 8, lx, nelv, time, step and the record code, the byte-order
+ * tag, element ids, the coordinates ('X', when x, y, z are given), one
+ * scalar as the pressure ('P', when p is given), then the per-element
+ * min/max metadata in single precision.  Host arrays of nelv lx^3 values in
+ * element order.  Host only. */
+nb_status nb_fld_write(const char *path, int nelv, int lx, const double *x, const double *y,
+                       const double *z, const double *p, double time, int step);
+
 /* Gather-scatter maps (and the neighbour per face, 6 per element, 1-based,
  * 0 on the boundary) of the unstructured mesh that nb_problem_create_mesh
  * takes, in the reference layout of gs_init_mapping.  Host only; call once

@@ -29,6 +29,7 @@ GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
 __all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "KspMonitor",
            "Jacobi", "Hsmg", "Batch", "Projection", "ortho", "read_nmsh", "write_nmsh",
+           "write_fld",
            "GS_OP_ADD", "NekoB200Error",
            "load", "version"]
 
@@ -376,6 +377,21 @@ def write_nmsh(path, vertex_ids, vertex_xyz):
     check(load().nb_mesh_write_nmsh(str(path).encode(), ids.shape[0],
                                     ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                     xyz.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+
+def write_fld(path, coef, p=None, time=0.0, step=0, mesh=True):
+    """Writes the problem's coordinates (mesh=True) and the field p (a
+    device tensor of n values, written as the pressure) to an fld file
+    (nb_fld_write)."""
+    import numpy as np
+    DP = ctypes.POINTER(ctypes.c_double)
+    arrs = [np.ascontiguousarray(coef.field(k).cpu().numpy()) for k in ("x", "y", "z")] \
+        if mesh else [None] * 3
+    pa = np.ascontiguousarray(p.detach().cpu().numpy(), dtype=np.float64) if p is not None \
+        else None
+    ptr = lambda a: a.ctypes.data_as(DP) if a is not None else None
+    check(load().nb_fld_write(str(path).encode(), coef.nelv, coef.lx, *(ptr(a) for a in arrs),
+                              ptr(pa), float(time), int(step)))
 
 
 def ortho(x, coef, stream=None):

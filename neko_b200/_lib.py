@@ -88,6 +88,7 @@ SIGNATURES = {
     "nb_box_gs_maps": (_I, [_IP, _IP, _I, _IP, _IP, _IP, _IP, _IP, _IP, _IP]),
     "nb_mesh_read_nmsh": (_I, [ctypes.c_char_p, _IP, _IP, _DP, _IP, _IP]),
     "nb_mesh_write_nmsh": (_I, [ctypes.c_char_p, _I, _IP, _DP]),
+    "nb_fld_write": (_I, [ctypes.c_char_p, _I, _I, _DP, _DP, _DP, _DP, ctypes.c_double, _I]),
     "nb_mesh_gs_maps": (_I, [_I, _IP, _I, _IP, _IP, _IP, _IP, _IP, _IP, _IP, _IP]),
     "nb_problem_create_box": (_I, [_IP, _DP, _DP, _IP, _I, ctypes.c_double, _I,
                                    ctypes.POINTER(_P)]),

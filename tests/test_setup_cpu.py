@@ -191,3 +191,41 @@ def test_nmsh_write_read_roundtrip(nblib, tmp_path):
     assert npz == 0
     np.testing.assert_array_equal(ids2, ids)
     np.testing.assert_array_equal(xyz2, xyz)
+
+
+def test_fld_write_layout(nblib, tmp_path):
+    """The fld file layout of fld_file_write (src/io/fld_file.f90:402-560):
+    header fields and Fortran e20.13 time, byte-order tag, element ids,
+    coordinates per element, the field, then per-element min/max."""
+    import struct
+    DP = ctypes.POINTER(ctypes.c_double)
+    nelv, lx = 3, 4
+    l3 = lx ** 3
+    rng = np.random.default_rng(2)
+    x, y, z, p = (rng.standard_normal(nelv * l3) for _ in range(4))
+    path = tmp_path / "field0.f00001"
+    assert nblib.nb_fld_write(str(path).encode(), nelv, lx, *(a.ctypes.data_as(DP)
+                              for a in (x, y, z, p)), 123.456, 7) == 0
+    raw = path.read_bytes()
+    hdr = raw[:132].decode()
+    assert hdr.startswith("#std 8  4  4  4          3          3  0.1234560000000E+03         7")
+    assert hdr.split()[-1] == "XP" and len(hdr) == 132
+    assert abs(struct.unpack("<f", raw[132:136])[0] - 6.54321) < 1e-6
+    off = 136
+    ids = np.frombuffer(raw, np.int32, nelv, off)
+    assert list(ids) == [1, 2, 3]
+    off += 4 * nelv
+    xyz = np.frombuffer(raw, np.float64, 3 * nelv * l3, off).reshape(nelv, 3, l3)
+    assert np.array_equal(xyz[:, 0], x.reshape(nelv, l3))
+    assert np.array_equal(xyz[:, 2], z.reshape(nelv, l3))
+    off += 8 * 3 * nelv * l3
+    pp = np.frombuffer(raw, np.float64, nelv * l3, off)
+    assert np.array_equal(pp, p)
+    off += 8 * nelv * l3
+    mx = np.frombuffer(raw, np.float32, 6 * nelv, off).reshape(nelv, 6)
+    assert np.allclose(mx[:, 0], x.reshape(nelv, l3).min(1).astype(np.float32))
+    assert np.allclose(mx[:, 5], z.reshape(nelv, l3).max(1).astype(np.float32))
+    off += 4 * 6 * nelv
+    mp = np.frombuffer(raw, np.float32, 2 * nelv, off).reshape(nelv, 2)
+    assert np.allclose(mp[:, 1], p.reshape(nelv, l3).max(1).astype(np.float32))
+    assert off + 4 * 2 * nelv == len(raw)
