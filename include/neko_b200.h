@@ -349,15 +349,18 @@ typedef struct {
   int coarse_iter;     /* hsmg coarse CG iterations (reference default 10) */
   double coarse_tol;   /* hsmg coarse CG absolute tolerance (default 1e-9) */
   int flexible;        /* 1: flexible CG (Polak-Ribiere beta) with a pc */
-  int ksp;             /* NB_KSP_CG (default) or NB_KSP_GMRES */
+  int ksp;             /* NB_KSP_CG (default), NB_KSP_GMRES or NB_KSP_PIPECG */
   int m_restart;       /* GMRES vectors per restart cycle (<= 0: 30, the
                           reference's default; at most 64) */
 } nb_solve_opts;
 
 typedef enum {
   NB_KSP_CG = 0,     /* cg_device_solve (flexible when opts.flexible) */
-  NB_KSP_GMRES = 1   /* gmres_device_solve: restarted flexible GMRES,
+  NB_KSP_GMRES = 1,  /* gmres_device_solve: restarted flexible GMRES,
                         src/krylov/bcknd/device/gmres_device.F90:319-487 */
+  NB_KSP_PIPECG = 2  /* pipecg_device_solve: pipelined PCG, one fused
+                        reduction an iteration (src/krylov/bcknd/device/
+                        pipecg_device.F90); a symmetric preconditioner */
 } nb_ksp_type;
 
 typedef struct {
@@ -384,9 +387,10 @@ nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r, void *s
 
 /* Solves A x = f (f already assembled and masked) from x0 = 0 with
  * preconditioned CG (opts.ksp = NB_KSP_CG; cg_device_solve,
- * src/krylov/bcknd/device/cg_device.f90:162-238) or restarted flexible
- * GMRES (NB_KSP_GMRES; gmres_device_solve), entirely on the device with
- * device-resident scalars.  x and f are device arrays of n doubles. */
+ * src/krylov/bcknd/device/cg_device.f90:162-238), restarted flexible
+ * GMRES (NB_KSP_GMRES; gmres_device_solve) or pipelined CG (NB_KSP_PIPECG;
+ * pipecg_device_solve), entirely on the device with device-resident
+ * scalars.  x and f are device arrays of n doubles. */
 nb_status nb_solve(nb_problem *p, double *x, const double *f,
                    const nb_solve_opts *opts, nb_solve_result *res,
                    void *stream);

@@ -27,7 +27,8 @@ from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpt
 
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
-__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "KspMonitor",
+__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "PipeCG",
+           "KspMonitor",
            "Jacobi", "Hsmg", "Batch", "Projection", "ortho", "read_nmsh", "write_nmsh",
            "write_fld",
            "GS_OP_ADD", "NekoB200Error",
@@ -289,6 +290,13 @@ class FCG(CG):
 
     def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9, mixed=False):
         super().__init__(n, max_iter, M, abs_tol, mixed, flexible=True)
+
+
+class PipeCG(CG):
+    """ksp_t of type 'pipecg': pipelined PCG (pipecg_device_t,
+    src/krylov/bcknd/device/pipecg_device.F90), one reduction an
+    iteration.  For a symmetric preconditioner (Jacobi)."""
+    ksp = _lib.NB_KSP_PIPECG
 
 
 class GMRES(CG):

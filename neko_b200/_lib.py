@@ -21,7 +21,7 @@ STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR
                 7: "NB_ERR_TIMEOUT"}
 
 NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED = 0, 1, 2, 3
-NB_KSP_CG, NB_KSP_GMRES = 0, 1
+NB_KSP_CG, NB_KSP_GMRES, NB_KSP_PIPECG = 0, 1, 2
 NB_OK, NB_ERR_ARG, NB_ERR_UNSUPPORTED, NB_ERR_OOM, NB_ERR_CUDA = 0, 1, 2, 3, 4
 NB_ERR_NOT_CONVERGED, NB_ERR_NAN, NB_ERR_TIMEOUT = 5, 6, 7
 

@@ -355,6 +355,7 @@ using namespace nb;
 
 void nb_problem::invalidate_solver_cache() {
   gmres_invalidate(this);
+  pipecg_invalidate(this);
   if (solver_ws) {
     CgWorkspace *W = (CgWorkspace *)solver_ws;
     if (W->graph_exec) {
@@ -529,6 +530,8 @@ extern "C" nb_status nb_solve(nb_problem *p, double *x, const double *f,
   }
   if (opts->ksp == NB_KSP_GMRES)
     return gmres_solve(p, x, f, *opts, pc, res, (cudaStream_t)stream);
+  if (opts->ksp == NB_KSP_PIPECG)
+    return pipecg_solve(p, x, f, *opts, pc, res, (cudaStream_t)stream);
   if (opts->ksp != NB_KSP_CG) {
     set_error("unknown Krylov method");
     return NB_ERR_ARG;

@@ -83,6 +83,9 @@ struct CgRun {
 nb_status cg_start(CgRun &R);
 nb_status cg_next_chunk(CgRun &R);
 int cg_poll(CgRun &R, bool wait, nb_solve_result *res, nb_status *status);
+// Pipelined CG (pipecg.cu).
+nb_status pipecg_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
+                       Precond *pc, nb_solve_result *res, cudaStream_t s);
 // Restarted flexible GMRES (gmres.cu).
 nb_status gmres_solve(nb_problem *P, double *x, const double *f, const nb_solve_opts &o,
                       Precond *pc, nb_solve_result *res, cudaStream_t s);

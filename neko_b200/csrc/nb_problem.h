@@ -63,6 +63,7 @@ struct nb_problem {
   // Krylov workspaces (allocated on first solve)
   void *solver_ws = nullptr;
   void *gmres_ws = nullptr;
+  void *pipe_ws = nullptr;
   size_t solver_ws_bytes = 0;
   nb::HsmgState *hsmg[2] = {nullptr, nullptr};  // hsmg: [0] FP64, [1] mixed
 
@@ -78,6 +79,8 @@ namespace nb {
 void hsmg_free(nb_problem *p);
 void gmres_free(nb_problem *p);
 void gmres_invalidate(nb_problem *p);
+void pipecg_free(nb_problem *p);
+void pipecg_invalidate(nb_problem *p);
 // After new h1: the coarse levels take the new h1 (hsmg_set_h).
 cudaError_t hsmg_refresh_coefficients(nb_problem *p);
 // The same for constant coefficients, asynchronously on stream s.

@@ -183,6 +183,7 @@ nb_problem::~nb_problem() {
   if (arena) cudaFree(arena);
   if (solver_ws) delete (nb::CgWorkspace *)solver_ws;
   gmres_free(this);
+  pipecg_free(this);
   hsmg_free(this);
 }
 

@@ -365,6 +365,75 @@ int or_gmres_solve_impl(const OrProblem &P, double *x, const double *f, int max_
   return iter;
 }
 
+// Pipelined PCG of pipecg_device_solve (src/krylov/bcknd/device/
+// pipecg_device.F90): the inner products of an iteration come from the
+// previous vector pass (pipecg_vecops_kernel, cuda/pipecg_kernel.h); x is
+// updated through p = beta p + u_old, x += alpha p as cg_update_xp_kernel
+// does (here every iteration).
+int or_pipecg_solve_impl(const OrProblem &P, double *x, const double *f, int max_iter,
+                         double abs_tol, const std::function<void(double *, const double *)> &M,
+                         double *res_start, double *res_final) {
+  const long n = P.n;
+  std::vector<double> p(n, 0.0), q(n, 0.0), r(n), s(n, 0.0), u(n), w(n), z(n, 0.0), mi(n), ni(n);
+  const double norm_fac = 1.0 / std::sqrt(P.volume);
+  for (long i = 0; i < n; i++) {
+    x[i] = 0.0;
+    r[i] = f[i];
+  }
+  M(u.data(), r.data());
+  ax_helm(P, w.data(), u.data());
+  or_gs_add_impl(P, w.data());
+  bc_apply(P, w.data());
+  double rtr = glsc3(r.data(), P.mult.data(), r.data(), n);
+  double rnorm = std::sqrt(rtr) * norm_fac;
+  *res_start = rnorm;
+  *res_final = rnorm;
+  if (rnorm == 0.0) return 0;
+  double gamma1 = 0.0, gamma2, delta, alpha = 0.0, beta;
+  double red[3] = {glsc3(r.data(), P.mult.data(), u.data(), n),
+                   glsc3(w.data(), P.mult.data(), u.data(), n), rtr};
+  int iter;
+  for (iter = 1; iter <= max_iter; iter++) {
+    M(mi.data(), w.data());
+    ax_helm(P, ni.data(), mi.data());
+    or_gs_add_impl(P, ni.data());
+    bc_apply(P, ni.data());
+    gamma2 = gamma1;
+    gamma1 = red[0];
+    delta = red[1];
+    rtr = red[2];
+    rnorm = std::sqrt(rtr) * norm_fac;
+    if (rnorm < abs_tol) break;
+    if (iter > 1) {
+      beta = gamma1 / gamma2;
+      alpha = gamma1 / (delta - (beta * gamma1 / alpha));
+    } else {
+      beta = 0.0;
+      alpha = gamma1 / delta;
+    }
+    double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    for (long i = 0; i < n; i++) {
+      const double u1 = u[i];
+      p[i] = beta * p[i] + u1;
+      x[i] = x[i] + alpha * p[i];
+      z[i] = beta * z[i] + ni[i];
+      q[i] = beta * q[i] + mi[i];
+      s[i] = beta * s[i] + w[i];
+      r[i] = r[i] - alpha * s[i];
+      u[i] = u1 - alpha * q[i];
+      w[i] = w[i] - alpha * z[i];
+      t1 = t1 + r[i] * P.mult[i] * u[i];
+      t2 = t2 + w[i] * P.mult[i] * u[i];
+      t3 = t3 + r[i] * P.mult[i] * r[i];
+    }
+    red[0] = t1;
+    red[1] = t2;
+    red[2] = t3;
+  }
+  *res_final = rnorm;
+  return iter > max_iter ? max_iter : iter;
+}
+
 // projection_t with the device forms of its steps (src/common/projection.f90):
 // device_project_on (:553-622), bcknd_project_back (:317-358) and
 // device_proj_ortho (:638-714); tol = 1e-7 (:101).  Inner products are
@@ -473,6 +542,17 @@ void or_projection_destroy(OrProjection *J) { delete J; }
 void or_projection_project_on(OrProjection *J, double *b) { proj_project_on(*J, b); }
 void or_projection_project_back(OrProjection *J, double *x) { proj_project_back(*J, x); }
 int or_projection_m(OrProjection *J) { return J->m; }
+
+// Jacobi-preconditioned pipelined CG.
+int or_pipecg_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double abs_tol,
+                     double *res_start, double *res_final) {
+  std::vector<double> d;
+  jacobi_update(*P, d);
+  auto M = [&](double *z, const double *r) {
+    for (long i = 0; i < P->n; i++) z[i] = d[i] * r[i];
+  };
+  return or_pipecg_solve_impl(*P, x, f, max_iter, abs_tol, M, res_start, res_final);
+}
 
 // Jacobi-preconditioned restarted GMRES (m vectors a cycle).
 int or_gmres_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double abs_tol,

@@ -84,6 +84,7 @@ def lib():
                                              ctypes.c_int, _D, _D]),
             "or_gmres_jacobi": (ctypes.c_int, [_P, _D, _D, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, _D, _D]),
+            "or_pipecg_jacobi": (ctypes.c_int, [_P, _D, _D, ctypes.c_int, ctypes.c_double, _D, _D]),
             "or_projection_create": (_P, [_P, ctypes.c_int]),
             "or_genmeshbox_nmsh": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int] * 3 +
                                    [ctypes.c_double] * 6 + [ctypes.c_int] * 3),
@@ -244,6 +245,16 @@ class OracleProblem:
         r1 = ctypes.c_double()
         it = lib().or_cg_jacobi(self.h, _dp(x), _dp(f), max_iter, abs_tol,
                                 ctypes.byref(r0), ctypes.byref(r1))
+        return x, it, r0.value, r1.value
+
+    def pipecg_jacobi(self, f, max_iter, abs_tol):
+        """Jacobi-preconditioned pipelined CG (pipecg_device_solve)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        x = np.zeros_like(f)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        it = lib().or_pipecg_jacobi(self.h, _dp(x), _dp(f), max_iter, abs_tol,
+                                    ctypes.byref(r0), ctypes.byref(r1))
         return x, it, r0.value, r1.value
 
     def gmres_jacobi(self, f, max_iter, abs_tol, m_restart=30):

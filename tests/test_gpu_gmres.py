@@ -115,3 +115,21 @@ def test_gmres_max_iter_and_repeat(nb, oracle):
     assert it_o == 12
     assert torch.equal(x1, x) and m1.res_final == m2.res_final
     assert _cmp(_np(x1), xo, False) < 1e-9
+
+
+@pytest.mark.parametrize("nel,lx,h2", [((4, 4, 4), 6, 0.0), ((3, 4, 3), 8, 25.0)])
+def test_pipecg_jacobi_matches_oracle(nb, oracle, nel, lx, h2):
+    """Pipelined CG (NB_KSP_PIPECG) against the oracle's restatement of
+    pipecg_device_solve: iterations within +-1, solution 1e-7."""
+    P, O, b, r0 = _setup(nb, oracle, nel, lx, (False,) * 3, 0.05, 1.0, 11)
+    if h2:
+        P.set_coefficients_const(1.0, h2)
+        O.set_f64("h2", np.full(P.n, h2))
+        O.set_ifh2(True)
+    xo, it_o, rs_o, _ = O.pipecg_jacobi(b, 2000, 1e-10 * r0)
+    x = P.zeros()
+    mon = nb.PipeCG(max_iter=2000, abs_tol=1e-10 * r0, M=nb.Jacobi()).solve(
+        nb.AxHelm(), x, _cuda(b), P.n, P)
+    assert mon.converged and abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    assert abs(mon.res_start - rs_o) <= 1e-12 * rs_o
+    assert _cmp(_np(x), xo, False) < 1e-7
