@@ -38,6 +38,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # counted).
 FUSED_TRAFFIC_B_PER_POINT = {}
 
+# Algorithmic bytes of one gather-scatter add per local entry (a point that
+# shares its node with another element): its value read and written, and its
+# 4-byte map index.
+GS_B_PER_ENTRY = 20
+
 
 def measured_peaks():
     try:
@@ -311,15 +316,31 @@ def kernel_only(args, cfg):
     z = torch.rand(P.n, dtype=torch.float64, device="cuda")
     w = P.zeros()
     s = torch.cuda.Stream()
-    for _ in range(args.warmup + args.steps):
+
+    def launch():
         if args.kernel_only == "ax":
             nb.AxHelm().compute(w, u, P, stream=s)
         elif args.kernel_only == "fused":
             nb.AxHelm().update_p_compute(w, u, z, 0.5, P, stream=s)
         else:
             P.gs.op(u, P.n, stream=s)
+    for _ in range(args.warmup):
+        launch()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    print(json.dumps({"kernel": args.kernel_only, "n": P.n, "launches": args.warmup + args.steps}))
+    e0.record(s)
+    for _ in range(args.steps):
+        launch()
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    nbytes = {"ax": 72 * P.n, "fused": 88 * P.n, "gs": GS_B_PER_ENTRY * P.nlocal}[args.kernel_only]
+    peaks, src = measured_peaks()
+    gbs = nbytes / ms / 1e6
+    print(json.dumps({"kernel": args.kernel_only, "n": P.n, "entries": P.nlocal,
+                      "launches": args.warmup + args.steps, "ms_per_launch": ms,
+                      "bytes_per_launch": nbytes, "achieved_gbs": gbs,
+                      "frac": gbs / peaks["hbm_gbs"], "peak_source": src}))
 
 
 def run_batch(args):
@@ -779,9 +800,13 @@ def main():
             return sorted(loops)[1]
         t_fused = loop_time(lambda: Ax.update_p_compute(w, pd, zd, 0.0, P, pap=pap, stream=stream))
         t_ax = loop_time(lambda: Ax.compute(w, x64, P, stream=stream))
+        # the fine-level gather-scatter add, in place on a copy of x
+        gu = x64.clone()
+        t_gs = loop_time(lambda: P.gs.op(gu, P.n, stream=stream))
     peaks, peak_src = measured_peaks()
     fused_bytes = 88 * P.n  # z, p read; p, w written; h1, G11..G23 read
     ax_bytes = 72 * P.n     # u, w, h1, G11..G23
+    gs_bytes = GS_B_PER_ENTRY * P.nlocal
     achieved = fused_bytes / t_fused / 1e9
     traffic_pp = FUSED_TRAFFIC_B_PER_POINT.get(cfg["lx"])
     singular = all(cfg["periodic"])
@@ -819,6 +844,13 @@ def main():
                     "frac": ax_bytes / t_ax / 1e9 / peaks["hbm_gbs"],
                     "bytes_per_launch": ax_bytes, "launch_ms": t_ax * 1e3,
                     "gdof_s": P.n / t_ax / 1e9},
+        "gs": {"kernel": "gs_add_fused_kernel<double>",
+               "achieved": gs_bytes / t_gs / 1e9, "unit": "GB/s",
+               "frac": gs_bytes / t_gs / 1e9 / peaks["hbm_gbs"],
+               "entries": P.nlocal, "bytes_per_launch": gs_bytes,
+               "bytes_definition": f"{GS_B_PER_ENTRY} B per local entry (value read and "
+                                   f"written, 4 B index)",
+               "launch_ms": t_gs * 1e3},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
