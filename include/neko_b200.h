@@ -60,6 +60,26 @@ void cuda_ax_helm_vector(void *au, void *av, void *aw, void *u, void *v, void *w
 void cuda_ax_helm_vector_part2(void *au, void *av, void *aw, void *u, void *v, void *w,
                                void *h2, void *B, int *n);
 
+/* The full-stress operator of the velocity solve with variable viscosity,
+ * (au, av, aw) = A_stress (u, v, w): per point the symmetric gradient
+ * h1 w3 / jac (G + G^T) of the three components, G = cofactors^T grad, back
+ * through the cofactors and the transposed derivatives.  Replaces
+ * cuda_ax_helm_stress_vector (src/math/bcknd/device/cuda/ax_helm_full.cu,
+ * called from ax_helm_full_device_compute_vector,
+ * src/math/bcknd/device/ax_helm_full_device.F90:190-259); dxt, dyt, dzt are
+ * accepted and not read (the transposes come from dx, dy, dz, as in the
+ * reference kernel).  lx 2..16; launches on glb_cmd_queue. */
+void cuda_ax_helm_stress_vector(void *au, void *av, void *aw, void *u, void *v, void *w,
+                                void *dx, void *dy, void *dz, void *dxt, void *dyt, void *dzt,
+                                void *h1, void *drdx, void *drdy, void *drdz, void *dsdx,
+                                void *dsdy, void *dsdz, void *dtdx, void *dtdy, void *dtdz,
+                                void *jacinv, void *w3, int *nelv, int *lx);
+/* au += h2 B u, av += h2 B v, aw += h2 B w.  Replaces
+ * cuda_ax_helm_stress_vector_part2 (ax_helm_full.cu); launches on
+ * glb_cmd_queue. */
+void cuda_ax_helm_stress_vector_part2(void *au, void *av, void *aw, void *u, void *v,
+                                      void *w, void *h2, void *B, int *n);
+
 /* au += h2 B u for one component.  Replaces the addcol4 used for the h2
  * term of the scalar Ax (ax_helm_device.F90:253-255 ->
  * src/math/bcknd/device/cuda/math.cu:641). */
@@ -311,6 +331,14 @@ nb_status nb_ax(nb_problem *p, double *w, const double *u, void *stream);
  * (src/math/ax_helm.f90).  Asynchronous on `stream`. */
 nb_status nb_ax_vector(nb_problem *p, double *au, double *av, double *aw, const double *u,
                        const double *v, const double *w, void *stream);
+/* (au, av, aw) = A_stress (u, v, w), the full-stress operator (incl. the
+ * h2 B term when enabled), ax_helm_full_t%compute_vector
+ * (src/math/ax_helm_full.f90).  The cofactors of the coordinate map and
+ * 1/jac (10 arrays of n doubles) are built on the first call and kept with
+ * the problem; nb_problem_field also hands them out ("drdx" ... "dtdz",
+ * "jacinv").  Asynchronous on `stream`. */
+nb_status nb_ax_stress(nb_problem *p, double *au, double *av, double *aw, const double *u,
+                       const double *v, const double *w, void *stream);
 /* Synchronises `stream` and reports (then clears) the problem's error word:
  * NB_ERR_TIMEOUT when an earlier asynchronous call on this problem had a
  * bounded device wait expire.  No counterpart in the reference, whose
@@ -370,6 +398,26 @@ typedef struct {
   int converged;
   int launches;  /* kernels this solve launched on the device */
 } nb_solve_result;
+
+/* Operators of the coupled three-component solve. */
+typedef enum {
+  NB_AX_HELM_VECTOR = 0, /* ax_helm on each component (ax_helm_t%compute_vector) */
+  NB_AX_STRESS = 1       /* the full-stress operator (ax_helm_full_t) */
+} nb_ax_op;
+
+/* Solves the coupled system A (x, y, z) = (fx, fy, fz) for the three
+ * velocity components from zero with CG sharing one set of scalars
+ * (cg_cpld_device_solve, src/krylov/bcknd/device/cg_cpld_device.f90:
+ * 292-417): inner products summed over the components, gs add and the
+ * zero-Dirichlet mask on each component, opts.pc NB_PC_JACOBI (the
+ * problem's Jacobi diagonal on each component) or NB_PC_NONE (anything
+ * else: NB_ERR_UNSUPPORTED), opts.max_iter and opts.abs_tol as nb_solve;
+ * the other options are ignored.  op is an nb_ax_op.  Device arrays of n
+ * doubles; synchronous on `stream`.  The reference's three monitors carry
+ * the same values; res is one of them. */
+nb_status nb_solve_coupled(nb_problem *p, int op, double *x, double *y, double *z,
+                           const double *fx, const double *fy, const double *fz,
+                           const nb_solve_opts *opts, nb_solve_result *res, void *stream);
 
 /* Builds (or rebuilds, when the settings changed) the problem's hsmg
  * preconditioner: levels lx -> 4 -> 2, Schwarz/FDM smoothers, coarse

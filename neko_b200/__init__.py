@@ -22,12 +22,13 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib
-from ._lib import (NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error, SolveOpts,
-                   SolveResult, check, load)
+from ._lib import (NB_ERR_ARG, NB_PC_HSMG, NB_PC_JACOBI, NB_PC_NONE, NekoB200Error,
+                   SolveOpts, SolveResult, check, load)
 
 GS_OP_ADD = 1  # src/gs/gs_ops.f90:36
 
-__all__ = ["Problem", "AxHelm", "GatherScatter", "BcList", "CG", "FCG", "GMRES", "PipeCG",
+__all__ = ["Problem", "AxHelm", "AxHelmFull", "CoupledCG", "GatherScatter", "BcList", "CG",
+           "FCG", "GMRES", "PipeCG",
            "KspMonitor",
            "Jacobi", "Hsmg", "Batch", "Projection", "ortho", "read_nmsh", "write_nmsh",
            "write_fld",
@@ -194,6 +195,23 @@ class AxHelm:
                                     _stream_handle(stream)))
 
 
+class AxHelmFull:
+    """ax_helm_full_t: the full-stress operator of the velocity solve with
+    variable viscosity (src/math/ax_helm_full.f90); it acts on the three
+    components together only, as the reference's does."""
+
+    op = _lib.NB_AX_STRESS
+
+    def compute(self, w, u, coef, msh=None, Xh=None, stream=None):
+        raise NekoB200Error(NB_ERR_ARG, "the full Helmholtz operator cannot be applied to a "
+                                        "single field; use compute_vector and a coupled "
+                                        "solver (CoupledCG)")
+
+    def compute_vector(self, au, av, aw, u, v, w, coef, msh=None, Xh=None, stream=None):
+        check(load().nb_ax_stress(coef.handle, _ptr(au), _ptr(av), _ptr(aw), _ptr(u), _ptr(v),
+                                  _ptr(w), _stream_handle(stream)))
+
+
 class GatherScatter:
     """gs_t of a problem: op(u, n, GS_OP_ADD) sums all local copies."""
 
@@ -309,6 +327,35 @@ class GMRES(CG):
                  m_restart=30):
         super().__init__(n, max_iter, M, abs_tol, mixed)
         self.m_restart = m_restart
+
+
+class CoupledCG:
+    """ksp_t of type 'cpldcg' (cg_cpld_device_t,
+    src/krylov/bcknd/device/cg_cpld_device.f90): CG on the three velocity
+    components with one set of scalars; Ax is AxHelm (ax_helm on each
+    component) or AxHelmFull (the full-stress operator); M is Jacobi or
+    None.  solve() on one field is refused, as in the reference."""
+
+    def __init__(self, n=None, max_iter=1000, M=None, abs_tol=1e-9):
+        self.max_iter, self.abs_tol = max_iter, abs_tol
+        self.M = M if M is not None else Jacobi()
+
+    def solve(self, *args, **kwargs):
+        raise NekoB200Error(NB_ERR_ARG, "the cpldcg solver is only defined for coupled solves")
+
+    def solve_coupled(self, Ax, x, y, z, fx, fy, fz, n=None, coef=None, blstx=None, blsty=None,
+                      blstz=None, gs_h=None, niter=None, stream=None):
+        o = SolveOpts()
+        o.max_iter = niter if niter is not None else self.max_iter
+        o.abs_tol = self.abs_tol
+        o.pc = getattr(self.M, "kind", NB_PC_NONE) if self.M is not None else NB_PC_NONE
+        op = getattr(Ax, "op", _lib.NB_AX_HELM_VECTOR)
+        r = SolveResult()
+        check(load().nb_solve_coupled(coef.handle, op, _ptr(x), _ptr(y), _ptr(z), _ptr(fx),
+                                      _ptr(fy), _ptr(fz), ctypes.byref(o), ctypes.byref(r),
+                                      _stream_handle(stream)))
+        mon = KspMonitor(r.iter, r.res_start, r.res_final, bool(r.converged), r.launches)
+        return [mon, mon, mon]
 
 
 class Projection:

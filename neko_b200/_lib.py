@@ -22,6 +22,7 @@ STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR
 
 NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED = 0, 1, 2, 3
 NB_KSP_CG, NB_KSP_GMRES, NB_KSP_PIPECG = 0, 1, 2
+NB_AX_HELM_VECTOR, NB_AX_STRESS = 0, 1
 NB_OK, NB_ERR_ARG, NB_ERR_UNSUPPORTED, NB_ERR_OOM, NB_ERR_CUDA = 0, 1, 2, 3, 4
 NB_ERR_NOT_CONVERGED, NB_ERR_NAN, NB_ERR_TIMEOUT = 5, 6, 7
 
@@ -52,6 +53,8 @@ SIGNATURES = {
     "cuda_addcol4": (None, [_P, _P, _P, _P, _IP, _P]),
     "cuda_ax_helm_vector": (None, [_P] * 19 + [_IP, _IP]),
     "cuda_ax_helm_vector_part2": (None, [_P] * 8 + [_IP]),
+    "cuda_ax_helm_stress_vector": (None, [_P] * 24 + [_IP, _IP]),
+    "cuda_ax_helm_stress_vector_part2": (None, [_P] * 8 + [_IP]),
     "cuda_gather_kernel": (None, [_P, _IP, _IP, _P, _P, _IP, _P, _IP, _P, _P, _IP, _P]),
     "cuda_scatter_kernel": (None, [_P, _IP, _P, _P, _IP, _P, _IP, _P, _P, _P]),
     "cuda_glsc3": (ctypes.c_double, [_P, _P, _P, _IP, _P]),
@@ -102,6 +105,9 @@ SIGNATURES = {
     "nb_ax": (_I, [_P, _P, _P, _P]),
     "nb_problem_sync": (_I, [_P, _P]),
     "nb_ax_vector": (_I, [_P] * 8),
+    "nb_ax_stress": (_I, [_P] * 8),
+    "nb_solve_coupled": (_I, [_P, _I] + [_P] * 6 + [ctypes.POINTER(SolveOpts),
+                                                  ctypes.POINTER(SolveResult), _P]),
     "nb_ax_update_p": (_I, [_P, _P, _P, _P, ctypes.c_double, _P, _P]),
     "nb_gs_add": (_I, [_P, _P, _P]),
     "nb_bc_apply": (_I, [_P, _P, _P]),

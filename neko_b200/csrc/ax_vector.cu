@@ -40,10 +40,12 @@ __global__ void __launch_bounds__(AxVecCfg<LX, S, KS>::THREADS)
                       const double *__restrict__ h1, const double *__restrict__ g11,
                       const double *__restrict__ g22, const double *__restrict__ g33,
                       const double *__restrict__ g12, const double *__restrict__ g13,
-                      const double *__restrict__ g23, const int nelv, int *__restrict__ err) {
+                      const double *__restrict__ g23, const int nelv, int *__restrict__ err,
+                      const int *__restrict__ skip) {
   using C = AxVecCfg<LX, S, KS>;
   constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS;
   static_assert(LX % KS == 0, "k split must divide lx");
+  if (skip && *skip) return;
   extern __shared__ __align__(128) unsigned char smem_vec[];
   double *stage = reinterpret_cast<double *>(smem_vec);
   double *sur = stage + S * NA * L3, *sus = sur + L3, *sut = sus + L3;
@@ -163,7 +165,8 @@ template <int LX, int S, int KS>
 static cudaError_t launch_vec(const VecIo &io, const double *D, const double *Dt,
                               const double *h1, const double *g11, const double *g22,
                               const double *g33, const double *g12, const double *g13,
-                              const double *g23, int nelv, cudaStream_t st, int *err) {
+                              const double *g23, int nelv, cudaStream_t st, int *err,
+                              const int *skip) {
   using C = AxVecCfg<LX, S, KS>;
   auto kern = ax_vec_tma_kernel<LX, S, KS>;
   static int grid_per_dev[64] = {0};
@@ -184,7 +187,7 @@ static cudaError_t launch_vec(const VecIo &io, const double *D, const double *Dt
   if (!err) return cudaErrorInvalidSymbol;
   const int grid = nelv < g ? nelv : g;
   kern<<<grid, C::THREADS, C::SMEM, st>>>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv,
-                                          err);
+                                          err, skip);
   return cudaGetLastError();
 }
 
@@ -196,7 +199,7 @@ cudaError_t ax_helm_vector(double *au, double *av, double *aw, const double *u,
                            const double *Dt, const double *h1, const double *g11,
                            const double *g22, const double *g33, const double *g12,
                            const double *g13, const double *g23, int nelv, int lx,
-                           cudaStream_t s, int *err) {
+                           cudaStream_t s, int *err, const int *skip) {
   VecIo io{{au, av, aw}, {u, v, w}};
   bool aligned = true;
   const void *ptrs[] = {u, v, w, h1, g11, g22, g33, g12, g13, g23};
@@ -204,16 +207,16 @@ cudaError_t ax_helm_vector(double *au, double *av, double *aw, const double *u,
     if (reinterpret_cast<uintptr_t>(q) & 15) aligned = false;
   if (aligned) {
     switch (lx) {
-      case 4: return launch_vec<4, 4, 1>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err);
-      case 6: return launch_vec<6, 3, 2>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err);
-      case 8: return launch_vec<8, 2, 2>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err);
-      case 10: return launch_vec<10, 2, 5>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err);
+      case 4: return launch_vec<4, 4, 1>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err, skip);
+      case 6: return launch_vec<6, 3, 2>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err, skip);
+      case 8: return launch_vec<8, 2, 2>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err, skip);
+      case 10: return launch_vec<10, 2, 5>(io, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, s, err, skip);
       default: break;
     }
   }
   for (int c = 0; c < 3; c++) {
     cudaError_t e = ax_helm<double>(io.out[c], io.in[c], D, D, D, Dt, Dt, Dt, h1, g11, g22, g33,
-                                    g12, g13, g23, nelv, lx, s, nullptr);
+                                    g12, g13, g23, nelv, lx, s, skip);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -356,6 +356,7 @@ using namespace nb;
 void nb_problem::invalidate_solver_cache() {
   gmres_invalidate(this);
   pipecg_invalidate(this);
+  cpld_invalidate(this);
   if (solver_ws) {
     CgWorkspace *W = (CgWorkspace *)solver_ws;
     if (W->graph_exec) {

@@ -64,6 +64,12 @@ struct nb_problem {
   void *solver_ws = nullptr;
   void *gmres_ws = nullptr;
   void *pipe_ws = nullptr;
+  void *cpld_ws = nullptr;  // coupled three-component CG
+  // Cofactors of the coordinate Jacobian and 1/jac for the full-stress
+  // operator: 10 x n doubles (drdx, drdy, drdz, dsdx, dsdy, dsdz, dtdx,
+  // dtdy, dtdz, jacinv), built on first use.
+  double *cof = nullptr;
+  cudaError_t ensure_cofactors(cudaStream_t s);
   size_t solver_ws_bytes = 0;
   nb::HsmgState *hsmg[2] = {nullptr, nullptr};  // hsmg: [0] FP64, [1] mixed
 
@@ -81,6 +87,8 @@ void gmres_free(nb_problem *p);
 void gmres_invalidate(nb_problem *p);
 void pipecg_free(nb_problem *p);
 void pipecg_invalidate(nb_problem *p);
+void cpld_free(nb_problem *p);
+void cpld_invalidate(nb_problem *p);
 // After new h1: the coarse levels take the new h1 (hsmg_set_h).
 cudaError_t hsmg_refresh_coefficients(nb_problem *p);
 // The same for constant coefficients, asynchronously on stream s.

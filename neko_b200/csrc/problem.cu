@@ -184,7 +184,9 @@ nb_problem::~nb_problem() {
   if (solver_ws) delete (nb::CgWorkspace *)solver_ws;
   gmres_free(this);
   pipecg_free(this);
+  cpld_free(this);
   hsmg_free(this);
+  if (cof) cudaFree(cof);
 }
 
 static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
@@ -493,6 +495,17 @@ extern "C" nb_status nb_problem_field(const nb_problem *p, const char *name, voi
   for (auto &e : t)
     if (!strcmp(e.k, name)) {
       *dptr = const_cast<void *>(e.v);
+      return NB_OK;
+    }
+  // cofactors of the full-stress operator, built on first request
+  const char *cofn[10] = {"drdx", "drdy", "drdz", "dsdx", "dsdy",
+                          "dsdz", "dtdx", "dtdy", "dtdz", "jacinv"};
+  for (int a = 0; a < 10; a++)
+    if (!strcmp(cofn[a], name)) {
+      nb_problem *q = const_cast<nb_problem *>(p);
+      NB_TRY(q->ensure_cofactors(nullptr));
+      NB_TRY(cudaDeviceSynchronize());
+      *dptr = q->cof + (size_t)a * q->n;
       return NB_OK;
     }
   return fail(NB_ERR_ARG, std::string("unknown field ") + name);

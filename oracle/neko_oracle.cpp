@@ -1105,6 +1105,9 @@ void coef_init(OrProblem &P) {
     tz[i] = xr[i] * ys[i] - xs[i] * yr[i];
     P.jacinv[i] = 1.0 / j;  // invers2
   }
+  P.drdx = rx; P.drdy = ry; P.drdz = rz;
+  P.dsdx = sx; P.dsdy = sy; P.dsdz = sz;
+  P.dtdx = tx; P.dtdy = ty; P.dtdz = tz;
   P.g11.assign(n, 0);
   P.g22.assign(n, 0);
   P.g33.assign(n, 0);
@@ -1372,6 +1375,16 @@ void or_get_f64(OrProblem *P, const char *name, double *out) {
   if (!strcmp(name, "g13")) v = &P->g13;
   if (!strcmp(name, "g23")) v = &P->g23;
   if (!strcmp(name, "jac")) v = &P->jac;
+  if (!strcmp(name, "jacinv")) v = &P->jacinv;
+  if (!strcmp(name, "drdx")) v = &P->drdx;
+  if (!strcmp(name, "drdy")) v = &P->drdy;
+  if (!strcmp(name, "drdz")) v = &P->drdz;
+  if (!strcmp(name, "dsdx")) v = &P->dsdx;
+  if (!strcmp(name, "dsdy")) v = &P->dsdy;
+  if (!strcmp(name, "dsdz")) v = &P->dsdz;
+  if (!strcmp(name, "dtdx")) v = &P->dtdx;
+  if (!strcmp(name, "dtdy")) v = &P->dtdy;
+  if (!strcmp(name, "dtdz")) v = &P->dtdz;
   if (!strcmp(name, "B")) v = &P->B;
   if (!strcmp(name, "mult")) v = &P->mult;
   if (!strcmp(name, "h1")) v = &P->h1;

@@ -30,6 +30,9 @@ struct OrProblem {
   std::vector<int> local_dof_gs, local_gs_dof, blk_len, blk_off;
   // coef_t (src/sem/coef.f90)
   std::vector<double> g11, g22, g33, g12, g13, g23, jac, jacinv, B, mult, h1, h2;
+  // cofactors of the coordinate Jacobian (coef%drdx ... coef%dtdz,
+  // coef.f90:869-905): jac times the derivatives of r, s, t in x, y, z
+  std::vector<double> drdx, drdy, drdz, dsdx, dsdy, dsdz, dtdx, dtdy, dtdz;
   double volume = 0;
   bool ifh2 = false;
   // zero Dirichlet mask, 1-based (src/bc/bc.f90:434-593)

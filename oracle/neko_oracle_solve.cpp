@@ -74,6 +74,108 @@ void ax_helm(const OrProblem &P, double *w, const double *u) {
     for (long i = 0; i < P.n; i++) w[i] = w[i] + P.h2[i] * P.B[i] * u[i];
 }
 
+// ax_helm_stress_lx (src/math/bcknd/cpu/ax_helm_full_cpu.f90:181-375): the
+// full-stress operator on three components, grad in r, s, t per component,
+// physical gradient with the cofactors, symmetric strain scaled by
+// dj = h1 w3 / jac, back through the cofactors and the transposed
+// derivatives; then the h2 B term of ax_helm_full_compute_vector
+// (ax_helm_full_cpu.f90:164-176).
+void ax_helm_stress(const OrProblem &P, double *au, double *av, double *aw, const double *u,
+                    const double *v, const double *w) {
+  const int lx = P.lx, lxy = lx * lx, lxyz = lxy * lx;
+  const double *Dx = P.dx.data(), *Dxt = P.dxt.data();
+  auto D = [&](int i, int k) { return Dx[i + lx * k]; };
+  auto Dt = [&](int i, int k) { return Dxt[i + lx * k]; };
+  parallel_for(P.nelv, [&](long e0, long e1) {
+  std::vector<double> wr[3], ws[3], wt[3];
+  for (int c = 0; c < 3; c++) {
+    wr[c].assign(lxyz, 0.0);
+    ws[c].assign(lxyz, 0.0);
+    wt[c].assign(lxyz, 0.0);
+  }
+  for (long e = e0; e < e1; e++) {
+    const size_t o = (size_t)e * lxyz;
+    const double *in[3] = {u + o, v + o, w + o};
+    double *out[3] = {au + o, av + o, aw + o};
+    for (int c = 0; c < 3; c++) {
+      const double *ue = in[c];
+      for (int j = 0; j < lxy; j++)
+        for (int i = 0; i < lx; i++) {
+          double t = 0.0;
+          for (int k = 0; k < lx; k++) t = t + D(i, k) * ue[k + lx * j];
+          wr[c][i + lx * j] = t;
+        }
+      for (int k = 0; k < lx; k++)
+        for (int j = 0; j < lx; j++)
+          for (int i = 0; i < lx; i++) {
+            double t = 0.0;
+            for (int l = 0; l < lx; l++) t = t + D(j, l) * ue[i + lx * l + lxy * k];
+            ws[c][i + lx * j + lxy * k] = t;
+          }
+      for (int k = 0; k < lx; k++)
+        for (int i = 0; i < lxy; i++) {
+          double t = 0.0;
+          for (int l = 0; l < lx; l++) t = t + D(k, l) * ue[i + lxy * l];
+          wt[c][i + lxy * k] = t;
+        }
+    }
+    for (int i = 0; i < lxyz; i++) {
+      const size_t g = o + i;
+      const double rx = P.drdx[g], ry = P.drdy[g], rz = P.drdz[g];
+      const double sx = P.dsdx[g], sy = P.dsdy[g], sz = P.dsdz[g];
+      const double tx = P.dtdx[g], ty = P.dtdy[g], tz = P.dtdz[g];
+      double gr[3][3];  // gr[c][d]: jac * d(component c)/d(x_d)
+      for (int c = 0; c < 3; c++) {
+        gr[c][0] = wr[c][i] * rx + ws[c][i] * sx + wt[c][i] * tx;
+        gr[c][1] = wr[c][i] * ry + ws[c][i] * sy + wt[c][i] * ty;
+        gr[c][2] = wr[c][i] * rz + ws[c][i] * sz + wt[c][i] * tz;
+      }
+      const double dj = P.h1[g] * P.w3[i] * P.jacinv[g];
+      const double s11 = dj * (gr[0][0] + gr[0][0]);
+      const double s22 = dj * (gr[1][1] + gr[1][1]);
+      const double s33 = dj * (gr[2][2] + gr[2][2]);
+      const double s12 = dj * (gr[0][1] + gr[1][0]);
+      const double s13 = dj * (gr[0][2] + gr[2][0]);
+      const double s23 = dj * (gr[1][2] + gr[2][1]);
+      const double S[3][3] = {{s11, s12, s13}, {s12, s22, s23}, {s13, s23, s33}};
+      for (int c = 0; c < 3; c++) {
+        wr[c][i] = rx * S[c][0] + ry * S[c][1] + rz * S[c][2];
+        ws[c][i] = sx * S[c][0] + sy * S[c][1] + sz * S[c][2];
+        wt[c][i] = tx * S[c][0] + ty * S[c][1] + tz * S[c][2];
+      }
+    }
+    for (int c = 0; c < 3; c++) {
+      double *we = out[c];
+      for (int j = 0; j < lxy; j++)
+        for (int i = 0; i < lx; i++) {
+          double t = 0.0;
+          for (int k = 0; k < lx; k++) t = t + Dt(i, k) * wr[c][k + lx * j];
+          we[i + lx * j] = t;
+        }
+      for (int k = 0; k < lx; k++)
+        for (int j = 0; j < lx; j++)
+          for (int i = 0; i < lx; i++) {
+            double t = 0.0;
+            for (int l = 0; l < lx; l++) t = t + Dt(j, l) * ws[c][i + lx * l + lxy * k];
+            we[i + lx * j + lxy * k] = we[i + lx * j + lxy * k] + t;
+          }
+      for (int k = 0; k < lx; k++)
+        for (int i = 0; i < lxy; i++) {
+          double t = 0.0;
+          for (int l = 0; l < lx; l++) t = t + Dt(k, l) * wt[c][i + lxy * l];
+          we[i + lxy * k] = we[i + lxy * k] + t;
+        }
+    }
+  }
+  });
+  if (P.ifh2)
+    for (long i = 0; i < P.n; i++) {
+      au[i] = au[i] + P.h2[i] * P.B[i] * u[i];
+      av[i] = av[i] + P.h2[i] * P.B[i] * v[i];
+      aw[i] = aw[i] + P.h2[i] * P.B[i] * w[i];
+    }
+}
+
 // zero_dirichlet apply (src/bc/zero_dirichlet.f90:92-172): x(msk) = 0.
 void bc_apply(const OrProblem &P, double *x) {
   for (int m : P.msk) x[m - 1] = 0.0;
@@ -527,6 +629,83 @@ int or_cg_jacobi(OrProblem *P, double *x, const double *f, int max_iter, double 
     for (long i = 0; i < P->n; i++) z[i] = r[i] * d[i];  // col3 (pc_jacobi.f90:86-92)
   };
   return or_cg_solve_impl(*P, x, f, max_iter, abs_tol, M, res_start, res_final);
+}
+
+void or_ax_helm_stress(OrProblem *P, double *au, double *av, double *aw, const double *u,
+                       const double *v, const double *w) {
+  ax_helm_stress(*P, au, av, aw, u, v, w);
+}
+
+// cg_cpld_device_solve (src/krylov/bcknd/device/cg_cpld_device.f90:292-417):
+// CG on three components with one set of scalars, z_c = M r_c per component
+// (Jacobi here, or none), (a, mult b) summed over the components
+// (device_vdot3 then glsc2), the operator either the full-stress one
+// (stress != 0) or ax_helm on each component; gs add and the mask per
+// component (rotate_cyc is the identity without cyclic boundaries).
+// Returns the iteration count.
+int or_cg_coupled(OrProblem *P, double *x, double *y, double *z, const double *fx,
+                  const double *fy, const double *fz, int max_iter, double abs_tol, int stress,
+                  int jacobi, double *res_start, double *res_final) {
+  const long n = P->n;
+  std::vector<double> d;
+  if (jacobi) jacobi_update(*P, d);
+  std::vector<double> r[3], zz[3], p[3], ww[3], tmp(n);
+  double *xs[3] = {x, y, z};
+  const double *fs[3] = {fx, fy, fz};
+  for (int c = 0; c < 3; c++) {
+    r[c].assign(fs[c], fs[c] + n);
+    zz[c].assign(n, 0.0);
+    p[c].assign(n, 0.0);
+    ww[c].assign(n, 0.0);
+    for (long i = 0; i < n; i++) xs[c][i] = 0.0;
+  }
+  const double norm_fac = 1.0 / std::sqrt(P->volume);
+  auto vdot3 = [&](std::vector<double> *a, std::vector<double> *b) {
+    for (long i = 0; i < n; i++)
+      tmp[i] = a[0][i] * b[0][i] + a[1][i] * b[1][i] + a[2][i] * b[2][i];
+    double s = 0.0;  // glsc2(tmp, mult)
+    for (long i = 0; i < n; i++) s = s + tmp[i] * P->mult[i];
+    return s;
+  };
+  double rtz1 = 1.0, rtz2;
+  double rtr = vdot3(r, r);
+  double rnorm = std::sqrt(rtr) * norm_fac;
+  *res_start = rnorm;
+  *res_final = rnorm;
+  if (rnorm == 0.0) return 0;
+  int iter;
+  for (iter = 1; iter <= max_iter; iter++) {
+    for (int c = 0; c < 3; c++)
+      for (long i = 0; i < n; i++) zz[c][i] = jacobi ? d[i] * r[c][i] : r[c][i];
+    rtz2 = rtz1;
+    rtz1 = vdot3(zz, r);
+    double beta = rtz1 / rtz2;
+    if (iter == 1) beta = 0.0;
+    for (int c = 0; c < 3; c++)
+      for (long i = 0; i < n; i++) p[c][i] = zz[c][i] + beta * p[c][i];  // add2s1
+    if (stress) {
+      ax_helm_stress(*P, ww[0].data(), ww[1].data(), ww[2].data(), p[0].data(), p[1].data(),
+                     p[2].data());
+    } else {
+      for (int c = 0; c < 3; c++) ax_helm(*P, ww[c].data(), p[c].data());
+    }
+    for (int c = 0; c < 3; c++) {
+      or_gs_add_impl(*P, ww[c].data());
+      bc_apply(*P, ww[c].data());
+    }
+    const double pap = vdot3(ww, p);
+    const double alpha = rtz1 / pap, alphm = -alpha;
+    for (int c = 0; c < 3; c++)
+      for (long i = 0; i < n; i++) {
+        xs[c][i] = xs[c][i] + alpha * p[c][i];  // opadd2cm
+        r[c][i] = r[c][i] + alphm * ww[c][i];
+      }
+    rtr = vdot3(r, r);
+    rnorm = std::sqrt(rtr) * norm_fac;
+    if (rnorm < abs_tol) break;
+  }
+  *res_final = rnorm;
+  return iter > max_iter ? max_iter : iter;
 }
 
 OrProjection *or_projection_create(OrProblem *P, int L) {

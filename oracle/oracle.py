@@ -92,6 +92,10 @@ def lib():
             "or_projection_project_on": (None, [_P, _D]),
             "or_projection_project_back": (None, [_P, _D]),
             "or_projection_m": (ctypes.c_int, [_P]),
+            "or_ax_helm_stress": (None, [_P, _D, _D, _D, _D, _D, _D]),
+            "or_cg_coupled": (ctypes.c_int, [_P, _D, _D, _D, _D, _D, _D, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
+                                             _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -227,6 +231,26 @@ class OracleProblem:
         w = np.zeros_like(u)
         lib().or_ax_helm(self.h, _dp(w), _dp(u))
         return w
+
+    def ax_helm_stress(self, u, v, w):
+        """Full-stress operator on three components (ax_helm_stress_lx)."""
+        u, v, w = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w))
+        au, av, aw = np.zeros_like(u), np.zeros_like(u), np.zeros_like(u)
+        lib().or_ax_helm_stress(self.h, _dp(au), _dp(av), _dp(aw), _dp(u), _dp(v), _dp(w))
+        return au, av, aw
+
+    def cg_coupled(self, f, max_iter, abs_tol, stress=True, jacobi=True):
+        """Coupled CG on three components (cg_cpld_device_solve); f is a
+        sequence of three right-hand sides.  Returns ((x, y, z), iterations,
+        res_start, res_final)."""
+        fx, fy, fz = (np.ascontiguousarray(a, dtype=np.float64) for a in f)
+        x, y, z = np.zeros_like(fx), np.zeros_like(fx), np.zeros_like(fx)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        it = lib().or_cg_coupled(self.h, _dp(x), _dp(y), _dp(z), _dp(fx), _dp(fy), _dp(fz),
+                                 max_iter, abs_tol, int(stress), int(jacobi), ctypes.byref(r0),
+                                 ctypes.byref(r1))
+        return (x, y, z), it, r0.value, r1.value
 
     def bc_apply(self, x):
         x = np.array(x, dtype=np.float64, copy=True)
