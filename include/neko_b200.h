@@ -281,9 +281,9 @@ nb_status nb_problem_create_box(const int nel[3], const double lo[3],
  * the optional sine deformation of nb_problem_create_box, the gather-scatter
  * maps follow gs_init_mapping entry for entry for any relative rotation of
  * neighbouring elements.  Faces with no neighbour become zero-Dirichlet when
- * dirichlet_boundary is non-zero.  Jacobi-preconditioned solves accept any
- * conforming mesh; hsmg needs neighbours that meet through opposite faces
- * with the same orientation (NB_ERR_UNSUPPORTED otherwise). */
+ * dirichlet_boundary is non-zero.  Every solver and preconditioner accepts
+ * any conforming mesh; hsmg's Schwarz ghost exchange follows each face
+ * pairing (neighbour face and in-face orientation from the corner ids). */
 nb_status nb_problem_create_mesh(int nelv, const int *vertex_ids, const double *vertex_xyz,
                                  int lx, double deform_amp, int dirichlet_boundary,
                                  nb_problem **out);

@@ -36,6 +36,19 @@ namespace nb {
 // Kernels
 // ---------------------------------------------------------------------------
 
+// Orientation of a face pairing (general meshes): bits 0-2 the neighbour's
+// face nf, bit 3 swaps the two in-face coordinates, bits 4 and 5 reverse the
+// first / second.  Maps the position (s1, s2) (1-based, 1..lx; s1 along the
+// lower of the two in-face axes) on this element's face to (t1, t2) on the
+// neighbour's face nf.
+__device__ __forceinline__ void face_map(unsigned code, int lx, int s1, int s2, int &nf, int &t1,
+                                         int &t2) {
+  nf = code & 7;
+  int u1 = (code & 8) ? s2 : s1, u2 = (code & 8) ? s1 : s2;
+  t1 = (code & 16) ? lx + 1 - u1 : u1;
+  t2 = (code & 32) ? lx + 1 - u2 : u2;
+}
+
 // e = S (D^-1) S' r on the extended element (NL = lx + 2 points a side),
 // ghost layer gathered from the neighbours (fn: 1-based neighbour per face,
 // 0 = none).  One block (one warp; two for NL >= 13) per element holds the
@@ -195,7 +208,8 @@ __device__ __forceinline__ void fdm_pass(const T *__restrict__ src, T *__restric
 
 template <typename TIN, typename T, int NL>
 __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
-    fdm_kernel(const TIN *__restrict__ r, const int *__restrict__ fn, const T *__restrict__ S,
+    fdm_kernel(const TIN *__restrict__ r, const int *__restrict__ fn,
+               const unsigned char *__restrict__ ornt, const T *__restrict__ S,
                const T *__restrict__ lam, const T *__restrict__ eps, T *__restrict__ out,
                int nelv, const int *__restrict__ skip) {
   if (skip && *skip) return;
@@ -226,10 +240,15 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
     for (int q = u; q < 6 * L2; q += LPE) {  // faces: the neighbour's first interior layer
       const int f = q / L2, w = q - f * L2, s1 = w % LX + 1, s2 = w / LX + 1, dir = f >> 1;
       const int cb = (f & 1) ? NL - 1 : 0;   // ghost coordinate across the face
-      const int cs = (f & 1) ? 2 : LX - 1;   // its source: the neighbour's layer 1 / LX-2
       const int a = dir == 0 ? cb : s1, b = dir == 1 ? cb : (dir == 0 ? s1 : s2),
                 c = dir == 2 ? cb : s2;
-      const int sa = dir == 0 ? cs : a, sb = dir == 1 ? cs : b, sc = dir == 2 ? cs : c;
+      // its source: the neighbour's first interior layer behind its face nf,
+      // at the face position (t1, t2) of (s1, s2) in the neighbour's frame
+      int nf = f ^ 1, t1 = s1, t2 = s2;
+      if (ornt) face_map(__ldg(ornt + e * 6 + f), LX, s1, s2, nf, t1, t2);
+      const int ndir = nf >> 1, cs = (nf & 1) ? LX - 1 : 2;
+      const int sa = ndir == 0 ? cs : t1, sb = ndir == 1 ? cs : (ndir == 0 ? t1 : t2),
+                sc = ndir == 2 ? cs : t2;
       const int nb = __ldg(fn + e * 6 + f);
       gather_elem<TIN, T>(b0 + C::pos(b + NL * c, a),
                           nb ? r + (long)(nb - 1) * L3 + (sa - 1) + LX * (sb - 1) + L2 * (sc - 1)
@@ -292,8 +311,8 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
 template <typename T, int LX>
 __global__ void __launch_bounds__(256)
     schwarz_post_kernel(const T *__restrict__ ext, const int *__restrict__ fn,
-                        const T *__restrict__ wt, T *__restrict__ out, long nelv,
-                        const int *__restrict__ skip) {
+                        const unsigned char *__restrict__ ornt, const T *__restrict__ wt,
+                        T *__restrict__ out, long nelv, const int *__restrict__ skip) {
   if (skip && *skip) return;
   constexpr int NL = LX + 2, L2 = LX * LX, L3 = L2 * LX, N2 = NL * NL, N3 = N2 * NL;
   const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -308,8 +327,22 @@ __global__ void __launch_bounds__(256)
                      j == LX - 2 && f[3], k == 1 && f[4], k == LX - 2 && f[5]};
   const long in = (long)NL * (j + 1) + (long)N2 * (k + 1), jn = (i + 1) + (long)N2 * (k + 1),
              kn = (i + 1) + (long)NL * (j + 1);
-  const long off[6] = {(NL - 1) + in, 0 + in, NL * (NL - 1) + jn, 0 + jn, N2 * (NL - 1) + kn,
-                       0 + kn};
+  long off[6] = {(NL - 1) + in, 0 + in, NL * (NL - 1) + jn, 0 + jn, N2 * (NL - 1) + kn,
+                 0 + kn};
+  if (ornt) {  // general mesh: the ghost result sits on the neighbour's face nf
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+      if (!c[d]) continue;
+      const int dir = d >> 1;
+      const int s1 = (dir == 0 ? j : i) + 1, s2 = (dir == 2 ? j : k) + 1;
+      int nf, t1, t2;
+      face_map(__ldg(ornt + e * 6 + d), LX, s1, s2, nf, t1, t2);
+      const int nd = nf >> 1, cg = (nf & 1) ? NL - 1 : 0;
+      const int a = nd == 0 ? cg : t1, b = nd == 1 ? cg : (nd == 0 ? t1 : t2),
+                cc = nd == 2 ? cg : t2;
+      off[d] = a + (long)NL * b + (long)N2 * cc;
+    }
+  }
   T g[6];
 #pragma unroll
   for (int d = 0; d < 6; d++) g[d] = c[d] ? ext[(long)(f[d] - 1) * N3 + off[d]] : T(0);
@@ -442,6 +475,7 @@ struct SchwarzLevel {
   nb_problem *P = nullptr;  // the level's problem (gs maps, mask)
   T *S = nullptr, *lam = nullptr, *eps = nullptr, *wt = nullptr, *ext = nullptr;
   int *fn = nullptr;
+  const unsigned char *ornt = nullptr;  // face pairings of a general mesh (null: aligned)
 };
 
 template <typename TIN, typename T, int LX>
@@ -460,11 +494,10 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
     attr_set = true;
   }
   kern<<<(unsigned)((L.nelv + C::EPW - 1) / C::EPW), C::TPE, C::SMEM, s>>>(
-      r, L.fn, L.S, L.lam, L.eps, L.ext, (int)L.nelv,
-                                                   skip);
+      r, L.fn, L.ornt, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
   const long n = L.nelv * LX * LX * LX;
-  schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.ext, L.fn, L.wt, e,
-                                                                        L.nelv, skip);
+  schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      L.ext, L.fn, L.ornt, L.wt, e, L.nelv, skip);
   return cudaGetLastError();
 }
 
@@ -705,6 +738,53 @@ struct SchwarzHost {
   std::vector<int> fn;
 };
 
+// Face pairings of a general mesh for the Schwarz ghost exchange: for every
+// element face with a neighbour, the neighbour's face that meets it (its
+// opposite face preferred when several qualify, as on a periodic direction
+// one element wide) and the map of the in-face coordinates, found by
+// matching the four corner vertex ids (symmetric vertex order: corner
+// (i, j, k) is vertex 1 + i + 2 j + 4 k).  The reference reaches the same
+// pairing through a gather-scatter on an (lx+2)-point numbering
+// (schwarz_init, src/math/schwarz.f90:112-171).  Codes as face_map reads
+// them; false when a face has no matching pairing.
+static bool face_pairings(long nelv, const std::vector<int> &ids, const std::vector<int> &fn,
+                          std::vector<unsigned char> &ornt) {
+  ornt.assign((size_t)nelv * 6, 0);
+  auto corner = [&](long e, int f, int b1, int b2) {
+    const int dir = f >> 1, side = f & 1;
+    const int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
+    const int v = (side << dir) | (b1 << a1) | (b2 << a2);
+    return ids[(size_t)e * 8 + v];
+  };
+  for (long e = 0; e < nelv; e++)
+    for (int f = 0; f < 6; f++) {
+      const int nb = fn[e * 6 + f];
+      if (!nb) continue;
+      const long n = nb - 1;
+      bool found = false;
+      for (int gi = 0; gi < 6 && !found; gi++) {
+        const int g = gi == 0 ? (f ^ 1) : (gi - 1 < (f ^ 1) ? gi - 1 : gi);
+        if (fn[n * 6 + g] != e + 1) continue;
+        for (int code = 0; code < 8 && !found; code++) {
+          const int sw = code & 1, f1 = (code >> 1) & 1, f2 = (code >> 2) & 1;
+          bool ok = true;
+          for (int b1 = 0; b1 < 2 && ok; b1++)
+            for (int b2 = 0; b2 < 2 && ok; b2++) {
+              const int u1 = sw ? b2 : b1, u2 = sw ? b1 : b2;
+              const int t1 = f1 ? 1 - u1 : u1, t2 = f2 ? 1 - u2 : u2;
+              ok = corner(e, f, b1, b2) == corner(n, g, t1, t2);
+            }
+          if (ok) {
+            ornt[e * 6 + f] = (unsigned char)(g | (sw << 3) | (f1 << 4) | (f2 << 5));
+            found = true;
+          }
+        }
+      }
+      if (!found) return false;
+    }
+  return true;
+}
+
 static nb_status build_schwarz_host(nb_problem *L, bool dirichlet, SchwarzHost &H) {
   std::vector<double> x(L->n), y(L->n), z(L->n);
   if (cudaMemcpy(x.data(), L->x, L->n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
@@ -741,7 +821,8 @@ static std::vector<T> cast_vec(const std::vector<double> &v) {
 // Allocates and fills the device side of HsmgImpl<T>.
 template <typename T>
 static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const SchwarzHost &hm,
-                             const std::vector<double> &Jfm, const std::vector<double> &Jmc) {
+                             const std::vector<double> &Jfm, const std::vector<double> &Jmc,
+                             const std::vector<unsigned char> &ornt) {
   nb_problem *P = H->fine, *M = H->mid, *C = H->crs;
   const long nelv = P->nelv, n = P->n, nm = M->n, nc = C->n;
   const int nlf = P->lx + 2, nlm = M->lx + 2;
@@ -756,6 +837,7 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
                o_Fm = c.take(hm.fn.size() * 4),
                o_Xm = c.take((size_t)nelv * nlm * nlm * nlm * sizeof(T));
   const size_t o_Jfm = c.take(Jfm.size() * sizeof(T)), o_Jmc = c.take(Jmc.size() * sizeof(T));
+  const size_t o_or = c.take(ornt.size());
   const size_t o_mf = f32 ? c.take(n * sizeof(T)) : 0, o_mm = c.take(nm * sizeof(T));
   const size_t o_zf = f32 ? c.take(n * sizeof(T)) : 0;
   const size_t o_wm = c.take(nm * sizeof(T)), o_em = c.take(nm * sizeof(T));
@@ -779,6 +861,7 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
   };
   setlev(H->sf, P, o_Sf, o_Lf, o_Ef, o_Wf, o_Ff, o_Xf);
   setlev(H->sm, M, o_Sm, o_Lm, o_Em, o_Wm, o_Fm, o_Xm);
+  if (!ornt.empty()) H->sf.ornt = H->sm.ornt = (const unsigned char *)(A + o_or);
   H->Jfm = Tp(o_Jfm), H->Jmc = Tp(o_Jmc);
   H->mult_f = f32 ? Tp(o_mf) : reinterpret_cast<T *>(P->mult);
   H->mult_m = Tp(o_mm);
@@ -824,6 +907,8 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
       upi(o_Ff, hf.fn) || upv(o_Sm, hm.S) || upv(o_Lm, hm.lam) || upv(o_Em, hm.eps) ||
       upv(o_Wm, hm.wt) || upi(o_Fm, hm.fn) || upv(o_Jfm, Jfm) || upv(o_Jmc, Jmc) ||
       upv(o_mm, hm_mult) || (f32 && upv(o_mf, hf_mult)) ||
+      (!ornt.empty() &&
+       cudaMemcpy(A + o_or, ornt.data(), ornt.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(A + o_st, &cs, sizeof(cs), cudaMemcpyHostToDevice) ||
       cudaMemset(A + o_part, 0, 2 * 2 * kCoarseMaxBlocks * sizeof(double) + 64))
     return hfail(NB_ERR_CUDA, "hsmg: upload failed");
@@ -846,11 +931,10 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   }
   const int lx = P->lx;
   if (lx < 3 || lx > 14) return hfail(NB_ERR_UNSUPPORTED, "hsmg supports lx 3..14");
-  if (!P->faces_aligned)
+  std::vector<unsigned char> ornt;  // face pairings (general meshes only)
+  if (!P->faces_aligned && !face_pairings(P->nelv, P->mesh_ids, P->fn, ornt))
     return hfail(NB_ERR_UNSUPPORTED,
-                 "hsmg needs every face neighbour to meet through the opposite face with the "
-                 "same orientation (the direct Schwarz ghost exchange); this mesh has rotated "
-                 "neighbours");
+                 "hsmg: a face neighbour shares no face with matching corner vertices");
   const int lx_mid = lx < 5 ? std::max(lx - 1, 3) : 4, lx_crs = 2;
   HsmgState *H = mixed ? (HsmgState *)new HsmgImpl<float>() : (HsmgState *)new HsmgImpl<double>();
   H->fine = P;
@@ -889,8 +973,8 @@ nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out) {
   gll_space(lx_crs, zc, tmp, t2, t3);
   lagrange_matrix(zf, zm, Jfm);
   lagrange_matrix(zm, zc, Jmc);
-  st = mixed ? upload_impl((HsmgImpl<float> *)H, hf, hm, Jfm, Jmc)
-             : upload_impl((HsmgImpl<double> *)H, hf, hm, Jfm, Jmc);
+  st = mixed ? upload_impl((HsmgImpl<float> *)H, hf, hm, Jfm, Jmc, ornt)
+             : upload_impl((HsmgImpl<double> *)H, hf, hm, Jfm, Jmc, ornt);
   // The uploads ran on the legacy stream (a pageable cudaMemcpy may return
   // before its DMA lands); finish them before any caller stream reads them.
   if (st == NB_OK && cudaDeviceSynchronize() != cudaSuccess)

@@ -5,7 +5,8 @@ gs_init_mapping, coef_t on the same vertex ids and coordinates).
 Meshes: a box whose elements' local frames are turned by random cube
 rotations, so neighbours meet with arbitrary relative orientation.  Bars as
 for the box: geometric factors 1e-12 of their scale, ax_helm 1e-12, gather-
-scatter bit-exact, Jacobi-PCG iterations within +-1 and solutions 1e-7."""
+scatter bit-exact, Jacobi-PCG / GMRES / hsmg-FCG iterations within +-1 and
+solutions 1e-7, one hsmg apply 1e-10."""
 import numpy as np
 import pytest
 import torch
@@ -73,10 +74,38 @@ def test_rotated_mesh_matches_oracle(nb, oracle, nel, lx, seed, deform):
                                                                           _cuda(b), P.n, P)
     xgo, it_go, _, _ = O.gmres_jacobi(b, 2000, 1e-10 * r0)
     assert mg.converged and abs(mg.iter - it_go) <= 1, (mg.iter, it_go)
-    # hsmg needs aligned neighbours: a rotated mesh is refused, not mis-solved
-    with pytest.raises(nb.NekoB200Error) as ei:
-        nb.Hsmg().solve(P.zeros(), _cuda(b), P)
-    assert ei.value.status == 2
+
+
+@pytest.mark.parametrize("nel,lx,seed", [((3, 2, 4), 6, 1), ((3, 3, 3), 8, 2), ((2, 3, 2), 5, 3)])
+def test_rotated_mesh_hsmg_matches_oracle(nb, oracle, nel, lx, seed):
+    """hsmg on neighbours that meet with arbitrary relative orientation: the
+    Schwarz ghost exchange follows each face pairing (the reference reaches
+    it through a gather-scatter on the (lx+2)-point numbering).  One apply
+    within 1e-10 of the oracle's, flexible CG within +-1 iteration and 1e-7,
+    the mixed-precision solve within 1e-6 of the oracle's solution."""
+    P, O = _pair(nb, oracle, nel, lx, seed, 0.05)
+    rng = np.random.default_rng(seed)
+    H = oracle.OracleHsmg(O)
+    r = O.bc_apply(O.gs_add(rng.standard_normal(P.n)))
+    z = P.zeros()
+    nb.Hsmg().solve(z, _cuda(r), P)
+    torch.cuda.synchronize()
+    zo = H.apply(r)
+    assert np.abs(_np(z) - zo).max() <= 1e-10 * np.abs(zo).max()
+    b = O.bc_apply(O.gs_add(O.f64("B") * rng.standard_normal(P.n)))
+    r0 = np.sqrt(np.sum(b * O.f64("mult") * b) / O.volume)
+    xo, it_o, _, _ = H.cg(b, 300, 1e-9 * r0, flexible=True)
+    for mixed in (False, True):
+        x = P.zeros()
+        mon = nb.FCG(max_iter=300, abs_tol=1e-9 * r0, M=nb.Hsmg(mixed=mixed)).solve(
+            nb.AxHelm(), x, _cuda(b), P.n, P)
+        assert mon.converged
+        if mixed:
+            assert mon.iter <= it_o + 3, (mon.iter, it_o)
+            assert np.linalg.norm(_np(x) - xo) / np.linalg.norm(xo) < 1e-6
+        else:
+            assert abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+            assert np.abs(_np(x) - xo).max() / np.abs(xo).max() < 1e-7
 
 
 @pytest.mark.parametrize("nel,lx,periodic", [((4, 3, 4), 8, (True,) * 3),
