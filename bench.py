@@ -317,11 +317,17 @@ def kernel_only(args, cfg):
     w = P.zeros()
     s = torch.cuda.Stream()
 
+    if args.kernel_only == "stress":
+        v3 = [torch.rand(P.n, dtype=torch.float64, device="cuda") for _ in range(3)]
+        o3 = [P.zeros() for _ in range(3)]
+
     def launch():
         if args.kernel_only == "ax":
             nb.AxHelm().compute(w, u, P, stream=s)
         elif args.kernel_only == "fused":
             nb.AxHelm().update_p_compute(w, u, z, 0.5, P, stream=s)
+        elif args.kernel_only == "stress":
+            nb.AxHelmFull().compute_vector(*o3, *v3, P, stream=s)
         else:
             P.gs.op(u, P.n, stream=s)
     for _ in range(args.warmup):
@@ -334,7 +340,8 @@ def kernel_only(args, cfg):
     e1.record(s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
-    nbytes = {"ax": 72 * P.n, "fused": 88 * P.n, "gs": GS_B_PER_ENTRY * P.nlocal}[args.kernel_only]
+    nbytes = {"ax": 72 * P.n, "fused": 88 * P.n, "stress": 136 * P.n,
+              "gs": GS_B_PER_ENTRY * P.nlocal}[args.kernel_only]
     peaks, src = measured_peaks()
     gbs = nbytes / ms / 1e6
     print(json.dumps({"kernel": args.kernel_only, "n": P.n, "entries": P.nlocal,
@@ -441,6 +448,86 @@ def run_batch(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_velocity(args):
+    """The velocity solve of a time step with variable viscosity on the
+    config-2 mesh (periodic deformed box 32^3 hex, lx 8, three components of
+    16.8 M points): coupled Jacobi-CG (cg_cpld) with the full-stress
+    operator, h1 = 1 + 0.5 sin x sin y sin z (the viscosity field), h2 = 10
+    (the BDF mass term), each component's right-hand side B f_c assembled,
+    to 1e-8 relative; solves/s timed on the device, and the full-stress
+    operator timed alone with events (136 algorithmic bytes a point: u, v,
+    w, h1, 1/jac and nine cofactors read, three outputs written)."""
+    import numpy as np
+    import torch
+    import neko_b200 as nb
+    from neko_b200 import workloads
+    torch.cuda.set_device(0)
+    cfg = dict(workloads.CONFIG2)
+    cfg["lx"] = args.lx
+    P = build_problem(nb, cfg)
+    x, y, z, B = (P.field(k) for k in ("x", "y", "z", "B"))
+    h1 = 1.0 + 0.5 * torch.sin(x) * torch.sin(y) * torch.sin(z)
+    P.set_coefficients(h1.contiguous(), torch.full_like(h1, 10.0))
+    f = []
+    for c in range(3):
+        fc = (B * torch.sin(x + c) * torch.cos(2 * y - c) * torch.sin(3 * z + 0.5 * c)).contiguous()
+        P.gs.op(fc, P.n)
+        f.append(fc)
+    mult = P.field("mult")
+    r0 = math.sqrt(sum(float((fc * mult * fc).sum()) for fc in f) / P.volume)
+    tol = cfg["rel_tol"] * r0
+    xs = [P.zeros() for _ in range(3)]
+    solver = nb.CoupledCG(max_iter=2000, abs_tol=tol, M=nb.Jacobi())
+    Ax = nb.AxHelmFull()
+    s = torch.cuda.Stream()
+    mons = None
+    for _ in range(args.warmup):
+        mons = solver.solve_coupled(Ax, *xs, *f, P.n, P, stream=s)
+    out = [P.zeros() for _ in range(3)]
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            mons = solver.solve_coupled(Ax, *xs, *f, P.n, P, stream=s)
+        e1.record(s)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        # the operator alone (its inputs, 15 arrays of 134 MB, exceed L2)
+        for _ in range(5):
+            Ax.compute_vector(*out, *xs, P, stream=s)
+        reps = args.ax_reps
+        torch.cuda.synchronize()
+        e0.record(s)
+        for _ in range(reps):
+            Ax.compute_vector(*out, *xs, P, stream=s)
+        e1.record(s)
+        torch.cuda.synchronize()
+    t_op = e0.elapsed_time(e1) / 1e3 / reps
+    peaks, src = measured_peaks()
+    nbytes = 136 * P.n
+    gbs = nbytes / t_op / 1e9
+    line = {
+        "metric": "velocity solves/s to 1e-8 rel (coupled CG, full-stress operator)",
+        "value": args.steps / t, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic", "vs_baseline": None,
+        "config": {"workload": workload_name(cfg, "coupled Jacobi-CG, full-stress operator, "
+                                             "h1 = 1 + 0.5 sin x sin y sin z, h2 = 10")
+                   + ", three components", "iterations": mons[0].iter,
+                   "converged": mons[0].converged, "r0": r0},
+        "roofline": {"bound": "hbm", "kernel": f"ax_stress_tma_kernel<{cfg['lx']}> "
+                     "(nb_ax_stress, three components)", "achieved": gbs,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+                     "peak_source": src, "bytes_per_launch": nbytes, "launch_ms": t_op * 1e3,
+                     "traffic": None},
+        "gpu_launches": mons[0].launches * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    P.close()
 
 
 def run_axgs(args):
@@ -603,12 +690,15 @@ def main():
                     help="skip the CPU oracle solve (cpu_baseline and the parity fields)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision solve measured beside the FP64 one")
-    ap.add_argument("--kernel-only", choices=["ax", "fused", "gs", "solve"], default=None,
+    ap.add_argument("--kernel-only", choices=["ax", "fused", "gs", "stress", "solve"],
+                    default=None,
                     help="run only this kernel (or one FP64 + one mixed solve inside a "
                          "profiler window) on an nel^3 box (profiling case)")
-    ap.add_argument("--workload", choices=["solve", "axgs", "batch", "serve"], default="solve",
+    ap.add_argument("--workload", choices=["solve", "axgs", "batch", "serve", "velocity"],
+                    default="solve",
                     help="solve: the hsmg-FCG config-2 line (default); batch: batched "
-                         "uneven solves; serve: the served request stream")
+                         "uneven solves; serve: the served request stream; velocity: the "
+                         "coupled full-stress velocity solve on the config-2 mesh")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--max-solves", type=int, default=64,
                     help="per-problem hsmg solves running at once in the batch / server")
@@ -637,6 +727,8 @@ def main():
         return run_serve(args)
     if args.workload == "axgs":
         return run_axgs(args)
+    if args.workload == "velocity":
+        return run_velocity(args)
     world, rank, local = dist_setup()
 
     if args.impl == "reference":
