@@ -320,6 +320,23 @@ def kernel_only(args, cfg):
     if args.kernel_only == "stress":
         v3 = [torch.rand(P.n, dtype=torch.float64, device="cuda") for _ in range(3)]
         o3 = [P.zeros() for _ in range(3)]
+    if args.kernel_only in ("dropin_fdm", "dropin_tnsr3d"):
+        import ctypes
+        lib = nb.load()
+        nel, nl = P.nelv, P.lx + 2
+        ci = lambda v: ctypes.byref(ctypes.c_int(v))
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())
+        if args.kernel_only == "dropin_fdm":
+            fr = torch.rand(nel * nl ** 3, dtype=torch.float64, device="cuda")
+            fe = torch.zeros_like(fr)
+            fd = torch.rand_like(fr)
+            fs = torch.rand(nel * 6 * nl * nl, dtype=torch.float64, device="cuda")
+        else:
+            tu = torch.rand(P.n, dtype=torch.float64, device="cuda")
+            tv = torch.zeros(nel * 64, dtype=torch.float64, device="cuda")
+            tJ = torch.rand(4 * P.lx, dtype=torch.float64, device="cuda")
+            tJt = torch.rand(4 * P.lx, dtype=torch.float64, device="cuda")
+        dstream = ctypes.c_void_p(s.cuda_stream)
 
     def launch():
         if args.kernel_only == "ax":
@@ -328,6 +345,13 @@ def kernel_only(args, cfg):
             nb.AxHelm().update_p_compute(w, u, z, 0.5, P, stream=s)
         elif args.kernel_only == "stress":
             nb.AxHelmFull().compute_vector(*o3, *v3, P, stream=s)
+        elif args.kernel_only == "dropin_fdm":
+            lib.cuda_fdm_do_fast(vp(fe), vp(fr), vp(fs), vp(fd), ci(nl), ci(nel), dstream)
+        elif args.kernel_only == "dropin_tnsr3d":
+            with torch.cuda.stream(s):  # cuda_tnsr3d launches on the drop-in default stream
+                lib.nb_set_default_stream(dstream)
+                lib.cuda_tnsr3d(vp(tv), ci(4), vp(tu), ci(P.lx), vp(tJ), vp(tJt), vp(tJt),
+                                ci(nel))
         else:
             P.gs.op(u, P.n, stream=s)
     for _ in range(args.warmup):
@@ -340,8 +364,13 @@ def kernel_only(args, cfg):
     e1.record(s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    nl = P.lx + 2
     nbytes = {"ax": 72 * P.n, "fused": 88 * P.n, "stress": 136 * P.n,
-              "gs": GS_B_PER_ENTRY * P.nlocal}[args.kernel_only]
+              "gs": GS_B_PER_ENTRY * P.nlocal,
+              # r read and written, e written, d read, six nl x nl matrices read
+              "dropin_fdm": P.nelv * (4 * nl ** 3 + 6 * nl * nl) * 8,
+              # u read, v written (lx -> 4 points a side)
+              "dropin_tnsr3d": (P.n + P.nelv * 64) * 8}[args.kernel_only]
     peaks, src = measured_peaks()
     gbs = nbytes / ms / 1e6
     print(json.dumps({"kernel": args.kernel_only, "n": P.n, "entries": P.nlocal,
@@ -690,7 +719,8 @@ def main():
                     help="skip the CPU oracle solve (cpu_baseline and the parity fields)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision solve measured beside the FP64 one")
-    ap.add_argument("--kernel-only", choices=["ax", "fused", "gs", "stress", "solve"],
+    ap.add_argument("--kernel-only", choices=["ax", "fused", "gs", "stress", "dropin_fdm",
+                                              "dropin_tnsr3d", "solve"],
                     default=None,
                     help="run only this kernel (or one FP64 + one mixed solve inside a "
                          "profiler window) on an nel^3 box (profiling case)")

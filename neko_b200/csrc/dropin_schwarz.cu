@@ -4,7 +4,10 @@
 // results of the reference's CUDA backend.  The native hsmg path does not
 // use them (its Schwarz step reads ghost layers from the neighbours
 // directly); they exist so a Neko build that calls the reference's
-// Schwarz/FDM device routines can link this library.
+// Schwarz/FDM device routines can link this library.  cuda_fdm_do_fast runs
+// the native FDM passes for nl >= 8 and cuda_tnsr3d a compile-time-size
+// kernel for hsmg's interpolation pairs; other sizes take the general
+// kernels here.
 //
 // tnsr3d: v = (C x B x A) u per element, contracting the first index with
 // A (nv x nu), then the second with B (Bt stored nu x nv), then the third
@@ -62,6 +65,63 @@ __global__ void __launch_bounds__(kTnsrThreads)
   __syncthreads();
   tnsr3d_el(sv, nv, su, nu, A, Bt, Ct, w1, w2);
   for (int q = threadIdx.x; q < nv3; q += blockDim.x) v[e * nv3 + q] = sv[q];
+}
+
+// The same contraction with compile-time sizes (the interpolation pairs of
+// hsmg: fine <-> middle, middle <-> coarse): every loop unrolls, and the
+// matrices sit in shared memory beside the element.
+template <int NU, int NV>
+__global__ void __launch_bounds__(kTnsrThreads)
+    tnsr3d_fixed_kernel(double *__restrict__ v, const double *__restrict__ u,
+                        const double *__restrict__ A, const double *__restrict__ Bt,
+                        const double *__restrict__ Ct) {
+  constexpr int NU3 = NU * NU * NU, NV3 = NV * NV * NV, W1 = NV * NU * NU, W2 = NV * NV * NU;
+  __shared__ double su[NU3], w1[W1], w2[W2], sA[NV * NU], sB[NU * NV], sC[NU * NV];
+  const long e = blockIdx.x;
+  for (int q = threadIdx.x; q < NU3; q += kTnsrThreads) su[q] = u[e * NU3 + q];
+  for (int q = threadIdx.x; q < NU * NV; q += kTnsrThreads) {
+    sA[q] = A[q];
+    sB[q] = Bt[q];
+    sC[q] = Ct[q];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < W1; q += kTnsrThreads) {  // w1(i, jk)
+    const int i = q % NV, jk = q / NV;
+    double s = 0;
+#pragma unroll
+    for (int l = 0; l < NU; l++) s += sA[i + NV * l] * su[l + NU * jk];
+    w1[q] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < W2; q += kTnsrThreads) {  // w2(i, j, k)
+    const int i = q % NV, j = (q / NV) % NV, k = q / (NV * NV);
+    double s = 0;
+#pragma unroll
+    for (int l = 0; l < NU; l++) s += sB[l + NU * j] * w1[i + NV * l + NV * NU * k];
+    w2[q] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < NV3; q += kTnsrThreads) {
+    const int ij = q % (NV * NV), k = q / (NV * NV);
+    double s = 0;
+#pragma unroll
+    for (int l = 0; l < NU; l++) s += sC[l + NU * k] * w2[ij + NV * NV * l];
+    v[e * NV3 + q] = s;
+  }
+}
+
+static bool tnsr3d_fixed(double *v, int nv, const double *u, int nu, const double *A,
+                         const double *Bt, const double *Ct, int nel, cudaStream_t st) {
+#define NB_T(a, b)                                                                    \
+  if (nu == a && nv == b) {                                                           \
+    tnsr3d_fixed_kernel<a, b><<<nel, kTnsrThreads, 0, st>>>(v, u, A, Bt, Ct);          \
+    return true;                                                                      \
+  }
+  NB_T(5, 4) NB_T(6, 4) NB_T(7, 4) NB_T(8, 4) NB_T(9, 4) NB_T(10, 4) NB_T(11, 4) NB_T(12, 4)
+  NB_T(4, 5) NB_T(4, 6) NB_T(4, 7) NB_T(4, 8) NB_T(4, 9) NB_T(4, 10) NB_T(4, 11) NB_T(4, 12)
+  NB_T(4, 2) NB_T(2, 4) NB_T(3, 2) NB_T(2, 3) NB_T(4, 3) NB_T(3, 4)
+#undef NB_T
+  return false;
 }
 
 // fdm_do_fast (src/math/bcknd/device/cuda/fdm_kernel.h:38-137): per element
@@ -168,6 +228,11 @@ extern "C" void cuda_tnsr3d(void *v, int *nv, void *u, int *nu, void *A, void *B
     exit(1);
   }
   if (*nel <= 0) return;
+  if (tnsr3d_fixed((double *)v, *nv, (const double *)u, *nu, (const double *)A,
+                   (const double *)Bt, (const double *)Ct, *nel, default_stream())) {
+    cuda_check_fatal(cudaGetLastError(), "cuda_tnsr3d");
+    return;
+  }
   const size_t smem = 4 * (size_t)N * N * N * sizeof(double);
   set_smem((const void *)tnsr3d_kernel<double>, smem);
   tnsr3d_kernel<double><<<*nel, kTnsrThreads, smem, default_stream()>>>(
@@ -183,6 +248,14 @@ extern "C" void cuda_fdm_do_fast(void *e, void *r, void *s, void *d, int *nl, in
     exit(1);
   }
   if (*nel <= 0) return;
+  // nl >= 8: the native FDM passes (one warp per element, matrix rows as
+  // vector loads); smaller nl: the general kernel below
+  const cudaError_t fe = fdm_dropin((double *)e, (double *)r, (const double *)s,
+                                    (const double *)d, *nl, *nel, (cudaStream_t)stream);
+  if (fe != cudaErrorNotSupported) {
+    cuda_check_fatal(fe, "cuda_fdm_do_fast");
+    return;
+  }
   const int N3 = *nl * *nl * *nl;
   const size_t smem = (4 * (size_t)N3 + 6 * (size_t)*nl * *nl) * sizeof(double);
   set_smem((const void *)fdm_do_fast_kernel<double>, smem);

@@ -69,6 +69,11 @@ cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, 
                         CgState *st, double beta, double *pap_out, double *partials,
                         unsigned *counter, int max_grid, cudaStream_t s, int *err);
 
+// cuda_fdm_do_fast for nl 8..16 with the native FDM passes (pc_hsmg.cu);
+// cudaErrorNotSupported for other nl.
+cudaError_t fdm_dropin(double *eo, double *r, const double *s, const double *d, int nl, int nel,
+                       cudaStream_t st);
+
 // Grid size for streaming kernels: a multiple of the SM count.
 int stream_grid(long n, int threads);
 

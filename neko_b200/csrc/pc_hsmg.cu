@@ -518,6 +518,87 @@ static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, c
   return gs_add_fused<T>(L.P->gsd, e, true, s, skip);
 }
 
+// Drop-in form of the FDM (cuda_fdm_do_fast, src/math/bcknd/device/cuda/
+// fdm_kernel.h): the input is the caller's extended element itself, the
+// matrices are the caller's s(:,:,m,d) (m = 2, the transposed eigenvectors,
+// for the forward transform; m = 1 for the backward one) and the scaling is
+// the caller's full diagonal d, applied between the transforms and written
+// back to r as the reference does.  The passes are those of fdm_kernel (one
+// warp per element, vector matrix rows), so nl >= 8 only.
+template <int NL>
+__global__ void __launch_bounds__(FdmCfg<double, NL>::TPE, FdmCfg<double, NL>::MINB)
+    fdm_dropin_kernel(double *__restrict__ eo, double *__restrict__ r,
+                      const double *__restrict__ s, const double *__restrict__ d, int nelv) {
+  using T = double;
+  using C = FdmCfg<T, NL>;
+  static_assert(C::VEC && C::EPW == 1, "vector form only");
+  constexpr int N2 = C::N2, N3 = C::N3, LPE = C::LPE, MS = NL * C::NLR;
+  static_assert(6 * N2 <= C::BUF, "matrix staging fits the second buffer");
+  extern __shared__ __align__(16) unsigned char fdm_smem[];
+  const int u = threadIdx.x;
+  T *b0 = reinterpret_cast<T *>(fdm_smem), *b1 = b0 + C::BUF;
+  T *sS = b0 + C::OFFM, *sL = sS + C::MAT, *stage = b1;
+  const long e = blockIdx.x;
+  if (e >= nelv) return;
+  for (int q = u; q < N3; q += LPE) cp_async_elem<T>(b0 + C::pos(q / NL, q % NL), r + e * N3 + q, true);
+  for (int q = u; q < 6 * N2; q += LPE) cp_async_elem<T>(stage + q, s + e * 6 * N2 + q, true);
+  cp_async_wait_all();
+  __syncthreads();
+  T *fwd = sS, *bwd = sS + 3 * MS;
+  for (int q = u; q < 3 * N2; q += LPE) {
+    const int dd = q / N2, rr = q - dd * N2, a = rr % NL, b = rr / NL;
+    fwd[dd * MS + a + C::NLR * b] = stage[(2 * dd + 1) * N2 + a + NL * b];  // s2(a, b)
+    bwd[dd * MS + a + C::NLR * b] = stage[(2 * dd) * N2 + a + NL * b];      // s1(a, b)
+  }
+  __syncthreads();
+  fdm_pass<T, NL, true, false>(b0, b1, fwd, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, true, false>(b1, b0, fwd + MS, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, true, false>(b0, b1, fwd + 2 * MS, sL, nullptr, u);
+  __syncthreads();
+  for (int q = u; q < N3; q += LPE) {  // r = d * (forward transform), kept for the backward one
+    const int p = C::pos(q / NL, q % NL);
+    const T v = b1[p] * d[e * N3 + q];
+    b1[p] = v;
+    r[e * N3 + q] = v;
+  }
+  __syncthreads();
+  fdm_pass<T, NL, false, false>(b1, b0, bwd, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, false, false>(b0, b1, bwd + MS, sL, nullptr, u);
+  __syncthreads();
+  fdm_pass<T, NL, false, false>(b1, nullptr, bwd + 2 * MS, sL, eo + e * N3, u);
+}
+
+template <int NL>
+static cudaError_t launch_fdm_dropin(double *eo, double *r, const double *s, const double *d,
+                                     int nel, cudaStream_t st) {
+  using C = FdmCfg<double, NL>;
+  auto kern = fdm_dropin_kernel<NL>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t err =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    if (err != cudaSuccess) return err;
+    attr_set = true;
+  }
+  kern<<<(unsigned)nel, C::TPE, C::SMEM, st>>>(eo, r, s, d, nel);
+  return cudaGetLastError();
+}
+
+cudaError_t fdm_dropin(double *eo, double *r, const double *s, const double *d, int nl, int nel,
+                       cudaStream_t st) {
+  if (nel <= 0) return cudaSuccess;
+  switch (nl) {
+#define NB_FD(N) \
+  case N: return launch_fdm_dropin<N>(eo, r, s, d, nel, st);
+    NB_FD(8) NB_FD(9) NB_FD(10) NB_FD(11) NB_FD(12) NB_FD(13) NB_FD(14) NB_FD(15) NB_FD(16)
+#undef NB_FD
+    default: return cudaErrorNotSupported;
+  }
+}
+
 // restriction (Jt x Jt x Jt)(in * scale) from ni to no points (J: ni x no);
 // scale_f, when given, holds the same values as scale exactly in FP32 and is
 // read instead

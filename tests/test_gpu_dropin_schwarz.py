@@ -56,7 +56,7 @@ def test_tnsr3d(oracle, nblib, nu, nv):
     assert _rel(v.cpu().numpy(), ref) < 1e-13
 
 
-@pytest.mark.parametrize("nl", [4, 6, 10, 12, 7])
+@pytest.mark.parametrize("nl", [4, 6, 7, 8, 10, 12, 16])
 def test_fdm_do_fast(oracle, nblib, nl):
     rng = np.random.default_rng(nl)
     nel = 29
