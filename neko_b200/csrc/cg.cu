@@ -184,11 +184,12 @@ __global__ void __launch_bounds__(kRedThreads)
 
 // x += alpha p; r -= alpha w; rtr = (r, mult r); convergence test.
 __global__ void __launch_bounds__(kRedThreads)
-    cg_update_xr_kernel(double *__restrict__ x, double *__restrict__ r,
+    cg_update_xr_kernel(double *__restrict__ r,
                         const double *__restrict__ p, const double *__restrict__ w,
                         const double *__restrict__ mult, const float *__restrict__ multf, long n, CgState *st,
                         double *partials, unsigned *counter) {
   if (st->done) return;
+  double *__restrict__ x = st->x;
   const double alpha = st->alpha, malpha = -alpha;
   double s = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
@@ -219,10 +220,11 @@ __global__ void __launch_bounds__(kRedThreads)
 // True residual: r = f - w (w = A x just computed), rtr, rnorm and the
 // convergence test redone on it; the next direction restarts (beta = 0).
 __global__ void __launch_bounds__(kRedThreads)
-    cg_true_residual_kernel(double *__restrict__ r, const double *__restrict__ f,
+    cg_true_residual_kernel(double *__restrict__ r,
                             const double *__restrict__ w, const double *__restrict__ mult, const float *__restrict__ multf, long n,
                             CgState *st, double *partials, unsigned *counter) {
   if (st->skip_rc) return;
+  const double *__restrict__ f = st->f;
   double s = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads) {
@@ -243,6 +245,15 @@ __global__ void __launch_bounds__(kRedThreads)
     }
     if (rn < st->abs_tol) st->done = 1;
   }
+}
+
+// y = st->x (the recompute's operator input), on scheduled iterations only
+__global__ void cg_copy_x_kernel(double *__restrict__ y, long n, const CgState *st) {
+  if (st->skip_rc) return;
+  const double *__restrict__ x = st->x;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    y[i] = x[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -299,8 +310,7 @@ cudaError_t CgWorkspace::ensure(long n_) {
 }
 
 // One CG iteration (all launches on s), precond chosen by pc.
-static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, double *x,
-                                const double *f, cudaStream_t s) {
+static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, cudaStream_t s) {
   const long n = P->n;
   const int rb = red_blocks(n), eg = stream_grid(n, 256);
   if (pc) {
@@ -335,15 +345,17 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, doub
   if (e != cudaSuccess) return e;
   if (!W.fused)
     cg_pap_kernel<<<rb, kRedThreads, 0, s>>>(W.w, W.p, P->mult, P->multf, n, W.st, W.partials, W.counter);
-  cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(x, W.r, W.p, W.w, P->mult, P->multf, n, W.st,
+  cg_update_xr_kernel<<<rb, kRedThreads, 0, s>>>(W.r, W.p, W.w, P->mult, P->multf, n, W.st,
                                                  W.partials, W.counter);
   if (W.recompute_every > 0) {  // w = A x, gs, mask; r = f - w (scheduled iterations only)
-    e = P->ax_raw(W.w, x, s, &W.st->skip_rc);
+    // x through z (free until the next preconditioner apply overwrites it)
+    cg_copy_x_kernel<<<eg, 256, 0, s>>>(W.z, n, W.st);
+    e = P->ax_raw(W.w, W.z, s, &W.st->skip_rc);
     if (e != cudaSuccess) return e;
-    if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, x, n, &W.st->skip_rc);
+    if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.z, n, &W.st->skip_rc);
     e = gs_add_fused<double>(P->gsd, W.w, true, s, &W.st->skip_rc);
     if (e != cudaSuccess) return e;
-    cg_true_residual_kernel<<<rb, kRedThreads, 0, s>>>(W.r, f, W.w, P->mult, P->multf, n, W.st,
+    cg_true_residual_kernel<<<rb, kRedThreads, 0, s>>>(W.r, W.w, P->mult, P->multf, n, W.st,
                                                        W.partials, W.counter);
   }
   return cudaGetLastError();
@@ -394,6 +406,8 @@ nb_status cg_start(CgRun &R) {
   init.abs_tol = o.abs_tol;
   init.max_iter = o.max_iter;
   init.recompute_every = W.recompute_every;
+  init.x = R.x;
+  init.f = R.f;
   init.skip_rc = 1;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
   const long n = P->n;
@@ -401,7 +415,8 @@ nb_status cg_start(CgRun &R) {
                                                         W.st, W.partials, W.counter, nullptr);
   NB_CUDA_TRY(cudaGetLastError());
   // (Re)capture the iteration graph when the operands changed.
-  const void *key[5] = {R.x, R.f, pc,
+  // x and f are read from the state: the graph depends on neither
+  const void *key[5] = {nullptr, nullptr, pc,
                         (const void *)(intptr_t)(W.use_jacobi | (W.flexible << 1) |
                                                  ((W.recompute_every > 0) << 2)),
                         (const void *)(intptr_t)P->ifh2};
@@ -418,9 +433,9 @@ nb_status cg_start(CgRun &R) {
     NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t ce = cudaSuccess;
     for (int k = 0; k < R.chunk && ce == cudaSuccess; k++)
-      ce = cg_iteration(P, W, pc, R.x, R.f, cs);
+      ce = cg_iteration(P, W, pc, cs);
     W.launches_per_iter = (W.fused ? 4 : 6 + (P->ifh2 ? 1 : 0)) + (pc ? pc->launches() : 0) +
-                          (W.recompute_every > 0 ? 3 + (P->ifh2 ? 1 : 0) : 0);
+                          (W.recompute_every > 0 ? 4 + (P->ifh2 ? 1 : 0) : 0);
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (ce != cudaSuccess) {

@@ -17,6 +17,10 @@ struct CgState {
   int recompute_every;  // > 0: r = f - A x every that many iterations
   int skip_rc;          // 0 when the current iteration ends with a recompute
   int restart;          // next beta is 0 (after a recompute)
+  // The solve's x and f: the kernels of a captured iteration read them
+  // here, so one graph serves every solve of the workspace.
+  double *x;
+  const double *f;
 };
 
 // pc_t%solve(z, r): z = M^-1 r on stream s; returns early when *skip != 0.
