@@ -108,10 +108,12 @@ __global__ void __launch_bounds__(kRedThreads)
 // x_c += alpha p_c, r_c -= alpha w_c; rnorm, the convergence test; then the
 // next iteration's z_c = d r_c, rtz and beta.
 __global__ void __launch_bounds__(kRedThreads)
-    cpld_update_kernel(V3 x, V3 r, V3 z, C3 p, C3 w, const double *__restrict__ d,
-                       const double *__restrict__ mult, const float *__restrict__ multf, long n,
-                       CgState *st, double *partials, unsigned *counter) {
+    cpld_update_kernel(const V3 *__restrict__ xp, V3 r, V3 z, C3 p, C3 w,
+                       const double *__restrict__ d, const double *__restrict__ mult,
+                       const float *__restrict__ multf, long n, CgState *st, double *partials,
+                       unsigned *counter) {
   if (st->done) return;
+  const V3 x = *xp;  // the solve's x, y, z (device copy: one graph for every solve)
   const double alpha = st->alpha, alphm = -alpha;
   double s0 = 0.0, s1 = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
@@ -158,6 +160,7 @@ struct CpldWorkspace {
   unsigned *counter = nullptr;
   CgState *st = nullptr;
   CgState *host = nullptr;
+  V3 *xdev = nullptr;  // the solve's x, y, z pointers
   cudaGraphExec_t graph = nullptr;
   const void *key[9] = {nullptr};
   int launches_per_iter = 0;
@@ -177,7 +180,7 @@ struct CpldWorkspace {
     n = n_;
     const size_t vec = ((size_t)n * 8 + 255) & ~size_t(255);
     const size_t red = 2 * (size_t)kMaxRedBlocks * sizeof(double) + 256;
-    cudaError_t e = cudaMalloc(&base, 12 * vec + red + sizeof(CgState) + 256);
+    cudaError_t e = cudaMalloc(&base, 12 * vec + red + sizeof(CgState) + 256 + sizeof(V3));
     if (e != cudaSuccess) {
       base = nullptr;
       return e;
@@ -187,6 +190,7 @@ struct CpldWorkspace {
     partials = (double *)(b + 12 * vec);
     counter = (unsigned *)(b + 12 * vec + 2 * (size_t)kMaxRedBlocks * sizeof(double));
     st = (CgState *)(b + 12 * vec + red);
+    xdev = (V3 *)(b + 12 * vec + red + ((sizeof(CgState) + 255) & ~size_t(255)));
     if ((e = cudaMemset(counter, 0, 256)) != cudaSuccess) return e;
     // legacy-stream set-up: finish it before a caller's non-blocking stream
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;
@@ -245,10 +249,13 @@ nb_status cpld_solve(nb_problem *P, int op, double *const xs[3], const double *c
   init.abs_tol = o.abs_tol;
   init.max_iter = o.max_iter;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  NB_CUDA_TRY(cudaMemcpyAsync(W.xdev, &x, sizeof(V3), cudaMemcpyHostToDevice, s));
   cpld_init_kernel<<<rb, kRedThreads, 0, s>>>(x, p, r, z, f, d, P->mult, P->multf, n, W.st,
                                               W.partials, W.counter);
   NB_CUDA_TRY(cudaGetLastError());
-  const void *key[9] = {xs[0], xs[1], xs[2], fs[0], fs[1], fs[2], d,
+  // x, y, z are read from the device copy: the graph depends on neither
+  // the solution nor the right-hand side pointers
+  const void *key[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, d,
                         (const void *)(intptr_t)op, (const void *)(intptr_t)P->ifh2};
   const int chunk = n > (1 << 22) ? 4 : 16;
   if (!W.graph || memcmp(key, W.key, sizeof(key))) {
@@ -268,8 +275,8 @@ nb_status cpld_solve(nb_problem *P, int op, double *const xs[3], const double *c
       if (ce == cudaSuccess) {
         cpld_pap_kernel<<<rb, kRedThreads, 0, cs>>>(wc, pc, P->mult, P->multf, n, W.st,
                                                     W.partials, W.counter);
-        cpld_update_kernel<<<rb, kRedThreads, 0, cs>>>(x, r, z, pc, wc, d, P->mult, P->multf, n,
-                                                       W.st, W.partials, W.counter);
+        cpld_update_kernel<<<rb, kRedThreads, 0, cs>>>(W.xdev, r, z, pc, wc, d, P->mult,
+                                                       P->multf, n, W.st, W.partials, W.counter);
         ce = cudaGetLastError();
       }
     }

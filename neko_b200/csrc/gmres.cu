@@ -43,6 +43,10 @@ struct GmresState {
   double rnorm, res_start, inv_scale;
   double h[kGmresMaxM * kGmresMaxM];  // h(i,j) at i + m j (0-based)
   double c[kGmresMaxM], s[kGmresMaxM], gam[kGmresMaxM + 1];
+  // the solve's x and f: read here by the captured cycle, so one graph
+  // serves every solve of the workspace
+  double *x;
+  const double *f;
 };
 
 // Sum over the block of CH values at once; results valid in thread 0.
@@ -68,10 +72,11 @@ __device__ __forceinline__ void block_sum_many(double (&v)[CH], double *sh) {
 // r = f - w (w = A x after gs and mask; x = 0 in the first cycle makes w
 // zero), gam(1) = sqrt((r, mult r)); starts the cycle.
 __global__ void __launch_bounds__(kRedThreads)
-    gm_cycle_start_kernel(double *__restrict__ r, const double *__restrict__ f,
+    gm_cycle_start_kernel(double *__restrict__ r,
                           const double *__restrict__ w, const double *__restrict__ mult,
                           const float *__restrict__ multf, long n, GmresState *st,
                           double *partials, unsigned *counter) {
+  const double *__restrict__ f = st->f;
   if (st->done) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       st->j_used = 0;  // a replay after the end changes nothing
@@ -244,8 +249,8 @@ __global__ void __launch_bounds__(kRedThreads)
 // End of a cycle: y = H^-1 gam by back substitution over the j_used
 // columns (every block computes it), then x += sum_k z_k y_k.
 __global__ void __launch_bounds__(kRedThreads)
-    gm_update_x_kernel(double *__restrict__ x, const double *const *__restrict__ Z, long n,
-                       const GmresState *st) {
+    gm_update_x_kernel(const double *const *__restrict__ Z, long n, const GmresState *st) {
+  double *__restrict__ x = st->x;
   const int j = st->j_used, m = st->m;
   if (j <= 0) return;
   __shared__ double y[kGmresMaxM];
@@ -338,6 +343,15 @@ struct GmresWorkspace {
   }
 };
 
+// y = st->x, the operator input of the cycle's residual
+__global__ void gm_copy_x_kernel(double *__restrict__ y, long n, const GmresState *st) {
+  if (st->done) return;
+  const double *__restrict__ x = st->x;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    y[i] = x[i];
+}
+
 // w = A u, gs add, mask (the operator as the Krylov loop applies it);
 // nothing when *skip != 0.
 static cudaError_t apply_op(nb_problem *P, double *w, const double *u, const int *skip,
@@ -351,14 +365,16 @@ static cudaError_t apply_op(nb_problem *P, double *w, const double *u, const int
 
 // One restart cycle: residual, m columns, x update.
 static cudaError_t gmres_cycle(nb_problem *P, GmresWorkspace &W, Precond *pc, bool jacobi,
-                               double *x, const double *f, cudaStream_t s, int *launches) {
+                               cudaStream_t s, int *launches) {
   const long n = P->n;
   const int rb = red_blocks(n), eg = stream_grid(n, 256);
   int L = 0;
-  cudaError_t e = apply_op(P, W.w, x, &W.st->done, s);
+  // x through Z[0], which this cycle's first preconditioner apply overwrites
+  gm_copy_x_kernel<<<eg, 256, 0, s>>>(W.Z[0], n, W.st);
+  cudaError_t e = apply_op(P, W.w, W.Z[0], &W.st->done, s);
   if (e != cudaSuccess) return e;
-  L += 2 + (P->ifh2 ? 1 : 0);
-  gm_cycle_start_kernel<<<rb, kRedThreads, 0, s>>>(W.r, f, W.w, P->mult, P->multf, n, W.st,
+  L += 3 + (P->ifh2 ? 1 : 0);
+  gm_cycle_start_kernel<<<rb, kRedThreads, 0, s>>>(W.r, W.w, P->mult, P->multf, n, W.st,
                                                    W.partials, W.counter);
   gm_scale_kernel<<<eg, 256, 0, s>>>(W.V[0], W.r, n, W.st);
   L += 2;
@@ -384,7 +400,7 @@ static cudaError_t gmres_cycle(nb_problem *P, GmresWorkspace &W, Precond *pc, bo
       L += 1;
     }
   }
-  gm_update_x_kernel<<<eg, kRedThreads, 0, s>>>(x, W.Zp, n, W.st);
+  gm_update_x_kernel<<<eg, kRedThreads, 0, s>>>(W.Zp, n, W.st);
   L += 1;
   *launches = L;
   return cudaGetLastError();
@@ -415,10 +431,12 @@ nb_status gmres_solve(nb_problem *P, double *x, const double *f, const nb_solve_
   init->m = m;
   init->max_iter = o.max_iter;
   for (int k = 0; k < m; k++) init->c[k] = init->s[k] = 1.0;
+  init->x = x;
+  init->f = f;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, init, sizeof(GmresState), cudaMemcpyHostToDevice, s));
   // the pinned staging buffer is read back below: the copy must be done first
   NB_CUDA_TRY(cudaStreamSynchronize(s));
-  const void *key[5] = {x, f, pc, (const void *)(intptr_t)(jacobi | (P->ifh2 << 1)),
+  const void *key[5] = {nullptr, nullptr, pc, (const void *)(intptr_t)(jacobi | (P->ifh2 << 1)),
                         (const void *)(intptr_t)m};
   if (!W.graph_exec || memcmp(key, W.graph_key, sizeof(key))) {
     if (W.graph_exec) {
@@ -429,7 +447,7 @@ nb_status gmres_solve(nb_problem *P, double *x, const double *f, const nb_solve_
     NB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g;
     NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    cudaError_t ce = gmres_cycle(P, W, pc, jacobi, x, f, cs, &W.launches_per_cycle);
+    cudaError_t ce = gmres_cycle(P, W, pc, jacobi, cs, &W.launches_per_cycle);
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (ce != cudaSuccess) {

@@ -35,6 +35,7 @@ struct PipeState {
   double red[3];  // gamma, delta, rtr of the last vector pass
   double gamma1, gamma2, delta, rtr, alpha, beta, rnorm, res_start;
   int iter, max_iter, done, nan;
+  double *x;  // the solve's x, read by the captured iterations
 };
 
 // (r, mult u), (w, mult u), (r, mult r) into st->red
@@ -154,13 +155,14 @@ __global__ void pipe_scalar_kernel(PipeState *st) {
 
 // The vector pass of one iteration and the next inner products.
 __global__ void __launch_bounds__(kRedThreads)
-    pipe_vecops_kernel(double *__restrict__ x, double *__restrict__ p, double *__restrict__ q,
+    pipe_vecops_kernel(double *__restrict__ p, double *__restrict__ q,
                        double *__restrict__ r, double *__restrict__ s, double *__restrict__ u,
                        double *__restrict__ w, double *__restrict__ z,
                        const double *__restrict__ ni, const double *__restrict__ mi,
                        const double *__restrict__ mult, const float *__restrict__ multf, long n,
                        PipeState *st, double *partials, unsigned *counter) {
   if (st->done) return;
+  double *__restrict__ x = st->x;
   const double alpha = st->alpha, beta = st->beta;
   double t1 = 0, t2 = 0, t3 = 0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
@@ -274,6 +276,7 @@ nb_status pipecg_solve(nb_problem *P, double *x, const double *f, const nb_solve
   init.norm_fac = 1.0 / std::sqrt(P->volume);
   init.abs_tol = o.abs_tol;
   init.max_iter = o.max_iter;
+  init.x = x;
   NB_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   // r = f, u = M r, w = A u and the first inner products (outside the graph)
   pipe_zero_kernel<<<eg, 256, 0, s>>>(x, p, z, q, sv, r, f, n);
@@ -284,7 +287,7 @@ nb_status pipecg_solve(nb_problem *P, double *x, const double *f, const nb_solve
                                                      W.partials, W.counter);
   pipe_start_kernel<<<1, 1, 0, s>>>(W.st);
   NB_CUDA_TRY(cudaGetLastError());
-  const void *key[4] = {x, f, pc, (const void *)(intptr_t)(jacobi | (P->ifh2 << 1))};
+  const void *key[4] = {nullptr, nullptr, pc, (const void *)(intptr_t)(jacobi | (P->ifh2 << 1))};
   const int chunk = n > (1 << 22) ? 4 : 16;
   if (!W.graph || memcmp(key, W.key, sizeof(key))) {
     if (W.graph) {
@@ -301,7 +304,7 @@ nb_status pipecg_solve(nb_problem *P, double *x, const double *f, const nb_solve
       if (ce == cudaSuccess) ce = pipe_op(P, ni, mi, &W.st->done, cs);
       if (ce == cudaSuccess) {
         pipe_scalar_kernel<<<1, 1, 0, cs>>>(W.st);
-        pipe_vecops_kernel<<<rb, kRedThreads, 0, cs>>>(x, p, q, r, sv, u, w, z, ni, mi, P->mult,
+        pipe_vecops_kernel<<<rb, kRedThreads, 0, cs>>>(p, q, r, sv, u, w, z, ni, mi, P->mult,
                                                        P->multf, n, W.st, W.partials, W.counter);
         ce = cudaGetLastError();
       }
