@@ -324,10 +324,10 @@ struct AxCgCfg {
   static constexpr size_t SMEM = S * NA * ABYTES + 3 * ABYTES + 2 * L2 * sizeof(double) + 16 * S;
 };
 
-template <int LX, int S, int KS>
+template <int LX, int S, int KS, typename TZ>
 __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
     ax_cg_fused_kernel(double *__restrict__ w, double *__restrict__ p,
-                       const double *__restrict__ z, const double *__restrict__ D,
+                       const TZ *__restrict__ z, const double *__restrict__ D,
                        const double *__restrict__ Dt, const double *__restrict__ h1,
                        const double *__restrict__ g11, const double *__restrict__ g22,
                        const double *__restrict__ g33, const double *__restrict__ g12,
@@ -357,12 +357,15 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
     sDt[q] = Dt[q];
   }
   __syncthreads();
-  const double *src[NA] = {z, p, h1, g11, g22, g33, g12, g13, g23};
+  // z (slot 0) arrives in its own precision: L3 values of TZ
+  constexpr uint32_t ZBYTES = (uint32_t)(L3 * sizeof(TZ));
+  const double *src[NA] = {nullptr, p, h1, g11, g22, g33, g12, g13, g23};
   auto issue = [&](int t, int s) {
     const long e = b + (long)t * G;
-    mbar_arrive_expect_tx(&full[s], (uint32_t)(NA * C::ABYTES));
+    mbar_arrive_expect_tx(&full[s], (uint32_t)((NA - 1) * C::ABYTES) + ZBYTES);
+    bulk_g2s(stage + (size_t)(s * NA) * L3, z + e * L3, ZBYTES, &full[s]);
 #pragma unroll
-    for (int a = 0; a < NA; a++)
+    for (int a = 1; a < NA; a++)
       bulk_g2s(stage + (size_t)(s * NA + a) * L3, src[a] + e * L3, (uint32_t)C::ABYTES, &full[s]);
   };
   if (tid == 0)
@@ -391,7 +394,7 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
       break;
     }
     const long e = b + (long)t * G;
-    const double *sz = stage + (size_t)s * NA * L3;
+    const TZ *sz = reinterpret_cast<const TZ *>(stage + (size_t)s * NA * L3);
     double *su = stage + (size_t)s * NA * L3 + L3;  // old p, replaced by the new
     const double *sh = su + L3, *s11 = su + 2 * L3, *s22 = su + 3 * L3, *s33 = su + 4 * L3,
                  *s12 = su + 5 * L3, *s13 = su + 6 * L3, *s23 = su + 7 * L3;
@@ -399,7 +402,7 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
         const int q = col + L2 * (k0 + kk);
-        const double pn = sz[q] + beta * su[q];
+        const double pn = (double)sz[q] + beta * su[q];
         su[q] = pn;
         p[e * L3 + q] = pn;
       }
@@ -470,15 +473,15 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
   }
 }
 
-template <int LX, int S, int KS>
-static cudaError_t launch_ax_cg(double *w, double *p, const double *z, const double *D,
+template <int LX, int S, int KS, typename TZ>
+static cudaError_t launch_ax_cg(double *w, double *p, const TZ *z, const double *D,
                                 const double *Dt, const double *h1, const double *g11,
                                 const double *g22, const double *g33, const double *g12,
                                 const double *g13, const double *g23, int nelv, CgState *st,
                                 double beta, double *pap_out, double *partials,
                                 unsigned *counter, int max_grid, cudaStream_t s, int *err) {
   using C = AxCgCfg<LX, S, KS>;
-  auto kern = ax_cg_fused_kernel<LX, S, KS>;
+  auto kern = ax_cg_fused_kernel<LX, S, KS, TZ>;
   static int grid_per_dev[64] = {0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -502,7 +505,8 @@ static cudaError_t launch_ax_cg(double *w, double *p, const double *z, const dou
   return cudaGetLastError();
 }
 
-cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, const double *Dt,
+template <typename TZ>
+cudaError_t ax_cg_fused(double *w, double *p, const TZ *z, const double *D, const double *Dt,
                         const double *h1, const double *g11, const double *g22, const double *g33,
                         const double *g12, const double *g13, const double *g23, int nelv, int lx,
                         CgState *st, double beta, double *pap_out, double *partials,
@@ -510,14 +514,26 @@ cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, 
   const void *ptrs[] = {z, p, h1, g11, g22, g33, g12, g13, g23};
   for (const void *q : ptrs)
     if (reinterpret_cast<uintptr_t>(q) & 15) return cudaErrorNotSupported;
-  if (((size_t)lx * lx * lx * sizeof(double)) % 16) return cudaErrorNotSupported;
+  if (((size_t)lx * lx * lx * sizeof(TZ)) % 16) return cudaErrorNotSupported;
   switch (lx) {
-    case 6: return launch_ax_cg<6, 3, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
-    case 8: return launch_ax_cg<8, 2, 2>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
-    case 10: return launch_ax_cg<10, 2, 5>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
+    case 6: return launch_ax_cg<6, 3, 2, TZ>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
+    case 8: return launch_ax_cg<8, 2, 2, TZ>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
+    case 10: return launch_ax_cg<10, 2, 5, TZ>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
     default: return cudaErrorNotSupported;
   }
 }
+template cudaError_t ax_cg_fused<double>(double *, double *, const double *, const double *,
+                                         const double *, const double *, const double *,
+                                         const double *, const double *, const double *,
+                                         const double *, const double *, int, int, CgState *,
+                                         double, double *, double *, unsigned *, int,
+                                         cudaStream_t, int *);
+template cudaError_t ax_cg_fused<float>(double *, double *, const float *, const double *,
+                                        const double *, const double *, const double *,
+                                        const double *, const double *, const double *,
+                                        const double *, const double *, int, int, CgState *,
+                                        double, double *, double *, unsigned *, int,
+                                        cudaStream_t, int *);
 
 int *dropin_error_word() {
   static int *cache[64] = {nullptr};

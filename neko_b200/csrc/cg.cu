@@ -113,15 +113,16 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 // rtz = (r, mult z) for an externally applied preconditioner.
+template <typename TZ>
 __global__ void __launch_bounds__(kRedThreads)
-    cg_dot_rz_kernel(const double *__restrict__ z, const double *__restrict__ r,
+    cg_dot_rz_kernel(const TZ *__restrict__ z, const double *__restrict__ r,
                      const double *__restrict__ mult, const float *__restrict__ multf, long n, CgState *st, double *partials,
                      unsigned *counter) {
   if (st->done) return;
   double s = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads)
-    s += r[i] * MW(i) * z[i];
+    s += r[i] * MW(i) * (double)z[i];
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {
     st->rtz2 = st->rtz1;
@@ -134,15 +135,16 @@ __global__ void __launch_bounds__(kRedThreads)
 // Flexible variant (Polak-Ribiere): rtz = (r, mult z) and rwz =
 // (w_prev, mult z); beta = -alpha_prev * rwz / rtz_prev, because
 // r_k - r_(k-1) = -alpha_(k-1) w_(k-1) and w still holds w_(k-1) here.
+template <typename TZ>
 __global__ void __launch_bounds__(kRedThreads)
-    cg_dot_rz_flex_kernel(const double *__restrict__ z, const double *__restrict__ r,
+    cg_dot_rz_flex_kernel(const TZ *__restrict__ z, const double *__restrict__ r,
                           const double *__restrict__ w_prev, const double *__restrict__ mult, const float *__restrict__ multf,
                           long n, CgState *st, double *partials, unsigned *counter) {
   if (st->done) return;
   double s0 = 0.0, s1 = 0.0;
   for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
        i += (long)gridDim.x * kRedThreads) {
-    const double mz = MW(i) * z[i];
+    const double mz = MW(i) * (double)z[i];
     s0 += r[i] * mz;
     s1 += w_prev[i] * mz;
   }
@@ -156,13 +158,14 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 // p = z + beta p
-__global__ void cg_update_p_kernel(double *__restrict__ p, const double *__restrict__ z,
+template <typename TZ>
+__global__ void cg_update_p_kernel(double *__restrict__ p, const TZ *__restrict__ z,
                                    long n, const CgState *st) {
   if (st->done) return;
   const double beta = st->beta;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
        i += (long)gridDim.x * blockDim.x)
-    p[i] = z[i] + beta * p[i];
+    p[i] = (double)z[i] + beta * p[i];
 }
 
 // pap = (w, mult p); alpha = rtz / pap
@@ -313,15 +316,29 @@ cudaError_t CgWorkspace::ensure(long n_) {
 static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, cudaStream_t s) {
   const long n = P->n;
   const int rb = red_blocks(n), eg = stream_grid(n, 256);
+  // A preconditioner that computes in FP32 leaves z in FP32 and the kernels
+  // below widen each value as they read it: the same numbers as converting
+  // z to FP64 first, without the conversion pass.
+  const float *zf = pc ? pc->output_f32() : nullptr;
   if (pc) {
-    cudaError_t e = pc->apply(W.z, W.r, &W.st->done, s);
+    cudaError_t e = zf ? pc->apply_f32(W.r, &W.st->done, s) : pc->apply(W.z, W.r, &W.st->done, s);
     if (e != cudaSuccess) return e;
-    if (W.flexible)
-      cg_dot_rz_flex_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.w, P->mult, P->multf, n, W.st,
-                                                       W.partials, W.counter);
-    else
-      cg_dot_rz_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, P->multf, n, W.st, W.partials,
-                                                  W.counter);
+    if (W.flexible) {
+      if (zf)
+        cg_dot_rz_flex_kernel<float><<<rb, kRedThreads, 0, s>>>(zf, W.r, W.w, P->mult, P->multf,
+                                                                n, W.st, W.partials, W.counter);
+      else
+        cg_dot_rz_flex_kernel<double><<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.w, P->mult,
+                                                                 P->multf, n, W.st, W.partials,
+                                                                 W.counter);
+    } else {
+      if (zf)
+        cg_dot_rz_kernel<float><<<rb, kRedThreads, 0, s>>>(zf, W.r, P->mult, P->multf, n, W.st,
+                                                           W.partials, W.counter);
+      else
+        cg_dot_rz_kernel<double><<<rb, kRedThreads, 0, s>>>(W.z, W.r, P->mult, P->multf, n,
+                                                            W.st, W.partials, W.counter);
+    }
   } else {
     cg_precond_dot_kernel<<<rb, kRedThreads, 0, s>>>(W.z, W.r, W.use_jacobi ? P->jdiag : nullptr,
                                                      P->mult, P->multf, n, W.st, W.partials, W.counter);
@@ -330,13 +347,19 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, cuda
   // no h2 term (the local form of pap needs p zero wherever w is masked)
   cudaError_t e = cudaErrorNotSupported;
   if (P->nmask == 0 && !P->ifh2 && P->use_stream_ax)
-    e = ax_cg_fused(W.w, W.p, W.z, P->D, P->Dt, P->h1, P->g11, P->g22, P->g33, P->g12, P->g13,
-                    P->g23, (int)P->nelv, P->lx, W.st, 0.0, nullptr, W.partials, W.counter,
-                    kCgMaxPartials, s, P->err);
+    e = zf ? ax_cg_fused(W.w, W.p, zf, P->D, P->Dt, P->h1, P->g11, P->g22, P->g33, P->g12,
+                         P->g13, P->g23, (int)P->nelv, P->lx, W.st, 0.0, nullptr, W.partials,
+                         W.counter, kCgMaxPartials, s, P->err)
+           : ax_cg_fused(W.w, W.p, (const double *)W.z, P->D, P->Dt, P->h1, P->g11, P->g22,
+                         P->g33, P->g12, P->g13, P->g23, (int)P->nelv, P->lx, W.st, 0.0, nullptr,
+                         W.partials, W.counter, kCgMaxPartials, s, P->err);
   W.fused = e == cudaSuccess;
   if (e != cudaSuccess && e != cudaErrorNotSupported) return e;
   if (!W.fused) {
-    cg_update_p_kernel<<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
+    if (zf)
+      cg_update_p_kernel<float><<<eg, 256, 0, s>>>(W.p, zf, n, W.st);
+    else
+      cg_update_p_kernel<double><<<eg, 256, 0, s>>>(W.p, W.z, n, W.st);
     e = P->ax_raw(W.w, W.p, s, &W.st->done);
     if (e != cudaSuccess) return e;
     if (P->ifh2) addcol4_kernel<<<eg, 256, 0, s>>>(W.w, P->h2, P->B, W.p, n, &W.st->done);
@@ -434,7 +457,9 @@ nb_status cg_start(CgRun &R) {
     cudaError_t ce = cudaSuccess;
     for (int k = 0; k < R.chunk && ce == cudaSuccess; k++)
       ce = cg_iteration(P, W, pc, cs);
-    W.launches_per_iter = (W.fused ? 4 : 6 + (P->ifh2 ? 1 : 0)) + (pc ? pc->launches() : 0) +
+    // an FP32-output preconditioner skips its conversion launch
+    const int pc_launches = pc ? pc->launches() - (pc->output_f32() ? 1 : 0) : 0;
+    W.launches_per_iter = (W.fused ? 4 : 6 + (P->ifh2 ? 1 : 0)) + pc_launches +
                           (W.recompute_every > 0 ? 4 + (P->ifh2 ? 1 : 0) : 0);
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);

@@ -63,7 +63,9 @@ struct CgState;
 // rtz / pap are written to it; without one, beta is the argument and pap
 // goes to *pap_out (device, may be null).  cudaErrorNotSupported when lx or
 // alignment is not covered.
-cudaError_t ax_cg_fused(double *w, double *p, const double *z, const double *D, const double *Dt,
+// z may be FP32 (a mixed-precision preconditioner's output), widened as read.
+template <typename TZ>
+cudaError_t ax_cg_fused(double *w, double *p, const TZ *z, const double *D, const double *Dt,
                         const double *h1, const double *g11, const double *g22, const double *g33,
                         const double *g12, const double *g13, const double *g23, int nelv, int lx,
                         CgState *st, double beta, double *pap_out, double *partials,

@@ -31,6 +31,15 @@ struct Precond {
   virtual int launches() const = 0;
   // nonzero when a bounded device wait of an apply expired; clears it
   virtual int take_error() { return 0; }
+  // A preconditioner that computes in FP32 may leave its output there: the
+  // FP32 array apply_f32 writes (its own buffer), else null.
+  virtual const float *output_f32() { return nullptr; }
+  virtual cudaError_t apply_f32(const double *r, const int *skip, cudaStream_t s) {
+    (void)r;
+    (void)skip;
+    (void)s;
+    return cudaErrorNotSupported;
+  }
 };
 
 // Blocks a CG reduction may use (its partial sums live in the workspace).

@@ -710,10 +710,28 @@ struct HsmgImpl : public HsmgState {
     return v;
   }
 
+  // FP32 smoothing levels: the output can stay in FP32 (zf)
+  const float *output_f32() override {
+    return sizeof(T) == 4 ? reinterpret_cast<const float *>(zf) : nullptr;
+  }
+  cudaError_t apply_f32(const double *r, const int *skip, cudaStream_t s) override {
+    if (sizeof(T) != 4) return cudaErrorNotSupported;
+    return apply_to(zf, r, skip, s);
+  }
+
   cudaError_t apply(double *z, const double *r, const int *skip, cudaStream_t s) override {
+    T *zs = sizeof(T) == 8 ? reinterpret_cast<T *>(z) : zf;
+    cudaError_t e = apply_to(zs, r, skip, s);
+    if (e != cudaSuccess) return e;
+    if (sizeof(T) == 4)
+      convert_kernel<T, double><<<stream_grid(fine->n, 256), 256, 0, s>>>(z, zs, fine->n, skip);
+    return cudaGetLastError();
+  }
+
+  // zs = M r in the smoothing precision
+  cudaError_t apply_to(T *zs, const double *r, const int *skip, cudaStream_t s) {
     cudaError_t e;
     const long nelv = fine->nelv;
-    T *zs = sizeof(T) == 8 ? reinterpret_cast<T *>(z) : zf;
     // fine Schwarz on the side stream: zs = S_f r
     if ((e = ensure_side()) != cudaSuccess || (e = cudaEventRecord(ev_fork, s)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(side, ev_fork, 0)) != cudaSuccess ||
@@ -752,8 +770,6 @@ struct HsmgImpl : public HsmgState {
     if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, merged ? nullptr : mult_f)) !=
         cudaSuccess)
       return e;
-    if (sizeof(T) == 4)
-      convert_kernel<T, double><<<stream_grid(fine->n, 256), 256, 0, s>>>(z, zs, fine->n, skip);
     return cudaGetLastError();
   }
 };
