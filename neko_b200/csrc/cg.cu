@@ -157,6 +157,28 @@ __global__ void __launch_bounds__(kRedThreads)
   }
 }
 
+// The flexible CG's scalars from per-element partial sums (2 per element:
+// (r, mult z), (w_prev, mult z)) that the preconditioner formed: one block,
+// fixed order.
+__global__ void __launch_bounds__(1024)
+    cg_finish_flex_kernel(const double *__restrict__ part, long nelv, CgState *st) {
+  if (st->done) return;
+  double s0 = 0.0, s1 = 0.0;
+  for (long e = threadIdx.x; e < nelv; e += 1024) {
+    s0 += part[2 * e];
+    s1 += part[2 * e + 1];
+  }
+  __shared__ double sh[32];
+  s0 = block_sum<1024>(s0, sh);
+  s1 = block_sum<1024>(s1, sh);
+  if (threadIdx.x == 0) {
+    st->beta = (st->iter == 0 || st->restart) ? 0.0 : -st->alpha * s1 / st->rtz1;
+    st->restart = 0;
+    st->rtz2 = st->rtz1;
+    st->rtz1 = s0;
+  }
+}
+
 // p = z + beta p
 template <typename TZ>
 __global__ void cg_update_p_kernel(double *__restrict__ p, const TZ *__restrict__ z,
@@ -268,6 +290,7 @@ static nb_status ws_fail(nb_status s, const std::string &m) {
 }
 
 CgWorkspace::~CgWorkspace() {
+  if (dots) cudaFree(dots);
   if (ev) cudaEventDestroy(ev);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   if (base) cudaFree(base);
@@ -320,7 +343,14 @@ static cudaError_t cg_iteration(nb_problem *P, CgWorkspace &W, Precond *pc, cuda
   // below widen each value as they read it: the same numbers as converting
   // z to FP64 first, without the conversion pass.
   const float *zf = pc ? pc->output_f32() : nullptr;
-  if (pc) {
+  if (pc && W.use_dots) {
+    // the preconditioner forms the two inner products of its output as it
+    // prolongs (continuous r and w: the sums over local points of the
+    // unassembled output equal the mult-weighted ones of the assembled z)
+    cudaError_t e = pc->apply_dots(W.z, W.r, W.w, W.dots, &W.st->done, s);
+    if (e != cudaSuccess) return e;
+    cg_finish_flex_kernel<<<1, 1024, 0, s>>>(W.dots, W.dots_n, W.st);
+  } else if (pc) {
     cudaError_t e = zf ? pc->apply_f32(W.r, &W.st->done, s) : pc->apply(W.z, W.r, &W.st->done, s);
     if (e != cudaSuccess) return e;
     if (W.flexible) {
@@ -424,6 +454,18 @@ nb_status cg_start(CgRun &R) {
   W.use_jacobi = o.pc == NB_PC_JACOBI;
   W.flexible = (o.flexible != 0 || o.mixed != 0) && pc != nullptr;
   W.recompute_every = o.mixed ? 50 : 0;
+  W.use_dots = W.flexible && pc->dots_in_apply();
+  if (W.use_dots && (!W.dots || W.dots_n != P->nelv)) {
+    if (W.dots) cudaFree(W.dots);
+    W.dots = nullptr;
+    cudaError_t ae = cudaMalloc(&W.dots, 2 * (size_t)P->nelv * sizeof(double));
+    if (ae != cudaSuccess) {
+      W.dots = nullptr;
+      return ws_fail(ae == cudaErrorMemoryAllocation ? NB_ERR_OOM : NB_ERR_CUDA,
+                     std::string("CG workspace: ") + cudaGetErrorString(ae));
+    }
+    W.dots_n = P->nelv;
+  }
   CgState init{};
   init.norm_fac = 1.0 / std::sqrt(P->volume);
   init.abs_tol = o.abs_tol;
@@ -441,7 +483,8 @@ nb_status cg_start(CgRun &R) {
   // x and f are read from the state: the graph depends on neither
   const void *key[5] = {nullptr, nullptr, pc,
                         (const void *)(intptr_t)(W.use_jacobi | (W.flexible << 1) |
-                                                 ((W.recompute_every > 0) << 2)),
+                                                 ((W.recompute_every > 0) << 2) |
+                                                 (W.use_dots << 3)),
                         (const void *)(intptr_t)P->ifh2};
   bool same = W.graph_exec && !memcmp(key, W.graph_key, sizeof(key));
   R.chunk = n > (1 << 22) ? 4 : 16;
@@ -457,7 +500,9 @@ nb_status cg_start(CgRun &R) {
     cudaError_t ce = cudaSuccess;
     for (int k = 0; k < R.chunk && ce == cudaSuccess; k++)
       ce = cg_iteration(P, W, pc, cs);
-    // an FP32-output preconditioner skips its conversion launch
+    // an FP32-output preconditioner skips its conversion launch; with the
+    // inner products formed by the preconditioner a one-block finishing
+    // launch replaces the dot pass
     const int pc_launches = pc ? pc->launches() - (pc->output_f32() ? 1 : 0) : 0;
     W.launches_per_iter = (W.fused ? 4 : 6 + (P->ifh2 ? 1 : 0)) + pc_launches +
                           (W.recompute_every > 0 ? 4 + (P->ifh2 ? 1 : 0) : 0);

@@ -40,6 +40,21 @@ struct Precond {
     (void)s;
     return cudaErrorNotSupported;
   }
+  // True when apply_dots can form the flexible CG's two inner products
+  // (r, mult z) and (w_prev, mult z) of its output: partial sums, two per
+  // element, in part; z is written as by apply (or left in FP32 when
+  // output_f32 is non-null).
+  virtual bool dots_in_apply() const { return false; }
+  virtual cudaError_t apply_dots(double *z, const double *r, const double *w_prev, double *part,
+                                 const int *skip, cudaStream_t s) {
+    (void)z;
+    (void)r;
+    (void)w_prev;
+    (void)part;
+    (void)skip;
+    (void)s;
+    return cudaErrorNotSupported;
+  }
 };
 
 // Blocks a CG reduction may use (its partial sums live in the workspace).
@@ -61,6 +76,11 @@ struct CgWorkspace {
   cudaGraphExec_t graph_exec = nullptr;
   cudaEvent_t ev = nullptr;  // behind the state copy of the last chunk
   const void *graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // per-element partial inner products of a preconditioner that forms them
+  // (Precond::apply_dots): 2 x nelv doubles, allocated on first use
+  double *dots = nullptr;
+  long dots_n = 0;
+  bool use_dots = false;  // this solve's iterations take them
   ~CgWorkspace();
   cudaError_t ensure(long n);
 };

@@ -362,12 +362,23 @@ __global__ void __launch_bounds__(256)
 // count, so a thread's global loads are all in flight together.
 constexpr int kT3Threads = 128;
 
-template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC>
+// With DOT (prolongation into the unassembled fine-level output), the
+// block also forms sum(out r) and sum(out w) over its element's points in
+// FP64 and writes them to dots[2e], dots[2e + 1]: the flexible CG's inner
+// products (r, mult z) and (w, mult z) of the assembled z = gs(out), since
+// r and w are continuous (see PrologDots).
+struct PrologDots {
+  const double *r = nullptr, *w = nullptr;
+  double *part = nullptr;  // 2 per element
+};
+
+template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC,
+          bool DOT = false>
 __global__ void __launch_bounds__(kT3Threads)
     tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
                    const float *__restrict__ scale_f,
                    const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
-                   const int *__restrict__ skip) {
+                   const int *__restrict__ skip, PrologDots dots = PrologDots{}) {
   if (skip && *skip) return;
   constexpr int I3 = NI * NI * NI, O3 = NO * NO * NO, NT = kT3Threads;
   __shared__ T su[I3], s1[NO * NI * NI], s2[NO * NO * NI], sA[NO * NI];
@@ -422,6 +433,7 @@ __global__ void __launch_bounds__(kT3Threads)
   constexpr int RO = (O3 + NT - 1) / NT;
   TOUT prev[RO];
   TIN oscale[RO];
+  double dr[DOT ? RO : 1], dw[DOT ? RO : 1];
   if (ACC) {
 #pragma unroll
     for (int g = 0; g < RO; g++) {
@@ -430,8 +442,13 @@ __global__ void __launch_bounds__(kT3Threads)
       oscale[g] = (scale && q < O3)
                       ? (scale_f ? (TIN)scale_f[e * O3 + q] : scale[e * O3 + q])
                       : TIN(1);
+      if constexpr (DOT) {
+        dr[g] = q < O3 ? __ldg(dots.r + e * O3 + q) : 0.0;
+        dw[g] = q < O3 ? __ldg(dots.w + e * O3 + q) : 0.0;
+      }
     }
   }
+  double s_r = 0.0, s_w = 0.0;
 #pragma unroll
   for (int g = 0; g < RO; g++) {  // z
     const int q = tid + g * NT;
@@ -440,12 +457,27 @@ __global__ void __launch_bounds__(kT3Threads)
       T acc = 0;
 #pragma unroll
       for (int k = 0; k < NI; k++) acc += sA[r + NO * k] * s2[op + NO * NO * k];
+      TOUT v;
       if (ACC && scale)
-        out[e * O3 + q] = (TOUT)((T)prev[g] + (T)oscale[g] * acc);
+        v = (TOUT)((T)prev[g] + (T)oscale[g] * acc);
       else if (ACC)
-        out[e * O3 + q] = (TOUT)((T)prev[g] + acc);
+        v = (TOUT)((T)prev[g] + acc);
       else
-        out[e * O3 + q] = (TOUT)acc;
+        v = (TOUT)acc;
+      out[e * O3 + q] = v;
+      if constexpr (DOT) {
+        s_r += (double)v * dr[g];
+        s_w += (double)v * dw[g];
+      }
+    }
+  }
+  if constexpr (DOT) {
+    __shared__ double sh[kT3Threads / 32];
+    s_r = block_sum<kT3Threads>(s_r, sh);
+    s_w = block_sum<kT3Threads>(s_w, sh);
+    if (tid == 0) {
+      dots.part[2 * e] = s_r;
+      dots.part[2 * e + 1] = s_w;
     }
   }
 }
@@ -622,11 +654,17 @@ static cudaError_t restrict_level(int ni, int no, const TIN *in, const TIN *scal
 template <typename TIN, typename TOUT, typename T>
 static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *out, long nelv,
                                const int *skip, cudaStream_t s, const TIN *oscale = nullptr,
-                               const float *oscale_f = nullptr) {
+                               const float *oscale_f = nullptr,
+                               const PrologDots *dots = nullptr) {
 #define NB_P(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
-    tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, kT3Threads, 0, s>>>(         \
-        in, oscale, oscale_f, J, out, nelv, skip);                                          \
+    if (dots)                                                                               \
+      tensor3_kernel<TIN, TOUT, T, A, B, false, true, true>                                 \
+          <<<(unsigned)nelv, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip,  \
+                                                 *dots);                                    \
+    else                                                                                    \
+      tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, kT3Threads, 0, s>>>(   \
+          in, oscale, oscale_f, J, out, nelv, skip);                                        \
     return cudaGetLastError();                                                              \
   }
   NB_P(2, 4) NB_P(2, 3) NB_P(4, 5) NB_P(4, 6) NB_P(4, 7) NB_P(4, 8) NB_P(4, 9) NB_P(4, 10)
@@ -719,6 +757,21 @@ struct HsmgImpl : public HsmgState {
     return apply_to(zf, r, skip, s);
   }
 
+  // Without a mask the output is assembled by one final gather-scatter of
+  // the prolongation's result, so the inner products with the continuous r
+  // and w_prev can be formed by the prolongation itself.
+  bool dots_in_apply() const override { return merged_assembly(); }
+  cudaError_t apply_dots(double *z, const double *r, const double *w_prev, double *part,
+                         const int *skip, cudaStream_t s) override {
+    if (!merged_assembly()) return cudaErrorNotSupported;
+    PrologDots d;
+    d.r = r;
+    d.w = w_prev;
+    d.part = part;
+    if (sizeof(T) == 4) return apply_to(zf, r, skip, s, &d);  // output stays in zf
+    return apply_to(reinterpret_cast<T *>(z), r, skip, s, &d);
+  }
+
   cudaError_t apply(double *z, const double *r, const int *skip, cudaStream_t s) override {
     T *zs = sizeof(T) == 8 ? reinterpret_cast<T *>(z) : zf;
     cudaError_t e = apply_to(zs, r, skip, s);
@@ -728,8 +781,9 @@ struct HsmgImpl : public HsmgState {
     return cudaGetLastError();
   }
 
-  // zs = M r in the smoothing precision
-  cudaError_t apply_to(T *zs, const double *r, const int *skip, cudaStream_t s) {
+  // zs = M r in the smoothing precision (dots: see apply_dots)
+  cudaError_t apply_to(T *zs, const double *r, const int *skip, cudaStream_t s,
+                       const PrologDots *dots = nullptr) {
     cudaError_t e;
     const long nelv = fine->nelv;
     // fine Schwarz on the side stream: zs = S_f r
@@ -764,7 +818,8 @@ struct HsmgImpl : public HsmgState {
     // mult gs(gs(wt e) + J e_mid) = gs(wt e + mult J e_mid).
     if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s,
                                   merged ? mult_f : nullptr,
-                                  merged && sizeof(T) == 8 ? fine->multf : nullptr)) !=
+                                  merged && sizeof(T) == 8 ? fine->multf : nullptr,
+                                  merged ? dots : nullptr)) !=
         cudaSuccess)
       return e;
     if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, merged ? nullptr : mult_f)) !=
