@@ -36,7 +36,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # case (dram__bytes_read.sum + dram__bytes_write.sum per launch over the
 # points; the part of p and w still dirty in L2 when the launch ends is not
 # counted).
-FUSED_TRAFFIC_B_PER_POINT = {}
+FUSED_TRAFFIC_B_PER_POINT = {8: 85.4}
 
 # Algorithmic bytes of one gather-scatter add per local entry (a point that
 # shares its node with another element): its value read and written, and its
