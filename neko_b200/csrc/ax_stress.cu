@@ -84,7 +84,8 @@ template <int LX, int S, int KS>
 __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
     ax_stress_tma_kernel(StressIo io, StressGeo geo, const double *__restrict__ dx,
                          const double *__restrict__ dy, const double *__restrict__ dz,
-                         const double *__restrict__ w3, const int nelv, int *__restrict__ err,
+                         const double *__restrict__ w3, const double *__restrict__ h2,
+                         const double *__restrict__ Bm, const int nelv, int *__restrict__ err,
                          const int *__restrict__ skip) {
   using C = StressCfg<LX, S, KS>;
   constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS;
@@ -111,15 +112,15 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
   }
   for (int q = tid; q < L3; q += C::THREADS) sW3[q] = w3[q];
   __syncthreads();
-  const double *src[NA] = {io.in[0],  io.in[1],  io.in[2],  geo.h1,   geo.jacinv,
-                           geo.c[0],  geo.c[1],  geo.c[2],  geo.c[3], geo.c[4],
-                           geo.c[5],  geo.c[6],  geo.c[7],  geo.c[8]};
+  // stage slot: u, v, w, h1, 1/jac, the nine cofactors
   auto issue = [&](int t, int s) {
     const long e = b + (long)t * G;
     mbar_arrive_expect_tx(&full[s], (uint32_t)(NA * C::ABYTES));
 #pragma unroll
-    for (int a = 0; a < NA; a++)
-      bulk_g2s(stage + (size_t)(s * NA + a) * L3, src[a] + e * L3, (uint32_t)C::ABYTES, &full[s]);
+    for (int a = 0; a < NA; a++) {
+      const double *src = a < 3 ? io.in[a] : (a == 3 ? geo.h1 : (a == 4 ? geo.jacinv : geo.c[a - 5]));
+      bulk_g2s(stage + (size_t)(s * NA + a) * L3, src + e * L3, (uint32_t)C::ABYTES, &full[s]);
+    }
   };
   if (tid == 0)
     for (int t = 0; t < S && t < nt; t++) issue(t, t);
@@ -148,12 +149,17 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
     }
     const long e = b + (long)t * G;
     const double *slot = stage + (size_t)s * NA * L3;
+    double uown[3][KP];  // u, v, w at this thread's points (for the h2 term)
     if (act) {
       double cu[3][LX];  // this thread's (i, j) column of u, v, w
 #pragma unroll
       for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int l = 0; l < LX; l++) cu[c][l] = slot[c * L3 + col + L2 * l];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int kk = 0; kk < KP; kk++) uown[c][kk] = slot[c * L3 + col + L2 * (k0 + kk)];
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
         const int k = k0 + kk;
@@ -188,7 +194,14 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
     __syncthreads();  // flux planes complete, stage s consumed
     if (tid == 0 && t + S < nt) issue(t + S, s);
     if (act) {
-#pragma unroll 1
+      // h2 B at this thread's points (the part2 term, folded in)
+      double hb[KP];
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) {
+        const long g = e * L3 + col + L2 * (k0 + kk);
+        hb[kk] = h2 ? __ldg(h2 + g) * __ldg(Bm + g) : 0.0;
+      }
+#pragma unroll
       for (int c = 0; c < 3; c++) {
         const double *fr = planes + (3 * c) * L3, *fs = fr + L3, *ft = fs + L3;
         double rt[LX];
@@ -205,7 +218,9 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
             cc += Dytj[l] * fs[i + LX * l + L2 * k];
             d += sDz[l + LX * k] * rt[l];
           }
-          wo[e * L3 + col + L2 * k] = a + cc + d;
+          double v = a + cc + d;
+          if (h2) v = v + hb[kk] * uown[c][kk];  // au + h2 B u, the part2 order
+          wo[e * L3 + col + L2 * k] = v;
         }
       }
     }
@@ -224,7 +239,8 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
 template <int LX, int S, int KS>
 static cudaError_t launch_stress_tma(const StressIo &io, const StressGeo &geo, const double *dx,
                                      const double *dy, const double *dz, const double *w3,
-                                     int nelv, cudaStream_t st, int *err, const int *skip) {
+                                     const double *h2, const double *Bm, int nelv,
+                                     cudaStream_t st, int *err, const int *skip) {
   using C = StressCfg<LX, S, KS>;
   auto kern = ax_stress_tma_kernel<LX, S, KS>;
   static int grid_per_dev[64] = {0};
@@ -244,7 +260,7 @@ static cudaError_t launch_stress_tma(const StressIo &io, const StressGeo &geo, c
   if (!err) err = dropin_error_word();
   if (!err) return cudaErrorInvalidSymbol;
   const int grid = nelv < g ? nelv : g;
-  kern<<<grid, C::THREADS, C::SMEM, st>>>(io, geo, dx, dy, dz, w3, nelv, err, skip);
+  kern<<<grid, C::THREADS, C::SMEM, st>>>(io, geo, dx, dy, dz, w3, h2, Bm, nelv, err, skip);
   return cudaGetLastError();
 }
 
@@ -397,7 +413,7 @@ cudaError_t ax_stress(double *au, double *av, double *aw, const double *u, const
                       const double *w, const double *dx, const double *dy, const double *dz,
                       const double *h1, const double *jacinv, const double *const cof[9],
                       const double *w3, int nelv, int lx, cudaStream_t s, int *err,
-                      const int *skip) {
+                      const int *skip, const double *h2, const double *Bm) {
   StressIo io{{au, av, aw}, {u, v, w}};
   StressGeo geo{h1, jacinv, {cof[0], cof[1], cof[2], cof[3], cof[4], cof[5], cof[6], cof[7],
                              cof[8]}};
@@ -408,21 +424,24 @@ cudaError_t ax_stress(double *au, double *av, double *aw, const double *u, const
     if (reinterpret_cast<uintptr_t>(q) & 15) aligned = false;
   if (aligned) {
     switch (lx) {
-      case 4: return launch_stress_tma<4, 4, 4>(io, geo, dx, dy, dz, w3, nelv, s, err, skip);
-      case 6: return launch_stress_tma<6, 3, 3>(io, geo, dx, dy, dz, w3, nelv, s, err, skip);
-      case 8: return launch_stress_tma<8, 3, 4>(io, geo, dx, dy, dz, w3, nelv, s, err, skip);
+      case 4: return launch_stress_tma<4, 4, 4>(io, geo, dx, dy, dz, w3, h2, Bm, nelv, s, err, skip);
+      case 6: return launch_stress_tma<6, 3, 3>(io, geo, dx, dy, dz, w3, h2, Bm, nelv, s, err, skip);
+      case 8: return launch_stress_tma<8, 3, 4>(io, geo, dx, dy, dz, w3, h2, Bm, nelv, s, err, skip);
       default: break;
     }
   }
+  cudaError_t e;
   switch (lx) {
 #define NB_STRESS_GEN(L) \
-  case L: return launch_stress_gen<L>(io, geo, dx, dy, dz, w3, nelv, s, skip);
+  case L: e = launch_stress_gen<L>(io, geo, dx, dy, dz, w3, nelv, s, skip); break;
     NB_STRESS_GEN(2) NB_STRESS_GEN(3) NB_STRESS_GEN(4) NB_STRESS_GEN(5) NB_STRESS_GEN(6)
     NB_STRESS_GEN(7) NB_STRESS_GEN(8) NB_STRESS_GEN(9) NB_STRESS_GEN(10) NB_STRESS_GEN(11)
     NB_STRESS_GEN(12) NB_STRESS_GEN(13) NB_STRESS_GEN(14) NB_STRESS_GEN(15) NB_STRESS_GEN(16)
 #undef NB_STRESS_GEN
     default: return cudaErrorNotSupported;
   }
+  if (e != cudaSuccess || !h2) return e;
+  return ax_stress_part2(au, av, aw, u, v, w, h2, Bm, (long)nelv * lx * lx * lx, s, skip);
 }
 
 // au += h2 B u, av += h2 B v, aw += h2 B w (the reference's part2 kernel,
@@ -559,7 +578,8 @@ extern "C" void cuda_ax_helm_stress_vector(void *au, void *av, void *aw, void *u
   const double *cof[9] = {d(drdx), d(drdy), d(drdz), d(dsdx), d(dsdy),
                           d(dsdz), d(dtdx), d(dtdy), d(dtdz)};
   stress_fatal(ax_stress(d(au), d(av), d(aw), d(u), d(v), d(w), d(dx), d(dy), d(dz), d(h1),
-                         d(jacinv), cof, d(w3), *nelv, *lx, default_stream(), nullptr, nullptr),
+                         d(jacinv), cof, d(w3), *nelv, *lx, default_stream(), nullptr, nullptr,
+                         nullptr, nullptr),
                "cuda_ax_helm_stress_vector");
 }
 
@@ -581,11 +601,10 @@ cudaError_t problem_ax_stress(nb_problem *P, double *au, double *av, double *aw,
   const long n = P->n;
   const double *cof[9];
   for (int a = 0; a < 9; a++) cof[a] = P->cof + (size_t)a * n;
-  e = ax_stress(au, av, aw, u, v, w, P->D, P->D, P->D, P->h1, P->cof + (size_t)9 * n, cof, P->w3,
-                P->nelv, P->lx, s, P->err, skip);
-  if (e != cudaSuccess) return e;
-  if (P->ifh2) e = ax_stress_part2(au, av, aw, u, v, w, P->h2, P->B, n, s, skip);
-  return e;
+  // the h2 B term in the same pass where the streaming kernel runs
+  return ax_stress(au, av, aw, u, v, w, P->D, P->D, P->D, P->h1, P->cof + (size_t)9 * n, cof,
+                   P->w3, P->nelv, P->lx, s, P->err, skip, P->ifh2 ? P->h2 : nullptr,
+                   P->ifh2 ? P->B : nullptr);
 }
 }  // namespace nb
 

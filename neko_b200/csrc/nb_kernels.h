@@ -43,14 +43,15 @@ cudaError_t ax_helm_vector(double *au, double *av, double *aw, const double *u,
                            const double *g13, const double *g23, int nelv, int lx,
                            cudaStream_t s, int *err, const int *skip = nullptr);
 
-// (au, av, aw) = A_stress (u, v, w), h1 part: the full-stress operator with
+// (au, av, aw) = A_stress (u, v, w): the full-stress operator with
 // cofactors cof[0..8] = drdx, drdy, drdz, dsdx, dsdy, dsdz, dtdx, dtdy, dtdz
-// (ax_stress.cu).  Returns at once when *skip is set.
+// (ax_stress.cu), plus h2 B (u, v, w) when h2 is given (in the same pass on
+// the streaming kernel).  Returns at once when *skip is set.
 cudaError_t ax_stress(double *au, double *av, double *aw, const double *u, const double *v,
                       const double *w, const double *dx, const double *dy, const double *dz,
                       const double *h1, const double *jacinv, const double *const cof[9],
                       const double *w3, int nelv, int lx, cudaStream_t s, int *err,
-                      const int *skip);
+                      const int *skip, const double *h2 = nullptr, const double *Bm = nullptr);
 // au += h2 B u, av += h2 B v, aw += h2 B w
 cudaError_t ax_stress_part2(double *au, double *av, double *aw, const double *u,
                             const double *v, const double *w, const double *h2,

@@ -576,11 +576,16 @@ __global__ void __launch_bounds__(FdmCfg<double, NL>::TPE, FdmCfg<double, NL>::M
   for (int q = u; q < 6 * N2; q += LPE) cp_async_elem<T>(stage + q, s + e * 6 * N2 + q, true);
   cp_async_wait_all();
   __syncthreads();
+  // Row l of a pass's matrix holds the weights of input l for outputs
+  // i = 0..nl-1.  The reference's transforms are tnsr3d(s(2,x), s(1,y),
+  // s(1,z)) forward and tnsr3d(s(1,x), s(2,y), s(2,z)) backward, whose
+  // first matrix contracts as A(i, l) and the other two as Bt(l, j).
   T *fwd = sS, *bwd = sS + 3 * MS;
   for (int q = u; q < 3 * N2; q += LPE) {
-    const int dd = q / N2, rr = q - dd * N2, a = rr % NL, b = rr / NL;
-    fwd[dd * MS + a + C::NLR * b] = stage[(2 * dd + 1) * N2 + a + NL * b];  // s2(a, b)
-    bwd[dd * MS + a + C::NLR * b] = stage[(2 * dd) * N2 + a + NL * b];      // s1(a, b)
+    const int dd = q / N2, rr = q - dd * N2, i = rr % NL, l = rr / NL;
+    const T *s1 = stage + (2 * dd) * N2, *s2 = stage + (2 * dd + 1) * N2;
+    fwd[dd * MS + i + C::NLR * l] = dd == 0 ? s2[i + NL * l] : s1[l + NL * i];
+    bwd[dd * MS + i + C::NLR * l] = dd == 0 ? s1[i + NL * l] : s2[l + NL * i];
   }
   __syncthreads();
   fdm_pass<T, NL, true, false>(b0, b1, fwd, sL, nullptr, u);
