@@ -163,11 +163,21 @@ __global__ void __launch_bounds__(kRedThreads)
 __global__ void __launch_bounds__(1024)
     cg_finish_flex_kernel(const double *__restrict__ part, long nelv, CgState *st) {
   if (st->done) return;
-  double s0 = 0.0, s1 = 0.0;
-  for (long e = threadIdx.x; e < nelv; e += 1024) {
-    s0 += part[2 * e];
-    s1 += part[2 * e + 1];
+  // four independent chains a thread (loads in flight together), summed in
+  // a fixed order
+  double a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
+  for (long e0 = threadIdx.x; e0 < nelv; e0 += 4 * 1024) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const long e = e0 + k * 1024;
+      if (e < nelv) {
+        const double2 v = reinterpret_cast<const double2 *>(part)[e];
+        a0[k] += v.x;
+        a1[k] += v.y;
+      }
+    }
   }
+  double s0 = (a0[0] + a0[1]) + (a0[2] + a0[3]), s1 = (a1[0] + a1[1]) + (a1[2] + a1[3]);
   __shared__ double sh[32];
   s0 = block_sum<1024>(s0, sh);
   s1 = block_sum<1024>(s1, sh);
@@ -217,12 +227,27 @@ __global__ void __launch_bounds__(kRedThreads)
   double *__restrict__ x = st->x;
   const double alpha = st->alpha, malpha = -alpha;
   double s = 0.0;
-  for (long i = blockIdx.x * (long)kRedThreads + threadIdx.x; i < n;
-       i += (long)gridDim.x * kRedThreads) {
-    x[i] = x[i] + alpha * p[i];
-    const double ri = r[i] + malpha * w[i];
-    r[i] = ri;
-    s += ri * MW(i) * ri;
+  // x comes from the state, so the compiler cannot tell it from r: every
+  // operand of a pair of points is loaded before anything is stored
+  const long stride = (long)gridDim.x * kRedThreads;
+  for (long i0 = blockIdx.x * (long)kRedThreads + threadIdx.x; i0 < n; i0 += 2 * stride) {
+    const long i1 = i0 + stride;
+    const bool two = i1 < n;
+    const double x0 = x[i0], p0 = p[i0], r0 = r[i0], w0 = w[i0], m0 = MW(i0);
+    double x1 = 0, p1 = 0, r1 = 0, w1 = 0, m1 = 0;
+    if (two) {
+      x1 = x[i1], p1 = p[i1], r1 = r[i1], w1 = w[i1], m1 = MW(i1);
+    }
+    const double ri0 = r0 + malpha * w0;
+    x[i0] = x0 + alpha * p0;
+    r[i0] = ri0;
+    s += ri0 * m0 * ri0;
+    if (two) {
+      const double ri1 = r1 + malpha * w1;
+      x[i1] = x1 + alpha * p1;
+      r[i1] = ri1;
+      s += ri1 * m1 * ri1;
+    }
   }
   double tot;
   if (grid_sum<kRedThreads>(s, partials, counter, &tot)) {

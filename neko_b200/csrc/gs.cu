@@ -138,49 +138,6 @@ void gs_relayout(const GsMaps &m, const std::vector<unsigned char> &masked, long
     if (masked[i] && !covered[i]) h.extra_mask.push_back((int)i);
 }
 
-// One item list for the whole gather-scatter: the facet pairs become
-// two-entry segments (a + b, the same sum as the pair's), and all items are
-// ordered by the lowest point index they touch, so that the items around
-// one element are summed together and each 32-byte sector of u is fetched
-// once instead of once for the pairs and again for the edge and vertex
-// segments.  Each item keeps its own summation order (map order), so the
-// results are unchanged.
-void gs_unify_sorted(GsHostLayout &h) {
-  const int nseg = (int)h.seg_ptr.size() - 1, npairs = (int)h.pairs.size();
-  const int nit = nseg + npairs;
-  std::vector<int> lo(nit);
-  for (int q = 0; q < nseg; q++) {
-    int m = h.seg_idx[h.seg_ptr[q]];
-    for (int k = h.seg_ptr[q] + 1; k < h.seg_ptr[q + 1]; k++) m = std::min(m, h.seg_idx[k]);
-    lo[q] = m;
-  }
-  for (int p = 0; p < npairs; p++) lo[nseg + p] = std::min(h.pairs[p].x, h.pairs[p].y);
-  std::vector<int> order(nit);
-  for (int q = 0; q < nit; q++) order[q] = q;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return lo[a] < lo[b]; });
-  std::vector<int> ptr(nit + 1, 0), idx;
-  std::vector<unsigned char> msk(nit, 0);
-  idx.reserve(h.seg_idx.size() + 2 * (size_t)npairs);
-  for (int q = 0; q < nit; q++) {
-    const int it = order[q];
-    if (it < nseg) {
-      for (int k = h.seg_ptr[it]; k < h.seg_ptr[it + 1]; k++) idx.push_back(h.seg_idx[k]);
-      msk[q] = h.seg_masked.empty() ? 0 : h.seg_masked[it];
-    } else {
-      const int2 pr = h.pairs[it - nseg];
-      idx.push_back(pr.x);
-      idx.push_back(pr.y);
-      msk[q] = h.pair_masked.empty() ? 0 : h.pair_masked[it - nseg];
-    }
-    ptr[q + 1] = (int)idx.size();
-  }
-  h.seg_ptr.swap(ptr);
-  h.seg_idx.swap(idx);
-  h.seg_masked.swap(msk);
-  h.pairs.clear();
-  h.pair_masked.clear();
-}
-
 // The fused form needs every facet id to occur exactly twice, in adjacent
 // entries (true for conforming meshes); otherwise callers use the
 // two-phase reference path.

@@ -30,9 +30,7 @@ struct GsDevice {
 void gs_relayout(const GsMaps &m, const std::vector<unsigned char> &masked, long n,
                  GsHostLayout &h);
 bool gs_pairs_regular(const GsMaps &m);
-// Pairs folded into the segment list, all items ordered by their lowest
-// point index (same sums, better sector reuse).
-void gs_unify_sorted(GsHostLayout &h);
+
 
 // u = gs_add(u) over g; masked entries become 0 when with_mask; when scale
 // is given every written entry is multiplied by scale[index] (points outside

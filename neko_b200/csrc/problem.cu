@@ -294,7 +294,6 @@ static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
   }
   GsHostLayout hl;
   gs_relayout(P->maps, masked, n, hl);
-  if (!getenv("NB_GS_SPLIT")) gs_unify_sorted(hl);
   // deformed-element flags as mesh_generate_flags (mesh.f90:437-467) computes
   // them from the vertices (always false on an axis-aligned box).
   std::vector<unsigned char> dfrmd(nelv, 0);
