@@ -25,7 +25,9 @@
 #include <cstdlib>
 
 #include "nb_kernels.h"
+#include "nb_precond.h"
 #include "nb_problem.h"
+#include "nb_reduce.cuh"
 #include "nb_tma.cuh"
 
 namespace nb {
@@ -37,6 +39,19 @@ struct StressIo {
 // h1, 1/jac, cofactors drdx, drdy, drdz, dsdx, dsdy, dsdz, dtdx, dtdy, dtdz
 struct StressGeo {
   const double *h1, *jacinv, *c[9];
+};
+
+// The CG step folded into the operator (coupled CG): p_c = z_c + beta p_c
+// formed from the stage and stored, the operator applied to the new p, and
+// pap = sum over local points of p . w with alpha = rtz / pap.  p is zero on
+// masked points (z is) and continuous, so the local sum equals the
+// mult-weighted one after the gather-scatter and mask.
+struct StressCg {
+  const double *z[3] = {nullptr, nullptr, nullptr};
+  double *pout[3] = {nullptr, nullptr, nullptr};
+  CgState *st = nullptr;
+  double *partials = nullptr;
+  unsigned *counter = nullptr;
 };
 
 // Strain and fluxes at one point: g[c][0..2] = (d/dr, d/ds, d/dt) of
@@ -71,26 +86,28 @@ __device__ __forceinline__ void stress_point(const double g[3][3], const double 
 // ---------------------------------------------------------------------------
 // Streaming kernel
 // ---------------------------------------------------------------------------
-template <int LX, int S, int KS>
+template <int LX, int S, int KS, bool CG = false>
 struct StressCfg {
-  static constexpr int L2 = LX * LX, L3 = L2 * LX, NA = 14, NP = 9;
+  static constexpr int L2 = LX * LX, L3 = L2 * LX, NA = CG ? 17 : 14, NP = 9;
   static constexpr int THREADS = ((L2 * KS + 31) / 32) * 32;
   static constexpr size_t ABYTES = (size_t)L3 * sizeof(double);
   static constexpr size_t SMEM =
       S * NA * ABYTES + NP * ABYTES + ABYTES + 3 * L2 * sizeof(double) + 16 * S;
 };
 
-template <int LX, int S, int KS>
-__global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
+template <int LX, int S, int KS, bool CG = false>
+__global__ void __launch_bounds__(StressCfg<LX, S, KS, CG>::THREADS)
     ax_stress_tma_kernel(StressIo io, StressGeo geo, const double *__restrict__ dx,
                          const double *__restrict__ dy, const double *__restrict__ dz,
                          const double *__restrict__ w3, const double *__restrict__ h2,
                          const double *__restrict__ Bm, const int nelv, int *__restrict__ err,
-                         const int *__restrict__ skip) {
-  using C = StressCfg<LX, S, KS>;
+                         const int *__restrict__ skip, StressCg cg) {
+  using C = StressCfg<LX, S, KS, CG>;
   constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS;
   static_assert(LX % KS == 0, "k split must divide lx");
   if (skip && *skip) return;
+  if (CG && cg.st->done) return;
+  const double beta = CG ? cg.st->beta : 0.0;
   extern __shared__ __align__(128) unsigned char smem_stress[];
   double *stage = reinterpret_cast<double *>(smem_stress);
   double *planes = stage + S * NA * L3;  // 9 flux planes: component-major, (r, s, t)
@@ -112,13 +129,16 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
   }
   for (int q = tid; q < L3; q += C::THREADS) sW3[q] = w3[q];
   __syncthreads();
-  // stage slot: u, v, w, h1, 1/jac, the nine cofactors
+  // stage slot: u, v, w, h1, 1/jac, the nine cofactors (+ z_1..z_3 in the
+  // CG form, where u, v, w are the old directions)
   auto issue = [&](int t, int s) {
     const long e = b + (long)t * G;
     mbar_arrive_expect_tx(&full[s], (uint32_t)(NA * C::ABYTES));
 #pragma unroll
     for (int a = 0; a < NA; a++) {
-      const double *src = a < 3 ? io.in[a] : (a == 3 ? geo.h1 : (a == 4 ? geo.jacinv : geo.c[a - 5]));
+      const double *src =
+          a < 3 ? io.in[a]
+                : (a == 3 ? geo.h1 : (a == 4 ? geo.jacinv : (a < 14 ? geo.c[a - 5] : cg.z[a - 14])));
       bulk_g2s(stage + (size_t)(s * NA + a) * L3, src + e * L3, (uint32_t)C::ABYTES, &full[s]);
     }
   };
@@ -140,6 +160,7 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
 
   int t = 0;
   bool failed = false;
+  double pap = 0.0;
   for (; t < nt; t++) {
     const int s = t % S;
     const bool ok = mbar_wait(&full[s], (uint32_t)((t / S) & 1));
@@ -149,6 +170,21 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
     }
     const long e = b + (long)t * G;
     const double *slot = stage + (size_t)s * NA * L3;
+    if constexpr (CG) {  // p = z + beta p for this thread's points, in the stage and stored
+      double *sp = stage + (size_t)s * NA * L3;
+      if (act) {
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int kk = 0; kk < KP; kk++) {
+            const int q = col + L2 * (k0 + kk);
+            const double pn = sp[(14 + c) * L3 + q] + beta * sp[c * L3 + q];
+            sp[c * L3 + q] = pn;
+            cg.pout[c][e * L3 + q] = pn;
+          }
+      }
+      __syncthreads();  // the element's new directions complete in the stage
+    }
     double uown[3][KP];  // u, v, w at this thread's points (for the h2 term)
     if (act) {
       double cu[3][LX];  // this thread's (i, j) column of u, v, w
@@ -221,6 +257,7 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
           double v = a + cc + d;
           if (h2) v = v + hb[kk] * uown[c][kk];  // au + h2 B u, the part2 order
           wo[e * L3 + col + L2 * k] = v;
+          if (CG) pap += uown[c][kk] * v;
         }
       }
     }
@@ -234,15 +271,23 @@ __global__ void __launch_bounds__(StressCfg<LX, S, KS>::THREADS)
     }
     __syncthreads();
   }
+  if constexpr (CG) {
+    double tot;  // every block takes part, a failed one with its partial sum
+    if (grid_sum<C::THREADS>(pap, cg.partials, cg.counter, &tot)) {
+      cg.st->pap = tot;
+      cg.st->alpha = cg.st->rtz1 / tot;
+    }
+  }
 }
 
-template <int LX, int S, int KS>
+template <int LX, int S, int KS, bool CG = false>
 static cudaError_t launch_stress_tma(const StressIo &io, const StressGeo &geo, const double *dx,
                                      const double *dy, const double *dz, const double *w3,
                                      const double *h2, const double *Bm, int nelv,
-                                     cudaStream_t st, int *err, const int *skip) {
-  using C = StressCfg<LX, S, KS>;
-  auto kern = ax_stress_tma_kernel<LX, S, KS>;
+                                     cudaStream_t st, int *err, const int *skip,
+                                     const StressCg &cg = StressCg{}) {
+  using C = StressCfg<LX, S, KS, CG>;
+  auto kern = ax_stress_tma_kernel<LX, S, KS, CG>;
   static int grid_per_dev[64] = {0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -260,7 +305,7 @@ static cudaError_t launch_stress_tma(const StressIo &io, const StressGeo &geo, c
   if (!err) err = dropin_error_word();
   if (!err) return cudaErrorInvalidSymbol;
   const int grid = nelv < g ? nelv : g;
-  kern<<<grid, C::THREADS, C::SMEM, st>>>(io, geo, dx, dy, dz, w3, h2, Bm, nelv, err, skip);
+  kern<<<grid, C::THREADS, C::SMEM, st>>>(io, geo, dx, dy, dz, w3, h2, Bm, nelv, err, skip, cg);
   return cudaGetLastError();
 }
 
@@ -605,6 +650,40 @@ cudaError_t problem_ax_stress(nb_problem *P, double *au, double *av, double *aw,
   return ax_stress(au, av, aw, u, v, w, P->D, P->D, P->D, P->h1, P->cof + (size_t)9 * n, cof,
                    P->w3, P->nelv, P->lx, s, P->err, skip, P->ifh2 ? P->h2 : nullptr,
                    P->ifh2 ? P->B : nullptr);
+}
+}  // namespace nb
+
+namespace nb {
+// The coupled CG's direction update, full-stress operator (with the h2 B
+// term) and curvature in one streaming pass (StressCg); returns
+// cudaErrorNotSupported where the streaming kernel does not apply.
+cudaError_t problem_ax_stress_cg(nb_problem *P, double *const w[3], double *const p[3],
+                                 const double *const z[3], CgState *st, double *partials,
+                                 unsigned *counter, cudaStream_t s) {
+  cudaError_t e = P->ensure_cofactors(s);
+  if (e != cudaSuccess) return e;
+  const long n = P->n;
+  StressIo io{{w[0], w[1], w[2]}, {p[0], p[1], p[2]}};
+  StressGeo geo{P->h1, P->cof + (size_t)9 * n, {}};
+  for (int a = 0; a < 9; a++) geo.c[a] = P->cof + (size_t)a * n;
+  StressCg cg;
+  for (int c = 0; c < 3; c++) {
+    cg.z[c] = z[c];
+    cg.pout[c] = p[c];
+  }
+  cg.st = st;
+  cg.partials = partials;
+  cg.counter = counter;
+  const void *ptrs[] = {p[0], p[1], p[2], z[0], z[1], z[2], P->h1, P->cof};
+  for (const void *q : ptrs)
+    if (reinterpret_cast<uintptr_t>(q) & 15) return cudaErrorNotSupported;
+  const double *h2 = P->ifh2 ? P->h2 : nullptr, *Bm = P->ifh2 ? P->B : nullptr;
+  switch (P->lx) {
+    case 4: return launch_stress_tma<4, 4, 4, true>(io, geo, P->D, P->D, P->D, P->w3, h2, Bm, P->nelv, s, P->err, nullptr, cg);
+    case 6: return launch_stress_tma<6, 3, 3, true>(io, geo, P->D, P->D, P->D, P->w3, h2, Bm, P->nelv, s, P->err, nullptr, cg);
+    case 8: return launch_stress_tma<8, 2, 4, true>(io, geo, P->D, P->D, P->D, P->w3, h2, Bm, P->nelv, s, P->err, nullptr, cg);
+    default: return cudaErrorNotSupported;
+  }
 }
 }  // namespace nb
 

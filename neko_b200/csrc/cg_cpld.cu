@@ -12,9 +12,12 @@
 // rotate_cyc is the identity here (no cyclic boundaries).
 //
 // Differences in form: the scalars live on the device; z_c = M r_c and the
-// next iteration's rtz are formed in the pass that updates x and r, so an
-// iteration is four vector passes (p update, operator, gather-scatter,
-// pap) plus that update; a chunk of iterations is one CUDA graph.
+// next iteration's rtz are formed in the pass that updates x and r; with the
+// full-stress operator on its streaming kernel (lx 4, 6, 8) the direction
+// update p = z + beta p and the curvature (p, w) (summed over local points
+// before the gather-scatter: p is continuous and zero on masked points) are
+// part of the operator's pass, so an iteration is the operator, three
+// gather-scatters and the update; a chunk of iterations is one CUDA graph.
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -31,6 +34,9 @@ namespace nb {
 cudaError_t problem_ax_stress(nb_problem *P, double *au, double *av, double *aw,
                               const double *u, const double *v, const double *w,
                               cudaStream_t s, const int *skip);
+cudaError_t problem_ax_stress_cg(nb_problem *P, double *const w[3], double *const p[3],
+                                 const double *const z[3], CgState *st, double *partials,
+                                 unsigned *counter, cudaStream_t s);
 
 struct V3 {
   double *c[3];
@@ -268,20 +274,40 @@ nb_status cpld_solve(nb_problem *P, int op, double *const xs[3], const double *c
     cudaGraph_t g;
     NB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     cudaError_t ce = cudaSuccess;
+    bool fused = false;
     for (int k = 0; k < chunk && ce == cudaSuccess; k++) {
-      cpld_update_p_kernel<<<eg, 256, 0, cs>>>(p, zc, n, W.st);
-      ce = cudaGetLastError();
-      if (ce == cudaSuccess) ce = cpld_op(P, op, w, p, &W.st->done, cs);
+      // the full-stress operator on the streaming kernel takes the direction
+      // update and the curvature into its pass; otherwise separate passes
+      const cudaError_t fe =
+          op == NB_AX_STRESS
+              ? problem_ax_stress_cg(P, w.c, p.c, zc.c, W.st, W.partials, W.counter, cs)
+              : cudaErrorNotSupported;
+      if (fe == cudaSuccess) {
+        fused = true;
+        for (int c = 0; c < 3 && ce == cudaSuccess; c++)
+          ce = gs_add_fused<double>(P->gsd, w.c[c], true, cs, &W.st->done);
+      } else if (fe != cudaErrorNotSupported) {
+        ce = fe;
+        break;
+      } else {
+        cpld_update_p_kernel<<<eg, 256, 0, cs>>>(p, zc, n, W.st);
+        ce = cudaGetLastError();
+        if (ce == cudaSuccess) ce = cpld_op(P, op, w, p, &W.st->done, cs);
+        if (ce == cudaSuccess)
+          cpld_pap_kernel<<<rb, kRedThreads, 0, cs>>>(wc, pc, P->mult, P->multf, n, W.st,
+                                                      W.partials, W.counter);
+      }
       if (ce == cudaSuccess) {
-        cpld_pap_kernel<<<rb, kRedThreads, 0, cs>>>(wc, pc, P->mult, P->multf, n, W.st,
-                                                    W.partials, W.counter);
         cpld_update_kernel<<<rb, kRedThreads, 0, cs>>>(W.xdev, r, z, pc, wc, d, P->mult,
                                                        P->multf, n, W.st, W.partials, W.counter);
         ce = cudaGetLastError();
       }
     }
-    const int op_launches = 1 + (P->ifh2 ? 1 : 0);
-    W.launches_per_iter = 1 + op_launches + 3 + 2;
+    // the operator: one launch, plus a separate h2 launch except on the
+    // full-stress streaming kernel, which folds the h2 term in
+    const bool h2_folded = op == NB_AX_STRESS && (P->lx == 4 || P->lx == 6 || P->lx == 8);
+    const int op_launches = 1 + (P->ifh2 && !h2_folded ? 1 : 0);
+    W.launches_per_iter = fused ? 1 + 3 + 1 : 1 + op_launches + 3 + 2;
     cudaError_t ee = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
     if (ce != cudaSuccess) {
