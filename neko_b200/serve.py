@@ -62,24 +62,42 @@ class InstancePool:
     """Problem instances for the per-problem solves (hsmg slots): a slot owns
     its instance until it is released, so concurrent requests of one shape
     get distinct instances.  The first instance of a shape is the
-    GeometryCache's problem; the others are created on demand and kept.
-    Every instance has its hsmg preconditioners (the `variants`: False for
-    FP64, True for mixed precision) built when it is created."""
+    GeometryCache's problem; the others are created on demand and kept while
+    the device has room: before a new instance is built, free extra
+    instances (least recently released first) are destroyed until at least
+    `reserve_gb` of device memory is free.  Every instance has its hsmg
+    preconditioners (the `variants`: False for FP64, True for mixed
+    precision) built when it is created."""
 
-    def __init__(self, cache, variants=(False,)):
+    def __init__(self, cache, variants=(False,), reserve_gb=16.0):
         self.cache, self.variants = cache, tuple(variants)
         self.free, self.count, self.setup_s = {}, {}, 0.0
         self.extra = []
+        self.reserve = int(reserve_gb * 1e9)
+        self.released = collections.OrderedDict()  # free extra instances, oldest first
+        self.evicted = 0
+
+    def _make_room(self):
+        while torch.cuda.mem_get_info()[0] < self.reserve and self.released:
+            Pid, (k, P) = self.released.popitem(last=False)
+            self.free[k].remove(P)
+            self.extra.remove(P)
+            self.count[k] -= 1
+            P.close()
+            self.evicted += 1
 
     def acquire(self, spec):
         k = self.cache.key(spec)
         fl = self.free.setdefault(k, [])
         if fl:
-            return fl.pop()
+            P = fl.pop()
+            self.released.pop(id(P), None)
+            return P
         t0 = time.perf_counter()
         if self.count.get(k, 0) == 0:
             P = self.cache.get(spec)
         else:
+            self._make_room()
             P = Problem((spec["n"],) * 3, spec["lx"],
                         deform=workloads.deform_amplitude(spec["dseed"]), dirichlet=True)
             self.extra.append(P)
@@ -90,7 +108,10 @@ class InstancePool:
         return P
 
     def release(self, spec, P):
-        self.free.setdefault(self.cache.key(spec), []).append(P)
+        k = self.cache.key(spec)
+        self.free.setdefault(k, []).append(P)
+        if any(P is q for q in self.extra):
+            self.released[id(P)] = (k, P)
 
     def instances(self):
         return sum(self.count.values())
