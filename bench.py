@@ -320,6 +320,14 @@ def kernel_only(args, cfg):
     if args.kernel_only == "stress":
         v3 = [torch.rand(P.n, dtype=torch.float64, device="cuda") for _ in range(3)]
         o3 = [P.zeros() for _ in range(3)]
+    if args.kernel_only == "dropin_ax":  # separate dx, dy, dz arrays, as Neko passes them
+        import ctypes
+        lib = nb.load()
+        mats = [P.field("dx").clone() for _ in range(3)] + [P.field("dxt").clone() for _ in range(3)]
+        geo = [P.field(k) for k in ("h1", "g11", "g22", "g33", "g12", "g13", "g23")]
+        ci = lambda v: ctypes.byref(ctypes.c_int(v))
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())
+        dstream = ctypes.c_void_p(s.cuda_stream)
     if args.kernel_only in ("dropin_fdm", "dropin_tnsr3d"):
         import ctypes
         lib = nb.load()
@@ -345,6 +353,10 @@ def kernel_only(args, cfg):
             nb.AxHelm().update_p_compute(w, u, z, 0.5, P, stream=s)
         elif args.kernel_only == "stress":
             nb.AxHelmFull().compute_vector(*o3, *v3, P, stream=s)
+        elif args.kernel_only == "dropin_ax":
+            lib.nb_set_default_stream(dstream)
+            lib.cuda_ax_helm(vp(w), vp(u), *(vp(m) for m in mats), *(vp(g) for g in geo),
+                             ci(P.nelv), ci(P.lx))
         elif args.kernel_only == "dropin_fdm":
             lib.cuda_fdm_do_fast(vp(fe), vp(fr), vp(fs), vp(fd), ci(nl), ci(nel), dstream)
         elif args.kernel_only == "dropin_tnsr3d":
@@ -365,7 +377,7 @@ def kernel_only(args, cfg):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
     nl = P.lx + 2
-    nbytes = {"ax": 72 * P.n, "fused": 88 * P.n, "stress": 136 * P.n,
+    nbytes = {"ax": 72 * P.n, "dropin_ax": 72 * P.n, "fused": 88 * P.n, "stress": 136 * P.n,
               "gs": GS_B_PER_ENTRY * P.nlocal,
               # r read and written, e written, d read, six nl x nl matrices read
               "dropin_fdm": P.nelv * (4 * nl ** 3 + 6 * nl * nl) * 8,
@@ -731,7 +743,8 @@ def main():
                     help="skip the CPU oracle solve (cpu_baseline and the parity fields)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision solve measured beside the FP64 one")
-    ap.add_argument("--kernel-only", choices=["ax", "fused", "gs", "stress", "dropin_fdm",
+    ap.add_argument("--kernel-only", choices=["ax", "dropin_ax", "fused", "gs", "stress",
+                                              "dropin_fdm",
                                               "dropin_tnsr3d", "solve"],
                     default=None,
                     help="run only this kernel (or one FP64 + one mixed solve inside a "

@@ -10,6 +10,11 @@
 // Follows the arithmetic of ax_helm_lx (src/math/bcknd/cpu/ax_helm_cpu.f90:
 // 180-290): ur = Dx u, us = Dy u, ut = Dz u; (ur,us,ut) <- h1 G (ur,us,ut);
 // w = Dxt ur + Dyt us + Dzt ut, with D matrices column-major as passed.
+#include <array>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
 #include <cstdio>
 #include <cstdlib>
 
@@ -626,6 +631,38 @@ template cudaError_t ax_helm<float>(float *, const float *, const float *, const
 
 }  // namespace nb
 
+namespace nb {
+// Whether a space's dx, dy, dz (and dxt, dyt, dzt) hold the same matrix.
+// Neko keeps them as three device arrays with equal contents for GLL
+// spaces; the streaming kernel needs one matrix, so the contents are
+// compared once per set of pointers (after the default stream has drained)
+// and the answer is kept.
+bool same_derivatives(const void *dx, const void *dy, const void *dz, const void *dxt,
+                      const void *dyt, const void *dzt, int lx) {
+  if (dx == dy && dx == dz && dxt == dyt && dxt == dzt) return true;
+  static std::mutex mu;
+  static std::map<std::array<const void *, 6>, std::pair<int, bool>> known;
+  const std::array<const void *, 6> key{dx, dy, dz, dxt, dyt, dzt};
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = known.find(key);
+  if (it != known.end() && it->second.first == lx) return it->second.second;
+  bool same = false;
+  if (cudaStreamSynchronize(default_stream()) == cudaSuccess) {
+    const size_t b = (size_t)lx * lx * sizeof(double);
+    std::vector<char> m[6];
+    bool ok = true;
+    for (int q = 0; q < 6 && ok; q++) {
+      m[q].resize(b);
+      ok = cudaMemcpy(m[q].data(), key[q], b, cudaMemcpyDeviceToHost) == cudaSuccess;
+    }
+    same = ok && !memcmp(m[0].data(), m[1].data(), b) && !memcmp(m[0].data(), m[2].data(), b) &&
+           !memcmp(m[3].data(), m[4].data(), b) && !memcmp(m[3].data(), m[5].data(), b);
+  }
+  known[key] = {lx, same};
+  return same;
+}
+}  // namespace nb
+
 extern "C" void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, void *dxt,
                              void *dyt, void *dzt, void *h1, void *g11, void *g22, void *g33,
                              void *g12, void *g13, void *g23, int *nelv, int *lx) {
@@ -634,7 +671,7 @@ extern "C" void cuda_ax_helm(void *w, void *u, void *dx, void *dy, void *dz, voi
     exit(1);
   }
   cudaError_t e = cudaErrorNotSupported;
-  if (dx == dy && dx == dz && dxt == dyt && dxt == dzt)
+  if (nb::same_derivatives(dx, dy, dz, dxt, dyt, dzt, *lx))
     e = nb::ax_helm_stream<double>((double *)w, (const double *)u, (const double *)dx,
                                    (const double *)dxt, (const double *)h1, (const double *)g11,
                                    (const double *)g22, (const double *)g33, (const double *)g12,

@@ -252,7 +252,7 @@ extern "C" void cuda_ax_helm_vector(void *au, void *av, void *aw, void *u, void 
   const cudaStream_t s = default_stream();
   cudaError_t e;
   auto d = [](void *p) { return (double *)p; };
-  if (dx == dy && dx == dz && dxt == dyt && dxt == dzt) {
+  if (same_derivatives(dx, dy, dz, dxt, dyt, dzt, *lx)) {
     e = ax_helm_vector(d(au), d(av), d(aw), d(u), d(v), d(w), d(dx), d(dxt), d(h1), d(g11),
                        d(g22), d(g33), d(g12), d(g13), d(g23), *nelv, *lx, s, nullptr);
   } else {

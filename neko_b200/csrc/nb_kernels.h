@@ -28,6 +28,11 @@ cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h
                            const T *g13, const T *g23, int nelv, int lx, cudaStream_t s,
                            const int *skip = nullptr, int *err = nullptr);
 
+// True when dx, dy, dz (and dxt, dyt, dzt) hold the same lx x lx matrix
+// (pointer-equal, or equal contents, compared once per pointer set).
+bool same_derivatives(const void *dx, const void *dy, const void *dz, const void *dxt,
+                      const void *dyt, const void *dzt, int lx);
+
 // Reads and clears the error word of the drop-in cuda_ax_helm (0 = no
 // error); kernels given a null error word record their timeouts there.
 int take_dropin_error();

@@ -142,6 +142,38 @@ def test_drop_in_ax_helm(nb, oracle, nblib):
     assert rel_err(_np(w), O.ax_helm(_np(u))) <= AX_RTOL
 
 
+@pytest.mark.parametrize("lx", [8, 7])
+def test_drop_in_ax_helm_separate_matrices(nb, oracle, nblib, lx):
+    """cuda_ax_helm with dx, dy, dz (and the transposes) as three separate
+    device arrays of equal contents, as Neko's space_t holds them: the
+    library recognises them as one matrix (the streaming kernel at lx 8) and
+    the result is the oracle's; then dy is changed, so the three differ and
+    the general kernel must take them as given."""
+    P, O = _pair(nb, oracle, (4, 3, 3), lx, (True,) * 3, 0.05, 0.0, 2 * np.pi)
+    rng = np.random.default_rng(13)
+    u = _cuda(rng.uniform(-1, 1, P.n))
+    f = {k: P.field(k) for k in ("dx", "dxt", "h1", "g11", "g22", "g33", "g12", "g13", "g23")}
+    dx, dy, dz = f["dx"].clone(), f["dx"].clone(), f["dx"].clone()
+    dxt, dyt, dzt = f["dxt"].clone(), f["dxt"].clone(), f["dxt"].clone()
+    nelv, lxc = ctypes.c_int(P.nelv), ctypes.c_int(P.lx)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def run():
+        w = P.zeros()
+        nblib.cuda_ax_helm(vp(w), vp(u), vp(dx), vp(dy), vp(dz), vp(dxt), vp(dyt), vp(dzt),
+                           *(vp(f[k]) for k in ("h1", "g11", "g22", "g33", "g12", "g13", "g23")),
+                           ctypes.byref(nelv), ctypes.byref(lxc))
+        torch.cuda.synchronize()
+        return _np(w)
+
+    assert rel_err(run(), O.ax_helm(_np(u))) <= AX_RTOL
+    # different dy (new arrays, so nothing cached applies): the general kernel
+    dy = f["dx"].clone() * 0.5
+    dyt = f["dxt"].clone() * 0.5
+    w2 = run()
+    assert not np.allclose(w2, O.ax_helm(_np(u)))
+
+
 @pytest.mark.parametrize("nel,lx,per,amp,lo,hi", CASES)
 def test_gs_add_bit_exact(nb, oracle, nel, lx, per, amp, lo, hi):
     P, O = _pair(nb, oracle, nel, lx, per, amp, lo, hi)
