@@ -306,19 +306,16 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
 
 // e(i,j,k) = ext interior + neighbours' ghost results on the first interior
 // layers (x, then y, then z, as the extrude passes add them), times the
-// overlap weight.  The neighbour table is read up front and every operand
-// load is issued before the first add, so a thread waits on one round trip.
+// overlap weight, for point q of element e.  The neighbour table is read up
+// front and every operand load is issued before the first add, so a thread
+// waits on one round trip.
 template <typename T, int LX>
-__global__ void __launch_bounds__(256)
-    schwarz_post_kernel(const T *__restrict__ ext, const int *__restrict__ fn,
-                        const unsigned char *__restrict__ ornt, const T *__restrict__ wt,
-                        T *__restrict__ out, long nelv, const int *__restrict__ skip) {
-  if (skip && *skip) return;
+__device__ __forceinline__ T schwarz_post_point(const T *__restrict__ ext,
+                                                const int *__restrict__ fn,
+                                                const unsigned char *__restrict__ ornt,
+                                                const T *__restrict__ wt, long e, int q) {
   constexpr int NL = LX + 2, L2 = LX * LX, L3 = L2 * LX, N2 = NL * NL, N3 = N2 * NL;
-  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (p >= nelv * L3) return;
-  const long e = p / L3;
-  const int q = (int)(p - e * L3), i = q % LX, j = (q / LX) % LX, k = q / L2;
+  const int i = q % LX, j = (q / LX) % LX, k = q / L2;
   const int2 *f2 = reinterpret_cast<const int2 *>(fn + e * 6);
   const int2 fa = __ldg(f2), fb = __ldg(f2 + 1), fc = __ldg(f2 + 2);
   const int f[6] = {fa.x, fa.y, fb.x, fb.y, fc.x, fc.y};
@@ -347,11 +344,24 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int d = 0; d < 6; d++) g[d] = c[d] ? ext[(long)(f[d] - 1) * N3 + off[d]] : T(0);
   T v = ext[e * N3 + (i + 1) + NL * (j + 1) + N2 * (k + 1)];
-  const T w = wt[p];
+  const T w = wt[e * L3 + q];
 #pragma unroll
   for (int d = 0; d < 6; d++)
     if (c[d]) v += g[d];
-  out[p] = v * w;
+  return v * w;
+}
+
+template <typename T, int LX>
+__global__ void __launch_bounds__(256)
+    schwarz_post_kernel(const T *__restrict__ ext, const int *__restrict__ fn,
+                        const unsigned char *__restrict__ ornt, const T *__restrict__ wt,
+                        T *__restrict__ out, long nelv, const int *__restrict__ skip) {
+  if (skip && *skip) return;
+  constexpr int L3 = LX * LX * LX;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= nelv * L3) return;
+  const long e = p / L3;
+  out[p] = schwarz_post_point<T, LX>(ext, fn, ornt, wt, e, (int)(p - e * L3));
 }
 
 // out = (A x A x A) in per element, A(o, i) = TR ? M[i + NI*o] : M[o + NO*i];
@@ -372,13 +382,25 @@ struct PrologDots {
   double *part = nullptr;  // 2 per element
 };
 
+// With POST (prolongation into the fine level), the value the prolongation
+// adds to is not read from `out` but formed here: the fine Schwarz post step
+// (schwarz_post_point) of the FDM output, so the post and the prolongation
+// are one pass over the fine level.
+template <typename T>
+struct PostArgs {
+  const T *ext = nullptr, *wt = nullptr;
+  const int *fn = nullptr;
+  const unsigned char *ornt = nullptr;
+};
+
 template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC,
-          bool DOT = false>
+          bool DOT = false, bool POST = false>
 __global__ void __launch_bounds__(kT3Threads)
     tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
                    const float *__restrict__ scale_f,
                    const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
-                   const int *__restrict__ skip, PrologDots dots = PrologDots{}) {
+                   const int *__restrict__ skip, PrologDots dots = PrologDots{},
+                   PostArgs<TOUT> post = PostArgs<TOUT>{}) {
   if (skip && *skip) return;
   constexpr int I3 = NI * NI * NI, O3 = NO * NO * NO, NT = kT3Threads;
   __shared__ T su[I3], s1[NO * NI * NI], s2[NO * NO * NI], sA[NO * NI];
@@ -438,7 +460,12 @@ __global__ void __launch_bounds__(kT3Threads)
 #pragma unroll
     for (int g = 0; g < RO; g++) {
       const int q = tid + g * NT;
-      prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
+      if constexpr (POST)
+        prev[g] = q < O3 ? schwarz_post_point<TOUT, NO>(post.ext, post.fn, post.ornt, post.wt,
+                                                         e, q)
+                         : TOUT(0);
+      else
+        prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
       oscale[g] = (scale && q < O3)
                       ? (scale_f ? (TIN)scale_f[e * O3 + q] : scale[e * O3 + q])
                       : TIN(1);
@@ -512,7 +539,7 @@ struct SchwarzLevel {
 
 template <typename TIN, typename T, int LX>
 static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
-                                   cudaStream_t s) {
+                                   cudaStream_t s, bool post = true) {
   constexpr int NL = LX + 2;
   using C = FdmCfg<T, NL>;
   auto kern = fdm_kernel<TIN, T, NL>;
@@ -527,6 +554,7 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
   }
   kern<<<(unsigned)((L.nelv + C::EPW - 1) / C::EPW), C::TPE, C::SMEM, s>>>(
       r, L.fn, L.ornt, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
+  if (!post) return cudaGetLastError();  // the prolongation forms the post step
   const long n = L.nelv * LX * LX * LX;
   schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       L.ext, L.fn, L.ornt, L.wt, e, L.nelv, skip);
@@ -536,11 +564,11 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
 // e = Schwarz(r) on level L (r already masked): FDM + overlap + gs + mask.
 template <typename TIN, typename T>
 static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
-                                 cudaStream_t s, bool assemble = true) {
+                                 cudaStream_t s, bool assemble = true, bool post = true) {
   cudaError_t err;
   switch (L.lx) {
 #define NB_S(N) \
-  case N: err = launch_fdm_post<TIN, T, N>(L, r, e, skip, s); break;
+  case N: err = launch_fdm_post<TIN, T, N>(L, r, e, skip, s, post); break;
     NB_S(3) NB_S(4) NB_S(5) NB_S(6) NB_S(7) NB_S(8) NB_S(9) NB_S(10) NB_S(11) NB_S(12)
     NB_S(13) NB_S(14)
 #undef NB_S
@@ -660,16 +688,25 @@ template <typename TIN, typename TOUT, typename T>
 static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *out, long nelv,
                                const int *skip, cudaStream_t s, const TIN *oscale = nullptr,
                                const float *oscale_f = nullptr,
-                               const PrologDots *dots = nullptr) {
+                               const PrologDots *dots = nullptr,
+                               const PostArgs<TOUT> *post = nullptr) {
+  const PrologDots d0 = dots ? *dots : PrologDots{};
+  const PostArgs<TOUT> p0 = post ? *post : PostArgs<TOUT>{};
 #define NB_P(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
-    if (dots)                                                                               \
+    const unsigned g = (unsigned)nelv;                                                      \
+    if (dots && post)                                                                       \
+      tensor3_kernel<TIN, TOUT, T, A, B, false, true, true, true>                           \
+          <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip, d0, p0);      \
+    else if (post)                                                                          \
+      tensor3_kernel<TIN, TOUT, T, A, B, false, true, false, true>                          \
+          <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip, d0, p0);      \
+    else if (dots)                                                                          \
       tensor3_kernel<TIN, TOUT, T, A, B, false, true, true>                                 \
-          <<<(unsigned)nelv, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip,  \
-                                                 *dots);                                    \
+          <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip, d0);          \
     else                                                                                    \
-      tensor3_kernel<TIN, TOUT, T, A, B, false, true><<<(unsigned)nelv, kT3Threads, 0, s>>>(   \
-          in, oscale, oscale_f, J, out, nelv, skip);                                        \
+      tensor3_kernel<TIN, TOUT, T, A, B, false, true>                                       \
+          <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip);              \
     return cudaGetLastError();                                                              \
   }
   NB_P(2, 4) NB_P(2, 3) NB_P(4, 5) NB_P(4, 6) NB_P(4, 7) NB_P(4, 8) NB_P(4, 9) NB_P(4, 10)
@@ -738,8 +775,9 @@ struct HsmgImpl : public HsmgState {
 
   int launches() const override {
     // 2 Schwarz x (fdm, post, gs) + restrict + gs + coarse (one launch) +
-    // prolong + final gs (+ convert); one gs fewer when merged
-    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0) - (merged_assembly() ? 1 : 0);
+    // prolong + final gs (+ convert); when merged the fine Schwarz has
+    // neither its own gs nor its own post launch
+    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0) - (merged_assembly() ? 2 : 0);
   }
 
   int take_error() override {
@@ -811,8 +849,12 @@ struct HsmgImpl : public HsmgState {
     if ((e = cudaEventRecord(ev_join_hi, hi)) != cudaSuccess) return e;
     // fine Schwarz on the side stream: zs = S_f r (left unassembled when the
     // final gather-scatter takes it, see below)
+    // Without a mask the post step of the fine Schwarz is left to the
+    // prolongation (one pass over the fine level after the join), so the
+    // side stream runs the FDM alone.
     const bool merged = merged_assembly();
-    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side, !merged)) != cudaSuccess) return e;
+    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side, !merged, !merged)) != cudaSuccess)
+      return e;
     if ((e = cudaEventRecord(ev_join, side)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s, ev_join, 0)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(s, ev_join_hi, 0)) != cudaSuccess)
@@ -821,10 +863,15 @@ struct HsmgImpl : public HsmgState {
     // Schwarz output's own gather-scatter is folded into this one: wt and
     // mult are the same at every copy of a point, so
     // mult gs(gs(wt e) + J e_mid) = gs(wt e + mult J e_mid).
+    PostArgs<T> post;
+    post.ext = sf.ext;
+    post.wt = sf.wt;
+    post.fn = sf.fn;
+    post.ornt = sf.ornt;
     if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s,
                                   merged ? mult_f : nullptr,
                                   merged && sizeof(T) == 8 ? fine->multf : nullptr,
-                                  merged ? dots : nullptr)) !=
+                                  merged ? dots : nullptr, merged ? &post : nullptr)) !=
         cudaSuccess)
       return e;
     if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, merged ? nullptr : mult_f)) !=
