@@ -663,10 +663,10 @@ def run_serve(args):
     B = nb.Batch(hbm_budget=max(int(args.serve_budget_gb * 1e9) - cache.device_bytes(), 1))
     zeros = np.zeros(len(cap_specs))
     serve.serve_batched(cap_specs, zeros, pool, 0, batch=B, mode="mixed", instances=inst,
-                        max_solves=args.max_solves, stream=stream)
+                        max_solves=args.max_solves, stream=stream, keep_solutions=False)
     _, _, _, span, _ = serve.serve_batched(cap_specs, zeros, pool, 0, batch=B, mode="mixed",
                                            instances=inst, max_solves=args.max_solves,
-                                           stream=stream)
+                                           stream=stream, keep_solutions=False)
     capacity = len(cap_specs) / span
     rates = [float(r) for r in args.serve_rates.split(",")]
     if min(rates) >= capacity:
@@ -684,13 +684,15 @@ def run_serve(args):
         head = specs[:min(len(specs), 2000)]
         for mode in ("mixed", "fp64"):
             serve.serve_batched(head, np.zeros(len(head)), pool, 0, batch=B, mode=mode,
-                                instances=inst, max_solves=args.max_solves, stream=stream)
+                                instances=inst, max_solves=args.max_solves, stream=stream,
+                                keep_solutions=False)
         r = {}
         for mode in ("mixed", "fp64"):
             status = []
             lat, it, conv, span, _ = serve.serve_batched(
                 specs, t_arr, pool, 0, batch=B, mode=mode, instances=inst,
-                max_solves=args.max_solves, stream=stream, status=status)
+                max_solves=args.max_solves, stream=stream, status=status,
+                keep_solutions=False)
             r[mode] = dict(serve.percentiles(lat), solves_per_s=len(specs) / span,
                            requests=len(specs), converged=int(sum(conv)),
                            mean_iter=float(np.mean(it)), span_s=span)

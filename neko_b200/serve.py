@@ -165,7 +165,7 @@ OK, NOT_CONVERGED, NAN, OOM_REJECTED, TIMEOUT, CANCELLED = (
 
 def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000, chunk_runs=1,
                   batch=None, stream=None, cancel=None, status=None, mode="jacobi",
-                  instances=None, max_solves=64):
+                  instances=None, max_solves=64, keep_solutions=True):
     """Continuous-batching server.  Returns per-request latency (s),
     iterations, convergence flags, the span of the run (s) and the solutions
     (request index -> device tensor).
@@ -177,6 +177,10 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
     smoothing with FP64 outer iteration for "mixed") on instances of
     `instances` (an InstancePool), at most `max_solves` at a time, all
     advanced together by the same run loop.
+
+    keep_solutions=False drops each request's solution once it has been
+    answered (a long stream's solutions would otherwise fill the device);
+    the returned dict is then empty.
 
     A request may set "max_iter" in its spec.  `cancel` maps request index ->
     time (s after the start) at which the client withdraws it; a withdrawn
@@ -213,6 +217,8 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
         i = active.pop(slot)
         if slot in owned:
             instances.release(specs[i], owned.pop(slot))
+        if not keep_solutions:
+            xs.pop(i, None)
         return i
 
     while done_count < n:
