@@ -321,16 +321,23 @@ cudaError_t ax_helm_stream(T *w, const T *u, const T *D, const T *Dt, const T *h
 // points, stores it, and the element's operator then reads it from the
 // stage.  Returns at once when st->done is set.
 // ---------------------------------------------------------------------------
-template <int LX, int S, int KS>
+// AL (lx = 10): the three work planes live in the stage itself, over the
+// G11, G22, G33 arrays of the element being computed (each thread reads the
+// six factors of a point before it writes that point's three fluxes, and no
+// thread reads another point's factors), which frees the room for a third
+// stage; the stage is then refilled after the second pass instead of the
+// first, so two elements are in flight while one is computed.
+template <int LX, int S, int KS, bool AL = false>
 struct AxCgCfg {
   static constexpr int L2 = LX * LX, L3 = L2 * LX, NA = 9;
   static constexpr int THREADS = ((L2 * KS + 31) / 32) * 32;
   static constexpr size_t ABYTES = (size_t)L3 * sizeof(double);
-  static constexpr size_t SMEM = S * NA * ABYTES + 3 * ABYTES + 2 * L2 * sizeof(double) + 16 * S;
+  static constexpr size_t SMEM =
+      S * NA * ABYTES + (AL ? 0 : 3 * ABYTES) + 2 * L2 * sizeof(double) + 16 * S;
 };
 
-template <int LX, int S, int KS, typename TZ>
-__global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
+template <int LX, int S, int KS, typename TZ, bool AL = false>
+__global__ void __launch_bounds__(AxCgCfg<LX, S, KS, AL>::THREADS)
     ax_cg_fused_kernel(double *__restrict__ w, double *__restrict__ p,
                        const TZ *__restrict__ z, const double *__restrict__ D,
                        const double *__restrict__ Dt, const double *__restrict__ h1,
@@ -339,14 +346,14 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
                        const double *__restrict__ g13, const double *__restrict__ g23,
                        const int nelv, CgState *st, double beta_arg, double *pap_out,
                        double *partials, unsigned *counter, int *__restrict__ err) {
-  using C = AxCgCfg<LX, S, KS>;
+  using C = AxCgCfg<LX, S, KS, AL>;
   constexpr int L2 = C::L2, L3 = C::L3, NA = C::NA, KP = LX / KS, THREADS = C::THREADS;
   static_assert(LX % KS == 0, "k split must divide lx");
   if (st && st->done) return;
   extern __shared__ __align__(128) unsigned char smem_ring[];
   double *stage = reinterpret_cast<double *>(smem_ring);
   double *sur = stage + S * NA * L3, *sus = sur + L3, *sut = sus + L3;
-  double *sD = sut + L3, *sDt = sD + L2;
+  double *sD = AL ? stage + S * NA * L3 : sut + L3, *sDt = sD + L2;
   uint64_t *full = reinterpret_cast<uint64_t *>(sDt + L2);
 
   const int tid = threadIdx.x;
@@ -403,6 +410,9 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
     double *su = stage + (size_t)s * NA * L3 + L3;  // old p, replaced by the new
     const double *sh = su + L3, *s11 = su + 2 * L3, *s22 = su + 3 * L3, *s33 = su + 4 * L3,
                  *s12 = su + 5 * L3, *s13 = su + 6 * L3, *s23 = su + 7 * L3;
+    // work planes: separate, or over this stage's G11, G22, G33 (AL)
+    double *wr = AL ? su + 2 * L3 : sur, *wsp = AL ? su + 3 * L3 : sus,
+           *wtp = AL ? su + 4 * L3 : sut;
     if (act) {
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
@@ -413,10 +423,12 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
       }
     }
     __syncthreads();  // the element's new p complete in the stage
-    double ru[LX];
+    double ru[LX], pown[KP];  // p column; p at this thread's points
     if (act) {
 #pragma unroll
       for (int l = 0; l < LX; l++) ru[l] = su[col + L2 * l];
+#pragma unroll
+      for (int kk = 0; kk < KP; kk++) pown[kk] = su[col + L2 * (k0 + kk)];
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
         const int k = k0 + kk;
@@ -431,33 +443,34 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
         const double H = sh[q];
         const double a11 = s11[q], a22 = s22[q], a33 = s33[q], a12 = s12[q], a13 = s13[q],
                      a23 = s23[q];
-        sur[q] = H * (a11 * ur + a12 * us + a13 * ut);
-        sus[q] = H * (a12 * ur + a22 * us + a23 * ut);
-        sut[q] = H * (a13 * ur + a23 * us + a33 * ut);
+        wr[q] = H * (a11 * ur + a12 * us + a13 * ut);
+        wsp[q] = H * (a12 * ur + a22 * us + a23 * ut);
+        wtp[q] = H * (a13 * ur + a23 * us + a33 * ut);
       }
     }
-    __syncthreads();  // stage s consumed, work planes complete
-    if (tid == 0 && t + S < nt) issue(t + S, s);
+    __syncthreads();  // stage s consumed (but for AL's planes), work planes complete
+    if (!AL && tid == 0 && t + S < nt) issue(t + S, s);
     if (act) {
       double rt[LX];
 #pragma unroll
-      for (int l = 0; l < LX; l++) rt[l] = sut[col + L2 * l];
+      for (int l = 0; l < LX; l++) rt[l] = wtp[col + L2 * l];
 #pragma unroll
       for (int kk = 0; kk < KP; kk++) {
         const int k = k0 + kk;
         double a = 0, c = 0, d = 0;
 #pragma unroll
         for (int l = 0; l < LX; l++) {
-          a += Dti[l] * sur[l + LX * j + L2 * k];
-          c += Dtj[l] * sus[i + LX * l + L2 * k];
+          a += Dti[l] * wr[l + LX * j + L2 * k];
+          c += Dtj[l] * wsp[i + LX * l + L2 * k];
           d += sDt[k + LX * l] * rt[l];
         }
         const double wq = a + c + d;
         w[e * L3 + col + L2 * k] = wq;
-        pap += ru[k] * wq;
+        pap += pown[kk] * wq;
       }
     }
     __syncthreads();  // work planes free for the next element
+    if (AL && tid == 0 && t + S < nt) issue(t + S, s);
   }
   if (failed) {
     if (tid == 0) {
@@ -478,15 +491,15 @@ __global__ void __launch_bounds__(AxCgCfg<LX, S, KS>::THREADS)
   }
 }
 
-template <int LX, int S, int KS, typename TZ>
+template <int LX, int S, int KS, typename TZ, bool AL = false>
 static cudaError_t launch_ax_cg(double *w, double *p, const TZ *z, const double *D,
                                 const double *Dt, const double *h1, const double *g11,
                                 const double *g22, const double *g33, const double *g12,
                                 const double *g13, const double *g23, int nelv, CgState *st,
                                 double beta, double *pap_out, double *partials,
                                 unsigned *counter, int max_grid, cudaStream_t s, int *err) {
-  using C = AxCgCfg<LX, S, KS>;
-  auto kern = ax_cg_fused_kernel<LX, S, KS, TZ>;
+  using C = AxCgCfg<LX, S, KS, AL>;
+  auto kern = ax_cg_fused_kernel<LX, S, KS, TZ, AL>;
   static int grid_per_dev[64] = {0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -523,7 +536,7 @@ cudaError_t ax_cg_fused(double *w, double *p, const TZ *z, const double *D, cons
   switch (lx) {
     case 6: return launch_ax_cg<6, 3, 2, TZ>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
     case 8: return launch_ax_cg<8, 2, 2, TZ>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
-    case 10: return launch_ax_cg<10, 2, 5, TZ>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
+    case 10: return launch_ax_cg<10, 3, 5, TZ, true>(w, p, z, D, Dt, h1, g11, g22, g33, g12, g13, g23, nelv, st, beta, pap_out, partials, counter, max_grid, s, err);
     default: return cudaErrorNotSupported;
   }
 }
