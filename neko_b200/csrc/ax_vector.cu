@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(AxVecCfg<LX, S, KS>::THREADS)
     const double *sh = slot + 3 * L3, *s11 = slot + 4 * L3, *s22 = slot + 5 * L3,
                  *s33 = slot + 6 * L3, *s12 = slot + 7 * L3, *s13 = slot + 8 * L3,
                  *s23 = slot + 9 * L3;
-#pragma unroll 1
+#pragma unroll
     for (int c = 0; c < 3; c++) {
       const double *su = slot + c * L3;
       if (act) {
