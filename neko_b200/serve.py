@@ -65,9 +65,10 @@ class InstancePool:
     GeometryCache's problem; the others are created on demand and kept while
     the device has room: before a new instance is built, free extra
     instances (least recently released first) are destroyed until at least
-    `reserve_gb` of device memory is free.  Every instance has its hsmg
-    preconditioners (the `variants`: False for FP64, True for mixed
-    precision) built when it is created."""
+    `reserve_gb` of device memory is free.  An instance's hsmg
+    preconditioner of a precision (False for FP64, True for mixed; one of
+    `variants`) is built the first time a request of that precision takes
+    the instance, so an instance holds only the precisions it served."""
 
     def __init__(self, cache, variants=(False,), reserve_gb=16.0):
         self.cache, self.variants = cache, tuple(variants)
@@ -76,6 +77,7 @@ class InstancePool:
         self.reserve = int(reserve_gb * 1e9)
         self.released = collections.OrderedDict()  # free extra instances, oldest first
         self.evicted = 0
+        self.built = {}  # id(instance) -> precisions whose hsmg exists
 
     def _make_room(self):
         while torch.cuda.mem_get_info()[0] < self.reserve and self.released:
@@ -83,15 +85,28 @@ class InstancePool:
             self.free[k].remove(P)
             self.extra.remove(P)
             self.count[k] -= 1
+            self.built.pop(Pid, None)
             P.close()
             self.evicted += 1
 
-    def acquire(self, spec):
+    def _ensure(self, P, mixed):
+        b = self.built.setdefault(id(P), set())
+        if mixed not in b:
+            t0 = time.perf_counter()
+            Hsmg(mixed=mixed).init(P)
+            self.setup_s += time.perf_counter() - t0
+            b.add(mixed)
+
+    def acquire(self, spec, mixed=None):
+        """An instance of spec's shape with the hsmg of precision `mixed`
+        built (the first of `variants` when None)."""
+        m = self.variants[0] if mixed is None else bool(mixed)
         k = self.cache.key(spec)
         fl = self.free.setdefault(k, [])
         if fl:
             P = fl.pop()
             self.released.pop(id(P), None)
+            self._ensure(P, m)
             return P
         t0 = time.perf_counter()
         if self.count.get(k, 0) == 0:
@@ -101,10 +116,9 @@ class InstancePool:
             P = Problem((spec["n"],) * 3, spec["lx"],
                         deform=workloads.deform_amplitude(spec["dseed"]), dirichlet=True)
             self.extra.append(P)
-        for m in self.variants:
-            Hsmg(mixed=m).init(P)
         self.count[k] = self.count.get(k, 0) + 1
         self.setup_s += time.perf_counter() - t0
+        self._ensure(P, m)
         return P
 
     def release(self, spec, P):
@@ -237,7 +251,7 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
                 break
             P, f, r0 = pool.get(sp)
             x = torch.empty(P.n, dtype=torch.float64, device="cuda")
-            Pi = instances.acquire(sp) if solo else None
+            Pi = instances.acquire(sp, mixed=mode == "mixed") if solo else None
             try:
                 if solo:
                     slot = B.submit_solve(Pi, f, x, rel_tol * r0, sp.get("max_iter", max_iter),

@@ -22,11 +22,13 @@ class FakeProblem:
 
 
 class FakeHsmg:
+    built = []
+
     def __init__(self, mixed=False):
-        pass
+        self.mixed = mixed
 
     def init(self, P):
-        pass
+        FakeHsmg.built.append((id(P), self.mixed))
 
 
 class FakeCache:
@@ -95,3 +97,16 @@ def test_in_use_instances_are_never_evicted(pool):
     p.acquire(spec(7))
     p.acquire(spec(7))
     assert p.evicted == 0 and not any(h.closed for h in held)
+
+
+def test_precisions_built_on_first_use(pool):
+    p, _ = pool
+    FakeHsmg.built.clear()
+    a = p.acquire(spec(3), mixed=True)
+    assert FakeHsmg.built == [(id(a), True)]
+    p.release(spec(3), a)
+    assert p.acquire(spec(3), mixed=True) is a
+    assert len(FakeHsmg.built) == 1  # nothing rebuilt
+    p.release(spec(3), a)
+    p.acquire(spec(3), mixed=False)
+    assert FakeHsmg.built[-1] == (id(a), False) and len(FakeHsmg.built) == 2
