@@ -382,25 +382,13 @@ struct PrologDots {
   double *part = nullptr;  // 2 per element
 };
 
-// With POST (prolongation into the fine level), the value the prolongation
-// adds to is not read from `out` but formed here: the fine Schwarz post step
-// (schwarz_post_point) of the FDM output, so the post and the prolongation
-// are one pass over the fine level.
-template <typename T>
-struct PostArgs {
-  const T *ext = nullptr, *wt = nullptr;
-  const int *fn = nullptr;
-  const unsigned char *ornt = nullptr;
-};
-
 template <typename TIN, typename TOUT, typename T, int NI, int NO, bool TR, bool ACC,
-          bool DOT = false, bool POST = false>
+          bool DOT = false>
 __global__ void __launch_bounds__(kT3Threads)
     tensor3_kernel(const TIN *__restrict__ in, const TIN *__restrict__ scale,
                    const float *__restrict__ scale_f,
                    const T *__restrict__ M, TOUT *__restrict__ out, long nelv,
-                   const int *__restrict__ skip, PrologDots dots = PrologDots{},
-                   PostArgs<TOUT> post = PostArgs<TOUT>{}) {
+                   const int *__restrict__ skip, PrologDots dots = PrologDots{}) {
   if (skip && *skip) return;
   constexpr int I3 = NI * NI * NI, O3 = NO * NO * NO, NT = kT3Threads;
   __shared__ T su[I3], s1[NO * NI * NI], s2[NO * NO * NI], sA[NO * NI];
@@ -460,12 +448,7 @@ __global__ void __launch_bounds__(kT3Threads)
 #pragma unroll
     for (int g = 0; g < RO; g++) {
       const int q = tid + g * NT;
-      if constexpr (POST)
-        prev[g] = q < O3 ? schwarz_post_point<TOUT, NO>(post.ext, post.fn, post.ornt, post.wt,
-                                                         e, q)
-                         : TOUT(0);
-      else
-        prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
+      prev[g] = q < O3 ? out[e * O3 + q] : TOUT(0);
       oscale[g] = (scale && q < O3)
                       ? (scale_f ? (TIN)scale_f[e * O3 + q] : scale[e * O3 + q])
                       : TIN(1);
@@ -539,7 +522,7 @@ struct SchwarzLevel {
 
 template <typename TIN, typename T, int LX>
 static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
-                                   cudaStream_t s, bool post = true) {
+                                   cudaStream_t s) {
   constexpr int NL = LX + 2;
   using C = FdmCfg<T, NL>;
   auto kern = fdm_kernel<TIN, T, NL>;
@@ -554,7 +537,6 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
   }
   kern<<<(unsigned)((L.nelv + C::EPW - 1) / C::EPW), C::TPE, C::SMEM, s>>>(
       r, L.fn, L.ornt, L.S, L.lam, L.eps, L.ext, (int)L.nelv, skip);
-  if (!post) return cudaGetLastError();  // the prolongation forms the post step
   const long n = L.nelv * LX * LX * LX;
   schwarz_post_kernel<T, LX><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
       L.ext, L.fn, L.ornt, L.wt, e, L.nelv, skip);
@@ -564,11 +546,11 @@ static cudaError_t launch_fdm_post(const SchwarzLevel<T> &L, const TIN *r, T *e,
 // e = Schwarz(r) on level L (r already masked): FDM + overlap + gs + mask.
 template <typename TIN, typename T>
 static cudaError_t schwarz_apply(const SchwarzLevel<T> &L, const TIN *r, T *e, const int *skip,
-                                 cudaStream_t s, bool assemble = true, bool post = true) {
+                                 cudaStream_t s, bool assemble = true) {
   cudaError_t err;
   switch (L.lx) {
 #define NB_S(N) \
-  case N: err = launch_fdm_post<TIN, T, N>(L, r, e, skip, s, post); break;
+  case N: err = launch_fdm_post<TIN, T, N>(L, r, e, skip, s); break;
     NB_S(3) NB_S(4) NB_S(5) NB_S(6) NB_S(7) NB_S(8) NB_S(9) NB_S(10) NB_S(11) NB_S(12)
     NB_S(13) NB_S(14)
 #undef NB_S
@@ -688,20 +670,12 @@ template <typename TIN, typename TOUT, typename T>
 static cudaError_t prolong_add(int ni, int no, const TIN *in, const T *J, TOUT *out, long nelv,
                                const int *skip, cudaStream_t s, const TIN *oscale = nullptr,
                                const float *oscale_f = nullptr,
-                               const PrologDots *dots = nullptr,
-                               const PostArgs<TOUT> *post = nullptr) {
+                               const PrologDots *dots = nullptr) {
   const PrologDots d0 = dots ? *dots : PrologDots{};
-  const PostArgs<TOUT> p0 = post ? *post : PostArgs<TOUT>{};
 #define NB_P(A, B)                                                                          \
   if (ni == A && no == B) {                                                                 \
     const unsigned g = (unsigned)nelv;                                                      \
-    if (dots && post)                                                                       \
-      tensor3_kernel<TIN, TOUT, T, A, B, false, true, true, true>                           \
-          <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip, d0, p0);      \
-    else if (post)                                                                          \
-      tensor3_kernel<TIN, TOUT, T, A, B, false, true, false, true>                          \
-          <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip, d0, p0);      \
-    else if (dots)                                                                          \
+    if (dots)                                                                               \
       tensor3_kernel<TIN, TOUT, T, A, B, false, true, true>                                 \
           <<<g, kT3Threads, 0, s>>>(in, oscale, oscale_f, J, out, nelv, skip, d0);          \
     else                                                                                    \
@@ -775,9 +749,8 @@ struct HsmgImpl : public HsmgState {
 
   int launches() const override {
     // 2 Schwarz x (fdm, post, gs) + restrict + gs + coarse (one launch) +
-    // prolong + final gs (+ convert); when merged the fine Schwarz has
-    // neither its own gs nor its own post launch
-    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0) - (merged_assembly() ? 2 : 0);
+    // prolong + final gs (+ convert); one gs fewer when merged
+    return 6 + 1 + 1 + 1 + 1 + 1 + (sizeof(T) == 4 ? 1 : 0) - (merged_assembly() ? 1 : 0);
   }
 
   int take_error() override {
@@ -849,12 +822,8 @@ struct HsmgImpl : public HsmgState {
     if ((e = cudaEventRecord(ev_join_hi, hi)) != cudaSuccess) return e;
     // fine Schwarz on the side stream: zs = S_f r (left unassembled when the
     // final gather-scatter takes it, see below)
-    // Without a mask the post step of the fine Schwarz is left to the
-    // prolongation (one pass over the fine level after the join), so the
-    // side stream runs the FDM alone.
     const bool merged = merged_assembly();
-    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side, !merged, !merged)) != cudaSuccess)
-      return e;
+    if ((e = schwarz_apply<double, T>(sf, r, zs, skip, side, !merged)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(ev_join, side)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s, ev_join, 0)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(s, ev_join_hi, 0)) != cudaSuccess)
@@ -863,15 +832,10 @@ struct HsmgImpl : public HsmgState {
     // Schwarz output's own gather-scatter is folded into this one: wt and
     // mult are the same at every copy of a point, so
     // mult gs(gs(wt e) + J e_mid) = gs(wt e + mult J e_mid).
-    PostArgs<T> post;
-    post.ext = sf.ext;
-    post.wt = sf.wt;
-    post.fn = sf.fn;
-    post.ornt = sf.ornt;
     if ((e = prolong_add<T, T, T>(mid->lx, fine->lx, e_mid, Jfm, zs, nelv, skip, s,
                                   merged ? mult_f : nullptr,
                                   merged && sizeof(T) == 8 ? fine->multf : nullptr,
-                                  merged ? dots : nullptr, merged ? &post : nullptr)) !=
+                                  merged ? dots : nullptr)) !=
         cudaSuccess)
       return e;
     if ((e = gs_add_fused<T>(fine->gsd, zs, false, s, skip, merged ? nullptr : mult_f)) !=
