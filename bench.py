@@ -640,8 +640,8 @@ def run_axgs(args):
 
 def run_serve(args):
     """Served request stream: open-loop Poisson arrivals at each of
-    --serve-rates (plus one rate at half the measured capacity when every
-    given rate is above it), --serve-requests requests per rate drawn as the
+    --serve-rates (plus one rate at half the measured capacity when no
+    given rate is below three quarters of it), --serve-requests requests per rate drawn as the
     batched workload, answered by the continuous-batching server under a
     --serve-budget-gb HBM budget in mixed precision and in FP64 (hsmg
     problems as per-problem solves, Jacobi ones in the persistent batched
@@ -669,7 +669,9 @@ def run_serve(args):
                                            stream=stream, keep_solutions=False)
     capacity = len(cap_specs) / span
     rates = [float(r) for r in args.serve_rates.split(",")]
-    if min(rates) >= capacity:
+    # a rate well below the capacity, so that one stream's latencies are
+    # service time rather than queueing
+    if min(rates) >= 0.75 * capacity:
         rates.insert(0, round(0.5 * capacity, 1))
     out = {}
     for q, rate in enumerate(rates):
