@@ -724,7 +724,7 @@ def run_serve(args):
                                   "their preconditioners built before each timed stream "
                                   "(an untimed pass over its first 2000 requests)",
                    "geometries": len(cache.problems), "instances": inst.instances(),
-                   "instances_evicted": inst.evicted,
+                   "instances_evicted": inst.evicted, "instance_waits": inst.deferred,
                    "setup_s": cache.setup_s + inst.setup_s},
         "rates": out,
     }

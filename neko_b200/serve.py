@@ -77,6 +77,7 @@ class InstancePool:
         self.reserve = int(reserve_gb * 1e9)
         self.released = collections.OrderedDict()  # free extra instances, oldest first
         self.evicted = 0
+        self.deferred = 0  # acquisitions answered "wait"
         self.built = {}  # id(instance) -> precisions whose hsmg exists
 
     def _make_room(self):
@@ -97,9 +98,12 @@ class InstancePool:
             self.setup_s += time.perf_counter() - t0
             b.add(mixed)
 
-    def acquire(self, spec, mixed=None):
+    def acquire(self, spec, mixed=None, wait=False):
         """An instance of spec's shape with the hsmg of precision `mixed`
-        built (the first of `variants` when None)."""
+        built (the first of `variants` when None).  With wait=True, None
+        when every instance of the shape is in use and the device is below
+        its memory reserve (the caller tries again later) rather than a new
+        instance built on the room of idle ones."""
         m = self.variants[0] if mixed is None else bool(mixed)
         k = self.cache.key(spec)
         fl = self.free.setdefault(k, [])
@@ -108,6 +112,9 @@ class InstancePool:
             self.released.pop(id(P), None)
             self._ensure(P, m)
             return P
+        if wait and self.count.get(k, 0) > 0 and torch.cuda.mem_get_info()[0] < self.reserve:
+            self.deferred += 1
+            return None
         t0 = time.perf_counter()
         if self.count.get(k, 0) == 0:
             P = self.cache.get(spec)
@@ -243,15 +250,25 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
         for i in [i for i in waiting if i in cancel and cancel[i] <= now]:
             waiting.remove(i)
             finish(i, CANCELLED, now)
+        deferred = []
         while waiting:  # admission in arrival order while the budget allows
             i = waiting[0]
             sp = specs[i]
             solo = per_problem and sp.get("pc", "jacobi") == "hsmg"
             if solo and len(owned) >= max_solves:
                 break
+            Pi = None
+            if solo:
+                # when every instance of the shape is busy and the device is
+                # short of memory the request waits for one to come free
+                # (building one would destroy idle instances that later
+                # requests need again); the requests behind it go on
+                Pi = instances.acquire(sp, mixed=mode == "mixed", wait=bool(active))
+                if Pi is None:
+                    deferred.append(waiting.popleft())
+                    continue
             P, f, r0 = pool.get(sp)
             x = torch.empty(P.n, dtype=torch.float64, device="cuda")
-            Pi = instances.acquire(sp, mixed=mode == "mixed") if solo else None
             try:
                 if solo:
                     slot = B.submit_solve(Pi, f, x, rel_tol * r0, sp.get("max_iter", max_iter),
@@ -275,6 +292,7 @@ def serve_batched(specs, t_arr, pool, budget_bytes, rel_tol=1e-8, max_iter=5000,
             if Pi is not None:
                 owned[slot] = Pi
             xs[i] = x
+        waiting.extendleft(reversed(deferred))  # deferred requests keep their places
         if not active:
             if nxt < n and not waiting:
                 time.sleep(max(0.0, t_arr[nxt] - (time.perf_counter() - t0)))

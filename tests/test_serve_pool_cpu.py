@@ -110,3 +110,16 @@ def test_precisions_built_on_first_use(pool):
     p.release(spec(3), a)
     p.acquire(spec(3), mixed=False)
     assert FakeHsmg.built[-1] == (id(a), False) and len(FakeHsmg.built) == 2
+
+
+def test_wait_instead_of_building_when_short(pool):
+    p, free = pool
+    s = spec(5)
+    a = p.acquire(s)                 # the cache's problem
+    b = p.acquire(s)                 # an extra one while memory allows
+    free["bytes"] = 1
+    assert p.acquire(s, wait=True) is None and p.deferred == 1
+    p.release(s, b)
+    assert p.acquire(s, wait=True) is b   # a free instance is always handed out
+    assert p.acquire(spec(9), wait=True) is not None  # a shape's first instance is built
+    assert not a.closed
