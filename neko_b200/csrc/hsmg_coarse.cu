@@ -11,8 +11,8 @@
 //
 //   restrict -> | gs + mask (f) -> | init x, r, z = d r, (r,r), (r,z) -> |
 //   per iteration: p = z + beta p, w = A p (element-local), (p, w) -> |
-//                  gs + mask (w) with, for each summed point, x += alpha p,
-//                  r -= alpha w, z = d r, (r, r), (r, z) -> |  ... -> prolong
+//                  gs + mask (w) -> | x += alpha p, r -= alpha w,
+//                  z = d r, (r, r), (r, z) -> |  ... -> prolong
 //
 // The arithmetic is that of cg_init / cg_precond_dot / cg_update_p /
 // ax_helm / gs / cg_update_xr, with one change of form: (p, mult gs(w)) is
@@ -347,74 +347,37 @@ __global__ void __launch_bounds__(kCoarseThreads)
     double pap, unused;
     if (!allsum2(s_pw, 0.0, pap, unused)) return;
     const double alpha = rtz / pap;
-    // gather-scatter of w and the vector update in one phase: each item's
-    // sum (the gs add's order) is used at once for its copies; x += alpha
-    // p, r -= alpha w, z = d r, (r, mult r), (r, mult z); points outside
-    // every item take their local w
+    gs_phase(a.w);
+    if (!grid_barrier(a.bar, a.err)) return;
+    // x += alpha p; r -= alpha w; z = d r; (r, mult r), (r, mult z)
     s_rr = 0.0;
     s_rz = 0.0;
     const double malpha = -alpha;
-    auto upd = [&](int idx, double wv) {
-      const double pi = a.p[idx], xo = a.x[idx], ro = a.r[idx];
-      const double dv = __ldg(a.dinv + idx), m = __ldg(a.mult + idx);
-      a.x[idx] = xo + alpha * pi;
-      const double ri = ro + malpha * wv;
-      a.r[idx] = ri;
-      const double zi = ri * dv;
-      a.z[idx] = zi;
-      s_rr += ri * m * ri;
-      s_rz += ri * m * zi;
-    };
-    auto item = [&](long t) {  // gs_add_item's sum, then the update of the copies
-      const GsDevice &g = a.gs;
-      if (t < g.npairs) {
-        const int2 pr = __ldg(g.pairs + t);
-        double sm = a.w[pr.x] + a.w[pr.y];
-        if (g.pair_masked && g.pair_masked[t]) sm = 0.0;
-        upd(pr.x, sm);
-        upd(pr.y, sm);
-        return;
-      }
-      long q = t - g.npairs;
-      if (q < g.nseg) {
-        const int lo = __ldg(g.seg_ptr + q), hi = __ldg(g.seg_ptr + q + 1);
-        double sm = a.w[__ldg(g.seg_idx + lo)];
-        for (int k = lo + 1; k < hi; k++) sm = sm + a.w[__ldg(g.seg_idx + k)];
-        if (g.seg_masked && g.seg_masked[q]) sm = 0.0;
-        for (int k = lo; k < hi; k++) upd(__ldg(g.seg_idx + k), sm);
-        return;
-      }
-      q -= g.nseg;
-      if (q < g.nextra) upd(__ldg(g.extra_mask + q), 0.0);
-    };
-    {
-      const GsSlot &c = gslot[threadIdx.x];
-      if (c.kind == 1) {
-        double sm = a.w[c.idx[0]] + a.w[c.idx[1]];
-        if (c.masked) sm = 0.0;
-        upd(c.idx[0], sm);
-        upd(c.idx[1], sm);
-      } else if (c.kind == 2) {
-        double v[kGsCache];
+    for (long q0 = t0; q0 < nc; q0 += kU * stride) {
+      double xq[kU], pq[kU], rq[kU], wq[kU], m[kU], dv[kU];
 #pragma unroll
-        for (int k = 0; k < kGsCache; k++) v[k] = k < c.len ? a.w[c.idx[k]] : 0.0;
-        double sm = v[0];
-#pragma unroll
-        for (int k = 1; k < kGsCache; k++)
-          if (k < c.len) sm = sm + v[k];
-        if (c.masked) sm = 0.0;
-#pragma unroll
-        for (int k = 0; k < kGsCache; k++)
-          if (k < c.len) upd(c.idx[k], sm);
-      } else if (c.kind == 3) {
-        upd(c.idx[0], 0.0);
-      } else if (c.kind == 4) {
-        item(t0);
+      for (int u = 0; u < kU; u++) {
+        const long q = q0 + u * stride;
+        const bool ok = q < nc;
+        xq[u] = ok ? a.x[q] : 0.0;
+        pq[u] = ok ? a.p[q] : 0.0;
+        rq[u] = ok ? a.r[q] : 0.0;
+        wq[u] = ok ? a.w[q] : 0.0;
+        m[u] = ok ? __ldg(a.mult + q) : 0.0;
+        dv[u] = ok ? __ldg(a.dinv + q) : 0.0;
       }
-      for (long t = t0 + stride; t < nitems; t += stride) item(t);
-      for (long q = t0; q < a.nsingle; q += stride) {
-        const int idx = __ldg(a.single + q);
-        upd(idx, a.w[idx]);
+#pragma unroll
+      for (int u = 0; u < kU; u++) {
+        const long q = q0 + u * stride;
+        if (q < nc) {
+          a.x[q] = xq[u] + alpha * pq[u];
+          const double ri = rq[u] + malpha * wq[u];
+          a.r[q] = ri;
+          const double zi = ri * dv[u];
+          a.z[q] = zi;
+          s_rr += ri * m[u] * ri;
+          s_rz += ri * m[u] * zi;
+        }
       }
     }
     double rtz_new;

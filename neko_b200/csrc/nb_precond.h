@@ -141,8 +141,6 @@ struct CoarseArgs {
   unsigned *bar = nullptr;  // grid-barrier word (reset with err after a timeout)
   int *err = nullptr;       // set to 1 when a barrier wait expired
   const int *skip = nullptr;
-  const int *single = nullptr;  // coarse points in no gather-scatter item
-  int nsingle = 0;
 };
 constexpr int kCoarseMaxBlocks = 1024;
 

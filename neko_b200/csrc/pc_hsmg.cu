@@ -1011,25 +1011,8 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
   const size_t o_wm = c.take(nm * sizeof(T)), o_em = c.take(nm * sizeof(T));
   const size_t o_rc = c.take(nc * 8), o_ec = c.take(nc * 8), o_r = c.take(nc * 8),
                o_z = c.take(nc * 8), o_p = c.take(nc * 8), o_w = c.take(nc * 8);
-  // coarse points outside every gather-scatter item (neither shared nor a
-  // masked item of their own): updated by the coarse kernel on their own
-  std::vector<int> single;
-  {
-    std::vector<unsigned char> covered(nc, 0);
-    for (int q = 0; q < C->maps.nlocal; q++) covered[C->maps.gs_dof[q] - 1] = 1;
-    if (C->gsd.nextra > 0) {
-      std::vector<int> ex(C->gsd.nextra);
-      if (cudaMemcpy(ex.data(), C->gsd.extra_mask, ex.size() * 4, cudaMemcpyDeviceToHost) !=
-          cudaSuccess)
-        return hfail(NB_ERR_CUDA, "hsmg: mask copy failed");
-      for (int q : ex) covered[q] = 1;
-    }
-    for (long q = 0; q < nc; q++)
-      if (!covered[q]) single.push_back((int)q);
-  }
   const size_t o_st = c.take(sizeof(CgState)),
-               o_part = c.take(2 * 2 * kCoarseMaxBlocks * sizeof(double) + 64),
-               o_single = c.take(single.size() * 4 + 4);
+               o_part = c.take(2 * 2 * kCoarseMaxBlocks * sizeof(double) + 64);
   if (cudaMalloc(&H->arena, c.off) != cudaSuccess) return hfail(NB_ERR_OOM, "hsmg: device arena");
   char *A = (char *)H->arena;
   auto Tp = [&](size_t o) { return (T *)(A + o); };
@@ -1067,8 +1050,6 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
   ca.part = Dp(o_part);
   ca.bar = (unsigned *)(A + o_part + 2 * 2 * kCoarseMaxBlocks * sizeof(double));
   ca.err = (int *)(ca.bar + 2);
-  ca.single = (const int *)(A + o_single);
-  ca.nsingle = (int)single.size();
   auto upv = [&](size_t o, const std::vector<double> &v) {
     std::vector<T> t = cast_vec<T>(v);
     return t.empty() ? cudaSuccess
@@ -1097,7 +1078,6 @@ static nb_status upload_impl(HsmgImpl<T> *H, const SchwarzHost &hf, const Schwar
       (!ornt.empty() &&
        cudaMemcpy(A + o_or, ornt.data(), ornt.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(A + o_st, &cs, sizeof(cs), cudaMemcpyHostToDevice) ||
-      (!single.empty() && upi(o_single, single)) ||
       cudaMemset(A + o_part, 0, 2 * 2 * kCoarseMaxBlocks * sizeof(double) + 64))
     return hfail(NB_ERR_CUDA, "hsmg: upload failed");
   return NB_OK;
