@@ -30,9 +30,11 @@
 // rebuilds the queues and the graph, so solves can join while others run
 // (continuous batching).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "nb_gs_dev.cuh"
@@ -976,13 +978,22 @@ static nb_status ksp_advance(nb_batch *b, int *left) {
   return NB_OK;
 }
 
-// Blocks until the first running per-problem solve has finished its chunk.
-static void ksp_wait_one(nb_batch *b) {
-  for (auto &k : b->kslots)
-    if (k.used && k.started && !k.finished) {
-      if (cg_poll(k.run, true, &k.res, &k.status)) k.finished = true;
-      return;
+// Waits until some running per-problem solve has finished its current
+// chunk (whichever comes first; polling every solve's event, with a short
+// sleep between rounds once the wait is not short), so that no solve that
+// could be relaunched sits idle behind a slower one.
+static void ksp_wait_any(nb_batch *b) {
+  for (int round = 0;; round++) {
+    bool running = false;
+    for (auto &k : b->kslots) {
+      if (!k.used || !k.started || k.finished) continue;
+      running = true;
+      const CgWorkspace *W = (const CgWorkspace *)k.run.P->solver_ws;
+      if (!W || !W->ev || cudaEventQuery(W->ev) != cudaErrorNotReady) return;
     }
+    if (!running) return;
+    if (round > 32) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
 }
 
 extern "C" nb_status nb_batch_release(nb_batch *b, int slot) {
@@ -1043,13 +1054,20 @@ extern "C" nb_status nb_batch_run(nb_batch *b, int max_chunks, int *active, void
     st = ksp_advance(b, &kleft);
     if (st != NB_OK) return st;
     if (jac) {
+      // while the Jacobi chunk runs, per-problem solves that finish a chunk
+      // are relaunched at once
+      for (int round = 0; kleft && cudaEventQuery(b->ev_jacobi) == cudaErrorNotReady; round++) {
+        st = ksp_advance(b, &kleft);
+        if (st != NB_OK) return st;
+        if (round > 32) std::this_thread::sleep_for(std::chrono::microseconds(20));
+      }
       NB_BTRY(cudaEventSynchronize(b->ev_jacobi));
       b->mirror_valid = true;
       jleft = 0;
       for (int q = 0; q < ns; q++)
         if (b->slots[q].used && !hs[q].done) jleft++;
     } else if (kleft) {
-      ksp_wait_one(b);
+      ksp_wait_any(b);
       st = ksp_advance(b, &kleft);
       if (st != NB_OK) return st;
     }
