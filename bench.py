@@ -175,7 +175,7 @@ def make_rhs(nb, P, seed):
     import torch
     from neko_b200 import workloads
     x, y, z, B = (P.field(k) for k in ("x", "y", "z", "B"))
-    b = workloads.config2_rhs_local(x, y, z, B, seed).contiguous()
+    b = workloads.periodic_box_rhs(x, y, z, B, seed).contiguous()
     P.gs.op(b, P.n)
     torch.cuda.synchronize()
     return b
@@ -254,7 +254,7 @@ def run_reference(args, cfg, world, rank):
     from neko_b200 import workloads
     O = oracle_problem(cfg)
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
-    b = O.gs_add(workloads.config2_rhs_local(x, y, z, B, args.seed))
+    b = O.gs_add(workloads.periodic_box_rhs(x, y, z, B, args.seed))
     mult = O.f64("mult")
     r0 = math.sqrt(float(np.sum(b * mult * b)) / O.volume)
     tol = cfg["rel_tol"] * r0
@@ -288,7 +288,7 @@ def run_reference(args, cfg, world, rank):
 
 def kernel_only(args, cfg):
     """A smaller case of one kernel for profilers: nel^3 elements of the
-    config-2 geometry, `--steps` launches after `--warmup`."""
+    periodic-box geometry, `--steps` launches after `--warmup`."""
     import torch
     import neko_b200 as nb
     cfg = dict(cfg, nel=(args.nel,) * 3, lx=args.lx)
@@ -493,7 +493,7 @@ def run_batch(args):
 
 def run_velocity(args):
     """The velocity solve of a time step with variable viscosity on the
-    config-2 mesh (periodic deformed box 32^3 hex, lx 8, three components of
+    periodic 32^3 box (periodic deformed box 32^3 hex, lx 8, three components of
     16.8 M points): coupled Jacobi-CG (cg_cpld) with the full-stress
     operator, h1 = 1 + 0.5 sin x sin y sin z (the viscosity field), h2 = 10
     (the BDF mass term), each component's right-hand side B f_c assembled,
@@ -505,7 +505,7 @@ def run_velocity(args):
     import neko_b200 as nb
     from neko_b200 import workloads
     torch.cuda.set_device(0)
-    cfg = dict(workloads.CONFIG2)
+    cfg = dict(workloads.PERIODIC_BOX_32)
     cfg["lx"] = args.lx
     P = build_problem(nb, cfg)
     x, y, z, B = (P.field(k) for k in ("x", "y", "z", "B"))
@@ -572,7 +572,7 @@ def run_velocity(args):
 
 
 def run_axgs(args):
-    """Config 1: unit box 8^3, lx = 8, zero Dirichlet.  (a) ax_helm followed
+    """Unit box 8^3, lx = 8, zero Dirichlet.  (a) ax_helm followed
     by gs add on a continuous u ~ U[-1,1] (h1 = 1, h2 = 0), 100 times,
     GDOF/s; (b) the Jacobi-PCG solve of the sin^3 + noise right-hand side to
     1e-10 relative, solves/s."""
@@ -580,7 +580,7 @@ def run_axgs(args):
     import neko_b200 as nb
     from neko_b200 import workloads
     torch.cuda.set_device(0)
-    c = workloads.CONFIG1
+    c = workloads.UNIT_BOX_8
     P = nb.Problem(c["nel"], c["lx"], lo=c["lo"], hi=c["hi"], periodic=c["periodic"],
                    deform=c["deform"], dirichlet=c["dirichlet"])
     g = torch.Generator(device="cuda").manual_seed(args.seed)
@@ -607,7 +607,7 @@ def run_axgs(args):
     xi = torch.randn(P.n, dtype=torch.float64, device="cuda", generator=g) * 1e-3
     P.gs.op(xi)
     xi *= P.field("mult")
-    f = workloads.config1_pointwise(x, y, z, xi) * P.field("B")
+    f = workloads.unit_box_pointwise(x, y, z, xi) * P.field("B")
     P.gs.op(f)
     P.bclst.apply(f)
     r0 = math.sqrt(float((f * P.field("mult") * f).sum()) / P.volume)
@@ -625,7 +625,7 @@ def run_axgs(args):
     err = float((xs - torch.sin(math.pi * x) * torch.sin(math.pi * y) *
                  torch.sin(math.pi * z)).abs().max())
     print(json.dumps({
-        "metric": "ax_helm + gs add GDOF/s (config 1)", "value": P.n / t / 1e9, "unit": "GDOF/s",
+        "metric": "ax_helm + gs add GDOF/s (unit box 8^3, lx 8)", "value": P.n / t / 1e9, "unit": "GDOF/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
         "vs_baseline": None,
         "config": {"workload": "unit box 8^3 hex, lx=8 (262,144 points), zero Dirichlet, "
@@ -755,15 +755,15 @@ def main():
                          "profiler window) on an nel^3 box (profiling case)")
     ap.add_argument("--workload", choices=["solve", "axgs", "batch", "serve", "velocity"],
                     default="solve",
-                    help="solve: the hsmg-FCG config-2 line (default); batch: batched "
+                    help="solve: the hsmg-FCG line on the periodic 32^3 box (default); batch: batched "
                          "uneven solves; serve: the served request stream; velocity: the "
-                         "coupled full-stress velocity solve on the config-2 mesh")
+                         "coupled full-stress velocity solve on the periodic 32^3 box")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--max-solves", type=int, default=64,
                     help="per-problem hsmg solves running at once in the batch / server")
     ap.add_argument("--coarse-tol", type=float, default=1e-9,
                     help="hsmg coarse CG absolute tolerance (reference KSP_ABS_TOL 1e-9; "
-                         "1e-4 is the config-2 variant)")
+                         "1e-4 is the weaker variant)")
     ap.add_argument("--serve-rates", default="200,1000,5000")
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-seq-requests", type=int, default=1000,
@@ -776,7 +776,7 @@ def main():
         ap.error("--warmup must be >= 3")
 
     from neko_b200 import workloads
-    cfg = dict(workloads.CONFIG2)
+    cfg = dict(workloads.PERIODIC_BOX_32)
     cfg["lx"] = args.lx
     if args.kernel_only:
         return kernel_only(args, cfg)

@@ -1,10 +1,10 @@
-"""Seeded synthetic workloads of the benchmark configurations (inputs only).
+"""Seeded synthetic workloads of the benchmarks (inputs only).
 
-* config 1: unit box 8^3, lx = 8, zero Dirichlet on every face,
+* unit box 8^3, lx = 8, zero Dirichlet on every face,
   f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z) + xi, xi ~ N(0, 1e-3) per local
   point made continuous by gs_add(xi) * mult; b = gs_add(B f), masked
   (the shape of examples/poisson/driver.f90 + setup.f90).
-* config 2: periodic box [0, 2 pi]^3, 32^3 elements, lx = 8, GLL points
+* periodic box [0, 2 pi]^3, 32^3 elements, lx = 8, GLL points
   displaced by 0.05 sin of the other two coordinates; f = sum over integer
   wave vectors 0 < |k| <= 4 (half space) of a_k cos(k.x) + b_k sin(k.x)
   with a_k, b_k ~ N(0, 1); b_local = B f, de-meaned as ortho does
@@ -15,10 +15,11 @@ import math
 import numpy as np
 import torch
 
-CONFIG1 = dict(nel=(8, 8, 8), lx=8, lo=(0.0,) * 3, hi=(1.0,) * 3, periodic=(False,) * 3,
-               deform=0.0, dirichlet=True, rel_tol=1e-10, max_iter=500)
-CONFIG2 = dict(nel=(32, 32, 32), lx=8, lo=(0.0,) * 3, hi=(2 * math.pi,) * 3,
-               periodic=(True,) * 3, deform=0.05, dirichlet=False, rel_tol=1e-8, max_iter=5000)
+UNIT_BOX_8 = dict(nel=(8, 8, 8), lx=8, lo=(0.0,) * 3, hi=(1.0,) * 3, periodic=(False,) * 3,
+                  deform=0.0, dirichlet=True, rel_tol=1e-10, max_iter=500)
+PERIODIC_BOX_32 = dict(nel=(32, 32, 32), lx=8, lo=(0.0,) * 3, hi=(2 * math.pi,) * 3,
+                       periodic=(True,) * 3, deform=0.05, dirichlet=False, rel_tol=1e-8,
+                       max_iter=5000)
 
 
 def fourier_modes(kmax=4):
@@ -50,13 +51,13 @@ def fourier_field(x, y, z, seed, kmax=4):
     return f.numpy() if is_np else f
 
 
-def config2_rhs_local(x, y, z, B, seed):
+def periodic_box_rhs(x, y, z, B, seed):
     """B f de-meaned over local points (before gs)."""
     bl = B * fourier_field(x, y, z, seed)
     return bl - bl.sum() / bl.numel() if isinstance(bl, torch.Tensor) else bl - bl.sum() / bl.size
 
 
-def config1_pointwise(x, y, z, xi_cont):
+def unit_box_pointwise(x, y, z, xi_cont):
     pi = math.pi
     if isinstance(x, torch.Tensor):
         s = torch.sin
@@ -65,7 +66,7 @@ def config1_pointwise(x, y, z, xi_cont):
     return 3 * pi ** 2 * s(pi * x) * s(pi * y) * s(pi * z) + xi_cont
 
 
-# --- config 4/5: uneven Helmholtz problems -----------------------------------
+# --- batched and served streams: uneven Helmholtz problems -----------------------------------
 N_DEFORM_SEEDS = 8
 
 

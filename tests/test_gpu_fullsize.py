@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 def _cfg(lx):
     from neko_b200 import workloads
-    c = dict(workloads.CONFIG2)
+    c = dict(workloads.PERIODIC_BOX_32)
     c["lx"] = lx
     return c
 
@@ -38,7 +38,7 @@ class _Case:
                             deform=c["deform"], dirichlet=c["dirichlet"])
         from neko_b200 import workloads
         P = self.P
-        b = workloads.config2_rhs_local(P.field("x"), P.field("y"), P.field("z"), P.field("B"),
+        b = workloads.periodic_box_rhs(P.field("x"), P.field("y"), P.field("z"), P.field("B"),
                                         2024).contiguous()
         P.gs.op(b, P.n)
         torch.cuda.synchronize()
@@ -92,7 +92,7 @@ def case10(nb, oracle):
 
 
 @pytest.mark.parametrize("coarse_tol", [1e-9, 1e-4])
-def test_config2_fp64_solve_matches_oracle(nb, case8, coarse_tol):
+def test_periodic_box_32_fp64_solve_matches_oracle(nb, case8, coarse_tol):
     """32^3 x lx 8: the reference's coarse solve (10 Jacobi-CG iterations at
     abs tol 1e-9) and the 1e-4 variant."""
     xo, it_o = case8.oracle_solution(coarse_tol)
@@ -103,7 +103,7 @@ def test_config2_fp64_solve_matches_oracle(nb, case8, coarse_tol):
     assert np.abs(a - r).max() / np.abs(r).max() < 1e-7
 
 
-def test_config3_lx8_mixed_vs_oracle(nb, case8):
+def test_periodic_box_32_lx8_mixed_vs_oracle(nb, case8):
     xo, it_o = case8.oracle_solution(1e-9)
     x, mon = case8.gpu_solve(nb, 1e-9, mixed=True)
     assert mon.converged and mon.res_final < case8.tol
@@ -113,7 +113,7 @@ def test_config3_lx8_mixed_vs_oracle(nb, case8):
     assert err < 1e-6, err
 
 
-def test_config3_lx10_fp64_and_mixed_vs_oracle(nb, case10):
+def test_periodic_box_32_lx10_fp64_and_mixed_vs_oracle(nb, case10):
     """lx = 10 (32.8 M points): the FP64 solve within +-1 iteration and 1e-7
     of the oracle, the mixed solve within 1e-6 of the oracle's solution."""
     xo, it_o = case10.oracle_solution(1e-9)

@@ -37,7 +37,7 @@ def _setup(nb, oracle, nel, lx, per, amp, hi, seed):
     if dirichlet:
         O.bc_boundary()
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
-    b = O.bc_apply(O.gs_add(workloads.config2_rhs_local(x, y, z, B, seed)))
+    b = O.bc_apply(O.gs_add(workloads.periodic_box_rhs(x, y, z, B, seed)))
     r0 = np.sqrt(np.sum(b * O.f64("mult") * b) / O.volume)
     return P, O, b, r0
 

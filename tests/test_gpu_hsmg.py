@@ -130,7 +130,7 @@ def test_fcg_hsmg_matches_oracle(nb, oracle, nel, lx, per, amp, hi, dirichlet=No
     singular = all(per) or dirichlet is False
     H = oracle.OracleHsmg(O)
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
-    rl = workloads.config2_rhs_local(x, y, z, B, 3)
+    rl = workloads.periodic_box_rhs(x, y, z, B, 3)
     if singular:  # consistent right-hand side: zero sum over the global points
         rl = rl - rl.sum() / rl.size
     b = O.gs_add(rl)
@@ -194,7 +194,7 @@ def test_mixed_fcg_reaches_fp64_solution(nb, oracle, nel, lx, per, amp, hi):
     P, O = _pair(nb, oracle, nel, lx, per, amp, hi)
     H = oracle.OracleHsmg(O)
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
-    b = O.bc_apply(O.gs_add(workloads.config2_rhs_local(x, y, z, B, 5)))
+    b = O.bc_apply(O.gs_add(workloads.periodic_box_rhs(x, y, z, B, 5)))
     mult = O.f64("mult")
     r0 = np.sqrt(np.sum(b * mult * b) / O.volume)
     xo, it_o, _, _ = H.cg(b, 200, 1e-8 * r0, flexible=True)

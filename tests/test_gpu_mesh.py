@@ -159,7 +159,7 @@ def test_problem_from_nmsh_file(nb, oracle, tmp_path):
     O.deform_sine(0.05)
     O.coef()
     x, y, z, B = O.f64("x"), O.f64("y"), O.f64("z"), O.f64("B")
-    b = O.gs_add(workloads.config2_rhs_local(x, y, z, B, 4))
+    b = O.gs_add(workloads.periodic_box_rhs(x, y, z, B, 4))
     r0 = np.sqrt(np.sum(b * O.f64("mult") * b) / O.volume)
     H = oracle.OracleHsmg(O)
     xo, it_o, _, _ = H.cg(b, 200, 1e-8 * r0, flexible=True)

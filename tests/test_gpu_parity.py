@@ -270,8 +270,8 @@ def test_jacobi_diag_matches_oracle(nb, oracle):
     assert rel_err(_np(P.field("jacobi")), O.jacobi_diag()) <= 1e-12
 
 
-def test_cg_jacobi_config1_shape(nb, oracle):
-    """Config-1 shape (unit box, Dirichlet, sin^3 RHS + continuous noise):
+def test_cg_jacobi_unit_box_8(nb, oracle):
+    """Unit-box 8^3 shape (Dirichlet, sin^3 RHS + continuous noise):
     iteration counts within +-1 of the oracle, same solution."""
     P, O = _pair(nb, oracle, (8, 8, 8), 8)
     x, y, z = O.f64("x"), O.f64("y"), O.f64("z")

@@ -80,7 +80,7 @@ def test_gll_known_values(oracle):
                                        atol=1e-11 * max(1, p))
 
 
-def test_box_counts_config1(oracle):
+def test_box_counts_unit_box_8(oracle):
     """512-element unit box at lx = 8: the map sizes gs_init_mapping gives
     (8 vertex + 12*6 edge entries per element, face pairs only for faces with
     a neighbour)."""
@@ -105,7 +105,7 @@ def test_periodic_box_numbering(oracle):
     assert P.glb_mpts == 125 and P.glb_meds == 192
 
 
-def test_config1_analytic_solution(oracle):
+def test_unit_box_8_analytic_solution(oracle):
     """Jacobi-PCG on -lap u = 3 pi^2 sin sin sin, u = 0 on the boundary of
     the unit box: spectral accuracy at lx = 8 (examples/poisson shape)."""
     P = oracle.OracleProblem.box((4, 4, 4), 8)
