@@ -364,7 +364,10 @@ typedef enum {
   NB_PC_JACOBI = 0,
   NB_PC_HSMG = 1,
   NB_PC_NONE = 2,
-  NB_PC_HSMG_MIXED = 3  /* nb_pc_apply only: hsmg with FP32 smoothing levels */
+  NB_PC_HSMG_MIXED = 3, /* nb_pc_apply only: hsmg with FP32 smoothing levels */
+  NB_PC_PHMG = 4        /* hybrid ph-multigrid (phmg_t): Chebyshev-Jacobi
+                           smoothing on the polynomial levels, tree AMG on
+                           the last (nb_phmg_init) */
 } nb_pc_type;
 
 typedef struct {
@@ -427,10 +430,51 @@ nb_status nb_solve_coupled(nb_problem *p, int op, double *x, double *y, double *
  * hsmg_init_from_components (src/krylov/pc_hsmg.f90:145-365). */
 nb_status nb_hsmg_init(nb_problem *p, int mixed, int coarse_iter, double coarse_tol);
 
+/* Settings of the hybrid ph-multigrid preconditioner; a field <= 0 takes
+ * the reference's default (src/multigrid/phmg.f90:141-180). */
+typedef struct {
+  int smoother_iterations; /* Chebyshev steps a level (default 3) */
+  int n_schedule;          /* entries of schedule; 0: the default {3, 1} */
+  int schedule[8];         /* polynomial degree of each coarser level, decreasing
+                              (level lx = degree + 1; default lx -> 4 -> 2) */
+  int coarse_levels;       /* tree-AMG levels on the last level (default 3) */
+  int coarse_iterations;   /* AMG V-cycles an application (default 1) */
+  int cheby_degree;        /* Chebyshev degree on the AMG levels (default 4) */
+} nb_phmg_opts;
+
+/* Builds (or rebuilds) the problem's phmg preconditioner: phmg_init_from_
+ * components (src/multigrid/phmg.f90:184-421) with the tree-AMG set-up
+ * (src/multigrid/tree_amg_multigrid.f90:111-228) and the eigenvalue
+ * estimates of its first solve (150 power steps a smoothed level and a
+ * level of the AMG).  The coarser levels take the first n values of the
+ * problem's h1 at build time, as the reference does.  opts may be null
+ * (defaults).  Synchronous.  The power steps' start vectors and the
+ * aggregation's element order come from splitmix64 seeded 3901 (the
+ * reference uses gfortran's random_number at seed 3901). */
+nb_status nb_phmg_init(nb_problem *p, const nb_phmg_opts *opts);
+
+/* Set-up figures of the problem's phmg (built with the defaults when
+ * absent): what = 0 levels, 1 lx of level i, 2/3/4 the Chebyshev tha/dlt/
+ * lambda_max of level i, 5 AMG levels, 6 entries of AMG level i, 7/8/9
+ * tha/dlt/lambda_max of AMG level i, 10 kernels an application launches. */
+nb_status nb_phmg_describe(nb_problem *p, int what, int i, double *out);
+
+/* The tree-AMG aggregation alone, on the host (no device use): for nelv
+ * elements of lx^3 points with face neighbours facet_neigh (6 per element,
+ * 1-based, 0 = none), asking for coarse_levels levels.  Writes *nlvls (the
+ * levels kept), nnodes[l-1] = aggregates of level l and finest[(l-1) * n0
+ * + i] = the 0-based aggregate of level-0 point i (n0 = nelv lx^3) for l =
+ * 1 .. nlvls-1.  aggregate_finest_level / aggregate_greedy
+ * (src/multigrid/tree_amg_aggregate.f90). */
+nb_status nb_tamg_aggregate(int nelv, int lx, const int *facet_neigh, int coarse_levels,
+                            int *nlvls, int *nnodes, int *finest);
+
 /* z = M r for preconditioner pc (NB_PC_HSMG, or NB_PC_HSMG_MIXED for the
- * FP32-smoother variant), r masked; uses the settings of the last
- * nb_hsmg_init of that variant (the defaults when there was none).  The
- * hsmg_solve of the reference (src/krylov/pc_hsmg.f90:481-627). */
+ * FP32-smoother variant, or NB_PC_PHMG), r masked; uses the settings of
+ * the last nb_hsmg_init / nb_phmg_init of that preconditioner (the
+ * defaults when there was none).  The hsmg_solve of the reference
+ * (src/krylov/pc_hsmg.f90:481-627); phmg_solve (src/multigrid/
+ * phmg.f90:462-498). */
 nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double *r, void *stream);
 
 /* Solves A x = f (f already assembled and masked) from x0 = 0 with

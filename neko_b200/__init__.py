@@ -271,8 +271,81 @@ class Hsmg:
         check(load().nb_pc_apply(coef.handle, kind, _ptr(z), _ptr(r), _stream_handle(stream)))
 
 
+class Phmg:
+    """phmg_t: hybrid ph-multigrid (src/multigrid/phmg.f90).  Polynomial
+    levels lx -> schedule + 1 (default lx -> 4 -> 2) smoothed by
+    `smoother_iterations` Jacobi-accelerated Chebyshev steps, a tree-AMG
+    V-cycle (`coarse_levels` levels, `cheby_degree` Chebyshev steps a
+    level, `coarse_iterations` cycles) on the last.  `solve(z, r, coef)` is
+    pc_t%solve: z = M r (r masked).  Built for a problem on first use and
+    kept, as the reference's phmg_init does (the coarser levels keep the h1
+    of that moment)."""
+    kind = _lib.NB_PC_PHMG
+
+    def __init__(self, smoother_iterations=3, schedule=(3, 1), coarse_levels=3,
+                 coarse_iterations=1, cheby_degree=4):
+        self.smoother_iterations = smoother_iterations
+        self.schedule = tuple(int(k) for k in schedule)
+        self.coarse_levels = coarse_levels
+        self.coarse_iterations = coarse_iterations
+        self.cheby_degree = cheby_degree
+
+    def _settings(self):
+        return (self.smoother_iterations, self.schedule, self.coarse_levels,
+                self.coarse_iterations, self.cheby_degree)
+
+    def init(self, coef):
+        """phmg_init: build the levels, the aggregation and the eigenvalue
+        estimates for this problem (again only when the settings differ from
+        those it was built with)."""
+        if getattr(coef, "_phmg_settings", None) == self._settings():
+            return
+        if not 1 <= len(self.schedule) <= 8:
+            raise NekoB200Error(NB_ERR_ARG, "phmg: 1 to 8 schedule entries")
+        o = _lib.PhmgOpts()
+        o.smoother_iterations = self.smoother_iterations
+        o.n_schedule = len(self.schedule)
+        for i, k in enumerate(self.schedule):
+            o.schedule[i] = k
+        o.coarse_levels = self.coarse_levels
+        o.coarse_iterations = self.coarse_iterations
+        o.cheby_degree = self.cheby_degree
+        check(load().nb_phmg_init(coef.handle, ctypes.byref(o)))
+        coef._phmg_settings = self._settings()
+
+    prepare = init
+
+    def describe(self, coef, what, i=0):
+        out = ctypes.c_double()
+        check(load().nb_phmg_describe(coef.handle, what, i, ctypes.byref(out)))
+        return out.value
+
+    def solve(self, z, r, coef, n=None, stream=None):
+        self.init(coef)
+        check(load().nb_pc_apply(coef.handle, _lib.NB_PC_PHMG, _ptr(z), _ptr(r),
+                                 _stream_handle(stream)))
+
+
+def tamg_aggregate(nelv, lx, facet_neigh, coarse_levels=3):
+    """The tree-AMG aggregation on the host: (levels kept, [aggregates of
+    level l], [level-0 point -> 0-based aggregate of level l]) for l = 1 ..
+    levels-1."""
+    import numpy as np
+    fn = np.ascontiguousarray(facet_neigh, dtype=np.int32)
+    n0 = nelv * lx ** 3
+    nl = ctypes.c_int()
+    nn = np.zeros(max(coarse_levels, 1), dtype=np.int32)
+    fin = np.zeros(max(coarse_levels, 1) * n0, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    check(load().nb_tamg_aggregate(nelv, lx, fn.ctypes.data_as(ip), coarse_levels,
+                                   ctypes.byref(nl), nn.ctypes.data_as(ip),
+                                   fin.ctypes.data_as(ip)))
+    k = nl.value - 1
+    return nl.value, [int(v) for v in nn[:k]], [fin[i * n0:(i + 1) * n0].copy() for i in range(k)]
+
+
 class CG:
-    """ksp_t of type 'cg' with preconditioner M (Jacobi, Hsmg or None);
+    """ksp_t of type 'cg' with preconditioner M (Jacobi, Hsmg, Phmg or None);
     stops when sqrt(r' mult r / volume) < abs_tol (krylov.f90:411-421).
     flexible=True uses the Polak-Ribiere beta of flexible CG, which keeps
     converging with a non-symmetric preconditioner such as hsmg."""
@@ -297,6 +370,8 @@ class CG:
         o.flexible = int(self.flexible)
         o.ksp = self.ksp
         o.m_restart = getattr(self, "m_restart", 0)
+        if hasattr(self.M, "prepare"):
+            self.M.prepare(coef)
         r = SolveResult()
         check(load().nb_solve(coef.handle, _ptr(x), _ptr(f), ctypes.byref(o), ctypes.byref(r),
                               _stream_handle(stream)))

@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "NB_OK", 1: "NB_ERR_ARG", 2: "NB_ERR_UNSUPPORTED", 3: "NB_ERR
                 4: "NB_ERR_CUDA", 5: "NB_ERR_NOT_CONVERGED", 6: "NB_ERR_NAN",
                 7: "NB_ERR_TIMEOUT"}
 
-NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED = 0, 1, 2, 3
+NB_PC_JACOBI, NB_PC_HSMG, NB_PC_NONE, NB_PC_HSMG_MIXED, NB_PC_PHMG = 0, 1, 2, 3, 4
 NB_KSP_CG, NB_KSP_GMRES, NB_KSP_PIPECG = 0, 1, 2
 NB_AX_HELM_VECTOR, NB_AX_STRESS = 0, 1
 NB_OK, NB_ERR_ARG, NB_ERR_UNSUPPORTED, NB_ERR_OOM, NB_ERR_CUDA = 0, 1, 2, 3, 4
@@ -32,6 +32,12 @@ class SolveOpts(ctypes.Structure):
                 ("pc", ctypes.c_int), ("mixed", ctypes.c_int),
                 ("coarse_iter", ctypes.c_int), ("coarse_tol", ctypes.c_double),
                 ("flexible", ctypes.c_int), ("ksp", ctypes.c_int), ("m_restart", ctypes.c_int)]
+
+
+class PhmgOpts(ctypes.Structure):
+    _fields_ = [("smoother_iterations", ctypes.c_int), ("n_schedule", ctypes.c_int),
+                ("schedule", ctypes.c_int * 8), ("coarse_levels", ctypes.c_int),
+                ("coarse_iterations", ctypes.c_int), ("cheby_degree", ctypes.c_int)]
 
 
 class SolveResult(ctypes.Structure):
@@ -115,6 +121,9 @@ SIGNATURES = {
     "nb_glsc3_noalloc": (_I, [_P, _P, _P, _I, _DP, _P]),
     "nb_pc_apply": (_I, [_P, _I, _P, _P, _P]),
     "nb_hsmg_init": (_I, [_P, _I, _I, ctypes.c_double]),
+    "nb_phmg_init": (_I, [_P, ctypes.POINTER(PhmgOpts)]),
+    "nb_phmg_describe": (_I, [_P, _I, _I, _DP]),
+    "nb_tamg_aggregate": (_I, [_I, _I, _IP, _I, _IP, _IP, _IP]),
     "nb_projection_create": (_I, [_P, _I, _P]),
     "nb_projection_destroy": (_I, [_P]),
     "nb_projection_clear": (_I, [_P, _P]),

@@ -635,6 +635,9 @@ extern "C" nb_status nb_solve(nb_problem *p, double *x, const double *f,
   if (opts->pc == NB_PC_HSMG) {
     nb_status st = hsmg_get(p, *opts, &pc);
     if (st != NB_OK) return st;
+  } else if (opts->pc == NB_PC_PHMG) {
+    nb_status st = phmg_get(p, &pc);
+    if (st != NB_OK) return st;
   } else if (opts->pc != NB_PC_JACOBI && opts->pc != NB_PC_NONE) {
     set_error("unknown preconditioner");
     return NB_ERR_ARG;

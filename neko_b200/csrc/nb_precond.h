@@ -151,4 +151,9 @@ cudaError_t hsmg_coarse_solve(const CoarseArgs<T> &a, int lm, int max_blocks, cu
 // hsmg preconditioner of problem P, built on first use (pc_hsmg.cu).
 nb_status hsmg_get(nb_problem *P, const nb_solve_opts &o, Precond **out);
 
+struct PhmgSettings;
+// phmg preconditioner of problem P (pc_phmg.cu): the existing one, or one
+// built with the defaults; with settings, rebuilt with those.
+nb_status phmg_get(nb_problem *P, Precond **out, const PhmgSettings *settings = nullptr);
+
 }  // namespace nb

@@ -72,6 +72,7 @@ struct nb_problem {
   cudaError_t ensure_cofactors(cudaStream_t s);
   size_t solver_ws_bytes = 0;
   nb::HsmgState *hsmg[2] = {nullptr, nullptr};  // hsmg: [0] FP64, [1] mixed
+  void *phmg = nullptr;                          // ph-multigrid, built on first use
 
   ~nb_problem();
   cudaError_t update_jacobi(cudaStream_t s);
@@ -83,6 +84,7 @@ struct nb_problem {
 
 namespace nb {
 void hsmg_free(nb_problem *p);
+void phmg_free(nb_problem *p);
 void gmres_free(nb_problem *p);
 void gmres_invalidate(nb_problem *p);
 void pipecg_free(nb_problem *p);

@@ -1199,8 +1199,20 @@ extern "C" nb_status nb_pc_apply(nb_problem *p, int pc, double *z, const double 
     set_error("null argument");
     return NB_ERR_ARG;
   }
+  if (pc == NB_PC_PHMG) {
+    Precond *M = nullptr;
+    nb_status st = phmg_get(p, &M);
+    if (st != NB_OK) return st;
+    NB_CUDA_TRY(M->apply(z, r, nullptr, (cudaStream_t)stream));
+    NB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    if (M->take_error()) {
+      set_error("a bounded device wait expired (phmg level operator)");
+      return NB_ERR_TIMEOUT;
+    }
+    return NB_OK;
+  }
   if (pc != NB_PC_HSMG && pc != NB_PC_HSMG_MIXED) {
-    set_error("nb_pc_apply: pc must be NB_PC_HSMG or NB_PC_HSMG_MIXED");
+    set_error("nb_pc_apply: pc must be NB_PC_HSMG, NB_PC_HSMG_MIXED or NB_PC_PHMG");
     return NB_ERR_ARG;
   }
   return hsmg_apply_once(p, z, r, (cudaStream_t)stream, pc == NB_PC_HSMG_MIXED);

@@ -186,6 +186,7 @@ nb_problem::~nb_problem() {
   pipecg_free(this);
   cpld_free(this);
   hsmg_free(this);
+  phmg_free(this);
   if (cof) cudaFree(cof);
 }
 

@@ -249,18 +249,20 @@ __global__ void k_jacobi_diag(double *__restrict__ d, const double *__restrict__
   const int ijk = (int)(idx - e * L3);
   const int i = ijk % LX, j = (ijk / LX) % LX, k = ijk / (LX * LX);
   const long o = e * L3;
+  // (g t) t in the device form (pc_jacobi.cu:62-78), g (t t) in the CPU
+  // form (pc_jacobi.f90:195-225)
   double s = 0.0;
   for (int l = 0; l < LX; l++) {
-    const double t = dxt[i + LX * l];
-    s += G11[o + l + LX * j + LX * LX * k] * (t * t);
+    const double t = dxt[i + LX * l], g = G11[o + l + LX * j + LX * LX * k];
+    s += DEVICE_FORM ? g * t * t : g * (t * t);
   }
   for (int l = 0; l < LX; l++) {
-    const double t = dyt[j + LX * l];
-    s += G22[o + i + LX * l + LX * LX * k] * (t * t);
+    const double t = dyt[j + LX * l], g = G22[o + i + LX * l + LX * LX * k];
+    s += DEVICE_FORM ? g * t * t : g * (t * t);
   }
   for (int l = 0; l < LX; l++) {
-    const double t = dzt[k + LX * l];
-    s += G33[o + i + LX * j + LX * LX * l] * (t * t);
+    const double t = dzt[k + LX * l], g = G33[o + i + LX * j + LX * LX * l];
+    s += DEVICE_FORM ? g * t * t : g * (t * t);
   }
   const long p = o + ijk;
   const double xi = dxt[i + LX * i], yj = dyt[j + LX * j], zk = dzt[k + LX * k];

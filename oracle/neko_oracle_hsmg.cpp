@@ -531,6 +531,12 @@ void schwarz_compute(Schwarz &S, double *e, double *r) {
 
 }  // namespace
 
+// setup_intp for the other multigrid of the oracle (phmg).
+void or_setup_intp(std::vector<double> &jh, std::vector<double> &jht, const double *z_to,
+                   const double *z_from, int n_to, int n_from) {
+  setup_intp(jh, jht, z_to, z_from, n_to, n_from);
+}
+
 // ---------------------------------------------------------------------------
 // hsmg_t (pc_hsmg.f90:191-379 setup, 574-625 CPU solve)
 // ---------------------------------------------------------------------------

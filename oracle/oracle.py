@@ -96,6 +96,16 @@ def lib():
             "or_cg_coupled": (ctypes.c_int, [_P, _D, _D, _D, _D, _D, _D, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
                                              _D]),
+            "or_phmg_create": (_P, [_P, ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int]),
+            "or_phmg_destroy": (None, [_P]),
+            "or_phmg_apply": (None, [_P, _D, _D]),
+            "or_phmg_info": (ctypes.c_double, [_P, ctypes.c_int, ctypes.c_int]),
+            "or_phmg_agg_map": (None, [_P, ctypes.c_int, _I]),
+            "or_phmg_dinv": (None, [_P, ctypes.c_int, _D]),
+            "or_phmg_tamg": (None, [_P, _D, _D]),
+            "or_phmg_krylov": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, _D, _D,
+                                              ctypes.c_int, ctypes.c_double, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -448,3 +458,86 @@ def schwarz_toreg3d(a, nx, nel):
     b = np.zeros(nel * nx ** 3)
     lib().or_schwarz_toreg3d(_dp(b), _dp(np.ascontiguousarray(a)), nx, nel)
     return b
+
+
+class OraclePhmg:
+    """phmg_t of an OracleProblem (coef, h1/h2 and bc set up first):
+    Jacobi-accelerated Chebyshev smoothing on levels lx -> schedule + 1,
+    tree AMG on the last level."""
+
+    def __init__(self, P, smoother_iterations=3, schedule=(3, 1), coarse_levels=3,
+                 coarse_iterations=1, cheby_degree=4):
+        self.P = P
+        sched = (ctypes.c_int * len(schedule))(*schedule)
+        self.h = lib().or_phmg_create(P.h, smoother_iterations, sched, len(schedule),
+                                      coarse_levels, coarse_iterations, cheby_degree)
+        if not self.h:
+            raise RuntimeError("phmg set-up failed (the reference stops with an error here)")
+
+    def apply(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        lib().or_phmg_apply(self.h, _dp(z), _dp(r))
+        return z
+
+    def info(self, what, i=0):
+        return lib().or_phmg_info(self.h, what, i)
+
+    @property
+    def levels(self):
+        return int(self.info(0))
+
+    def level_lx(self, i):
+        return int(self.info(1, i))
+
+    def cheby(self, i):
+        """(tha, dlt, lambda_max) of level i's smoother."""
+        return self.info(2, i), self.info(3, i), self.info(4, i)
+
+    @property
+    def amg_levels(self):
+        return int(self.info(5))
+
+    def amg_nodes(self, i):
+        return int(self.info(6, i))
+
+    def amg_cheby(self, i):
+        return self.info(7, i), self.info(8, i), self.info(9, i)
+
+    def agg_map(self, lvl, n0):
+        out = np.zeros(n0, dtype=np.int32)
+        lib().or_phmg_agg_map(self.h, lvl, out.ctypes.data_as(_I))
+        return out
+
+    def dinv(self, i, n):
+        out = np.zeros(n)
+        lib().or_phmg_dinv(self.h, i, _dp(out))
+        return out
+
+    def tamg(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        lib().or_phmg_tamg(self.h, _dp(z), _dp(r))
+        return z
+
+    def krylov(self, f, max_iter, abs_tol, kind="cg", m=30):
+        """Solve with M = phmg: kind "cg", "fcg" or "gmres"."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        x = np.zeros_like(f)
+        r0 = ctypes.c_double()
+        r1 = ctypes.c_double()
+        k = {"cg": 0, "fcg": 1, "gmres": 2}[kind]
+        it = lib().or_phmg_krylov(self.P.h, self.h, k, m, _dp(x), _dp(f), max_iter, abs_tol,
+                                  ctypes.byref(r0), ctypes.byref(r1))
+        return x, it, r0.value, r1.value
+
+    def close(self):
+        if self.h:
+            lib().or_phmg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
