@@ -217,6 +217,14 @@ def oracle_solve(O, b, pc, tol, coarse_tol, max_iter):
         x, it, _, _ = H.cg(b, max_iter, tol, flexible=True)
         dt = time.perf_counter() - t0
         H.close()
+    elif pc == "phmg":
+        t0 = time.perf_counter()
+        H = orc.OraclePhmg(O)
+        t_setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        x, it, _, _ = H.krylov(b, max_iter, tol, kind="cg")
+        dt = time.perf_counter() - t0
+        H.close()
     else:
         t_setup = 0.0
         t0 = time.perf_counter()
@@ -740,13 +748,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--pc", default="hsmg", choices=["jacobi", "hsmg"])
+    ap.add_argument("--pc", default="hsmg", choices=["jacobi", "hsmg", "phmg"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--ax-reps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the CPU oracle solve (cpu_baseline and the parity fields)")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision solve measured beside the FP64 one")
+    ap.add_argument("--no-phmg", action="store_true",
+                    help="skip the phmg-CG solve measured beside the hsmg-FCG one")
     ap.add_argument("--kernel-only", choices=["ax", "dropin_ax", "fused", "gs", "stress",
                                               "dropin_fdm",
                                               "dropin_tnsr3d", "solve"],
@@ -805,6 +815,8 @@ def main():
     tol = cfg["rel_tol"] * r0
     if args.pc == "jacobi":
         solver = nb.CG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Jacobi())
+    elif args.pc == "phmg":  # Chebyshev smoothing and an AMG V-cycle: symmetric, plain CG
+        solver = nb.CG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Phmg())
     else:  # hsmg is not symmetric: flexible CG (plain CG stalls with it)
         solver = nb.FCG(max_iter=cfg["max_iter"], abs_tol=tol,
                         M=nb.Hsmg(coarse_tol=args.coarse_tol))
@@ -931,6 +943,33 @@ def main():
                                   "FP64 outer FCG, inner products, coarse CG, true residual "
                                   "every 50 iterations"}
 
+        # --- phmg-CG beside it: the other multigrid of the reference --------
+        phmg = None
+        if args.pc == "hsmg" and not args.no_phmg:
+            psolver = nb.CG(max_iter=cfg["max_iter"], abs_tol=tol, M=nb.Phmg())
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            psolver.M.init(P)  # levels, aggregation, 150-step eigenvalue estimates
+            t_setup = time.perf_counter() - t0
+            for _ in range(args.warmup):
+                mon_p = psolver.solve(Ax, x, b, P.n, P, stream=stream)
+            torch.cuda.synchronize()
+            if not mon_p.converged:
+                raise RuntimeError(f"phmg warm-up solve did not converge: {mon_p}")
+            t_p, mons_p = timed(lambda: psolver.solve(Ax, x, b, P.n, P, stream=stream),
+                                args.steps)
+            v_p = world * args.steps / t_p
+            phmg = {"value": v_p, "unit": "solves/s", "ms_per_step": t_p / args.steps * 1e3,
+                    "iterations": mons_p[-1].iter, "res_final": mons_p[-1].res_final,
+                    "abs_tol": tol, "speedup_vs_hsmg_fp64": v_p / value,
+                    "err_vs_hsmg_fp64": rel_err_mean_free(x.cpu().numpy(), x64.cpu().numpy(),
+                                                          all(cfg["periodic"])),
+                    "setup_s": t_setup,
+                    "gpu_launches": sum(m.launches for m in mons_p),
+                    "settings": "levels lx 8 -> 4 -> 2, 3 Chebyshev-Jacobi steps a level, "
+                                "tree AMG of 3 levels (Chebyshev degree 4, one V-cycle); "
+                                "plain CG, FP64"}
+
         # --- the dominant kernel of the solve, timed with events ----------
         # The fused CG step (p = z + beta p, w = A p, sum p w: 88 B/point) is
         # the largest share of the solve's device time; it is timed on its
@@ -968,7 +1007,8 @@ def main():
         "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_name(
-                       cfg, f"FP64 {'Jacobi-PCG' if args.pc == 'jacobi' else 'hsmg-FCG'}")
+                       cfg, "FP64 " + {"jacobi": "Jacobi-PCG", "hsmg": "hsmg-FCG",
+                                       "phmg": "phmg-CG"}[args.pc])
                        + ", one solve per step per GPU",
                    "pc": args.pc, "iterations": iters[-1], "r0": r0, "seed": args.seed,
                    "coarse": f"10 Jacobi-CG iterations, abs tol {args.coarse_tol:g}",
@@ -1007,6 +1047,8 @@ def main():
     }
     if mixed is not None:
         line["mixed"] = mixed
+    if phmg is not None:
+        line["phmg"] = phmg
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # One complete FP64 solve of the CPU oracle on the same right-hand
         # side: the CPU baseline (whole solve, host threads), and the parity
@@ -1016,7 +1058,7 @@ def main():
                                          cfg["max_iter"])
         O.close()
         cores = host_threads()
-        name = "hsmg-FCG" if args.pc == "hsmg" else "Jacobi-PCG"
+        name = {"hsmg": "hsmg-FCG", "phmg": "phmg-CG", "jacobi": "Jacobi-PCG"}[args.pc]
         line["cpu_baseline"] = {
             "value": 1.0 / dt_o, "unit": "solves/s", "cores": cores, "kind": "port",
             "sample": f"one complete FP64 {name} solve of the same problem and right-hand "
