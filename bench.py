@@ -1035,7 +1035,7 @@ def main():
                     "frac": ax_bytes / t_ax / 1e9 / peaks["hbm_gbs"],
                     "bytes_per_launch": ax_bytes, "launch_ms": t_ax * 1e3,
                     "gdof_s": P.n / t_ax / 1e9},
-        "gs": {"kernel": "gs_add_fused_kernel<double>",
+        "gs": {"kernel": "gs_add_warp_kernel<double,4>",
                "achieved": gs_bytes / t_gs / 1e9, "unit": "GB/s",
                "frac": gs_bytes / t_gs / 1e9 / peaks["hbm_gbs"],
                "entries": P.nlocal, "bytes_per_launch": gs_bytes,

@@ -331,6 +331,8 @@ static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
                o_pr = c.take<int2>(hl.pairs.size()), o_ex = c.take<int>(hl.extra_mask.size()),
                o_sm = c.take<unsigned char>(hl.seg_masked.size()),
                o_pm = c.take<unsigned char>(hl.pair_masked.size());
+  const size_t o_li = c.take<int>(hl.lane_idx.size()), o_lh = c.take<unsigned>(hl.lane_head.size()),
+               o_lz = c.take<unsigned>(hl.lane_zero.size()), o_sl = c.take<int>(hl.seg_long.size());
   const size_t o_df = c.take<unsigned char>(nelv), o_mf = c.take<float>(n);
   const size_t o_red = c.take<double>(kMaxRedBlocks + 64);
   const size_t o_err = c.take<int>(1);
@@ -381,6 +383,12 @@ static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
   P->gsd.extra_mask = (const int *)(A + o_ex);
   P->gsd.seg_masked = (const unsigned char *)(A + o_sm);
   P->gsd.pair_masked = (const unsigned char *)(A + o_pm);
+  P->gsd.nchunk = (int)hl.lane_head.size();
+  P->gsd.nlong = (int)hl.seg_long.size();
+  P->gsd.lane_idx = (const int *)(A + o_li);
+  P->gsd.lane_head = (const unsigned *)(A + o_lh);
+  P->gsd.lane_zero = (const unsigned *)(A + o_lz);
+  P->gsd.seg_long = (const int *)(A + o_sl);
 
   nb_problem_guard guard(P);
   auto up = [&](void *dst, const void *src, size_t bytes) {
@@ -404,6 +412,10 @@ static nb_status finish_problem(nb_problem *P, const std::vector<double> &xyz8,
   NB_TRY(up((void *)P->gsd.extra_mask, hl.extra_mask.data(), hl.extra_mask.size() * 4));
   NB_TRY(up((void *)P->gsd.seg_masked, hl.seg_masked.data(), hl.seg_masked.size()));
   NB_TRY(up((void *)P->gsd.pair_masked, hl.pair_masked.data(), hl.pair_masked.size()));
+  NB_TRY(up((void *)P->gsd.lane_idx, hl.lane_idx.data(), hl.lane_idx.size() * 4));
+  NB_TRY(up((void *)P->gsd.lane_head, hl.lane_head.data(), hl.lane_head.size() * 4));
+  NB_TRY(up((void *)P->gsd.lane_zero, hl.lane_zero.data(), hl.lane_zero.size() * 4));
+  NB_TRY(up((void *)P->gsd.seg_long, hl.seg_long.data(), hl.seg_long.size() * 4));
   NB_TRY(up(P->dfrmd, dfrmd.data(), dfrmd.size()));
 
   // geometry on the device
