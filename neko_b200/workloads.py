@@ -157,3 +157,15 @@ def box_mesh(nel, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), periodic=(False, False
                 ids.append(vid)
                 xyz.append(vx)
     return np.array(ids, dtype=np.int32), np.array(xyz, dtype=np.float64)
+
+
+def hub_mesh(nel, k, rotate_seed=None):
+    """box_mesh(nel) plus k elements that share only the first vertex of
+    element 0 with the rest of the mesh (each a copy of element 0's
+    hexahedron with seven new vertex ids): one point with more copies than
+    a warp has lanes, as at the singular vertices of unstructured meshes."""
+    ids, xyz = box_mesh(nel, rotate_seed=rotate_seed)
+    nid = int(ids.max()) + 1
+    extra = [[int(ids[0, 0])] + list(range(nid + 7 * e, nid + 7 * e + 7)) for e in range(k)]
+    return (np.concatenate([ids, np.array(extra, dtype=np.int32)]),
+            np.concatenate([xyz, np.repeat(xyz[:1], k, axis=0)]))

@@ -103,6 +103,22 @@ def test_mesh_gs_maps_bit_exact(nblib, oracle, nel, lx, seed, periodic):
     np.testing.assert_array_equal(bo, P.i32("blk_off"))
 
 
+@pytest.mark.parametrize("k,lx", [(36, 4), (60, 3)])
+def test_high_valence_vertex_maps_bit_exact(nblib, oracle, k, lx):
+    """A point shared by more elements than a warp has lanes (8 + k copies):
+    its gs block is longer than 32 entries."""
+    from neko_b200 import workloads
+    ids, xyz = workloads.hub_mesh((2, 2, 2), k, rotate_seed=1)
+    P = oracle.OracleProblem.from_elements(ids, xyz, lx)
+    fo, fn, dg, gd, bl, bo = nb_mesh_maps(nblib, ids, lx)
+    assert bl.max() == 8 + k
+    assert fo == P.local_facet_offset
+    np.testing.assert_array_equal(dg, P.i32("dof_gs"))
+    np.testing.assert_array_equal(gd, P.i32("gs_dof"))
+    np.testing.assert_array_equal(bl, P.i32("blk_len"))
+    np.testing.assert_array_equal(bo, P.i32("blk_off"))
+
+
 @pytest.mark.parametrize("nel,periodic,lx", CASES[:7])
 def test_unrotated_mesh_maps_equal_box_maps(nblib, nel, periodic, lx):
     from neko_b200 import workloads
