@@ -76,6 +76,34 @@ def test_rotated_mesh_matches_oracle(nb, oracle, nel, lx, seed, deform):
     assert mg.converged and abs(mg.iter - it_go) <= 1, (mg.iter, it_go)
 
 
+@pytest.mark.parametrize("k,lx", [(36, 4), (60, 5)])
+def test_high_valence_vertex_matches_oracle(nb, oracle, k, lx):
+    """A point with 8 + k copies, more than a warp has lanes: the gather-
+    scatter sums it as a long segment (one thread) beside the warp chunks.
+    gs bit-exact without and with the mask (a Jacobi-PCG solve, whose
+    operator gather-scatter masks the boundary)."""
+    from neko_b200 import workloads
+    ids, xyz = workloads.hub_mesh((2, 2, 2), k, rotate_seed=1)
+    P = nb.Problem.from_mesh(ids, xyz, lx, deform=0.0, dirichlet=True)
+    O = oracle.OracleProblem.from_elements(ids, xyz, lx)
+    O.coef()
+    O.bc_boundary()
+    rng = np.random.default_rng(k)
+    u = rng.uniform(-1, 1, P.n)
+    g = _cuda(u)
+    P.gs.op(g)
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(g), O.gs_add(u))
+    b = O.bc_apply(O.gs_add(O.f64("B") * rng.standard_normal(P.n)))
+    r0 = np.sqrt(np.sum(b * O.f64("mult") * b) / O.volume)
+    xo, it_o, _, _ = O.cg_jacobi(b, 2000, 1e-10 * r0)
+    x = P.zeros()
+    mon = nb.CG(max_iter=2000, abs_tol=1e-10 * r0, M=nb.Jacobi()).solve(nb.AxHelm(), x, _cuda(b),
+                                                                       P.n, P)
+    assert mon.converged and abs(mon.iter - it_o) <= 1, (mon.iter, it_o)
+    assert np.abs(_np(x) - xo).max() / np.abs(xo).max() < 1e-7
+
+
 @pytest.mark.parametrize("nel,lx,seed", [((3, 2, 4), 6, 1), ((3, 3, 3), 8, 2), ((2, 3, 2), 5, 3)])
 def test_rotated_mesh_hsmg_matches_oracle(nb, oracle, nel, lx, seed):
     """hsmg on neighbours that meet with arbitrary relative orientation: the
