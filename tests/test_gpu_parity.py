@@ -262,6 +262,22 @@ def test_vector_ops(nblib):
     np.testing.assert_array_equal(_np(A), b * c)
     nblib.cuda_invcol1(vp(A.data_ptr()), ctypes.byref(nn), s)
     np.testing.assert_array_equal(_np(A), 1.0 / (b * c))
+    # a += b c d (the h2 term's addcol4)
+    d = rng.standard_normal(n)
+    A, D = _cuda(a), _cuda(d)
+    nblib.cuda_addcol4(vp(A.data_ptr()), vp(Bt.data_ptr()), vp(C.data_ptr()), vp(D.data_ptr()),
+                       ctypes.byref(nn), s)
+    np.testing.assert_allclose(_np(A), a + b * c * d, rtol=1e-14, atol=1e-14)
+    # zero-Dirichlet: msk(0) holds the count, msk(1..count) 1-based points,
+    # called with m = count + 1 as zero_dirichlet.f90 passes size(msk)
+    pts = np.sort(rng.choice(n, 777, replace=False))
+    msk = _cuda(np.concatenate([[len(pts)], pts + 1]).astype(np.int32))
+    X = _cuda(a)
+    nblib.cuda_zero_dirichlet_apply_scalar(vp(msk.data_ptr()), vp(X.data_ptr()),
+                                           ctypes.byref(ctypes.c_int(len(pts) + 1)), s)
+    ref = a.copy()
+    ref[pts] = 0.0
+    np.testing.assert_array_equal(_np(X), ref)
 
 
 def test_jacobi_diag_matches_oracle(nb, oracle):
