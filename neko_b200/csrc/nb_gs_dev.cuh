@@ -1,6 +1,8 @@
-// nb_gs_dev.cuh -- one work item of the fused gather-scatter add, shared by
-// the standalone gs kernel and the kernels that run gs as one phase of a
-// persistent launch.
+// nb_gs_dev.cuh -- one work item of the fused gather-scatter add (one thread
+// a pair or segment), for the kernels that run gs as one phase of a
+// persistent launch (the hsmg coarse solve, the batched engine).  The
+// standalone gather-scatter runs the warp-shuffle form of the same sums
+// (gs.cu, gs_add_warp_kernel).
 //
 // Items 0..npairs-1 are facet pairs, then nseg shared-point segments, then
 // (when masking) the masked points that no segment or pair covers.  Each
