@@ -91,7 +91,14 @@ struct FdmCfg {
   static constexpr bool VEC = EPW == 1;
   static constexpr int VW = 16 / (int)sizeof(T);            // values per vector
   static constexpr int NLR = (NL + VW - 1) / VW * VW;        // row pitch
-  static constexpr int OFFM = (2 * BUF + VW - 1) / VW * VW;  // matrices, aligned
+  // FP32 one-element blocks pass in place: every lane reads its lines, the
+  // block meets at a barrier, then the rotated output overwrites the same
+  // buffer; the second buffer shrinks to the matrix staging area (3 N2), so
+  // more blocks fit an SM.  FP64 keeps two buffers (its registers, not its
+  // shared memory, bound its residency).
+  static constexpr bool INPLACE = VEC && sizeof(T) == 4;
+  static constexpr int BUF2 = INPLACE ? (3 * N2 + 1) / 2 * 2 : BUF;
+  static constexpr int OFFM = (BUF + BUF2 + VW - 1) / VW * VW;  // matrices, aligned
   static constexpr int MAT = VEC ? 6 * NL * NLR : 3 * N2;
   static constexpr int STR0 = VEC ? OFFM + MAT + 3 * NL + 1 : 2 * BUF + 3 * N2 + 3 * NL + 1;
   // per-element stride; with several elements in a warp it is 9 mod 16
@@ -102,7 +109,7 @@ struct FdmCfg {
   // shared memory allows (228 KB, 1 KB reserved per block), fewer if the
   // M x NL sums and the operands in flight would not fit in the registers
   static constexpr int OCC = (int)(233472 / (SMEM + 1024));
-  static constexpr int REGS = 3 * M * NL + 48;
+  static constexpr int REGS = sizeof(T) == 8 ? 3 * M * NL + 48 : 2 * M * NL + 4;
   static constexpr int RB = 65536 / (TPE * REGS);
   static constexpr int MINB0 = OCC < RB ? OCC : RB;
   static constexpr int MINB = MINB0 < 1 ? 1 : MINB0 > 32 / W ? 32 / W : MINB0;
@@ -142,7 +149,10 @@ __device__ __forceinline__ void fdm_pass(const T *__restrict__ src, T *__restric
                                          T *__restrict__ out, int u) {
   using C = FdmCfg<T, NL>;
   constexpr int N2 = C::N2, M = C::M, LA = C::LA;
-  if (u >= LA) return;
+  // in place (src == dst), lanes without lines still meet the barrier
+  // between the reads and the writes
+  if (!C::INPLACE && u >= LA) return;
+  const bool lines = u < LA;
   T o[M][NL];
   int base[M];
   T ljk[M];  // SCALE: spectra sum of the line's second index, added to the first's
@@ -160,7 +170,7 @@ __device__ __forceinline__ void fdm_pass(const T *__restrict__ src, T *__restric
     for (int i = 0; i < NL; i++) o[j][i] = T(0);
   }
 #pragma unroll 2
-  for (int l = 0; l < NL; l++) {
+  for (int l = 0; l < (lines ? NL : 0); l++) {
     T x[M];
 #pragma unroll
     for (int j = 0; j < M; j++) {
@@ -190,6 +200,10 @@ __device__ __forceinline__ void fdm_pass(const T *__restrict__ src, T *__restric
         for (int j = 0; j < M; j++) o[j][i] += mv * x[j];
       }
     }
+  }
+  if constexpr (C::INPLACE) {
+    if (!out) __syncthreads();  // every read of src done before dst (= src) is written
+    if (!lines) return;
   }
 #pragma unroll
   for (int j = 0; j < M; j++) {
@@ -291,6 +305,8 @@ __global__ void __launch_bounds__(FdmCfg<T, NL>::TPE, FdmCfg<T, NL>::MINB)
     __syncthreads();
   }
   // forward: b0 -> b1 -> b0 -> b1; backward (D^-1 on the first read): b1 -> b0 -> b1 -> out
+  // (in place: b0 -> b0 throughout)
+  if constexpr (C::INPLACE) b1 = b0;
   fdm_pass<T, NL, true, false>(b0, b1, fwd, sL, nullptr, u);
   __syncthreads();
   fdm_pass<T, NL, true, false>(b1, b0, fwd + MS, sL, nullptr, u);
