@@ -99,6 +99,7 @@ struct FdmCfg {
   static constexpr bool INPLACE = VEC && sizeof(T) == 4;
   static constexpr int BUF2 = INPLACE ? (3 * N2 + 1) / 2 * 2 : BUF;
   static constexpr int OFFM = (BUF + BUF2 + VW - 1) / VW * VW;  // matrices, aligned
+  static_assert(!INPLACE || BUF2 >= 3 * N2, "the staging area holds the three raw matrices");
   static constexpr int MAT = VEC ? 6 * NL * NLR : 3 * N2;
   static constexpr int STR0 = VEC ? OFFM + MAT + 3 * NL + 1 : 2 * BUF + 3 * N2 + 3 * NL + 1;
   // per-element stride; with several elements in a warp it is 9 mod 16
